@@ -1,0 +1,166 @@
+"""ORACLE (test infrastructure only): float64 restatement of the MD updates
+on the reference's hot path.
+
+  * velocity Verlet (jax_md.simulate.nve / velocity_verlet, wrapped by
+    deepmd_jax/routine.py:139-144);
+  * Martyna-Tuckerman-Klein Nose-Hoover chain (jax_md.simulate.nvt_nose_hoover
+    and nose_hoover_chain, wrapped by deepmd_jax/routine.py:147-158), chain
+    masses Q = kT tau^2 (Q0 *= DOF), DOF = 3N; invariant per
+    deepmd_jax/routine.py:9-25;
+  * PIMD BAOAB with exact free ring-polymer propagation and the PILE-L
+    thermostat (deepmd_jax/pimd.py:22-44,92-111,114-207,210-247);
+  * min_image_unwrap (deepmd_jax/md_utils.py:162-169).
+
+jax_md is a third-party dependency that is absent here (unpinned git HEAD,
+setup.py:13); the Nose-Hoover substep below restates its published MTK
+algorithm (Martyna, Tuckerman, Tobias, Klein, Mol. Phys. 87, 1117 (1996)) with
+the operator order used by jax_md.  Parity of that order is unpinned.
+The Gaussian noise of the stochastic steps comes from oracle/philox.py, the
+same counter-based stream the device kernels draw, so a step can be compared
+deterministically.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+HBAR = 6.582119569e-16 * 1e15  # eV fs (deepmd_jax/pimd.py:19)
+
+
+def kinetic_energy(p, m):
+    return 0.5 * float((p * p / m).sum())
+
+
+def vv_step(r, p, F, m, dt, force_fn):
+    """One velocity-Verlet step; returns (r, p, F, extra) with extra from force_fn."""
+    p = p + 0.5 * dt * F
+    r = r + dt * p / m
+    F, extra = force_fn(r)
+    p = p + 0.5 * dt * F
+    return r, p, F, extra
+
+
+class NHChain:
+    """Nose-Hoover chain state (float64)."""
+
+    def __init__(self, chain_length, dof, kT, tau, KE):
+        self.L = chain_length
+        self.xi = np.zeros(chain_length)
+        self.p = np.zeros(chain_length)
+        self.Q = kT * tau ** 2 * np.ones(chain_length)
+        self.Q[0] *= dof
+        self.dof = dof
+        self.tau = tau
+        self.KE = KE
+
+    def update_mass(self, kT):
+        self.Q = kT * self.tau ** 2 * np.ones(self.L)
+        self.Q[0] *= self.dof
+
+    def substep(self, delta, P, kT):
+        """One MTK chain substep of length delta/2 (jax_md nose_hoover_chain)."""
+        d2, d4, d8 = delta / 2, delta / 4, delta / 8
+        p, Q = self.p.copy(), self.Q
+        M = self.L - 1
+        G = p[M - 1] ** 2 / Q[M - 1] - kT
+        p[M] += d4 * G
+        for m in range(M - 1, 0, -1):
+            G = p[m - 1] ** 2 / Q[m - 1] - kT
+            scale = np.exp(-d8 * p[m + 1] / Q[m + 1])
+            p[m] = scale * (scale * p[m] + d4 * G)
+        G = 2.0 * self.KE - self.dof * kT
+        scale = np.exp(-d8 * p[1] / Q[1])
+        p[0] = scale * (scale * p[0] + d4 * G)
+        scale = np.exp(-d2 * p[0] / Q[0])
+        self.KE = self.KE * scale ** 2
+        P = P * scale
+        self.xi = self.xi + d2 * p / Q
+        G = 2.0 * self.KE - self.dof * kT
+        for m in range(M):
+            scale = np.exp(-d8 * p[m + 1] / Q[m + 1])
+            p[m] = scale * (scale * p[m] + d4 * G)
+            G = p[m] ** 2 / Q[m] - kT
+        p[M] += d4 * G
+        self.p = p
+        return P
+
+    def invariant_terms(self, kT):
+        """Chain part of the NH invariant (deepmd_jax/routine.py:19-24)."""
+        E = self.p[0] ** 2 / (2 * self.Q[0]) + self.dof * kT * self.xi[0]
+        for r, p, q in zip(self.xi[1:], self.p[1:], self.Q[1:]):
+            E += p ** 2 / (2 * q) + kT * r
+        return E
+
+
+def nvt_step(r, p, F, m, dt, kT, chain: NHChain, force_fn):
+    chain.update_mass(kT)
+    p = chain.substep(dt, p, kT)
+    r, p, F, extra = vv_step(r, p, F, m, dt, force_fn)
+    chain.KE = kinetic_energy(p, m)
+    p = chain.substep(dt, p, kT)
+    return r, p, F, extra
+
+
+def normal_mode_transform(n_bead, kT):
+    """(freqs (P,), C (P,P)) exactly as deepmd_jax/pimd.py:22-44 (numpy eigh)."""
+    ring_poly_freq = n_bead * kT / HBAR
+    A = (2 * np.eye(n_bead) - np.roll(np.eye(n_bead), 1, axis=0) - np.roll(np.eye(n_bead), -1, axis=0))
+    eva, eve = np.linalg.eigh(A)
+    order = np.argsort(eva)
+    eva = eva[order]
+    eve = eve[:, order]
+    if n_bead >= 2:
+        eva[0] = 0.0
+    return ring_poly_freq * np.sqrt(np.maximum(eva, 0.0)), eve
+
+
+def unwrap_across_beads(R, box3):
+    ref = R[0:1]
+    d = R - ref
+    d = d - box3 * np.round(d / box3)
+    return ref + d
+
+
+def free_ring_step(R, P, m, C, w, h, box3):
+    """Exact free ring-polymer propagation for time h (pimd.py:160-179).
+    R, P: (P, N, 3); m: (N, 1)."""
+    R = unwrap_across_beads(R, box3)
+    Q = np.tensordot(C.T, R, axes=(1, 0))
+    Pn = np.tensordot(C.T, P, axes=(1, 0))
+    w = w[:, None, None]
+    c, s = np.cos(w * h), np.sin(w * h)
+    sw = np.where(w == 0, 1.0, w)
+    Qn = np.empty_like(Q)
+    Pm = np.empty_like(Pn)
+    Qn[0] = Q[0] + h * Pn[0] / m
+    Pm[0] = Pn[0]
+    Qn[1:] = Q[1:] * c[1:] + Pn[1:] * s[1:] / (m * sw[1:])
+    Pm[1:] = Pn[1:] * c[1:] - m * sw[1:] * Q[1:] * s[1:]
+    return np.tensordot(C, Qn, axes=(1, 0)), np.tensordot(C, Pm, axes=(1, 0))
+
+
+def pile_l_step(P, m, C, gamma, dt, kT, noise):
+    """PILE-L O step in normal modes (pimd.py:92-111); noise (P, N, 3) ~ N(0,1).
+    Returns (P_new, delta_KE)."""
+    nb = C.shape[0]
+    Pn = np.tensordot(C.T, P, axes=(1, 0))
+    c1 = np.exp(-gamma * dt)[:, None, None]
+    c2 = np.sqrt(np.maximum(kT * nb * (1.0 - c1 ** 2), 0.0))
+    Pn = c1 * Pn + c2 * np.sqrt(m) * noise
+    Pnew = np.tensordot(C, Pn, axes=(1, 0))
+    dKE = 0.5 * float(((Pnew ** 2 - P ** 2) / m).sum())
+    return Pnew, dKE
+
+
+def pimd_step(R, P, F, m, dt, kT, C, w, gamma, box3, noise, force_fn):
+    """One BAOAB PIMD step (pimd.py:193-205); returns (R, P, F, dKE, extra)."""
+    P = P + 0.5 * dt * F
+    R, P = free_ring_step(R, P, m, C, w, dt / 2, box3)
+    P, dKE = pile_l_step(P, m, C, gamma, dt, kT, noise)
+    R, P = free_ring_step(R, P, m, C, w, dt / 2, box3)
+    F, extra = force_fn(R)
+    P = P + 0.5 * dt * F
+    return R, P, F, dKE, extra
+
+
+def min_image_unwrap(prev, cur, box3):
+    return prev + np.remainder(cur - prev + box3 / 2, box3) - box3 / 2

@@ -1,0 +1,52 @@
+"""The oracle against golden vectors produced by the reference's own model
+source (tests/golden/make_golden.py).  CPU only."""
+import numpy as np
+import pytest
+import torch
+
+from make_golden import golden_models
+from oracle import model as om
+
+G = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "golden_model.npz"))
+MODELS = golden_models()
+
+CASES = [("A", "A", "A", None), ("B", "A", "B", None), ("C", "A", "C", None),
+         ("D", "D", "B", "D_nbrs"), ("E", "E", "B", None)]
+
+
+@pytest.mark.parametrize("key,sysk,mk,nb", CASES)
+def test_oracle_matches_reference_source(key, sysk, mk, nb):
+    p, v = MODELS[mk]
+    m = om.OracleModel(p, v, torch.float64)
+    r = om.energy_force(m, G[sysk + "_pos"], G[sysk + "_box"], G[sysk + "_type"],
+                        nbrs=(G[nb] if nb else None), sel=[46, 92])
+    assert abs(r["energy"] - float(G[key + "_E"])) <= 1e-12 * max(1.0, abs(float(G[key + "_E"])))
+    assert np.abs(r["force"] - G[key + "_F"]).max() <= 1e-12
+
+
+def test_oracle_force_is_gradient():
+    """Central finite differences of the oracle energy (h = 1e-4 A)."""
+    p, v = MODELS["B"]
+    m = om.OracleModel(p, v, torch.float64)
+    pos, box, typ = G["A_pos"], G["A_box"], G["A_type"]
+    F = om.energy_force(m, pos, box, typ)["force"]
+    rng = np.random.default_rng(0)
+    for _ in range(6):
+        a, c = rng.integers(len(pos)), rng.integers(3)
+        h = 1e-4
+        pp = pos.copy(); pp[a, c] += h
+        pm = pos.copy(); pm[a, c] -= h
+        fd = -(om.energy_only(m, pp, box, typ)[0] - om.energy_only(m, pm, box, typ)[0]) / (2 * h)
+        assert abs(fd - F[a, c]) < 1e-7
+
+
+def test_oracle_virial_trace_is_strain_derivative():
+    p, v = MODELS["B"]
+    m = om.OracleModel(p, v, torch.float64)
+    pos, box, typ = G["E_pos"], G["E_box"], G["E_type"]
+    W = om.energy_force(m, pos, box, typ)["virial"]
+    eps = 1e-6
+    ep = om.energy_only(m, pos * (1 + eps), box * (1 + eps), typ)[0]
+    em = om.energy_only(m, pos * (1 - eps), box * (1 - eps), typ)[0]
+    assert abs((ep - em) / (2 * eps) + np.trace(W)) < 1e-6
+    assert np.abs(W - W.T).max() < 1e-10      # rotation invariance -> symmetric
