@@ -1,0 +1,297 @@
+// C ABI of libdpb200: model upload, workspace sizing and evaluation dispatch.
+#include "eval_common.cuh"
+#include <cuda_bf16.h>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+namespace dpb {
+std::atomic<uint64_t> g_launches{0};
+
+// fp32 path (eval_fp32.cu)
+template <int E0, int E1, int E2>
+int launch_embed_fwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                     const int32_t *, float *, float *, cudaStream_t);
+template <int E0, int E1, int E2>
+int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                     const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
+int launch_sgemm(int, int, int, const float *, int, RowMap, const float *, const Epi &, cudaStream_t);
+int launch_fit_energy(int, RowMap, int, const float *, const float *, const float *, const float *,
+                      const float *, float *, float *, double *, int, cudaStream_t);
+int launch_finalize(int, int, const float4 *, float *, const float *, const int32_t *, float *, double *, int,
+                    const float *, uint32_t *, cudaStream_t);
+// mixed path (mixed.cu)
+int mixed_supported(const DevModel &M);
+size_t mixed_workspace_per_atom(const DevModel &M);
+int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+               const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
+               cudaStream_t st);
+}  // namespace dpb
+
+using namespace dpb;
+
+struct dpb_model {
+  DevModel dm;
+  std::vector<void *> allocs;
+  int device;
+};
+
+
+static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <class T>
+static int upload(dpb_model *m, const T *host, size_t n, const T **dev) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return DPB_ERR_CUDA;
+  m->allocs.push_back(p);
+  if (cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+  *dev = (const T *)p;
+  return DPB_OK;
+}
+
+static int upload_bf16(dpb_model *m, const std::vector<float> &v, const __nv_bfloat16 **dev) {
+  std::vector<__nv_bfloat16> b(v.size());
+  for (size_t i = 0; i < v.size(); ++i) b[i] = __float2bfloat16_rn(v[i]);
+  return upload(m, b.data(), b.size(), dev);
+}
+
+static bool embed_supported(const DevModel &M) {
+  return (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
+}
+
+extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
+  if (!d || !out) return DPB_ERR_INVALID_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DPB_ERR_NO_DEVICE;
+  const int nt = d->ntypes;
+  if (nt < 1 || nt > kMaxTypes || d->n_embed != 3 || d->n_fit < 1 || d->n_fit > kMaxFitLayers)
+    return DPB_ERR_UNSUPPORTED;
+  dpb_model *m = new dpb_model();
+  cudaGetDevice(&m->device);
+  DevModel &M = m->dm;
+  std::memset(&M, 0, sizeof(M));
+  M.ntypes = nt;
+  M.E0 = d->embed_widths[0]; M.E1 = d->embed_widths[1]; M.E2 = d->embed_widths[2];
+  M.A = d->axis;
+  M.nfit = d->n_fit;
+  for (int l = 0; l < d->n_fit; ++l) M.FW[l] = d->fit_widths[l];
+  M.rcut = (float)d->rcut;
+  M.inv_nnbrs = (float)(1.0 / d->nnbrs);
+  if (!embed_supported(M) || M.A < 1 || 2 * M.A > 32 || 2 * M.A > M.E2) {
+    delete m;
+    return DPB_ERR_UNSUPPORTED;
+  }
+  for (int l = 1; l < d->n_fit; ++l)
+    if (M.FW[l] != M.FW[0]) { delete m; return DPB_ERR_UNSUPPORTED; }
+  for (int t = 0; t < nt; ++t) {
+    M.mean[t] = (float)d->sr_mean[t];
+    M.inv_std[t] = (float)(1.0 / d->sr_std[t]);
+  }
+  const int ew_in[3] = {1, M.E0, M.E1}, ew_out[3] = {M.E0, M.E1, M.E2};
+  int rc = DPB_OK;
+  for (int k = 0; k < nt * nt && rc == DPB_OK; ++k)
+    for (int l = 0; l < 3 && rc == DPB_OK; ++l) {
+      rc = upload(m, d->embed_kernel[k * 3 + l], (size_t)ew_in[l] * ew_out[l], &M.ew[k][l]);
+      if (rc == DPB_OK) rc = upload(m, d->embed_bias[k * 3 + l], (size_t)ew_out[l], &M.eb[k][l]);
+      if (rc == DPB_OK) {
+        std::vector<float> v(d->embed_kernel[k * 3 + l], d->embed_kernel[k * 3 + l] + (size_t)ew_in[l] * ew_out[l]);
+        rc = upload_bf16(m, v, &M.ew_bf[k][l]);
+      }
+    }
+  if (rc == DPB_OK) rc = upload(m, d->tbias, (size_t)M.E2, &M.tbias);
+  const int K0 = M.A * M.E2;
+  for (int t = 0; t < nt && rc == DPB_OK; ++t) {
+    for (int l = 0; l <= M.nfit && rc == DPB_OK; ++l) {
+      const int in = l == 0 ? K0 : M.FW[l - 1];
+      const int outw = l == M.nfit ? 1 : M.FW[l];
+      const float *kh = d->fit_kernel[t * (M.nfit + 1) + l];
+      const float *bh = d->fit_bias[t * (M.nfit + 1) + l];
+      std::vector<float> kv(kh, kh + (size_t)in * outw), bv(bh, bh + outw);
+      if (l == M.nfit) {  // fold out_norm and Ebias into the output layer
+        for (auto &x : kv) x = (float)(x * d->out_norm);
+        for (auto &x : bv) x = (float)((x + d->ebias[t]) * d->out_norm);
+      }
+      rc = upload(m, kv.data(), kv.size(), &M.fw[t][l]);
+      if (rc == DPB_OK) rc = upload(m, bv.data(), bv.size(), &M.fb[t][l]);
+      std::vector<float> kt((size_t)in * outw);
+      for (int i = 0; i < in; ++i)
+        for (int o = 0; o < outw; ++o) kt[(size_t)o * in + i] = kv[(size_t)i * outw + o];
+      if (rc == DPB_OK) rc = upload(m, kt.data(), kt.size(), &M.fwT[t][l]);
+      if (rc == DPB_OK) rc = upload_bf16(m, kv, &M.fw_bf[t][l]);
+      if (rc == DPB_OK) rc = upload_bf16(m, kt, &M.fwT_bf[t][l]);
+      if (rc == DPB_OK && l < M.nfit) {
+        const float *dt = d->fit_dt ? d->fit_dt[t * M.nfit + l] : nullptr;
+        if (dt) rc = upload(m, dt, (size_t)outw, &M.fdt[t][l]);
+      }
+    }
+  }
+  if (rc != DPB_OK) {
+    dpb_model_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return DPB_OK;
+}
+
+extern "C" int dpb_model_destroy(dpb_model *m) {
+  if (!m) return DPB_ERR_INVALID_ARG;
+  for (void *p : m->allocs) cudaFree(p);
+  delete m;
+  return DPB_OK;
+}
+
+static size_t fp32_ws_per_atom(const DevModel &M) {
+  const int FW = M.FW[0];
+  return (size_t)(10 * M.E2 + M.A * M.E2 + 2 * M.nfit * FW + 4 * FW + 1) * 4 + 16;
+}
+
+extern "C" int dpb_eval_workspace_bytes(const dpb_model *m, int natoms, int nframes, size_t *bytes) {
+  if (!m || !bytes || natoms <= 0 || nframes <= 0) return DPB_ERR_INVALID_ARG;
+  const size_t NF = (size_t)natoms * nframes;
+  size_t a = al(NF * fp32_ws_per_atom(m->dm)) + 16 * 256 + al((size_t)nframes * 9 * 8);
+  size_t b = al(NF * mixed_workspace_per_atom(m->dm)) + al(NF * 16) + al(NF * 4) + al((size_t)nframes * 9 * 8) +
+             16 * 256;
+  *bytes = std::max(a, b);
+  return DPB_OK;
+}
+
+static int fill_sys(const dpb_model *m, int natoms, int nframes, const int *type_count, const int *sel,
+                    SysDesc &D) {
+  const int nt = m->dm.ntypes;
+  D.N = natoms; D.F = nframes; D.ntypes = nt;
+  int off = 0, col = 0;
+  for (int t = 0; t < nt; ++t) {
+    if (type_count[t] < 0 || sel[t] < 0) return DPB_ERR_INVALID_ARG;
+    D.offs[t] = off; off += type_count[t];
+    D.sel[t] = sel[t]; D.col[t] = col; col += sel[t];
+  }
+  if (off != natoms) return DPB_ERR_INVALID_ARG;
+  for (int t = nt; t <= kMaxTypes; ++t) D.offs[t] = natoms;
+  D.col[nt] = col;
+  D.S = col;
+  return DPB_OK;
+}
+
+static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
+                     const float *box, const int32_t *nbrs, double *energy, float4 *F4, float *Eatom,
+                     double *virial, char *w, cudaStream_t st) {
+  const size_t NF = (size_t)D.N * D.F;
+  const int E2 = M.E2, A = M.A, K0 = A * E2, FW = M.FW[0], L = M.nfit;
+  float *T = (float *)w; w += al(NF * 10 * E2 * 4);
+  float *G = (float *)w; w += al(NF * K0 * 4);  // G, later dE/dG
+  float *tb[kMaxFitLayers], *hb[kMaxFitLayers];
+  for (int l = 0; l < L; ++l) { tb[l] = (float *)w; w += al(NF * FW * 4); }
+  for (int l = 0; l < L; ++l) { hb[l] = (float *)w; w += al(NF * FW * 4); }
+  float *gz[2], *gh[2];
+  gz[0] = (float *)w; w += al(NF * FW * 4);
+  gz[1] = (float *)w; w += al(NF * FW * 4);
+  gh[0] = (float *)w; w += al(NF * FW * 4);
+  gh[1] = (float *)w; w += al(NF * FW * 4);
+  int rc;
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    else rc = launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    if (rc) return rc;
+  }
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    const int cnt = D.offs[ti + 1] - D.offs[ti];
+    if (!cnt) continue;
+    const RowMap rm{cnt, D.N, D.offs[ti]};
+    const int Mrows = cnt * D.F;
+    for (int l = 0; l < L; ++l) {
+      Epi ep{};
+      ep.bias = M.fb[ti][l];
+      ep.out1 = tb[l];
+      ep.out2 = hb[l];
+      ep.ld = FW;
+      if (l > 0 && M.fdt[ti][l]) {
+        ep.mode = EPI_TANH_RES;
+        ep.dt = M.fdt[ti][l];
+        ep.hprev = hb[l - 1];
+      } else {
+        ep.mode = EPI_TANH;
+      }
+      if (l == 0) rc = launch_sgemm(Mrows, FW, K0, G, K0, rm, M.fw[ti][0], ep, st);
+      else rc = launch_sgemm(Mrows, FW, FW, hb[l - 1], FW, rm, M.fw[ti][l], ep, st);
+      if (rc) return rc;
+    }
+    int cur = 0;
+    rc = launch_fit_energy(Mrows, rm, FW, hb[L - 1], tb[L - 1], M.fw[ti][L], M.fb[ti][L], M.fdt[ti][L - 1], Eatom,
+                           gz[cur], energy, D.N, st);
+    if (rc) return rc;
+    for (int l = L - 1; l >= 1; --l) {
+      Epi ep{};
+      ep.ld = FW;
+      ep.tin = tb[l - 1];
+      if (M.fdt[ti][l]) {  // residual at layer l: gH_{l-1} += gH_l
+        if (l == L - 1) ep.gvec = M.fw[ti][L];
+        else ep.gmat = gh[cur];
+      }
+      ep.out1 = gz[cur ^ 1];
+      if (l - 1 > 0 && M.fdt[ti][l - 1]) {
+        ep.mode = EPI_GRAD_RES;
+        ep.dt = M.fdt[ti][l - 1];
+        ep.out2 = gh[cur ^ 1];
+      } else {
+        ep.mode = EPI_GRAD;
+      }
+      rc = launch_sgemm(Mrows, FW, FW, gz[cur], FW, rm, M.fwT[ti][l], ep, st);
+      if (rc) return rc;
+      cur ^= 1;
+    }
+    Epi ep{};
+    ep.mode = EPI_STORE;
+    ep.out1 = G;
+    ep.ld = K0;
+    rc = launch_sgemm(Mrows, K0, FW, gz[cur], FW, rm, M.fwT[ti][0], ep, st);
+    if (rc) return rc;
+  }
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    if (M.E2 == 100) rc = launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    else rc = launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    if (rc) return rc;
+  }
+  return DPB_OK;
+}
+
+extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,
+                        int nframes, const int *type_count, const float *box, const int32_t *nbrs, const int *sel,
+                        double *energy, float *atom_energy, float *force, double *virial, uint32_t *status,
+                        void *workspace, size_t ws_bytes, void *stream_) {
+  if (!m || !pos || !box || !nbrs || !energy || !force || !status || !type_count || !sel || natoms <= 0 ||
+      nframes <= 0)
+    return DPB_ERR_INVALID_ARG;
+  if (precision != DPB_PREC_FP32 && precision != DPB_PREC_MIXED) return DPB_ERR_INVALID_ARG;
+  if (natoms >= (1 << 24)) return DPB_ERR_UNSUPPORTED;
+  size_t need = 0;
+  dpb_eval_workspace_bytes(m, natoms, nframes, &need);
+  if (!workspace || ws_bytes < need) return DPB_ERR_WORKSPACE;
+  SysDesc D;
+  int rc = fill_sys(m, natoms, nframes, type_count, sel, D);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream_;
+  const DevModel &M = m->dm;
+  const size_t NF = (size_t)natoms * nframes;
+  char *w = (char *)workspace;
+  float4 *F4 = (float4 *)w; w += al(NF * 16);
+  float *Eatom = (float *)w; w += al(NF * 4);
+  double *vir = virial;
+  double *vscratch = (double *)w; w += al((size_t)nframes * 9 * 8);
+  if (!vir) vir = vscratch;
+  DPB_CUDA_TRY(cudaMemsetAsync(F4, 0, NF * 16, st));
+  DPB_CUDA_TRY(cudaMemsetAsync(energy, 0, (size_t)nframes * 8, st));
+  DPB_CUDA_TRY(cudaMemsetAsync(vir, 0, (size_t)nframes * 72, st));
+  if (precision == DPB_PREC_FP32) {
+    rc = eval_fp32(M, D, pos, perm, box, nbrs, energy, F4, Eatom, vir, w, st);
+  } else {
+    if (!mixed_supported(M)) return DPB_ERR_UNSUPPORTED;
+    rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st);
+  }
+  if (rc) return rc;
+  return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, nframes, pos, status, st);
+}
+
+extern "C" uint64_t dpb_kernel_launch_count(void) { return g_launches.load(); }
+
+extern "C" const char *dpb_version(void) { return "dpb200 0.1 (sm_100a)"; }

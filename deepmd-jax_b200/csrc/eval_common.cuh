@@ -1,0 +1,78 @@
+// Device-side model description shared by the FP32 and mixed evaluation paths.
+#pragma once
+#include "dpb_common.cuh"
+#include <cuda_bf16.h>
+
+namespace dpb {
+
+constexpr int kMaxEmbedLayers = 3;
+constexpr int kMaxFitLayers = 4;  // hidden layers
+
+struct DevModel {
+  int ntypes;
+  int E0, E1, E2;      // embedding widths
+  int A;               // axis neurons
+  int nfit;            // hidden fitting layers
+  int FW[kMaxFitLayers];
+  float rcut;
+  float inv_nnbrs;
+  float mean[kMaxTypes];
+  float inv_std[kMaxTypes];
+  // FP32 weights (device), per embedding net k = i*ntypes + j
+  const float *ew[kMaxTypes * kMaxTypes][kMaxEmbedLayers];
+  const float *eb[kMaxTypes * kMaxTypes][kMaxEmbedLayers];
+  const float *tbias;
+  // fitting per centre type: kernels (in,out), biases, dt (NULL if none);
+  // the final layer (index nfit) has out_norm folded into kernel and
+  // out_norm * (bias + Ebias) as its bias.
+  const float *fw[kMaxTypes][kMaxFitLayers + 1];
+  const float *fb[kMaxTypes][kMaxFitLayers + 1];
+  const float *fdt[kMaxTypes][kMaxFitLayers];
+  // transposed fitting kernels (out,in) for the adjoint GEMMs
+  const float *fwT[kMaxTypes][kMaxFitLayers + 1];
+  // BF16 copies for the mixed path (layouts documented in mixed.cu)
+  const __nv_bfloat16 *ew_bf[kMaxTypes * kMaxTypes][kMaxEmbedLayers];
+  const __nv_bfloat16 *fw_bf[kMaxTypes][kMaxFitLayers + 1];
+  const __nv_bfloat16 *fwT_bf[kMaxTypes][kMaxFitLayers + 1];
+};
+
+// Frame/type geometry of one evaluation call.
+struct SysDesc {
+  int N, F, ntypes, S;
+  int offs[kMaxTypes + 1];
+  int sel[kMaxTypes];
+  int col[kMaxTypes + 1];
+};
+
+// Rows of the fitting GEMMs are the atoms of one centre type across frames:
+// row r -> atom (r / cnt) * N + off + r % cnt.
+struct RowMap {
+  int cnt, N, off;
+  __host__ __device__ __forceinline__ size_t atom(int r) const {
+    int f = r / cnt;
+    return (size_t)f * N + off + (r - f * cnt);
+  }
+};
+
+enum EpiMode : int {
+  EPI_STORE = 0,      // out1 = acc
+  EPI_TANH = 1,       // t = tanh(acc + b); out1 = t; out2 = t (H = t)
+  EPI_TANH_RES = 2,   // t = tanh(acc + b); out1 = t; out2 = t * dt + Hprev
+  EPI_GRAD_RES = 3,   // gH = acc + gadd; out2 = gH; out1 = gZ = gH * dt * (1 - t^2)
+  EPI_GRAD = 4,       // gH = acc + gadd; out1 = gZ = gH * (1 - t^2)
+};
+
+// Fused epilogue of one fitting-layer GEMM (forward or adjoint).
+struct Epi {
+  int mode;
+  const float *bias;    // [Nc]
+  const float *dt;      // [Nc]
+  const float *hprev;   // per atom, ld
+  const float *tin;     // per atom tanh values of the layer below, ld
+  const float *gvec;    // [Nc] broadcast addend (or NULL)
+  const float *gmat;    // per atom addend (or NULL)
+  float *out1, *out2;   // per atom, ld
+  int ld;
+};
+
+}  // namespace dpb

@@ -1,0 +1,328 @@
+// Typed neighbour list (cell binning + per-centre scan), sm_100a.
+//
+// Semantics (bit-exact target): the reference canonicalises coordinates as
+// (coord % box) * (ref/box) * (1 - 5e-7) in float32 and sorts atoms by type
+// (deepmd_jax/md_utils.py:364-373); jax_md's dense neighbour list keeps j != i
+// with float32 d2 < cutoff^2 where d = mod(Ri - Rj + L/2, L) - L/2; get_nm
+// (md_utils.py:431-459) then keeps per neighbour type the sel_j smallest
+// indices in ascending order, type-local, padded with N, and flags overflow
+// when more than sel_j exist.
+//
+// Layout: cells are binned per frame; a warp owns one centre atom, walks the
+// 27 (or fewer, for 2-cell or 1-cell axes) neighbouring cells, appends hits
+// per type into shared memory with ballots, then ranks the hits (indices are
+// distinct, so rank = number of smaller hits) and writes the sorted prefix.
+#include "dpb_common.cuh"
+#include <algorithm>
+#include <cmath>
+
+namespace dpb {
+
+struct NlGrid {
+  int nc[3];
+  int ncell;      // per frame
+  int image_mode; // 1: explicit images (min(L) < 2 rc)
+  int nimg[3];    // image range per axis in image mode
+};
+
+static NlGrid make_grid(const float box[3], float rc) {
+  NlGrid g;
+  g.image_mode = 0;
+  for (int d = 0; d < 3; ++d) {
+    int n = (int)floorf(box[d] / rc);
+    g.nc[d] = std::max(1, std::min(n, 512));
+    if (box[d] < 2.f * rc) g.image_mode = 1;
+    g.nimg[d] = (int)floorf(rc / box[d] + 0.5f);  // images with |minimg + m L| < rc
+  }
+  if (g.image_mode) {
+    g.nc[0] = g.nc[1] = g.nc[2] = 1;
+  }
+  g.ncell = g.nc[0] * g.nc[1] * g.nc[2];
+  return g;
+}
+
+__global__ void nl_canon_kernel(const float *__restrict__ pos, const int32_t *__restrict__ perm,
+                                int N, int F, float3 L, float3 scale, float3 RB, int3 nc,
+                                float *__restrict__ canon, int *__restrict__ atom_cell,
+                                int *__restrict__ cell_count) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N * F) return;
+  int f = g / N, k = g - f * N;
+  int src = perm ? perm[k] : k;
+  const float *p = pos + ((size_t)f * N + src) * 3;
+  const float shrink = 0.9999995f;  // float32(1 - 5e-7)
+  float c0 = __fmul_rn(__fmul_rn(jmod(p[0], L.x), scale.x), shrink);
+  float c1 = __fmul_rn(__fmul_rn(jmod(p[1], L.y), scale.y), shrink);
+  float c2 = __fmul_rn(__fmul_rn(jmod(p[2], L.z), scale.z), shrink);
+  canon[(size_t)g * 3 + 0] = c0;
+  canon[(size_t)g * 3 + 1] = c1;
+  canon[(size_t)g * 3 + 2] = c2;
+  // cell bins of the reference box (canonical coordinates live in [0, ref))
+  int ix = min(max((int)(c0 / RB.x * nc.x), 0), nc.x - 1);
+  int iy = min(max((int)(c1 / RB.y * nc.y), 0), nc.y - 1);
+  int iz = min(max((int)(c2 / RB.z * nc.z), 0), nc.z - 1);
+  int cell = (ix * nc.y + iy) * nc.z + iz;
+  atom_cell[g] = cell;
+  atomicAdd(&cell_count[f * (nc.x * nc.y * nc.z) + cell], 1);
+}
+
+// Exclusive scan of n ints with one block (n up to a few million).
+__global__ void nl_scan_kernel(const int *__restrict__ in, int *__restrict__ out, int n) {
+  __shared__ int part[1024];
+  int t = threadIdx.x;
+  int per = (n + blockDim.x - 1) / blockDim.x;
+  int b = t * per, e = min(b + per, n);
+  int s = 0;
+  for (int i = b; i < e; ++i) s += in[i];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = t ? part[t - 1] : 0;
+  for (int i = b; i < e; ++i) {
+    out[i] = run;
+    run += in[i];
+  }
+  if (t == blockDim.x - 1) out[n] = part[t];
+}
+
+__global__ void nl_scatter_kernel(const int *__restrict__ atom_cell, const int *__restrict__ cell_start,
+                                  int *__restrict__ cursor, int *__restrict__ cell_atoms, int N, int F,
+                                  int ncell) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N * F) return;
+  int f = g / N;
+  int c = f * ncell + atom_cell[g];
+  int slot = atomicAdd(&cursor[c], 1);
+  cell_atoms[cell_start[c] + slot] = g - f * N;  // frame-local sorted index
+}
+
+struct NlParams {
+  int N, F, ntypes, cap;
+  int offs[kMaxTypes + 1];
+  int sel[kMaxTypes];
+  int col[kMaxTypes + 1];
+  float3 L;      // reference box (canonical frame)
+  float rc2;
+  int3 nc;
+  int image_mode;
+  int3 nimg;
+};
+
+// Append the hits of one 32-candidate round into the per-type lists.
+__device__ __forceinline__ void append_hits(bool hit, int t, int key, int ntypes, int cap, int *cnt,
+                                            int *lists) {
+  unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+#pragma unroll
+  for (int tt = 0; tt < kMaxTypes; ++tt) {
+    if (tt >= ntypes) break;
+    unsigned m = __ballot_sync(0xffffffffu, hit && t == tt);
+    if (m == 0u) continue;
+    int base = cnt[tt];
+    if (hit && t == tt) {
+      int p = base + __popc(m & lt);
+      if (p < cap) lists[tt * cap + p] = key;
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) cnt[tt] = base + __popc(m);
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ bool pair_hit(float3 ci, float3 cj, float3 L, float rc2) {
+  // jax_md.space.periodic displacement, centre minus neighbour, float32
+  float hx = 0.5f * L.x, hy = 0.5f * L.y, hz = 0.5f * L.z;
+  float dx = __fsub_rn(jmod(__fadd_rn(__fsub_rn(ci.x, cj.x), hx), L.x), hx);
+  float dy = __fsub_rn(jmod(__fadd_rn(__fsub_rn(ci.y, cj.y), hy), L.y), hy);
+  float dz = __fsub_rn(jmod(__fadd_rn(__fsub_rn(ci.z, cj.z), hz), L.z), hz);
+  float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+  return d2 < rc2;
+}
+
+__global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float *__restrict__ canon,
+                                                        const int *__restrict__ cell_start,
+                                                        const int *__restrict__ cell_atoms,
+                                                        int32_t *__restrict__ nbrs,
+                                                        int32_t *__restrict__ counts,
+                                                        uint32_t *__restrict__ status) {
+  extern __shared__ int smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  int *cnt = smem + warp * kMaxTypes;
+  int *lists = smem + wpb * kMaxTypes + warp * P.ntypes * P.cap;
+  int g = blockIdx.x * wpb + warp;
+  if (g >= P.N * P.F) return;
+  const int f = g / P.N, i = g - f * P.N;
+  const float *cf = canon + (size_t)f * P.N * 3;
+  float3 ci = make_float3(cf[i * 3], cf[i * 3 + 1], cf[i * 3 + 2]);
+  if (lane < kMaxTypes) cnt[lane] = 0;
+  __syncwarp();
+
+  if (!P.image_mode) {
+    const int ncell = P.nc.x * P.nc.y * P.nc.z;
+    const int *cs = cell_start + f * ncell;
+    int ix = min(max((int)(ci.x / P.L.x * P.nc.x), 0), P.nc.x - 1);
+    int iy = min(max((int)(ci.y / P.L.y * P.nc.y), 0), P.nc.y - 1);
+    int iz = min(max((int)(ci.z / P.L.z * P.nc.z), 0), P.nc.z - 1);
+    int lox = P.nc.x >= 3 ? -1 : 0, hix = P.nc.x >= 2 ? 1 : 0;
+    int loy = P.nc.y >= 3 ? -1 : 0, hiy = P.nc.y >= 2 ? 1 : 0;
+    int loz = P.nc.z >= 3 ? -1 : 0, hiz = P.nc.z >= 2 ? 1 : 0;
+    for (int ox = lox; ox <= hix; ++ox)
+      for (int oy = loy; oy <= hiy; ++oy)
+        for (int oz = loz; oz <= hiz; ++oz) {
+          int cx = (ix + ox + P.nc.x) % P.nc.x;
+          int cy = (iy + oy + P.nc.y) % P.nc.y;
+          int cz = (iz + oz + P.nc.z) % P.nc.z;
+          int c = (cx * P.nc.y + cy) * P.nc.z + cz;
+          int b = cs[c], e = cs[c + 1];
+          for (int base = b; base < e; base += 32) {
+            int q = base + lane;
+            bool hit = false;
+            int j = 0, t = 0;
+            if (q < e) {
+              j = cell_atoms[q];
+              float3 cj = make_float3(cf[j * 3], cf[j * 3 + 1], cf[j * 3 + 2]);
+              hit = (j != i) && pair_hit(ci, cj, P.L, P.rc2);
+              t = type_of(j, P.offs, P.ntypes);
+            }
+            append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
+          }
+        }
+  } else {
+    // small box: j is listed once if any periodic image lies within rc
+    const int nx = 2 * P.nimg.x + 1, ny = 2 * P.nimg.y + 1, nz = 2 * P.nimg.z + 1;
+    const int nim = nx * ny * nz;
+    for (int base = 0; base < P.N; base += 32) {
+      const int j = base + lane;
+      bool hit = false;
+      int t = 0;
+      if (j < P.N) {
+        const float3 cj = make_float3(cf[j * 3], cf[j * 3 + 1], cf[j * 3 + 2]);
+        const float3 d0 = make_float3(shift_ortho(cj.x - ci.x, P.L.x), shift_ortho(cj.y - ci.y, P.L.y),
+                                      shift_ortho(cj.z - ci.z, P.L.z));
+        for (int m = 0; m < nim && !hit; ++m) {
+          const int a = m / (ny * nz) - P.nimg.x, bb = (m / nz) % ny - P.nimg.y, cc = m % nz - P.nimg.z;
+          if (j == i && a == 0 && bb == 0 && cc == 0) continue;
+          const float x = d0.x + a * P.L.x, y = d0.y + bb * P.L.y, z = d0.z + cc * P.L.z;
+          hit = x * x + y * y + z * z < P.rc2;
+        }
+        t = type_of(j, P.offs, P.ntypes);
+      }
+      append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
+    }
+  }
+  __syncwarp();
+  // rank-sort each type's hits and write the sel_t smallest
+  const int S = P.col[P.ntypes];
+  int32_t *out = nbrs + (size_t)g * S;
+  bool ovf = false;
+  for (int t = 0; t < P.ntypes; ++t) {
+    int n = cnt[t];
+    if (counts && lane == 0) counts[(size_t)g * P.ntypes + t] = n;
+    ovf |= (n > P.sel[t]) || (n > P.cap);
+    int nn = min(n, P.cap);
+    const int *L_ = lists + t * P.cap;
+    for (int e = lane; e < nn; e += 32) {
+      int key = L_[e];
+      int rank = 0;
+      for (int e2 = 0; e2 < nn; ++e2) rank += (L_[e2] < key);
+      if (rank < P.sel[t]) out[P.col[t] + rank] = key - P.offs[t];
+    }
+    for (int e = nn + lane; e < P.sel[t]; e += 32) out[P.col[t] + e] = P.N;
+  }
+  if (ovf && lane == 0) atomicOr(status, DPB_ST_NLIST_OVERFLOW);
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" int dpb_nlist_workspace_bytes(int natoms, int nframes, const float box[3], float rc,
+                                         size_t *bytes) {
+  if (!bytes || natoms <= 0 || nframes <= 0 || !box || rc <= 0) return DPB_ERR_INVALID_ARG;
+  NlGrid g = make_grid(box, rc);
+  size_t NF = (size_t)natoms * nframes, C = (size_t)g.ncell * nframes;
+  *bytes = align_up(C * 4) * 2 + align_up((C + 1) * 4) + align_up(NF * 4) * 2 + align_up(NF * 12);
+  return DPB_OK;
+}
+
+extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
+                               const int *type_count, const int *sel, const float box[3],
+                               const float *ref_box, float rc, int32_t *nbrs, float *ref_pos,
+                               int32_t *counts, uint32_t *status, void *workspace, size_t ws_bytes,
+                               void *stream_) {
+  if (!pos || natoms <= 0 || nframes <= 0 || ntypes < 1 || ntypes > kMaxTypes || !type_count || !sel ||
+      !box || !nbrs || !status || rc <= 0)
+    return DPB_ERR_INVALID_ARG;
+  if (natoms >= (1 << 24)) return DPB_ERR_UNSUPPORTED;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  float rb[3] = {box[0], box[1], box[2]};
+  if (ref_box) { rb[0] = ref_box[0]; rb[1] = ref_box[1]; rb[2] = ref_box[2]; }
+  // jax_md receives rcut * max(ref/box) as float32 and squares it in float32
+  float smax = std::max(rb[0] / box[0], std::max(rb[1] / box[1], rb[2] / box[2]));
+  float rc_eff = rc * smax;
+  NlGrid g = make_grid(rb, rc_eff);
+  if (g.image_mode && (g.nimg[0] > 4 || g.nimg[1] > 4 || g.nimg[2] > 4)) return DPB_ERR_UNSUPPORTED;
+  size_t need = 0;
+  dpb_nlist_workspace_bytes(natoms, nframes, rb, rc_eff, &need);
+  if (!workspace || ws_bytes < need) return DPB_ERR_WORKSPACE;
+  NlParams P;
+  P.N = natoms; P.F = nframes; P.ntypes = ntypes;
+  int smax_sel = 0, off = 0, col = 0;
+  for (int t = 0; t < ntypes; ++t) {
+    if (type_count[t] < 0 || sel[t] < 0) return DPB_ERR_INVALID_ARG;
+    P.offs[t] = off; off += type_count[t];
+    P.sel[t] = sel[t]; P.col[t] = col; col += sel[t];
+    smax_sel = std::max(smax_sel, sel[t]);
+  }
+  if (off != natoms) return DPB_ERR_INVALID_ARG;
+  for (int t = ntypes; t <= kMaxTypes; ++t) P.offs[t] = natoms;
+  P.col[ntypes] = col;
+  // hit buffer per type: the sorted prefix is exact whenever a type's count
+  // fits (counts above cap only occur with overflow already flagged)
+  int cap = 256;
+  while (cap < smax_sel + 1) cap <<= 1;
+  if (cap > 1024) return DPB_ERR_UNSUPPORTED;
+  P.cap = cap;
+  P.L = make_float3(rb[0], rb[1], rb[2]);
+  P.rc2 = rc_eff * rc_eff;
+  P.nc = make_int3(g.nc[0], g.nc[1], g.nc[2]);
+  P.image_mode = g.image_mode;
+  P.nimg = make_int3(g.nimg[0], g.nimg[1], g.nimg[2]);
+
+  size_t NF = (size_t)natoms * nframes, C = (size_t)g.ncell * nframes;
+  char *w = (char *)workspace;
+  int *cell_count = (int *)w; w += align_up(C * 4);
+  int *cursor = (int *)w; w += align_up(C * 4);
+  int *cell_start = (int *)w; w += align_up((C + 1) * 4);
+  int *atom_cell = (int *)w; w += align_up(NF * 4);
+  int *cell_atoms = (int *)w; w += align_up(NF * 4);
+  float *canon = ref_pos ? ref_pos : (float *)w;
+
+  DPB_CUDA_TRY(cudaMemsetAsync(cell_count, 0, C * 4, stream));
+  DPB_CUDA_TRY(cudaMemsetAsync(cursor, 0, C * 4, stream));
+  float3 L = make_float3(box[0], box[1], box[2]);
+  float3 scale = make_float3(rb[0] / box[0], rb[1] / box[1], rb[2] / box[2]);
+  int nb = (int)((NF + 255) / 256);
+  nl_canon_kernel<<<nb, 256, 0, stream>>>(pos, perm, natoms, nframes, L, scale, P.L, P.nc, canon, atom_cell,
+                                          cell_count);
+  nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C);
+  nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, natoms, nframes,
+                                            g.ncell);
+  const int threads = 256, wpb = threads / 32;
+  size_t smem = (size_t)wpb * kMaxTypes * 4 + (size_t)wpb * ntypes * cap * 4;
+  if (smem > 48 * 1024) {
+    DPB_CUDA_TRY(cudaFuncSetAttribute(nl_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  nl_search_kernel<<<(int)((NF + wpb - 1) / wpb), threads, smem, stream>>>(P, canon, cell_start, cell_atoms,
+                                                                           nbrs, counts, status);
+  count_launch(4);
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}

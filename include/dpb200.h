@@ -1,0 +1,159 @@
+/*
+ * dpb200.h — C ABI of the B200-native Deep Potential (se_a) evaluation and MD
+ * step library (libdpb200.so).
+ *
+ * Conventions
+ *   - Every compute entry point takes caller-owned DEVICE pointers and a
+ *     cudaStream_t (passed as void*); nothing is synchronised unless stated.
+ *   - Return value: 0 on success, or a DPB_ERR_* code (>= 256) for host-side
+ *     failures.  Conditions detected on the device are OR-ed into a caller
+ *     owned uint32 status word with the bit meanings of the reference's error
+ *     code (deepmd_jax/md.py:618-641): 1 box shrank, 2 neighbour overflow,
+ *     4 overflow in a previous chunk, 8 lattice overflow, 16 NaN/Inf.
+ *   - Atoms inside a frame are in type-sorted order (stable sort of the user
+ *     order, deepmd_jax/utils.py:329-340) unless a permutation is passed.
+ *   - Frames: `nframes` frames of `natoms` atoms share type counts; arrays are
+ *     frame-major ((F,N,3) positions, (F,N,S) neighbour lists, (F,3) boxes).
+ *
+ * Reference interfaces each entry point replaces are cited per function.
+ */
+#ifndef DPB200_H
+#define DPB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DPB_API __attribute__((visibility("default")))
+#else
+#define DPB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPB_OK 0
+#define DPB_ST_BOX_SHRUNK 1u
+#define DPB_ST_NLIST_OVERFLOW 2u
+#define DPB_ST_NLIST_OVERFLOW_PREV 4u
+#define DPB_ST_LATTICE_OVERFLOW 8u
+#define DPB_ST_NONFINITE 16u
+
+#define DPB_ERR_INVALID_ARG 256
+#define DPB_ERR_CUDA 257
+#define DPB_ERR_UNSUPPORTED 258
+#define DPB_ERR_WORKSPACE 259
+#define DPB_ERR_NO_DEVICE 260
+
+/* Precision of the evaluation.
+ * DPB_PREC_FP32:  all arithmetic in FP32 (the reference's float32 with
+ *                 jax_default_matmul_precision='float32', deepmd_jax/__init__.py:10).
+ * DPB_PREC_MIXED: embedding/fitting contractions in BF16 on the tensor cores
+ *                 with FP32 accumulation; s(r), env matrix, first embedding
+ *                 layer, per-atom energies and forces in FP32. */
+#define DPB_PREC_FP32 0
+#define DPB_PREC_MIXED 1
+
+/* Neighbour entries are type-local atom indices (int32, < 2^24); the value
+ * natoms marks an empty slot, as in the reference's nbrs_nm padding.
+ * Small boxes (some L < 2 * cutoff): an entry means "some periodic image of
+ * j lies within the cutoff" and dpb_eval sums every image of j within rcut,
+ * the reference's lattice path (deepmd_jax/utils.py:66-78). */
+#define DPB_NBR_INDEX_MASK 0x00FFFFFF
+
+typedef struct dpb_model dpb_model;
+
+/* Model description.  Host pointers, float32 arrays in the reference's
+ * parameter pytree layout (deepmd_jax/train.py:288-304,
+ * deepmd_jax/dpmodel.py:50-81): kernels are (in, out) row-major. */
+typedef struct {
+  int ntypes;                 /* 1..4 */
+  int n_embed;                /* number of embedding layers (3) */
+  int embed_widths[4];        /* e.g. 25,50,100 */
+  int n_fit;                  /* number of hidden fitting layers (3) */
+  int fit_widths[4];          /* e.g. 240,240,240 */
+  int axis;                   /* axis_neuron A (16) */
+  double rcut;
+  double nnbrs;               /* params['Nnbrs'] */
+  double out_norm;
+  const double *sr_mean;      /* [ntypes] */
+  const double *sr_std;       /* [ntypes] */
+  const double *ebias;        /* [ntypes] */
+  const float *const *embed_kernel; /* [ntypes*ntypes*n_embed], net k = i*ntypes+j */
+  const float *const *embed_bias;   /* same */
+  const float *tbias;               /* [W] */
+  const float *const *fit_kernel;   /* [ntypes*(n_fit+1)] */
+  const float *const *fit_bias;     /* same */
+  const float *const *fit_dt;       /* [ntypes*n_fit], NULL where the layer has no dt */
+} dpb_model_desc;
+
+/* Upload the weights (FP32 and BF16 copies) to the current device.
+ * Replaces: model loading + replication, deepmd_jax/utils.py:230-237. */
+DPB_API int dpb_model_create(const dpb_model_desc *desc, dpb_model **out);
+DPB_API int dpb_model_destroy(dpb_model *model);
+
+/* ---------------------------------------------------------------- neighbour list */
+
+/* Workspace bytes needed by dpb_nlist_build for one frame layout. */
+DPB_API int dpb_nlist_workspace_bytes(int natoms, int nframes, const float box[3],
+                              float rcut_plus_skin, size_t *bytes);
+
+/* Typed neighbour list in the reference's nbrs_nm semantics.
+ * Replaces: typed_neighbor_list(...).allocate/.update, get_nm
+ * (deepmd_jax/md_utils.py:353-461) over jax_md.partition.neighbor_list.
+ *   pos        (F,N,3) float32 device; type-sorted order unless perm != NULL
+ *   perm       (N) int32 device: sorted index -> user index, or NULL
+ *   type_count [ntypes] host; sel [ntypes] host (capacity per neighbour type)
+ *   box        [3] host, the current box; ref_box [3] host or NULL (= box)
+ *   nbrs       (F,N,sum(sel)) int32 device out: block j holds the type-j
+ *              neighbours' type-local indices in ascending order, pad = N
+ *   ref_pos    (F,N,3) float32 device out or NULL: canonical coordinates used
+ *              for the drift test (reference_position)
+ *   counts     (F,N,ntypes) int32 device out or NULL: neighbours per type
+ *   status     device word, DPB_ST_NLIST_OVERFLOW is OR-ed in when a count
+ *              exceeds sel (the reference's did_buffer_overflow).
+ * Boxes with min(L) < 2*rcut_plus_skin list j once if any image of j is
+ * within the cutoff (j == i included when a non-zero image is). */
+DPB_API int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms, int nframes,
+                    int ntypes, const int *type_count, const int *sel,
+                    const float box[3], const float *ref_box, float rcut_plus_skin,
+                    int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status,
+                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------- evaluation */
+
+/* Workspace bytes needed by dpb_eval for F frames of N atoms. */
+DPB_API int dpb_eval_workspace_bytes(const dpb_model *model, int natoms, int nframes, size_t *bytes);
+
+/* Energy, per-atom energy, forces and virial of F frames.
+ * Replaces: DPModel.apply / energy_and_force (deepmd_jax/dpmodel.py:30-108)
+ * and the energy_fn / force_fn pair of deepmd_jax/md.py:292,416-444.
+ *   pos      (F,N,3) float32 device (type-sorted unless perm != NULL)
+ *   perm     (N) int32 device or NULL; outputs are written in the same order
+ *            as the positions
+ *   box      (F,3) float32 device (orthorhombic box lengths)
+ *   nbrs     (F,N,sum(sel)) int32 device, layout of dpb_nlist_build
+ *   energy   (F) float64 device out (total energy per frame)
+ *   atom_energy (F,N) float32 device out or NULL
+ *   force    (F,N,3) float32 device out, -dE/dpos
+ *   virial   (F,9) float64 device out or NULL: W_ab = -sum_pairs x_a dE/dx_b
+ *            with x = r_j - r_i; trace(W) = -dU/deps of a uniform strain
+ *            (deepmd_jax/md_utils.py:139-159)
+ *   status   device word (DPB_ST_NONFINITE on NaN/Inf energies). */
+DPB_API int dpb_eval(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
+             int natoms, int nframes, const int *type_count, const float *box,
+             const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,
+             float *force, double *virial, uint32_t *status, void *workspace,
+             size_t workspace_bytes, void *stream);
+
+/* Number of kernels the library launched since load (for launch accounting). */
+DPB_API uint64_t dpb_kernel_launch_count(void);
+
+/* Library version string. */
+DPB_API const char *dpb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DPB200_H */

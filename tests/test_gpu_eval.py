@@ -1,0 +1,82 @@
+"""FP32 evaluation on the GPU vs the float64 oracle and vs the golden
+vectors produced from the reference's own model source.
+
+Tolerances (FP32 kernels against FP64): energy |dE| <= 2e-6 * sum|E_atom| +
+1e-6 eV; forces max|dF| <= 2e-4 * max|F|; virial max|dW| <= 2e-4 * max|W|.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_helpers import run_gpu
+from make_golden import golden_models
+from oracle import model as om
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_model.npz"))
+MODELS = golden_models()
+
+
+def check_close(got, ref, name):
+    eabs = np.abs(ref["atom_energy"]).sum()
+    assert abs(got["energy"] - ref["energy"]) <= 2e-6 * eabs + 1e-6, (name, got["energy"], ref["energy"])
+    fmax = np.abs(ref["force"]).max()
+    assert np.abs(got["force"] - ref["force"]).max() <= 2e-4 * fmax, (name, np.abs(got["force"] - ref["force"]).max(), fmax)
+    if ref.get("virial") is not None:
+        wmax = np.abs(ref["virial"]).max()
+        assert np.abs(got["virial"] - ref["virial"]).max() <= 2e-4 * wmax + 1e-9, name
+    if ref.get("atom_energy") is not None:
+        assert np.abs(got["atom_energy"] - ref["atom_energy"]).max() <= 2e-6 * np.abs(ref["atom_energy"]).max() + 1e-6
+
+
+@pytest.mark.parametrize("key,sysk,mk", [("A", "A", "A"), ("B", "A", "B"), ("D", "D", "B"), ("E", "E", "B")])
+def test_fp32_vs_reference_golden(key, sysk, mk):
+    p, v = MODELS[mk]
+    pos, box, typ = G[sysk + "_pos"], G[sysk + "_box"], G[sysk + "_type"]
+    got = run_gpu(p, v, pos, box, typ)
+    assert got["status"] == 0
+    ref_o = om.energy_force(om.OracleModel(p, v, torch.float64), pos, box, typ)
+    ref = dict(energy=float(G[key + "_E"]), force=G[key + "_F"], atom_energy=ref_o["atom_energy"],
+               virial=ref_o["virial"])
+    check_close(dict(energy=got["energy"][0], force=got["force"][0], virial=got["virial"][0],
+                     atom_energy=got["atom_energy"][0]), ref, key)
+
+
+def test_fp32_batched_frames_match_single():
+    from deepmd_jax_b200.systems import water_box
+    p, v = MODELS["B"]
+    ws = [water_box(8, 24.83, seed=s) for s in (11, 12, 13)]
+    pos = np.stack([w["position"] for w in ws])
+    got = run_gpu(p, v, pos, ws[0]["box"], ws[0]["type_idx"])
+    m = om.OracleModel(p, v, torch.float64)
+    for f, w in enumerate(ws):
+        ref = om.energy_force(m, w["position"], w["box"], w["type_idx"],
+                              nbrs=got["nbrs"][f], sel=[46, 92])
+        check_close(dict(energy=got["energy"][f], force=got["force"][f], virial=got["virial"][f],
+                         atom_energy=got["atom_energy"][f]), ref, "frame%d" % f)
+
+
+def test_fp32_default_train_widths():
+    """The reference train() default architecture (embed 32-32-64, fit
+    128^3, axis 12; deepmd_jax/train.py:24-27)."""
+    from deepmd_jax_b200.systems import water_box, init_dp_params
+    from make_golden import randomize_model
+    w = water_box(8, 24.83, seed=5)
+    p, v = randomize_model(*init_dp_params(embed_widths=(32, 32, 64), fit_widths=(128, 128, 128), axis=12,
+                                           nnbrs=90.0, seed=3), seed=4)
+    got = run_gpu(p, v, w["position"], w["box"], w["type_idx"])
+    ref = om.energy_force(om.OracleModel(p, v, torch.float64), w["position"], w["box"], w["type_idx"],
+                          nbrs=got["nbrs"][0], sel=[46, 92])
+    check_close(dict(energy=got["energy"][0], force=got["force"][0], virial=got["virial"][0],
+                     atom_energy=got["atom_energy"][0]), ref, "default")
+
+
+def test_nonfinite_sets_status_bit():
+    p, v = MODELS["B"]
+    pos = G["A_pos"].copy()
+    pos[3, 0] = np.nan
+    got = run_gpu(p, v, pos, G["A_box"], G["A_type"])
+    assert got["status"] & 16
