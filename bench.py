@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark: MD throughput (atom-steps/s) of 98,304-atom water NVE on one
+B200, BF16/FP32 mixed form beside the plain FP32 form.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One "step" is one velocity-Verlet MD step of the whole box through the
+device-resident engine: drift test + gated neighbour rebuild, status checks,
+the force/virial evaluation and both half kicks (deepmd_jax/md.py:763-795).
+Synthetic input: the water builder (O on a 32^3 lattice with N(0, 0.1 A)
+jitter, H at gas-phase geometry, Maxwell-Boltzmann velocities at 300 K) and
+the random-init se_a model (25-50-100 / 240^3 / axis 16, rcut 6 A).
+Multi-GPU: the MD path does not shard here (replicas only) - each rank runs
+its own replica and the job value is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "deepmd-jax_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s, 98k-atom water MD (NVE, dt 0.5 fs), mixed vs plain FP32 on 1 B200"
+N_SIDE, BOX = 32, 99.3
+DT = 0.5
+CHUNK = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------- work model
+EMB_FWD_FLOP_ROW = 2 * (25 + 25 * 50 + 50 * 100) + 2 * 10 * 100          # 14,550
+EMB_BWD_FLOP_ROW = 2 * (25 + 2 * 25 * 50 + 2 * 50 * 100) + 2 * 2 * 10 * 100  # 29,050
+FIT_FLOP_ATOM = 2 * 2 * (1600 * 240 + 2 * 240 * 240)                       # fwd + adjoint GEMMs
+G_FLOP_ATOM = 2 * 16 * 100 * 10 * 3                                        # G and its adjoint
+
+
+def rows_within_rcut(pos_sorted, nbrs, type_count, sel, box, rcut):
+    """Average number of (centre, neighbour) rows with 0 < r < rcut."""
+    import torch
+    N = pos_sorted.shape[0]
+    offs = [0]
+    for c in type_count:
+        offs.append(offs[-1] + c)
+    col = 0
+    total = 0
+    L = torch.tensor(box, dtype=torch.float32, device=pos_sorted.device)
+    for j, s in enumerate(sel):
+        idx = nbrs[:, col:col + s].long()
+        valid = idx < type_count[j]
+        g = offs[j] + idx.clamp(max=type_count[j] - 1)
+        d = pos_sorted[g] - pos_sorted[:, None, :]
+        d = torch.remainder(d - L / 2, L) - L / 2
+        r = d.norm(dim=-1)
+        total += int(((r < rcut) & (r > 1e-14) & valid).sum())
+        col += s
+    return total / N
+
+
+# ----------------------------------------------------------------------------- reference arm
+def reference_arm(args):
+    """The reference's own CPU implementation cannot run here (pure JAX, jax is
+    not installed); its CPU restatement (oracle, torch FP32 on all host cores)
+    is timed instead on MD steps of the 12,288-atom box."""
+    import torch
+    import numpy as np
+    from deepmd_jax_b200.systems import water_box, init_dp_params, nnbrs_rule, MASS_UNIT_CONVERSION
+    from oracle import model as om, nlist as onl
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    w0 = water_box(4, 12.42, seed=0)
+    params, variables = init_dp_params(nnbrs=nnbrs_rule(w0["position"], w0["box"], w0["type_idx"], 6.0))
+    w = water_box(16, 49.66, seed=0)
+    m = om.OracleModel(params, variables, torch.float32)
+    cnt = np.bincount(w["type_idx"], minlength=2)
+    sel = [46, 92]
+
+    # the neighbour list (skin 0.3 A) stays valid over the few timed steps,
+    # as in the reference's soft update; it is built once, outside the timing
+    c = onl.canonicalize(w["position"], w["box"], w["type_idx"])
+    nb, _, _ = onl.typed_nlist(c, w["box"].astype(np.float32), onl.cutoff_sq(6.3), cnt, sel)
+
+    def forces(pos):
+        r = om.energy_force(m, pos, w["box"], w["type_idx"], nbrs=nb, sel=sel, virial=False)
+        return r["force"]
+
+    mass = (w["mass"] * MASS_UNIT_CONVERSION)[:, None]
+    r, p = w["position"].copy(), w["velocity"] * mass
+    F = forces(r)
+    steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p = p + 0.5 * DT * F
+        r = r + DT * p / mass
+        F = forces(r)
+        p = p + 0.5 * DT * F
+    dt = time.perf_counter() - t0
+    N = len(r)
+    val = N * steps / dt
+    return {"metric": METRIC, "value": val, "unit": "atom-steps/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "water MD NVE; CPU sample: 12,288-atom box (4,096 H2O, L=49.66 A)",
+                       "sample_atoms": N},
+            "cpu_baseline": {"value": val, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+                             "sample": "%d velocity-Verlet steps of the 12,288-atom water box with the FP32 "
+                                       "torch restatement of the reference model (the reference is JAX and "
+                                       "cannot be installed here)" % steps},
+            "e2e": {"value": val, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline_sample():
+    """Short CPU sample for the GPU arm's cpu_baseline key (same port)."""
+    class A:
+        steps, warmup, gpus = 1, 0, 1
+    r = reference_arm(A)
+    return r["cpu_baseline"]
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def gpu_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from deepmd_jax_b200 import _lib
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import water_box, init_dp_params, nnbrs_rule
+    torch.cuda.set_device(local_rank)
+    lib = _lib.load()
+    lib.dpb_profile_enable.argtypes = [ctypes.c_int]
+    lib.dpb_profile_read.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w0 = water_box(4, 12.42, seed=0)
+    params, variables = init_dp_params(nnbrs=nnbrs_rule(w0["position"], w0["box"], w0["type_idx"], 6.0))
+    w = water_box(N_SIDE, BOX, seed=rank)
+    N = len(w["position"])
+
+    def make_sim(precision):
+        return Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVE", DT,
+                          w["position"], initial_velocity=w["velocity"], report_interval=10 ** 9,
+                          precision=precision, verbose=False)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed_device_steps(sim, K, graph=True):
+        sim._use_graph = graph
+        n_full, rem = divmod(K, CHUNK)
+        barrier()
+        torch.cuda.synchronize()
+        l0 = lib.dpb_kernel_launch_count()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(n_full):
+            sim._run_chunk(CHUNK, None, None)
+        if rem:
+            sim._run_chunk(rem, None, None)
+        e.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = s.elapsed_time(e)
+        launches = lib.dpb_kernel_launch_count() - l0
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), launches
+
+    results = {}
+    for prec in (["fp32", "mixed"] if args.precision == "mixed" else ["fp32"]):
+        try:
+            sim = make_sim(prec)
+        except Exception as ex:  # precision not available
+            results[prec] = {"error": str(ex)}
+            continue
+        timed_device_steps(sim, max(args.warmup, 3))
+        with ClockSampler(local_rank) as clk:
+            ms, launches = timed_device_steps(sim, args.steps)
+        r = sim._report_struct()
+        # per-stage durations, live, with CUDA events on the launching stream (direct launches)
+        lib.dpb_profile_enable(1)
+        _, _ = timed_device_steps(sim, min(args.steps, 10), graph=False)
+        stages = {}
+        for sid, name in enumerate(["nlist", "embed_fwd", "fit", "embed_bwd", "integrate",
+                                    "mixed_embed_fwd", "mixed_fit", "mixed_embed_bwd"]):
+            msr, cnt = ctypes.c_double(), ctypes.c_uint64()
+            lib.dpb_profile_read(sid, ctypes.byref(msr), ctypes.byref(cnt))
+            if cnt.value:
+                stages[name] = (msr.value / cnt.value, cnt.value)
+        lib.dpb_profile_enable(0)
+        results[prec] = dict(ms=ms, launches=launches, clocks=clk.summary(), stages=stages, sim=sim,
+                             status=int(r.status), rebuilds=int(r.rebuilds), steps=int(r.steps))
+    head = "mixed" if "mixed" in results and "error" not in results["mixed"] else "fp32"
+    R = results[head]
+    K = args.steps
+    value = N * K * world / (R["ms"] / 1e3)
+    # rows with s(r) != 0 (the work the kernels do; padded slots are skipped)
+    sim = R["sim"]
+    ptrs = None
+    pos_sorted = torch.tensor(np.ascontiguousarray(w["position"][sim._perm]), dtype=torch.float32, device="cuda")
+    from deepmd_jax_b200.engine import NeighborBuilder
+    nbb = NeighborBuilder(N, 1, sim._type_count, sim._sel, w["box"], 6.3)
+    nb, _ = nbb.build(pos_sorted[None].contiguous())
+    rows = rows_within_rcut(pos_sorted, nb[0], list(sim._type_count), list(sim._sel), list(w["box"]), 6.0)
+    flop_atom = rows * (EMB_FWD_FLOP_ROW + EMB_BWD_FLOP_ROW) + FIT_FLOP_ATOM + G_FLOP_ATOM
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak_src = "of measured"
+    except Exception:
+        peak_src = "of fallback"
+    pk_tensor = float(peaks.get("bf16_tflops", 1590.0))
+    stg = R["stages"]
+    pref = "mixed_" if head == "mixed" else ""
+    cand = {k: v for k, v in stg.items() if k.startswith(pref) or head == "fp32"}
+    dom = max(cand, key=lambda k: cand[k][0]) if cand else None
+    flop_stage = {"embed_fwd": rows * EMB_FWD_FLOP_ROW, "embed_bwd": rows * EMB_BWD_FLOP_ROW,
+                  "fit": FIT_FLOP_ATOM}
+    roof = None
+    if dom:
+        key = dom.replace("mixed_", "")
+        fl = flop_stage.get(key, 0) * N
+        t_ms = cand[dom][0]
+        ach = fl / (t_ms / 1e3) / 1e12 if fl else 0.0
+        roof = {"bound": "tensor", "achieved": ach, "peak": pk_tensor, "unit": "TFLOP/s",
+                "frac": ach / pk_tensor, "traffic": None, "kernel": dom, "launch_ms": t_ms,
+                "algorithmic_flop_per_launch": fl, "peak_source": peak_src + " (bf16 dense, burst)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,
+        "warmup": max(args.warmup, 3), "ms_per_step": R["ms"] / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16+f32" if head == "mixed" else "f32", "data": "synthetic",
+        "config": {"workload": "98,304-atom water (32,768 H2O, L=99.3 A), NVE velocity Verlet dt 0.5 fs, "
+                               "random-init se_a model 25-50-100/240^3/axis 16, rcut 6 A, skin 0.3 A",
+                   "form": head, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set > L2 (per-step scratch ~2 GB)", "rows_per_atom_within_rcut": rows,
+                   "algorithmic_gflop_per_step": flop_atom * N / 1e9},
+        "ns_per_day": 1e-6 * DT * 86400 * K / (R["ms"] / 1e3),
+        "gpu_launches": int(R["launches"]),
+        "clocks": R["clocks"],
+        "roofline": roof,
+        "forms": {p: {"atom_steps_per_s": N * K * world / (v["ms"] / 1e3), "ms_per_step": v["ms"] / K,
+                      "stage_ms": {k: s[0] for k, s in v["stages"].items()}, "status": v["status"],
+                      "rebuilds": v["rebuilds"]} if "error" not in v else v
+                  for p, v in results.items()},
+    }
+    if "mixed" in line["forms"] and "fp32" in line["forms"] and "error" not in results.get("mixed", {"error": 1}):
+        line["mixed_over_fp32"] = line["forms"]["mixed"]["atom_steps_per_s"] / line["forms"]["fp32"]["atom_steps_per_s"]
+    # e2e through the public API: host state in, trajectory of every step out
+    if not args.no_e2e:
+        sim2 = R["sim"]
+        sim2._use_graph = True
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim2.setPosition(w["position"])
+        sim2.setVelocity(w["velocity"])
+        traj = sim2.run(K)
+        torch.cuda.synchronize()
+        dt_e2e = time.perf_counter() - t0
+        barrier()
+        t = torch.tensor([dt_e2e], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt_e2e = float(t.item())
+        line["e2e"] = {"value": N * K * world / dt_e2e, "unit": "atom-steps/s",
+                       "h2d_bytes_per_step": int(2 * N * 3 * 8 / K),
+                       "d2h_bytes_per_step": int(2 * N * 3 * 4),
+                       "api": "Simulation.setPosition + setVelocity + run(K) returning the per-step trajectory"}
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    for v in results.values():
+        v.pop("sim", None)
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(reference_arm(args)))
+        return 0
+    line = gpu_arm(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

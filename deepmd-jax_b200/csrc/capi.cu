@@ -1,5 +1,5 @@
 // C ABI of libdpb200: model upload, workspace sizing and evaluation dispatch.
-#include "eval_common.cuh"
+#include "internal.cuh"
 #include <cuda_bf16.h>
 #include <cstring>
 #include <vector>
@@ -7,6 +7,53 @@
 
 namespace dpb {
 std::atomic<uint64_t> g_launches{0};
+
+// ---- per-kernel event timing (dpb_profile_*)
+static bool g_prof_on = false;
+static std::vector<cudaEvent_t> g_prof_pool;
+static size_t g_prof_next = 0;
+struct ProfRec { int id; cudaEvent_t a, b; };
+static std::vector<ProfRec> g_prof_open, g_prof_done;
+static double g_prof_ms[PROF_COUNT];
+static uint64_t g_prof_n[PROF_COUNT];
+
+static cudaEvent_t prof_event() {
+  if (g_prof_next == g_prof_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    g_prof_pool.push_back(e);
+  }
+  return g_prof_pool[g_prof_next++];
+}
+void prof_begin(int id, cudaStream_t st) {
+  if (!g_prof_on) return;
+  ProfRec r{id, prof_event(), nullptr};
+  cudaEventRecord(r.a, st);
+  g_prof_open.push_back(r);
+}
+void prof_end(int id, cudaStream_t st) {
+  if (!g_prof_on) return;
+  for (size_t k = g_prof_open.size(); k-- > 0;)
+    if (g_prof_open[k].id == id) {
+      ProfRec r = g_prof_open[k];
+      g_prof_open.erase(g_prof_open.begin() + k);
+      r.b = prof_event();
+      cudaEventRecord(r.b, st);
+      g_prof_done.push_back(r);
+      return;
+    }
+}
+static void prof_collect() {
+  for (auto &r : g_prof_done) {
+    cudaEventSynchronize(r.b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    g_prof_ms[r.id] += ms;
+    g_prof_n[r.id] += 1;
+  }
+  g_prof_done.clear();
+  g_prof_next = 0;
+}
 
 // fp32 path (eval_fp32.cu)
 template <int E0, int E1, int E2>
@@ -30,11 +77,6 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
 
 using namespace dpb;
 
-struct dpb_model {
-  DevModel dm;
-  std::vector<void *> allocs;
-  int device;
-};
 
 
 static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -189,11 +231,14 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
   gh[0] = (float *)w; w += al(NF * FW * 4);
   gh[1] = (float *)w; w += al(NF * FW * 4);
   int rc;
+  prof_begin(PROF_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
     else rc = launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
     if (rc) return rc;
   }
+  prof_end(PROF_EMBED_FWD, st);
+  prof_begin(PROF_FIT, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
     if (!cnt) continue;
@@ -247,18 +292,21 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
     rc = launch_sgemm(Mrows, K0, FW, gz[cur], FW, rm, M.fwT[ti][0], ep, st);
     if (rc) return rc;
   }
+  prof_end(PROF_FIT, st);
+  prof_begin(PROF_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     if (M.E2 == 100) rc = launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
     else rc = launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
     if (rc) return rc;
   }
+  prof_end(PROF_EMBED_BWD, st);
   return DPB_OK;
 }
 
-extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,
-                        int nframes, const int *type_count, const float *box, const int32_t *nbrs, const int *sel,
-                        double *energy, float *atom_energy, float *force, double *virial, uint32_t *status,
-                        void *workspace, size_t ws_bytes, void *stream_) {
+int dpb::eval_impl(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,
+                   int nframes, const int *type_count, const float *box, const int32_t *nbrs, const int *sel,
+                   double *energy, float *atom_energy, float *force, double *virial, uint32_t *status,
+                   void *workspace, size_t ws_bytes, cudaStream_t st) {
   if (!m || !pos || !box || !nbrs || !energy || !force || !status || !type_count || !sel || natoms <= 0 ||
       nframes <= 0)
     return DPB_ERR_INVALID_ARG;
@@ -270,7 +318,6 @@ extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, con
   SysDesc D;
   int rc = fill_sys(m, natoms, nframes, type_count, sel, D);
   if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream_;
   const DevModel &M = m->dm;
   const size_t NF = (size_t)natoms * nframes;
   char *w = (char *)workspace;
@@ -290,6 +337,29 @@ extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, con
   }
   if (rc) return rc;
   return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, nframes, pos, status, st);
+}
+
+extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,
+                        int nframes, const int *type_count, const float *box, const int32_t *nbrs, const int *sel,
+                        double *energy, float *atom_energy, float *force, double *virial, uint32_t *status,
+                        void *workspace, size_t ws_bytes, void *stream) {
+  return dpb::eval_impl(m, precision, pos, perm, natoms, nframes, type_count, box, nbrs, sel, energy, atom_energy,
+                        force, virial, status, workspace, ws_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int dpb_profile_enable(int on) {
+  dpb::prof_collect();
+  for (int k = 0; k < dpb::PROF_COUNT; ++k) { dpb::g_prof_ms[k] = 0.0; dpb::g_prof_n[k] = 0; }
+  dpb::g_prof_on = on != 0;
+  return DPB_OK;
+}
+
+extern "C" int dpb_profile_read(int id, double *ms, uint64_t *count) {
+  if (id < 0 || id >= dpb::PROF_COUNT || !ms || !count) return DPB_ERR_INVALID_ARG;
+  dpb::prof_collect();
+  *ms = dpb::g_prof_ms[id];
+  *count = dpb::g_prof_n[id];
+  return DPB_OK;
 }
 
 extern "C" uint64_t dpb_kernel_launch_count(void) { return g_launches.load(); }

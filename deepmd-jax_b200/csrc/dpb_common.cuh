@@ -14,6 +14,22 @@ constexpr float kSqrt3 = 1.73205080756887719f;
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Optional per-kernel timing with CUDA events on the launching stream
+// (diagnostics; off by default and never used inside graph capture).
+enum ProfId : int {
+  PROF_NLIST = 0,
+  PROF_EMBED_FWD = 1,
+  PROF_FIT = 2,
+  PROF_EMBED_BWD = 3,
+  PROF_INTEGRATE = 4,
+  PROF_MIXED_EMBED_FWD = 5,
+  PROF_MIXED_FIT = 6,
+  PROF_MIXED_EMBED_BWD = 7,
+  PROF_COUNT = 8
+};
+void prof_begin(int id, cudaStream_t st);
+void prof_end(int id, cudaStream_t st);
+
 #define DPB_CUDA_TRY(expr)                                   \
   do {                                                       \
     cudaError_t _e = (expr);                                 \

@@ -41,10 +41,22 @@ static NlGrid make_grid(const float box[3], float rc) {
   return g;
 }
 
+// A non-null gate makes every kernel of the build a no-op unless *gate != 0,
+// so the rebuild can sit inside a captured MD step and run only when the
+// drift test asks for it.
+__global__ void nl_zero_kernel(int *__restrict__ a, int na, int *__restrict__ b, int nb,
+                               const unsigned *__restrict__ gate) {
+  if (gate && *gate == 0u) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < na) a[i] = 0;
+  if (i < nb) b[i] = 0;
+}
+
 __global__ void nl_canon_kernel(const float *__restrict__ pos, const int32_t *__restrict__ perm,
                                 int N, int F, float3 L, float3 scale, float3 RB, int3 nc,
                                 float *__restrict__ canon, int *__restrict__ atom_cell,
-                                int *__restrict__ cell_count) {
+                                int *__restrict__ cell_count, const unsigned *__restrict__ gate) {
+  if (gate && *gate == 0u) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= N * F) return;
   int f = g / N, k = g - f * N;
@@ -67,7 +79,9 @@ __global__ void nl_canon_kernel(const float *__restrict__ pos, const int32_t *__
 }
 
 // Exclusive scan of n ints with one block (n up to a few million).
-__global__ void nl_scan_kernel(const int *__restrict__ in, int *__restrict__ out, int n) {
+__global__ void nl_scan_kernel(const int *__restrict__ in, int *__restrict__ out, int n,
+                               const unsigned *__restrict__ gate) {
+  if (gate && *gate == 0u) return;
   __shared__ int part[1024];
   int t = threadIdx.x;
   int per = (n + blockDim.x - 1) / blockDim.x;
@@ -92,7 +106,8 @@ __global__ void nl_scan_kernel(const int *__restrict__ in, int *__restrict__ out
 
 __global__ void nl_scatter_kernel(const int *__restrict__ atom_cell, const int *__restrict__ cell_start,
                                   int *__restrict__ cursor, int *__restrict__ cell_atoms, int N, int F,
-                                  int ncell) {
+                                  int ncell, const unsigned *__restrict__ gate) {
+  if (gate && *gate == 0u) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= N * F) return;
   int f = g / N;
@@ -148,7 +163,9 @@ __global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float 
                                                         const int *__restrict__ cell_atoms,
                                                         int32_t *__restrict__ nbrs,
                                                         int32_t *__restrict__ counts,
-                                                        uint32_t *__restrict__ status) {
+                                                        uint32_t *__restrict__ status,
+                                                        const unsigned *__restrict__ gate) {
+  if (gate && *gate == 0u) return;
   extern __shared__ int smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
@@ -252,16 +269,15 @@ extern "C" int dpb_nlist_workspace_bytes(int natoms, int nframes, const float bo
   return DPB_OK;
 }
 
-extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
-                               const int *type_count, const int *sel, const float box[3],
-                               const float *ref_box, float rc, int32_t *nbrs, float *ref_pos,
-                               int32_t *counts, uint32_t *status, void *workspace, size_t ws_bytes,
-                               void *stream_) {
+namespace dpb {
+int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
+                     const int *type_count, const int *sel, const float box[3], const float *ref_box, float rc,
+                     int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status, void *workspace,
+                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream) {
   if (!pos || natoms <= 0 || nframes <= 0 || ntypes < 1 || ntypes > kMaxTypes || !type_count || !sel ||
       !box || !nbrs || !status || rc <= 0)
     return DPB_ERR_INVALID_ARG;
   if (natoms >= (1 << 24)) return DPB_ERR_UNSUPPORTED;
-  cudaStream_t stream = (cudaStream_t)stream_;
   float rb[3] = {box[0], box[1], box[2]};
   if (ref_box) { rb[0] = ref_box[0]; rb[1] = ref_box[1]; rb[2] = ref_box[2]; }
   // jax_md receives rcut * max(ref/box) as float32 and squares it in float32
@@ -305,24 +321,33 @@ extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms
   int *cell_atoms = (int *)w; w += align_up(NF * 4);
   float *canon = ref_pos ? ref_pos : (float *)w;
 
-  DPB_CUDA_TRY(cudaMemsetAsync(cell_count, 0, C * 4, stream));
-  DPB_CUDA_TRY(cudaMemsetAsync(cursor, 0, C * 4, stream));
+  nl_zero_kernel<<<(int)((C + 255) / 256), 256, 0, stream>>>(cell_count, (int)C, cursor, (int)C, gate);
   float3 L = make_float3(box[0], box[1], box[2]);
   float3 scale = make_float3(rb[0] / box[0], rb[1] / box[1], rb[2] / box[2]);
   int nb = (int)((NF + 255) / 256);
   nl_canon_kernel<<<nb, 256, 0, stream>>>(pos, perm, natoms, nframes, L, scale, P.L, P.nc, canon, atom_cell,
-                                          cell_count);
-  nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C);
+                                          cell_count, gate);
+  nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C, gate);
   nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, natoms, nframes,
-                                            g.ncell);
+                                            g.ncell, gate);
   const int threads = 256, wpb = threads / 32;
   size_t smem = (size_t)wpb * kMaxTypes * 4 + (size_t)wpb * ntypes * cap * 4;
   if (smem > 48 * 1024) {
     DPB_CUDA_TRY(cudaFuncSetAttribute(nl_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   nl_search_kernel<<<(int)((NF + wpb - 1) / wpb), threads, smem, stream>>>(P, canon, cell_start, cell_atoms,
-                                                                           nbrs, counts, status);
-  count_launch(4);
+                                                                           nbrs, counts, status, gate);
+  count_launch(5);
   DPB_LAUNCH_CHECK();
   return DPB_OK;
+}
+}  // namespace dpb
+
+extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
+                               const int *type_count, const int *sel, const float box[3],
+                               const float *ref_box, float rc, int32_t *nbrs, float *ref_pos,
+                               int32_t *counts, uint32_t *status, void *workspace, size_t ws_bytes,
+                               void *stream) {
+  return dpb::nlist_build_impl(pos, perm, natoms, nframes, ntypes, type_count, sel, box, ref_box, rc, nbrs,
+                               ref_pos, counts, status, workspace, ws_bytes, nullptr, (cudaStream_t)stream);
 }

@@ -1,0 +1,448 @@
+"""Simulation: the reference's MD driver on the device-resident engine.
+
+Mirrors deepmd_jax/md.py:48-1091 (constructor arguments, run(), getters and
+setters, report rows, error-code handling and chunked re-runs) for the
+routines on the hot path: 'NVE' (velocity Verlet), 'NVT' (Nose-Hoover chain)
+and 'NVT' with n_bead > 1 (ring-polymer BAOAB with PILE-L).  All device work
+runs in libdpb200.so through dpb_md_*; a chunk of steps is captured once into
+a CUDA graph and replayed.
+"""
+from __future__ import annotations
+
+import ctypes
+from time import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import DeviceModel, NeighborBuilder, sort_by_type, _ptr, _stream
+from .systems import MASS_UNIT_CONVERSION, TEMP_UNIT_CONVERSION
+from .utils import load_model
+
+HBAR = 6.582119569e-16 * 1e15  # eV fs (deepmd_jax/pimd.py:19)
+
+
+class MDDesc(ctypes.Structure):
+    _fields_ = [
+        ("routine", ctypes.c_int), ("natoms", ctypes.c_int), ("nbeads", ctypes.c_int),
+        ("type_idx", ctypes.POINTER(ctypes.c_int)), ("mass_per_type", ctypes.POINTER(ctypes.c_double)),
+        ("sel", ctypes.POINTER(ctypes.c_int)), ("box", ctypes.c_double * 3), ("skin", ctypes.c_double),
+        ("dt", ctypes.c_double), ("temperature", ctypes.c_double), ("chain_length", ctypes.c_int),
+        ("tau_t", ctypes.c_double), ("pimd_lambda", ctypes.c_double),
+        ("nm_transform", ctypes.POINTER(ctypes.c_double)), ("nm_freqs", ctypes.POINTER(ctypes.c_double)),
+        ("seed", ctypes.c_uint64), ("precision", ctypes.c_int),
+    ]
+
+
+class MDReport(ctypes.Structure):
+    _fields_ = [
+        ("potential_energy", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
+        ("virial", ctypes.c_double * 9), ("thermostat_work", ctypes.c_double), ("status", ctypes.c_uint32),
+        ("steps", ctypes.c_uint64), ("rebuilds", ctypes.c_uint64), ("rebuild_rate", ctypes.c_double),
+        ("chain_length", ctypes.c_int), ("chain_dof", ctypes.c_double),
+        ("chain_xi", ctypes.c_double * 8), ("chain_p", ctypes.c_double * 8), ("chain_Q", ctypes.c_double * 8),
+    ]
+
+
+def _declare(lib):
+    if getattr(lib, "_md_declared", False):
+        return
+    vp = ctypes.c_void_p
+    d64 = ctypes.POINTER(ctypes.c_double)
+    lib.dpb_md_create.argtypes = [vp, ctypes.POINTER(MDDesc), ctypes.POINTER(vp)]
+    lib.dpb_md_destroy.argtypes = [vp]
+    lib.dpb_md_set_positions.argtypes = [vp, d64]
+    lib.dpb_md_set_velocities.argtypes = [vp, d64]
+    lib.dpb_md_get_state.argtypes = [vp, d64, d64, d64]
+    lib.dpb_md_init.argtypes = [vp, ctypes.c_int, vp]
+    lib.dpb_md_run.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+    lib.dpb_md_report.argtypes = [vp, ctypes.POINTER(MDReport)]
+    lib.dpb_md_clear_status.argtypes = [vp, ctypes.c_uint32]
+    lib.dpb_md_snapshot.argtypes = [vp, ctypes.c_int]
+    lib.dpb_md_set_capacity.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp]
+    lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
+              "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
+              "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_device_bytes"):
+        getattr(lib, f).restype = ctypes.c_int
+    lib._md_declared = True
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def normal_mode_transform(n_bead, kT):
+    """Ring-polymer normal modes (deepmd_jax/pimd.py:22-44), numpy eigh."""
+    ring_poly_freq = n_bead * kT / HBAR
+    A = 2 * np.eye(n_bead) - np.roll(np.eye(n_bead), 1, axis=0) - np.roll(np.eye(n_bead), -1, axis=0)
+    eva, eve = np.linalg.eigh(A)
+    order = np.argsort(eva)
+    eva = eva[order]
+    eve = eve[:, order]
+    if n_bead >= 2:
+        eva[0] = 0.0
+    return ring_poly_freq * np.sqrt(np.maximum(eva, 0.0)), eve
+
+
+def knbr_from_counts(max_counts, buffer_ratio):
+    """Capacity rule of the reference allocate_fn (md_utils.py:394-403);
+    returns the number of kept columns (knbr - 1) per type."""
+    k = np.asarray(max_counts, float)
+    knbr = np.where(k == 0, 1, 1 + (k * buffer_ratio + np.maximum(20 - k, 0) * max(buffer_ratio - 1.2, 0)))
+    return [max(int(x) - 1, 1) for x in knbr.astype(int)]
+
+
+class Simulation:
+    """Two-step usage, as in the reference: ``sim = Simulation(...)`` then
+    ``traj = sim.run(steps)``.  Extra keyword ``precision`` selects 'fp32'
+    (default, the reference's float32) or 'mixed' (BF16 tensor-core GEMMs)."""
+
+    def __init__(self, model_path, box, type_idx, mass, routine, dt, initial_position, initial_velocity=None,
+                 report_interval=200, temperature=None, pressure=None, debug=False, seed=0,
+                 model_deviation_paths=(), use_neighbor_list_when_possible=True, neighbor_skin=None,
+                 neighbor_buffer_ratio=1.2, remove_com_motion=False, tau_t=100., tau_p=1000., chain_length_t=3,
+                 chain_length_p=3, chain_steps_t=1, chain_steps_p=1, sy_steps_t=1, sy_steps_p=1,
+                 fixed_indices=None, couple_axes=((0, 1, 2),), n_bead=1, type_symbols=None, pimd_lambda=1.0,
+                 pimd_print_invariant=False, precision="fp32", use_cuda_graph=True, verbose=True):
+        self.lib = _lib.load()
+        _declare(self.lib)
+        self.verbose = verbose
+        if isinstance(model_path, (tuple, list)):
+            params, variables = model_path
+        else:
+            model, variables = load_model(model_path)
+            params = model.params
+        self._params = params
+        self.model = DeviceModel(params, variables)
+        if routine not in ("NVE", "NVT"):
+            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NVT PIMD)" % routine)
+        if len(model_deviation_paths) or fixed_indices is not None or remove_com_motion:
+            raise NotImplementedError("model deviation / fixed atoms / COM removal are not supported")
+        if chain_steps_t != 1 or sy_steps_t != 1:
+            raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
+        if pressure is not None:
+            raise NotImplementedError("NPT is not supported")
+        self._n_bead = int(n_bead)
+        self._is_pimd = self._n_bead > 1
+        if self._is_pimd and routine != "NVT":
+            raise NotImplementedError("Path-integral MD (n_bead > 1) supports routine='NVT'.")
+        pos0 = np.asarray(initial_position, dtype=np.float64)
+        if self._is_pimd:
+            if pos0.ndim == 2:
+                pos0 = np.broadcast_to(pos0, (self._n_bead,) + pos0.shape).copy()
+            elif pos0.shape[0] != self._n_bead:
+                raise ValueError("initial_position leading axis %d does not match n_bead=%d"
+                                 % (pos0.shape[0], self._n_bead))
+            self._natoms = pos0.shape[1]
+        else:
+            self._natoms = pos0.shape[0]
+        box = np.asarray(box, dtype=np.float64)
+        if box.size == 1:
+            box = box.item() * np.ones(3)
+        elif box.shape == (3, 3):
+            if not np.allclose(box, np.diag(np.diag(box))):
+                raise NotImplementedError("non-orthorhombic boxes are not supported")
+            box = np.diag(box).copy()
+        self._box = box
+        self._routine = routine
+        self._dt = float(dt)
+        self._temperature = temperature
+        self.report_interval = int(report_interval)
+        self.step = 0
+        self.log = []
+        self._debug = debug
+        self.precision = precision
+        self._type_idx = np.asarray(type_idx, dtype=np.int32)
+        ct = params.get("chemical_types")
+        if ct is not None:
+            z2i = {z: i for i, z in enumerate(ct)}
+            self._type_idx = np.array([z2i[int(z)] for z in self._type_idx], dtype=np.int32)
+        self._mass_per_type = np.asarray(mass, dtype=np.float64)
+        self._mass = self._mass_per_type[self._type_idx]
+        self._step_chunk_size = max(10, min(100, 100000 // (self._natoms * self._n_bead)))
+        self._neighbor_skin = (0.3 if neighbor_skin is None else float(neighbor_skin))
+        self._buffer_ratio = float(neighbor_buffer_ratio)
+        self._kT = (temperature if temperature is not None else 0.0) * TEMP_UNIT_CONVERSION
+        self._use_graph = use_cuda_graph
+        self._graphs = {}
+        nt = int(params["ntypes"])
+        self._perm, self._type_count = sort_by_type(self._type_idx, nt)
+        # neighbour capacity from a measurement at the initial positions (allocate_fn)
+        self._sel = self._measure_capacity(pos0)
+        desc = MDDesc()
+        desc.routine = 2 if self._is_pimd else (0 if routine == "NVE" else 1)
+        desc.natoms = self._natoms
+        desc.nbeads = self._n_bead
+        self._keep = [np.ascontiguousarray(self._type_idx, dtype=np.int32), np.ascontiguousarray(self._mass_per_type)]
+        desc.type_idx = self._keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        desc.mass_per_type = _dptr(self._keep[1])
+        self._sel_arr = (ctypes.c_int * nt)(*self._sel)
+        desc.sel = self._sel_arr
+        for k in range(3):
+            desc.box[k] = float(box[k])
+        desc.skin = self._neighbor_skin
+        desc.dt = self._dt
+        desc.temperature = float(temperature or 0.0)
+        desc.chain_length = int(chain_length_t)
+        desc.tau_t = float(tau_t)
+        desc.pimd_lambda = float(pimd_lambda)
+        desc.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        desc.precision = {"fp32": 0, "mixed": 1}[precision]
+        if self._is_pimd:
+            self._nm_freqs, self._nm_trans = normal_mode_transform(self._n_bead, self._kT)
+            self._keep += [np.ascontiguousarray(self._nm_trans), np.ascontiguousarray(self._nm_freqs)]
+            desc.nm_transform = _dptr(self._keep[-2])
+            desc.nm_freqs = _dptr(self._keep[-1])
+        self._desc = desc
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.dpb_md_create(self.model.handle, ctypes.byref(desc), ctypes.byref(h)), "dpb_md_create")
+        self._h = h
+        self._set_pos(pos0)
+        if initial_velocity is not None:
+            vel = np.asarray(initial_velocity, dtype=np.float64)
+        else:
+            vel = self._initial_velocity(seed)
+        self._set_vel(vel)
+        _lib.check(self.lib.dpb_md_init(self._h, 1, _stream()), "dpb_md_init")
+        self._is_initial_state = True
+        self._error_code = 0
+        if verbose:
+            label = "NVT PIMD run" if self._is_pimd else ("%s run" % routine)
+            print("# Initialized %s with %d atoms" % (label, self._natoms))
+
+    # ------------------------------------------------------------------ helpers
+    def _measure_capacity(self, pos0):
+        frames = pos0.reshape(self._n_bead, self._natoms, 3)
+        pm = torch.tensor(self._perm.astype(np.int32), device="cuda")
+        big = [256] * len(self._type_count)
+        nb = NeighborBuilder(self._natoms, self._n_bead, self._type_count, big, self._box,
+                             float(self._params["rcut"]) + self._neighbor_skin)
+        p = torch.tensor(np.ascontiguousarray(frames), dtype=torch.float32, device="cuda")
+        counts = torch.empty((self._n_bead, self._natoms, len(big)), dtype=torch.int32, device="cuda")
+        nb.build(p, perm=pm, counts=counts)
+        mx = counts.reshape(-1, len(big)).max(0).values.cpu().numpy()
+        return knbr_from_counts(mx, self._buffer_ratio)
+
+    def _initial_velocity(self, seed):
+        """Maxwell-Boltzmann momenta sqrt(m kT) N(0,1) with the mean momentum
+        removed (jax_md initialize_momenta); PIMD beads at P kT
+        (pimd.py:72-79).  numpy's generator replaces jax.random."""
+        if self._kT == 0:
+            return np.zeros((self._n_bead, self._natoms, 3) if self._is_pimd else (self._natoms, 3))
+        rng = np.random.default_rng(seed)
+        m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
+        if self._is_pimd:
+            p = np.sqrt(m * self._kT * self._n_bead) * rng.normal(size=(self._n_bead, self._natoms, 3))
+        else:
+            p = np.sqrt(m * self._kT) * rng.normal(size=(self._natoms, 3))
+            p = p - p.mean(0, keepdims=True)
+        return p / m
+
+    def _set_pos(self, pos):
+        a = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).reshape(-1))
+        _lib.check(self.lib.dpb_md_set_positions(self._h, _dptr(a)), "dpb_md_set_positions")
+
+    def _set_vel(self, vel):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(vel, dtype=np.float64),
+                                                 (self._n_bead, self._natoms, 3)).reshape(-1))
+        _lib.check(self.lib.dpb_md_set_velocities(self._h, _dptr(a)), "dpb_md_set_velocities")
+
+    def _report_struct(self):
+        r = MDReport()
+        _lib.check(self.lib.dpb_md_report(self._h, ctypes.byref(r)), "dpb_md_report")
+        return r
+
+    def _frame_shape(self):
+        return (self._n_bead, self._natoms, 3) if self._is_pimd else (self._natoms, 3)
+
+    def _run_chunk(self, n, traj_p, traj_v):
+        stream = torch.cuda.current_stream()
+        if not self._use_graph:
+            _lib.check(self.lib.dpb_md_run(self._h, n, _ptr(traj_p), _ptr(traj_v), _stream()), "dpb_md_run")
+            return
+        key = (n, traj_p.data_ptr() if traj_p is not None else 0)
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                with torch.cuda.graph(g, stream=side, capture_error_mode="relaxed"):
+                    rc = self.lib.dpb_md_run(self._h, n, _ptr(traj_p), _ptr(traj_v),
+                                             ctypes.c_void_p(side.cuda_stream))
+            stream.wait_stream(side)
+            _lib.check(rc, "dpb_md_run (capture)")
+            self._graphs[key] = g
+        g.replay()
+
+    # ------------------------------------------------------------------ reports
+    def _temperature_of(self, KE):
+        return 2 * KE / (3 * self._natoms * self._n_bead) / TEMP_UNIT_CONVERSION / self._n_bead * self._n_bead
+
+    def _report_row(self, tic):
+        r = self._report_struct()
+        KE = r.kinetic_energy / self._n_bead ** 2 if self._is_pimd else r.kinetic_energy
+        PE = r.potential_energy / self._n_bead
+        T = 2 * r.kinetic_energy / (3 * self._natoms * self._n_bead) / TEMP_UNIT_CONVERSION / self._n_bead
+        row = [self.step, T, KE, PE]
+        headers = ["Step", "Temperature", "KE", "PE"]
+        if self._routine == "NVE":
+            row.append(KE + PE)
+            headers.append("Invariant")
+        elif not self._is_pimd:
+            kT = self._kT
+            E = PE + KE + r.chain_p[0] ** 2 / (2 * r.chain_Q[0]) + r.chain_dof * kT * r.chain_xi[0]
+            for k in range(1, r.chain_length):
+                E += r.chain_p[k] ** 2 / (2 * r.chain_Q[k]) + kT * r.chain_xi[k]
+            row.append(E)
+            headers.append("Invariant")
+        row.append(time() - tic)
+        headers.append("Time")
+        if self.verbose:
+            if not self.log:
+                print(" ".join("%-12s" % h for h in headers))
+            print("%-8d " % row[0] + " ".join("%-12.3f" % v for v in row[1:]))
+        self.log.append(row)
+        return r
+
+    # ------------------------------------------------------------------ public API
+    def run(self, steps, dump_interval=None, dump_prefix=None, dump_content="positions", dump_mode="overwrite"):
+        """Run ``steps`` steps; returns the trajectory dict of every step
+        (deepmd_jax/md.py:874-964)."""
+        if dump_prefix is not None:
+            raise NotImplementedError("XYZ dumping is outside this engine; use the returned trajectory")
+        steps = int(steps)
+        first = self._is_initial_state
+        L = steps + int(first)
+        fs = self._frame_shape()
+        traj = {"position": np.zeros((L,) + fs), "velocity": np.zeros((L,) + fs),
+                "box": np.tile(self._box, (L, 1))}
+        if first:
+            traj["position"][0] = self.getPosition()
+            traj["velocity"][0] = self.getVelocity()
+        tic_run = tic = time()
+        if first:
+            self._report_row(tic)
+        self._is_initial_state = False
+        NF3 = self._natoms * self._n_bead * 3
+        cap = min(self._step_chunk_size, steps) if steps else 0
+        buf_p = torch.empty((max(cap, 1), NF3), dtype=torch.float32, device="cuda")
+        buf_v = torch.empty((max(cap, 1), NF3), dtype=torch.float32, device="cuda")
+        done, idx = 0, int(first)
+        overflow_twice = False
+        while done < steps:
+            n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
+            _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
+            self._run_chunk(n, buf_p[:n] if n == cap else buf_p[:n].contiguous(), buf_v[:n] if n == cap else
+                            buf_v[:n].contiguous())
+            r = self._report_struct()
+            code = int(r.status)
+            if code & 16:
+                print("# Warning: Nan or Inf encountered in simulation. Terminating.")
+                self._error_code = code
+                break
+            if code & 2:
+                # reallocate (grow the buffer ratio on a repeat) and re-run the chunk (md.py:657-668,913-916)
+                _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
+                if overflow_twice:
+                    self._buffer_ratio += 0.05
+                overflow_twice = True
+                self._resize_capacity()
+                continue
+            overflow_twice = False
+            pos_chunk = buf_p[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
+            mom_chunk = buf_v[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
+            pos_u = np.empty_like(pos_chunk)
+            mom_u = np.empty_like(mom_chunk)
+            pos_u[:, :, self._perm] = pos_chunk
+            mom_u[:, :, self._perm] = mom_chunk
+            vel_u = mom_u / (self._mass * MASS_UNIT_CONVERSION)[None, None, :, None]
+            if not self._is_pimd:
+                pos_u, vel_u = pos_u[:, 0], vel_u[:, 0]
+            traj["position"][idx:idx + n] = pos_u
+            traj["velocity"][idx:idx + n] = vel_u
+            idx += n
+            done += n
+            self.step += n
+            if self.step % self.report_interval == 0 or done == steps:
+                self._report_row(tic)
+                tic = time()
+        elapsed = time() - tic_run
+        if self.verbose:
+            nsd = 1e-6 * steps * self._dt * (86400 / max(elapsed, 1e-9))
+            print("# Finished %d steps in %.2f s." % (steps, elapsed))
+            print("# Performance: %.3f ns/day, %.3f step/us/atom" %
+                  (nsd, 1e-6 * steps * self._natoms * self._n_bead / (elapsed + 1e-6)))
+        if self._is_pimd:
+            traj["centroid"] = np.stack([self._centroid(p) for p in traj["position"]])
+        return traj
+
+    def _resize_capacity(self):
+        pos = self.getPosition()
+        self._sel = self._measure_capacity(pos)
+        arr = (ctypes.c_int * len(self._sel))(*self._sel)
+        _lib.check(self.lib.dpb_md_set_capacity(self._h, arr, _stream()), "dpb_md_set_capacity")
+        _lib.check(self.lib.dpb_md_clear_status(self._h, ~2 & 0xFFFFFFFF), "dpb_md_clear_status")
+        self._graphs = {}
+        if self.verbose:
+            print("# Neighborlist reallocated with size %s" % (self._sel,))
+
+    def _centroid(self, R):
+        ref = R[0:1]
+        d = R - ref
+        d = d - self._box * np.round(d / self._box)
+        return (ref + d).mean(0)
+
+    def _state(self):
+        shape = (self._n_bead * self._natoms * 3,)
+        p, v, f = np.empty(shape), np.empty(shape), np.empty(shape)
+        _lib.check(self.lib.dpb_md_get_state(self._h, _dptr(p), _dptr(v), _dptr(f)), "dpb_md_get_state")
+        fs = self._frame_shape()
+        return p.reshape(fs), v.reshape(fs), f.reshape(fs)
+
+    def getPosition(self):
+        return self._state()[0]
+
+    def getVelocity(self):
+        return self._state()[1]
+
+    def getForce(self):
+        return self._state()[2]
+
+    def getCentroidPosition(self):
+        p = self.getPosition()
+        return self._centroid(p) if self._is_pimd else p
+
+    def getBox(self):
+        return np.array(self._box)
+
+    def getEnergy(self):
+        r = self._report_struct()
+        return r.potential_energy / self._n_bead
+
+    def getVirial(self):
+        return np.array(self._report_struct().virial).reshape(3, 3)
+
+    def setPosition(self, position, box=None):
+        if box is not None:
+            raise ValueError("Box can only be changed in NPT simulations.")
+        pos = np.asarray(position, dtype=np.float64)
+        if self._is_pimd and pos.ndim == 2:
+            pos = np.broadcast_to(pos, self._frame_shape())
+        if pos.shape != self._frame_shape():
+            raise ValueError("Position must have the same shape as the initial position.")
+        self._set_pos(pos)
+        _lib.check(self.lib.dpb_md_init(self._h, 0, _stream()), "dpb_md_init")
+
+    def setVelocity(self, velocity):
+        self._set_vel(velocity)
+
+    def __del__(self):
+        try:
+            self._graphs = {}
+            if getattr(self, "_h", None) is not None and self._h.value:
+                self.lib.dpb_md_destroy(self._h)
+        except Exception:
+            pass

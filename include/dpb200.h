@@ -147,6 +147,96 @@ DPB_API int dpb_eval(const dpb_model *model, int precision, const float *pos, co
              float *force, double *virial, uint32_t *status, void *workspace,
              size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------- MD engine */
+
+#define DPB_MD_NVE 0
+#define DPB_MD_NVT_NHC 1
+#define DPB_MD_PIMD_PILE 2
+
+typedef struct dpb_md dpb_md;
+
+/* Host-side description of an MD run (deepmd_jax/md.py:61-282 constructor
+ * arguments).  Units: Angstrom, fs, Dalton, Kelvin. */
+typedef struct {
+  int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE */
+  int natoms;
+  int nbeads;                  /* 1, or P ring-polymer beads for PIMD */
+  const int *type_idx;         /* [natoms] user order */
+  const double *mass_per_type; /* Dalton */
+  const int *sel;              /* neighbour capacity per type */
+  double box[3];
+  double skin;                 /* neighbour skin (0.3 for NVE/NVT, md.py:203-206) */
+  double dt;                   /* fs */
+  double temperature;          /* K (NVT / PIMD) */
+  int chain_length;            /* Nose-Hoover chain length (3) */
+  double tau_t;                /* fs: NHC tau; PIMD centroid friction 1/tau_t */
+  double pimd_lambda;          /* PILE internal-mode damping scale */
+  const double *nm_transform;  /* PIMD: (P,P) C, primitive <- normal mode */
+  const double *nm_freqs;      /* PIMD: (P) normal-mode frequencies, 1/fs */
+  uint64_t seed;               /* Philox key of the stochastic steps */
+  int precision;               /* DPB_PREC_* of the force evaluations */
+} dpb_md_desc;
+
+typedef struct {
+  double potential_energy;     /* sum over beads of the last force evaluation */
+  double kinetic_energy;       /* of the current momenta */
+  double virial[9];            /* sum over beads */
+  double thermostat_work;      /* PILE-L cumulative work */
+  uint32_t status;             /* OR of the device status bits */
+  uint64_t steps, rebuilds;
+  double rebuild_rate;         /* EMA of rebuilds per step (md.py:733) */
+  int chain_length;
+  double chain_dof;
+  double chain_xi[8], chain_p[8], chain_Q[8];
+} dpb_md_report_t;
+
+typedef struct {
+  float *pos, *mom, *force;    /* (P,N,3) type-sorted */
+  int32_t *nbrs;
+  double *energy, *virial;
+  uint32_t *status;
+  int32_t *perm_sorted_to_user;
+} dpb_md_pointers_t;
+
+/* Create an MD context on the current device; allocates the state and the
+ * workspaces of the neighbour list and the evaluation.
+ * Replaces: Simulation.__init__ state set-up (deepmd_jax/md.py:61-282) and the
+ * routine constructors (deepmd_jax/routine.py:139-158, deepmd_jax/pimd.py:114-207). */
+DPB_API int dpb_md_create(const dpb_model *model, const dpb_md_desc *desc, dpb_md **out);
+DPB_API int dpb_md_destroy(dpb_md *md);
+DPB_API int dpb_md_device_bytes(const dpb_md *md, size_t *bytes);
+/* State in user atom order, (P,N,3) float64 host arrays; velocities in A/fs.
+ * Replaces: setPosition / setVelocity / getPosition / getVelocity / getForce
+ * (deepmd_jax/md.py:969-1047). */
+DPB_API int dpb_md_set_positions(dpb_md *md, const double *pos);
+DPB_API int dpb_md_set_velocities(dpb_md *md, const double *vel);
+DPB_API int dpb_md_get_state(const dpb_md *md, double *pos, double *vel, double *force);
+/* Neighbour list and forces of the current positions; with reset_thermostat
+ * the chain / thermostat state restarts from the current kinetic energy (the
+ * routine's init_fn).  Synchronous. */
+DPB_API int dpb_md_init(dpb_md *md, int reset_thermostat, void *stream);
+/* Enqueue nsteps steps (drift test, gated rebuild, status, integrator, force
+ * evaluation); no host synchronisation, capturable in a CUDA graph.
+ * traj_pos / traj_mom: optional device buffers (nsteps,P,N,3) float32 in
+ * type-sorted order.  Replaces: the jitted lax.scan chunk
+ * (deepmd_jax/md.py:759-804). */
+DPB_API int dpb_md_run(dpb_md *md, int nsteps, float *traj_pos, float *traj_mom, void *stream);
+/* Synchronous read of the energies, status word and thermostat state. */
+DPB_API int dpb_md_report(dpb_md *md, dpb_md_report_t *report);
+DPB_API int dpb_md_clear_status(dpb_md *md, uint32_t keep_bits);
+/* restore == 0: save the state (chunk start); 1: restore it (chunk re-run). */
+DPB_API int dpb_md_snapshot(dpb_md *md, int restore);
+/* New neighbour capacity and a rebuild (overflow resolution, md.py:657-668). */
+DPB_API int dpb_md_set_capacity(dpb_md *md, const int *sel, void *stream);
+DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
+
+/* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
+ * default; not for use inside graph capture).  Stage ids: 0 neighbour
+ * drift/rebuild, 1 embedding forward, 2 fitting chain, 3 embedding adjoint,
+ * 4 integrator, 5/6/7 the same three stages of the mixed path. */
+DPB_API int dpb_profile_enable(int on);
+DPB_API int dpb_profile_read(int stage, double *ms, uint64_t *count);
+
 /* Number of kernels the library launched since load (for launch accounting). */
 DPB_API uint64_t dpb_kernel_launch_count(void);
 
