@@ -16,13 +16,13 @@ DPB_OK = 0
 STATUS_BITS = {1: "box shrank past the skin", 2: "neighbour list overflow", 4: "overflow in previous chunk",
                8: "lattice overflow", 16: "NaN/Inf encountered"}
 ERRORS = {256: "DPB_ERR_INVALID_ARG", 257: "DPB_ERR_CUDA", 258: "DPB_ERR_UNSUPPORTED",
-          259: "DPB_ERR_WORKSPACE", 260: "DPB_ERR_NO_DEVICE"}
+          259: "DPB_ERR_WORKSPACE", 260: "DPB_ERR_NO_DEVICE", 261: "DPB_ERR_SCRATCH_LIMIT"}
 PREC_FP32 = 0
 PREC_MIXED = 1
 NBR_INDEX_MASK = 0x00FFFFFF
 
 EXPORTED = ["dpb_model_create", "dpb_model_destroy", "dpb_nlist_workspace_bytes", "dpb_nlist_build",
-            "dpb_eval_workspace_bytes", "dpb_eval", "dpb_kernel_launch_count", "dpb_version"]
+            "dpb_eval_workspace_bytes", "dpb_eval", "dpb_eval_noalloc", "dpb_kernel_launch_count", "dpb_version"]
 
 
 class DPBError(RuntimeError):
@@ -83,6 +83,9 @@ def load():
     lib.dpb_eval.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, ctypes.c_int, c_int_p, f32p, i32p,
                              c_int_p, f64p, f32p, f32p, f64p, vp, vp, ctypes.c_size_t, vp]
     lib.dpb_eval.restype = ctypes.c_int
+    lib.dpb_eval_noalloc.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, ctypes.c_int, c_int_p, f32p, i32p,
+                                     c_int_p, f64p, f32p, f32p, f64p, vp, vp]
+    lib.dpb_eval_noalloc.restype = ctypes.c_int
     lib.dpb_kernel_launch_count.argtypes = []
     lib.dpb_kernel_launch_count.restype = ctypes.c_uint64
     lib.dpb_version.argtypes = []

@@ -45,6 +45,7 @@ extern "C" {
 #define DPB_ERR_UNSUPPORTED 258
 #define DPB_ERR_WORKSPACE 259
 #define DPB_ERR_NO_DEVICE 260
+#define DPB_ERR_SCRATCH_LIMIT 261
 
 /* Precision of the evaluation.
  * DPB_PREC_FP32:  all arithmetic in FP32 (the reference's float32 with
@@ -146,6 +147,21 @@ DPB_API int dpb_eval(const dpb_model *model, int precision, const float *pos, co
              const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,
              float *force, double *virial, uint32_t *status, void *workspace,
              size_t workspace_bytes, void *stream);
+
+/* dpb_eval without a caller workspace, for callers that cannot allocate
+ * device memory (a host code that keeps the force field inside its own fixed
+ * memory pool, a plugin whose process forbids foreign cudaMalloc calls, code
+ * that must not allocate between steps).  No counterpart in the reference:
+ * its JAX path has no notion of caller-provided scratch.  The scratch is a
+ * 64 MiB array inside the library image on each device that loads it; calls
+ * whose dpb_eval_workspace_bytes exceed it return DPB_ERR_SCRATCH_LIMIT.
+ * The first call on a device resolves the array's address (make it before any
+ * stream capture).  Calls share the array: calls that overlap on the GPU race.
+ * Arguments and outputs as dpb_eval.  Allocates nothing. */
+DPB_API int dpb_eval_noalloc(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
+                             int natoms, int nframes, const int *type_count, const float *box,
+                             const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,
+                             float *force, double *virial, uint32_t *status, void *stream);
 
 /* ---------------------------------------------------------------- MD engine */
 
