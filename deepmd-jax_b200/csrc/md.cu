@@ -534,7 +534,12 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
     cudaMemcpy(&h, sc, sizeof(h), cudaMemcpyDeviceToHost);
     h.chain_ke = h.ke;
     h.dof = 3.0 * (double)m->N;
-    for (int k = 0; k < kMaxChain; ++k) { h.xi[k] = 0.0; h.pxi[k] = 0.0; h.Q[k] = 0.0; }
+    for (int k = 0; k < kMaxChain; ++k) {
+      h.xi[k] = 0.0;
+      h.pxi[k] = 0.0;
+      h.Q[k] = k < m->d.chain_length ? m->kT * m->d.tau_t * m->d.tau_t : 0.0;  // chain masses at init
+    }
+    h.Q[0] *= h.dof;
     h.scale = 1.0;
     h.twork = 0.0;
     cudaMemcpy(sc, &h, sizeof(h), cudaMemcpyHostToDevice);
