@@ -73,6 +73,10 @@ size_t mixed_workspace_per_atom(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
                cudaStream_t st);
+int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+                      const int32_t *nbrs, float *T, float *G, int *err, cudaStream_t st);
+int fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Eatom, double *energy, char *w,
+                   cudaStream_t st);
 }  // namespace dpb
 
 using namespace dpb;
@@ -215,13 +219,13 @@ static int fill_sys(const dpb_model *m, int natoms, int nframes, const int *type
   return DPB_OK;
 }
 
-static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
-                     const float *box, const int32_t *nbrs, double *energy, float4 *F4, float *Eatom,
-                     double *virial, char *w, cudaStream_t st) {
+// FP32 fitting chain (tiled SGEMMs with fused epilogues) for every centre
+// type: G -> per-atom energies (FP64 frame sums) and dE/dG written over G.
+// w: scratch for the per-layer activations and adjoints.
+int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Eatom, double *energy, char *w,
+                        cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
   const int E2 = M.E2, A = M.A, K0 = A * E2, FW = M.FW[0], L = M.nfit;
-  float *T = (float *)w; w += al(NF * 10 * E2 * 4);
-  float *G = (float *)w; w += al(NF * K0 * 4);  // G, later dE/dG
   float *tb[kMaxFitLayers], *hb[kMaxFitLayers];
   for (int l = 0; l < L; ++l) { tb[l] = (float *)w; w += al(NF * FW * 4); }
   for (int l = 0; l < L; ++l) { hb[l] = (float *)w; w += al(NF * FW * 4); }
@@ -231,14 +235,6 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
   gh[0] = (float *)w; w += al(NF * FW * 4);
   gh[1] = (float *)w; w += al(NF * FW * 4);
   int rc;
-  prof_begin(PROF_EMBED_FWD, st);
-  for (int ti = 0; ti < M.ntypes; ++ti) {
-    if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
-    else rc = launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
-    if (rc) return rc;
-  }
-  prof_end(PROF_EMBED_FWD, st);
-  prof_begin(PROF_FIT, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
     if (!cnt) continue;
@@ -292,6 +288,27 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
     rc = launch_sgemm(Mrows, K0, FW, gz[cur], FW, rm, M.fwT[ti][0], ep, st);
     if (rc) return rc;
   }
+  return DPB_OK;
+}
+
+static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
+                     const float *box, const int32_t *nbrs, double *energy, float4 *F4, float *Eatom,
+                     double *virial, char *w, cudaStream_t st) {
+  const size_t NF = (size_t)D.N * D.F;
+  const int E2 = M.E2, A = M.A, K0 = A * E2, FW = M.FW[0], L = M.nfit;
+  float *T = (float *)w; w += al(NF * 10 * E2 * 4);
+  float *G = (float *)w; w += al(NF * K0 * 4);  // G, later dE/dG
+  int rc;
+  prof_begin(PROF_EMBED_FWD, st);
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    else rc = launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    if (rc) return rc;
+  }
+  prof_end(PROF_EMBED_FWD, st);
+  prof_begin(PROF_FIT, st);
+  rc = fit_fp32_chain(M, D, G, Eatom, energy, w, st);
+  if (rc) return rc;
   prof_end(PROF_FIT, st);
   prof_begin(PROF_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
@@ -360,6 +377,35 @@ extern "C" int dpb_profile_read(int id, double *ms, uint64_t *count) {
   *ms = dpb::g_prof_ms[id];
   *count = dpb::g_prof_n[id];
   return DPB_OK;
+}
+
+// fp32 descriptor stage (eval_fp32.cu kernels), T and G of every atom
+static int descriptors_fp32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
+                            const float *box, const int32_t *nbrs, float *T, float *G, cudaStream_t st) {
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    int rc = (M.E2 == 100) ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st)
+                           : launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    if (rc) return rc;
+  }
+  return DPB_OK;
+}
+
+extern "C" int dpb_eval_descriptors(const dpb_model *m, int precision, const float *pos, const int32_t *perm,
+                                    int natoms, int nframes, const int *type_count, const float *box,
+                                    const int32_t *nbrs, const int *sel, float *T, float *G, int *err,
+                                    void *stream) {
+  if (!m || !pos || !box || !nbrs || !T || !G || !err || !type_count || !sel || natoms <= 0 || nframes <= 0)
+    return DPB_ERR_INVALID_ARG;
+  SysDesc D;
+  int rc = fill_sys(m, natoms, nframes, type_count, sel, D);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == DPB_PREC_FP32) return descriptors_fp32(m->dm, D, pos, perm, box, nbrs, T, G, st);
+  if (precision == DPB_PREC_MIXED) {
+    if (!mixed_supported(m->dm)) return DPB_ERR_UNSUPPORTED;
+    return mixed_descriptors(m->dm, D, pos, perm, box, nbrs, T, G, err, st);
+  }
+  return DPB_ERR_INVALID_ARG;
 }
 
 extern "C" uint64_t dpb_kernel_launch_count(void) { return g_launches.load(); }

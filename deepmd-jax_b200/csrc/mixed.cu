@@ -1,11 +1,545 @@
 // Mixed-precision (BF16 tensor-core) evaluation path.
-#include "eval_common.cuh"
+#include "internal.cuh"
+#include "tc.cuh"
 
 namespace dpb {
-int mixed_supported(const DevModel &) { return 0; }
-size_t mixed_workspace_per_atom(const DevModel &) { return 0; }
-int mixed_eval(const DevModel &, const SysDesc &, const float *, const int32_t *, const float *, const int32_t *,
-               double *, float *, float4 *, double *, void *, cudaStream_t) {
-  return DPB_ERR_UNSUPPORTED;
+
+// ---------------------------------------------------------------- self-test
+// Known-answer test of the tcgen05 path: D(128x64) = A(128x32) B(32x64) with
+// A[m][k] = ((m*3 + k*5) % 17 - 8) / 8, B[k][n] = ((k*7 + n*11) % 13 - 6) / 4
+// (all exact in bf16).  variant 0: A and B K-major; 1: A and B MN-major.
+// Writes D row-major to out; err gets 1 on an mbarrier timeout.
+__global__ void __launch_bounds__(128) k_selftest_umma(int variant, float *out, int *err) {
+  constexpr int M = 128, N = 64, K = 32;
+  __shared__ __align__(128) __nv_bfloat16 As[M * K];
+  __shared__ __align__(128) __nv_bfloat16 Bs[N * K];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x;
+  char *Ab = reinterpret_cast<char *>(As), *Bb = reinterpret_cast<char *>(Bs);
+  for (int e = tid; e < M * K; e += 128) {
+    const int m = e / K, k = e % K;
+    const float v = (float)((m * 3 + k * 5) % 17 - 8) / 8.f;
+    const uint32_t off = variant == 0 ? tc::kmajor_off(m, k, K) : tc::mnmajor_off(k, m, M);
+    *reinterpret_cast<__nv_bfloat16 *>(Ab + off) = __float2bfloat16_rn(v);
+  }
+  for (int e = tid; e < N * K; e += 128) {
+    const int k = e / N, n = e % N;
+    const float v = (float)((k * 7 + n * 11) % 13 - 6) / 4.f;
+    const uint32_t off = variant == 0 ? tc::kmajor_off(n, k, K) : tc::mnmajor_off(k, n, N);
+    *reinterpret_cast<__nv_bfloat16 *>(Bb + off) = __float2bfloat16_rn(v);
+  }
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  if (tid < 32) tc::tmem_alloc(&tbase, 64);
+  tc::fence_proxy_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t d = tbase;
+  if (tid == 0) {
+    const uint32_t idesc = tc::idesc_bf16(M, N, variant, variant);
+    const uint32_t a0 = tc::smem_u32(As), b0 = tc::smem_u32(Bs);
+    for (int ks = 0; ks < K / 16; ++ks) {
+      uint64_t ad, bd;
+      if (variant == 0) {
+        ad = tc::make_desc(a0 + tc::kmajor_off(0, ks * 16, K), 128, (K / 8) * 128);
+        bd = tc::make_desc(b0 + tc::kmajor_off(0, ks * 16, K), 128, (K / 8) * 128);
+      } else {
+        ad = tc::make_desc(a0 + tc::mnmajor_off(ks * 16, 0, M), (M / 8) * 128, 128);
+        bd = tc::make_desc(b0 + tc::mnmajor_off(ks * 16, 0, N), (N / 8) * 128, 128);
+      }
+      tc::mma_bf16(d, ad, bd, idesc, ks > 0);
+    }
+    tc::commit(&mbar);
+  }
+  if (!tc::mbar_wait(&mbar, 0)) atomicOr(err, 1);
+  tc::fence_after_sync();
+  const int warp = tid >> 5;
+  for (int c = 0; c < N; c += 16) {
+    float v[16];
+    tc::tmem_ld16(d + ((uint32_t)(warp * 32) << 16) + c, v);
+    for (int i = 0; i < 16; ++i) out[tid * N + c + i] = v[i];
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) tc::tmem_dealloc(d, 64);
 }
+
+// ---------------------------------------------------------------- shared pieces
+template <int E0, int E1, int E2>
+struct MixDims {
+  static constexpr int K1 = (E0 + 15) / 16 * 16;
+  static constexpr int N1 = (E1 + 15) / 16 * 16;
+  static constexpr int K2 = N1;
+  static constexpr int N2 = (E2 + 15) / 16 * 16;
+  static constexpr int W1B = N1 * K1 * 2;  // bytes of the layer-1 B tile (K-major)
+  static constexpr int W2B = N2 * K2 * 2;  // bytes of the layer-2 B tile (K-major)
+  static constexpr int NETB = W1B + W2B;
+  static constexpr int NSMALL = 2 * E0 + E1 + E2;  // w0, b0, b1, b2 (fp32)
+  static constexpr int OPA_A0 = 128 * K1 * 2, OPA_A1 = 128 * K2 * 2, OPA_H2 = 128 * N2 * 2;
+  static constexpr int OPA = OPA_A0 > OPA_A1 ? (OPA_A0 > OPA_H2 ? OPA_A0 : OPA_H2) : (OPA_A1 > OPA_H2 ? OPA_A1 : OPA_H2);
+  static constexpr int Z1 = E1 / E0, Z2 = E2 / E1;
+};
+
+constexpr int kBlkAtoms = 8;    // centre atoms per block (T accumulators: 8 slots x 16 channels = 128 lanes)
+constexpr int kRowCap = 256;    // compacted-row buffer (one tile + the carry of the next compaction round)
+constexpr int kRblkBytes = 128 * 128 * 2;
+
+// Bounded wait on the block's MMA barrier, made uniform across the block.
+#define MIX_WAIT()                                  \
+  do {                                              \
+    const bool w_ = tc::mbar_wait(&mbar, ph);       \
+    ph ^= 1;                                        \
+    ok = __syncthreads_and(w_ && ok) != 0;          \
+    tc::fence_after_sync();                         \
+  } while (0)
+
+// Weights of nets (ti, tj), tj < ntypes, as BF16 B tiles (K-major, zero
+// padded) plus the FP32 first layer and biases.
+template <int E0, int E1, int E2>
+__device__ void mix_load_nets(const DevModel &M, int ti, char *netb, float *small) {
+  using D = MixDims<E0, E1, E2>;
+  for (int tj = 0; tj < M.ntypes; ++tj) {
+    const int k = ti * M.ntypes + tj;
+    char *w1 = netb + tj * D::NETB, *w2 = w1 + D::W1B;
+    const float *W1 = M.ew[k][1], *W2 = M.ew[k][2];
+    for (int e = threadIdx.x; e < D::N1 * D::K1; e += blockDim.x) {
+      const int n = e / D::K1, kk = e - n * D::K1;
+      const float v = (n < E1 && kk < E0) ? W1[kk * E1 + n] : 0.f;
+      *reinterpret_cast<__nv_bfloat16 *>(w1 + tc::kmajor_off(n, kk, D::K1)) = __float2bfloat16_rn(v);
+    }
+    for (int e = threadIdx.x; e < D::N2 * D::K2; e += blockDim.x) {
+      const int n = e / D::K2, kk = e - n * D::K2;
+      const float v = (n < E2 && kk < E1) ? W2[kk * E2 + n] : 0.f;
+      *reinterpret_cast<__nv_bfloat16 *>(w2 + tc::kmajor_off(n, kk, D::K2)) = __float2bfloat16_rn(v);
+    }
+    float *sm = small + tj * D::NSMALL;
+    for (int e = threadIdx.x; e < E0; e += blockDim.x) {
+      sm[e] = M.ew[k][0][e];
+      sm[E0 + e] = M.eb[k][0][e];
+    }
+    for (int e = threadIdx.x; e < E1; e += blockDim.x) sm[2 * E0 + e] = M.eb[k][1][e];
+    for (int e = threadIdx.x; e < E2; e += blockDim.x) sm[2 * E0 + E1 + e] = M.eb[k][2][e];
+  }
+}
+
+// Block-wide stream compaction of one 128-candidate round: returns this
+// thread's slot among the kept candidates; *total gets the round's count.
+__device__ __forceinline__ int block_compact(bool keep, int *wcnt, int *total) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) wcnt[warp] = __popc(m);
+  __syncthreads();
+  int off = 0, tot = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    if (w < warp) off += wcnt[w];
+    tot += wcnt[w];
+  }
+  __syncthreads();
+  *total = tot;
+  return off + __popc(m & ((1u << lane) - 1u));
+}
+
+// Geometry of a compacted row and the 10-channel env row (FP32).
+__device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std, float mean, RowGeom &gm,
+                                            float &st, float R[10]) {
+  row_geom(make_float3(rb.x, rb.y, rb.z), rcut, gm);
+  const float sn = gm.s * inv_std;
+  st = (gm.s - mean) * inv_std;
+  const float inv_rp = 1.f / (gm.r + 1e-16f);
+  const float xh[3] = {gm.x[0] * inv_rp, gm.x[1] * inv_rp, gm.x[2] * inv_rp};
+  env_row(sn, xh, R);
+}
+
+// ---------------------------------------------------------------- embedding forward (BF16 tcgen05)
+// Per block of 8 centre atoms of type ti: neighbour rows with s(r) != 0 are
+// compacted block-wide into 128-row tiles.  Per tile (thread = row = TMEM lane):
+//   layer 0 (1 -> E0) FP32 on CUDA cores, h0 -> A0 (bf16)
+//   D  = A0 . W1   (tcgen05, 128 x N1)   -> h1 = tanh(D + b1) + rep(h0) -> A1
+//   D  = A1 . W2   (tcgen05, 128 x N2)   -> h2 = tanh(D + b2) + rep(h1) -> H2
+//   D3 += Rblk . H2 (tcgen05, M = 8 slots x 16 channels, K = 128 rows)
+// where Rblk holds each row's env row R~ in its atom's 16-lane slot (zero
+// elsewhere), so D3 accumulates T_a = sum_rows R~^T h2 for the 8 atoms in
+// TMEM across all tiles of both neighbour types.  The block epilogue writes
+// T / Nnbrs (FP32) and the descriptor G (dpmodel.py:74-78).
+template <int E0, int E1, int E2>
+__global__ void __launch_bounds__(128) k_mix_embed_fwd(DevModel M, SysDesc D, int ti, const float *__restrict__ pos,
+                                                       const int32_t *__restrict__ perm,
+                                                       const float *__restrict__ box, const int32_t *__restrict__ nbrs,
+                                                       float *__restrict__ Tout, float *__restrict__ Gout,
+                                                       int *__restrict__ err) {
+  using MD = MixDims<E0, E1, E2>;
+  extern __shared__ __align__(1024) char smem[];
+  char *netb = smem;
+  float *small = reinterpret_cast<float *>(netb + M.ntypes * MD::NETB);
+  char *opa = reinterpret_cast<char *>(small) + ((M.ntypes * MD::NSMALL * 4 + 1023) / 1024) * 1024;
+  char *rblk = opa + ((MD::OPA + 1023) / 1024) * 1024;
+  float4 *rowbuf = reinterpret_cast<float4 *>(rblk + kRblkBytes);
+  __shared__ int wcnt[4];
+  __shared__ float3 ri_s[kBlkAtoms];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase_s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  mix_load_nets<E0, E1, E2>(M, ti, netb, small);
+  for (int e = tid; e < kRblkBytes / 16; e += 128) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  if (warp == 0) tc::tmem_alloc(&tbase_s, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tbase_s;
+  const uint32_t tD = tbase, tD3 = tbase + 128, lane_off = (uint32_t)(warp * 32) << 16;
+  uint32_t ph = 0;
+  bool ok = true;
+
+  const int cnt_i = D.offs[ti + 1] - D.offs[ti];
+  const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
+  const int nblk = nbpf * D.F;
+  const float inv_std = M.inv_std[ti], mean = M.mean[ti];
+  const uint32_t idesc1 = tc::idesc_bf16(128, MD::N1, 0, 0);
+  const uint32_t idesc2 = tc::idesc_bf16(128, MD::N2, 0, 0);
+  const uint32_t idesc3 = tc::idesc_bf16(128, MD::N2, 1, 1);
+  const uint32_t opa_u = tc::smem_u32(opa), rblk_u = tc::smem_u32(rblk), net_u = tc::smem_u32(netb);
+
+  for (int blk = blockIdx.x; blk < nblk && ok; blk += gridDim.x) {
+    const int f = blk / nbpf, a0 = (blk - f * nbpf) * kBlkAtoms;
+    const int nb = min(kBlkAtoms, cnt_i - a0);
+    const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
+    const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+    const int3 ni = image_range(L, M.rcut);
+    const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
+    if (tid < nb) {
+      const int src = perm ? perm[D.offs[ti] + a0 + tid] : D.offs[ti] + a0 + tid;
+      const float *p = pos + ((size_t)f * D.N + src) * 3;
+      ri_s[tid] = make_float3(p[0], p[1], p[2]);
+    }
+    __syncthreads();
+    int ntile = 0;           // tiles issued for this block
+    bool pending = false;    // an MMA3 in flight
+    int my_slot = -1;        // Rblk slot written by this thread's row in the pending tile
+    int rowcount = 0;
+    for (int tj = 0; tj < D.ntypes && ok; ++tj) {
+      const int sel = D.sel[tj], cnt_j = D.offs[tj + 1] - D.offs[tj];
+      const int per_atom = sel * nim, total = nb * per_atom;
+      const char *w1t = netb + tj * MD::NETB;
+      const uint32_t w1_u = net_u + tj * MD::NETB, w2_u = w1_u + MD::W1B;
+      const float *sm = small + tj * MD::NSMALL;
+      for (int base = 0; base < total + 128 && ok; base += 128) {
+        // ---- compaction round (the extra round flushes the tail of this type)
+        const bool flush = base >= total;
+        if (!flush) {
+          const int p = base + tid;
+          bool keep = false;
+          float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (p < total) {
+            const int slot = p / per_atom, rem = p - slot * per_atom;
+            const int sidx = nim == 1 ? rem : rem / nim, mimg = rem - sidx * nim;
+            const int idx = nbrs[(g0 + slot) * D.S + D.col[tj] + sidx] & DPB_NBR_INDEX_MASK;
+            if (idx < cnt_j) {
+              const int js = D.offs[tj] + idx;
+              const int src = perm ? perm[js] : js;
+              const float *pj = pos + ((size_t)f * D.N + src) * 3;
+              const float3 x = rel_coord(ri_s[slot], make_float3(pj[0], pj[1], pj[2]), L, ni, mimg);
+              RowGeom gm;
+              row_geom(x, M.rcut, gm);
+              if (gm.s != 0.f) {
+                keep = true;
+                rv = make_float4(x.x, x.y, x.z, __int_as_float(slot));
+              }
+            }
+          }
+          int tot;
+          const int pos_ = block_compact(keep, wcnt, &tot);
+          if (keep) rowbuf[rowcount + pos_] = rv;
+          rowcount += tot;
+          __syncthreads();
+        }
+        while (rowcount >= 128 || (flush && rowcount > 0)) {
+          const int nrows = min(rowcount, 128);
+          // ---- wait for the previous contraction, clear its Rblk entries
+          if (pending) {
+            MIX_WAIT();
+            if (!ok) break;
+            if (my_slot >= 0) {
+              const uint32_t o = tc::mnmajor_off(tid, 16 * my_slot, 128);
+              *reinterpret_cast<uint4 *>(rblk + o) = make_uint4(0, 0, 0, 0);
+              *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(0, 0, 0, 0);
+            }
+            pending = false;
+          }
+          // ---- row data, layer 0 (FP32), A0 and Rblk
+          const bool act = tid < nrows;
+          const float4 rv = act ? rowbuf[tid] : make_float4(100.f, 100.f, 100.f, 0.f);
+          const int slot = act ? __float_as_int(rv.w) : -1;
+          RowGeom gm;
+          float st, R[10];
+          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
+          float h0[E0];
+#pragma unroll
+          for (int k = 0; k < E0; ++k) h0[k] = tanhf(fmaf(st, sm[k], sm[E0 + k]));
+#pragma unroll
+          for (int k8 = 0; k8 < MD::K1; k8 += 8) {
+            uint4 q;
+            q.x = tc::pack_bf16(k8 + 0 < E0 ? h0[min(k8 + 0, E0 - 1)] : 0.f, k8 + 1 < E0 ? h0[min(k8 + 1, E0 - 1)] : 0.f);
+            q.y = tc::pack_bf16(k8 + 2 < E0 ? h0[min(k8 + 2, E0 - 1)] : 0.f, k8 + 3 < E0 ? h0[min(k8 + 3, E0 - 1)] : 0.f);
+            q.z = tc::pack_bf16(k8 + 4 < E0 ? h0[min(k8 + 4, E0 - 1)] : 0.f, k8 + 5 < E0 ? h0[min(k8 + 5, E0 - 1)] : 0.f);
+            q.w = tc::pack_bf16(k8 + 6 < E0 ? h0[min(k8 + 6, E0 - 1)] : 0.f, k8 + 7 < E0 ? h0[min(k8 + 7, E0 - 1)] : 0.f);
+            *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(tid, k8, MD::K1)) = q;
+          }
+          my_slot = slot;
+          if (act) {
+            const uint32_t o = tc::mnmajor_off(tid, 16 * slot, 128);
+            *reinterpret_cast<uint4 *>(rblk + o) =
+                make_uint4(tc::pack_bf16(R[0], R[1]), tc::pack_bf16(R[2], R[3]), tc::pack_bf16(R[4], R[5]),
+                           tc::pack_bf16(R[6], R[7]));
+            *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(tc::pack_bf16(R[8], R[9]), 0u, 0u, 0u);
+          }
+          tc::fence_proxy_async();
+          tc::fence_before_sync();
+          __syncthreads();
+          if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < MD::K1 / 16; ++ks)
+              tc::mma_bf16(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128),
+                           tc::make_desc(w1_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128),
+                           idesc1, ks > 0);
+            tc::commit(&mbar);
+          }
+          MIX_WAIT();
+          if (!ok) break;
+          // ---- layer 1 epilogue: h1 = tanh(z + b1) + rep(h0) -> A1
+          float h1[E1];
+#pragma unroll
+          for (int c0 = 0; c0 < MD::N1; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tD + lane_off + c0, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (c0 + i < E1) h1[c0 + i] = tc::tanh_fast(v[i] + sm[2 * E0 + c0 + i]) + h0[(c0 + i) / MD::Z1];
+          }
+#pragma unroll
+          for (int k8 = 0; k8 < MD::K2; k8 += 8) {
+            float t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = (k8 + u < E1) ? h1[min(k8 + u, E1 - 1)] : 0.f;
+            *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(tid, k8, MD::K2)) =
+                make_uint4(tc::pack_bf16(t[0], t[1]), tc::pack_bf16(t[2], t[3]), tc::pack_bf16(t[4], t[5]),
+                           tc::pack_bf16(t[6], t[7]));
+          }
+          tc::fence_proxy_async();
+          tc::fence_before_sync();
+          __syncthreads();
+          if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < MD::K2 / 16; ++ks)
+              tc::mma_bf16(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128),
+                           tc::make_desc(w2_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128),
+                           idesc2, ks > 0);
+            tc::commit(&mbar);
+          }
+          MIX_WAIT();
+          if (!ok) break;
+          // ---- layer 2 epilogue: h2 = tanh(z + b2) + rep(h1) -> H2 (MN-major B of the contraction)
+#pragma unroll
+          for (int c0 = 0; c0 < MD::N2; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tD + lane_off + c0, v);
+            float h2[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              h2[i] = (c0 + i < E2) ? tc::tanh_fast(v[i] + sm[2 * E0 + E1 + min(c0 + i, E2 - 1)]) +
+                                          h1[min((c0 + i) / MD::Z2, E1 - 1)]
+                                    : 0.f;
+#pragma unroll
+            for (int h = 0; h < 16; h += 8)
+              *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(tid, c0 + h, MD::N2)) =
+                  make_uint4(tc::pack_bf16(h2[h], h2[h + 1]), tc::pack_bf16(h2[h + 2], h2[h + 3]),
+                             tc::pack_bf16(h2[h + 4], h2[h + 5]), tc::pack_bf16(h2[h + 6], h2[h + 7]));
+          }
+          tc::fence_proxy_async();
+          tc::fence_before_sync();
+          __syncthreads();
+          if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks)
+              tc::mma_bf16(tD3, tc::make_desc(rblk_u + tc::mnmajor_off(16 * ks, 0, 128), (128 / 8) * 128, 128),
+                           tc::make_desc(opa_u + tc::mnmajor_off(16 * ks, 0, MD::N2), (MD::N2 / 8) * 128, 128),
+                           idesc3, (ntile > 0 || ks > 0) ? 1u : 0u);
+            tc::commit(&mbar);
+          }
+          pending = true;
+          ++ntile;
+          // ---- drop the processed rows, keep the carry
+          const int rem = rowcount - nrows;
+          float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (tid < rem) carry = rowbuf[nrows + tid];
+          __syncthreads();
+          if (tid < rem) rowbuf[tid] = carry;
+          rowcount = rem;
+          __syncthreads();
+        }
+      }
+    }
+    // ---- block epilogue: T (FP32) and G from the TMEM accumulators
+    if (!ok) break;
+    if (pending) {
+      MIX_WAIT();
+      pending = false;
+      if (!ok) break;
+      if (my_slot >= 0) {
+        const uint32_t o = tc::mnmajor_off(tid, 16 * my_slot, 128);
+        *reinterpret_cast<uint4 *>(rblk + o) = make_uint4(0, 0, 0, 0);
+        *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(0, 0, 0, 0);
+      }
+    }
+    float *Xs = reinterpret_cast<float *>(rblk);  // staging [slot][c][w], 8 x 10 x E2 floats
+    {
+      const int slot = tid >> 4, c = tid & 15;
+#pragma unroll
+      for (int c0 = 0; c0 < MD::N2; c0 += 16) {
+        float v[16];
+        if (ntile > 0) {
+          tc::tmem_ld16(tD3 + lane_off + c0, v);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] = 0.f;
+        }
+        if (slot < nb && c < 10) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int w = c0 + i;
+            if (w < E2) {
+              const float t = v[i] * M.inv_nnbrs;
+              Tout[(g0 + slot) * 10 * E2 + c * E2 + w] = t;
+              Xs[(slot * 10 + c) * E2 + w] = t + (c == 0 ? M.tbias[w] : 0.f);
+            }
+          }
+        }
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    const int A = M.A;
+    for (int idx = tid; idx < nb * A * E2; idx += 128) {
+      const int slot = idx / (A * E2), rem = idx - slot * A * E2, aa = rem / E2, w = rem - aa * E2;
+      const float *X = Xs + slot * 10 * E2;
+      const float y1 = X[1 * E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
+      float v = X[aa] * X[w] + X[E2 + aa] * X[E2 + w] + X[2 * E2 + aa] * X[2 * E2 + w] + X[3 * E2 + aa] * X[3 * E2 + w];
+      v = fmaf(y1 * y1 + X[4 * E2 + A + aa], X[4 * E2 + w], v);
+      v = fmaf(y2 * y2 + X[5 * E2 + A + aa], X[5 * E2 + w], v);
+      v = fmaf(y3 * y3 + X[6 * E2 + A + aa], X[6 * E2 + w], v);
+      v = fmaf(kSqrt2 * y1 * y3 + X[7 * E2 + A + aa], X[7 * E2 + w], v);
+      v = fmaf(kSqrt2 * y2 * y1 + X[8 * E2 + A + aa], X[8 * E2 + w], v);
+      v = fmaf(kSqrt2 * y3 * y2 + X[9 * E2 + A + aa], X[9 * E2 + w], v);
+      Gout[(g0 + slot) * (size_t)A * E2 + aa * E2 + w] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < kRblkBytes / 16; e += 128) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+  }
+  if (!ok) {
+    // a wait gave up: flag it, give in-flight MMAs one more bounded wait, release TMEM
+    if (tid == 0) atomicOr(err, 1);
+    tc::mbar_wait(&mbar, ph);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tbase, 256);
+}
+
+template <int E0, int E1, int E2>
+size_t mix_fwd_smem(int ntypes) {
+  using MD = MixDims<E0, E1, E2>;
+  return (size_t)ntypes * MD::NETB + ((ntypes * MD::NSMALL * 4 + 1023) / 1024) * 1024 +
+         ((MD::OPA + 1023) / 1024) * 1024 + kRblkBytes + kRowCap * 16 + 1024;
+}
+
+template <int E0, int E1, int E2>
+int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+                         const float *box, const int32_t *nbrs, float *T, float *G, int *err, cudaStream_t st) {
+  const int cnt = D.offs[ti + 1] - D.offs[ti];
+  if (cnt == 0) return DPB_OK;
+  const int nblk = (cnt + kBlkAtoms - 1) / kBlkAtoms * D.F;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = mix_fwd_smem<E0, E1, E2>(M.ntypes);
+  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_fwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  const int grid = nblk < 2 * nsm ? nblk : 2 * nsm;
+  k_mix_embed_fwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G, err);
+  count_launch();
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}
+
+// ---------------------------------------------------------------- dispatch
+template <int E0, int E1, int E2>
+int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                     const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
+int launch_sgemm(int, int, int, const float *, int, RowMap, const float *, const Epi &, cudaStream_t);
+int launch_fit_energy(int, RowMap, int, const float *, const float *, const float *, const float *, const float *,
+                      float *, float *, double *, int, cudaStream_t);
+int fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Eatom, double *energy, char *w,
+                   cudaStream_t st);
+
+int mixed_supported(const DevModel &M) {
+  return (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
+}
+
+size_t mixed_workspace_per_atom(const DevModel &M) {
+  const int FW = M.FW[0];
+  return (size_t)(10 * M.E2 + M.A * M.E2 + 2 * M.nfit * FW + 4 * FW + 1) * 4 + 16 + 64;
+}
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+                      const int32_t *nbrs, float *T, float *G, int *err, cudaStream_t st) {
+  prof_begin(PROF_MIXED_EMBED_FWD, st);
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, err, st)
+                           : launch_mix_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, err, st);
+    if (rc) return rc;
+  }
+  prof_end(PROF_MIXED_EMBED_FWD, st);
+  return DPB_OK;
+}
+
+int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+               const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
+               cudaStream_t st) {
+  const size_t NF = (size_t)D.N * D.F;
+  char *w = (char *)ws;
+  int *err = (int *)w; w += 256;
+  float *T = (float *)w; w += al256(NF * 10 * M.E2 * 4);
+  float *G = (float *)w; w += al256(NF * M.A * M.E2 * 4);
+  DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+  int rc = mixed_descriptors(M, D, pos, perm, box, nbrs, T, G, err, st);
+  if (rc) return rc;
+  prof_begin(PROF_MIXED_FIT, st);
+  rc = fit_fp32_chain(M, D, G, Eatom, energy, w, st);
+  prof_end(PROF_MIXED_FIT, st);
+  if (rc) return rc;
+  prof_begin(PROF_MIXED_EMBED_BWD, st);
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    rc = (M.E2 == 100) ? launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st)
+                       : launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    if (rc) return rc;
+  }
+  prof_end(PROF_MIXED_EMBED_BWD, st);
+  return DPB_OK;
+}
+
 }  // namespace dpb
+
+extern "C" int dpb_selftest_tcgen05(int variant, float *out, int *err, void *stream) {
+  if (!out || !err || variant < 0 || variant > 1) return DPB_ERR_INVALID_ARG;
+  dpb::k_selftest_umma<<<1, 128, 0, (cudaStream_t)stream>>>(variant, out, err);
+  dpb::count_launch();
+  return cudaGetLastError() == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
+}

@@ -251,7 +251,19 @@ DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
  * drift/rebuild, 1 embedding forward, 2 fitting chain, 3 embedding adjoint,
  * 4 integrator, 5/6/7 the same three stages of the mixed path. */
 DPB_API int dpb_profile_enable(int on);
+/* Diagnostics: known-answer test of the tcgen05 tensor-core path, a
+ * 128x64x32 BF16 product into TMEM (variant 0: K-major operands, 1: MN-major);
+ * out: 128*64 floats (device), err: device int set on a barrier timeout. */
+DPB_API int dpb_selftest_tcgen05(int variant, float *out, int *err, void *stream);
 DPB_API int dpb_profile_read(int stage, double *ms, uint64_t *count);
+
+/* The descriptor stage alone: T (F,N,10,W) = sum_j R~^T h2 / Nnbrs and
+ * G (F,N,A*W) float32, type-sorted atom order (deepmd_jax/dpmodel.py:50-78);
+ * err: device int set when a tensor-core wait gave up (mixed path). */
+DPB_API int dpb_eval_descriptors(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
+                                 int natoms, int nframes, const int *type_count, const float *box,
+                                 const int32_t *nbrs, const int *sel, float *T, float *G, int *err,
+                                 void *stream);
 
 /* Number of kernels the library launched since load (for launch accounting). */
 DPB_API uint64_t dpb_kernel_launch_count(void);
