@@ -477,6 +477,431 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
   return DPB_OK;
 }
 
+// ---------------------------------------------------------------- embedding adjoint (BF16 tcgen05)
+// Per block of 8 centre atoms: dE/dT of each atom (adjoint of
+// dpmodel.py:74-78, FP32) is written, scaled by 1/Nnbrs, into the B tile DTB
+// (N = 8 slots x 16 channels, K = W).  The rows are recomputed with their
+// tangent along s~ (forward mode): [h0, dh0] -> tcgen05 -> [h1, dh1] ->
+// tcgen05 -> [h2, dh2], then U = H2 . DTB and V = dH2 . DTB on the tensor
+// cores; a row reads its atom's slot: u = dE/dR~, dE/ds~ = R~ . v.  The FP32
+// row adjoint gives dE/dx, scattered as forces and reduced into the virial.
+template <int E0, int E1, int E2>
+__global__ void __launch_bounds__(128, 1) k_mix_embed_bwd(DevModel M, SysDesc D, int ti,
+                                                          const float *__restrict__ pos,
+                                                          const int32_t *__restrict__ perm,
+                                                          const float *__restrict__ box,
+                                                          const int32_t *__restrict__ nbrs,
+                                                          const float *__restrict__ Tin, const float *__restrict__ dG,
+                                                          float4 *__restrict__ F4, double *__restrict__ virial,
+                                                          int *__restrict__ err) {
+  using MD = MixDims<E0, E1, E2>;
+  constexpr int DTB_BYTES = 128 * MD::N2 * 2;
+  constexpr int OPB = 2 * MD::OPA_H2;  // H2 + dH2 (largest pair)
+  extern __shared__ __align__(1024) char smem[];
+  char *netb = smem;
+  float *small = reinterpret_cast<float *>(netb + M.ntypes * MD::NETB);
+  char *dtb = reinterpret_cast<char *>(small) + ((M.ntypes * MD::NSMALL * 4 + 1023) / 1024) * 1024;
+  char *opb = dtb + ((DTB_BYTES + 1023) / 1024) * 1024;
+  float4 *rowbuf = reinterpret_cast<float4 *>(opb + ((OPB + 1023) / 1024) * 1024);
+  __shared__ int wcnt[4];
+  __shared__ float3 ri_s[kBlkAtoms];
+  __shared__ float fi_s[kBlkAtoms * 3];
+  __shared__ double vir_s[9];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase_s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  mix_load_nets<E0, E1, E2>(M, ti, netb, small);
+  if (tid < 9) vir_s[tid] = 0.0;
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  if (warp == 0) tc::tmem_alloc(&tbase_s, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tbase_s, lane_off = (uint32_t)(warp * 32) << 16;
+  uint32_t ph = 0;
+  bool ok = true;
+  float vir[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) vir[k] = 0.f;
+
+  const int cnt_i = D.offs[ti + 1] - D.offs[ti];
+  const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
+  const int nblk = nbpf * D.F;
+  const float inv_std = M.inv_std[ti], mean = M.mean[ti];
+  const int A = M.A;
+  const uint32_t idesc1 = tc::idesc_bf16(128, MD::N1, 0, 0);
+  const uint32_t idesc2 = tc::idesc_bf16(128, MD::N2, 0, 0);
+  const uint32_t idesc3 = tc::idesc_bf16(128, 128, 0, 0);
+  const uint32_t opb_u = tc::smem_u32(opb), dtb_u = tc::smem_u32(dtb), net_u = tc::smem_u32(netb);
+  // operand placements inside opb (byte offsets)
+  const uint32_t oA0 = 0, oA0t = MD::OPA_A0, oA1 = 0, oA1t = MD::OPA_A1, oH2 = 0, oH2t = MD::OPA_H2;
+
+  for (int blk = blockIdx.x; blk < nblk && ok; blk += gridDim.x) {
+    const int f = blk / nbpf, a0 = (blk - f * nbpf) * kBlkAtoms;
+    const int nb = min(kBlkAtoms, cnt_i - a0);
+    const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
+    const size_t frame_base = (size_t)f * D.N;
+    const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+    const int3 ni = image_range(L, M.rcut);
+    const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
+    if (tid < nb) {
+      const int src = perm ? perm[D.offs[ti] + a0 + tid] : D.offs[ti] + a0 + tid;
+      const float *p = pos + (frame_base + src) * 3;
+      ri_s[tid] = make_float3(p[0], p[1], p[2]);
+    }
+    if (tid < kBlkAtoms * 3) fi_s[tid] = 0.f;
+    // ---- dE/dT per atom -> DTB (bf16, K-major [n = 16 slot + c][k = w])
+    for (int e = tid; e < DTB_BYTES / 16; e += 128) reinterpret_cast<uint4 *>(dtb)[e] = make_uint4(0, 0, 0, 0);
+    float *Xs = reinterpret_cast<float *>(opb);      // 10 x E2
+    float *dGs = Xs + 10 * E2;                       // A x E2
+    float *Qs = dGs + A * E2;                        // 10 x A
+    float *dQs = Qs + 10 * A;                        // 10 x A
+    float *dXs = dQs + 10 * A;                       // 10 x E2
+    __syncthreads();
+    for (int a = 0; a < nb; ++a) {
+      const size_t g = g0 + a;
+      for (int e = tid; e < 10 * E2; e += 128) Xs[e] = Tin[g * 10 * E2 + e] + (e < E2 ? M.tbias[e] : 0.f);
+      for (int e = tid; e < A * E2; e += 128) dGs[e] = dG[g * (size_t)A * E2 + e];
+      __syncthreads();
+      for (int e = tid; e < 10 * A; e += 128) {
+        const int c = e / A, aa = e - c * A;
+        float qv;
+        if (c < 4) {
+          qv = Xs[c * E2 + aa];
+        } else {
+          const float y1 = Xs[E2 + A + aa], y2 = Xs[2 * E2 + A + aa], y3 = Xs[3 * E2 + A + aa];
+          const int m = c - 4;
+          const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
+          qv = b6[m] + Xs[c * E2 + A + aa];
+        }
+        Qs[e] = qv;
+        float dq = 0.f;
+        for (int w = 0; w < E2; ++w) dq = fmaf(dGs[aa * E2 + w], Xs[c * E2 + w], dq);
+        dQs[e] = dq;
+      }
+      __syncthreads();
+      for (int e = tid; e < 10 * E2; e += 128) {
+        const int c = e / E2, w = e - c * E2;
+        float v = 0.f;
+        for (int aa = 0; aa < A; ++aa) v = fmaf(dGs[aa * E2 + w], Qs[c * A + aa], v);
+        if (w < A && c < 4) v += dQs[c * A + w];
+        if (w >= A && w < 2 * A) {
+          const int aa = w - A;
+          if (c >= 4) {
+            v += dQs[c * A + aa];
+          } else if (c >= 1) {
+            const float y1 = Xs[E2 + w], y2 = Xs[2 * E2 + w], y3 = Xs[3 * E2 + w];
+            const float d0 = dQs[4 * A + aa], d1 = dQs[5 * A + aa], d2 = dQs[6 * A + aa], d3 = dQs[7 * A + aa],
+                        d4 = dQs[8 * A + aa], d5 = dQs[9 * A + aa];
+            if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
+            if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
+            if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
+          }
+        }
+        dXs[e] = v * M.inv_nnbrs;
+      }
+      __syncthreads();
+      for (int e = tid; e < 10 * MD::N2; e += 128) {
+        const int c = e / MD::N2, w = e - c * MD::N2;
+        const float v = w < E2 ? dXs[c * E2 + w] : 0.f;
+        *reinterpret_cast<__nv_bfloat16 *>(dtb + tc::kmajor_off(16 * a + c, w, MD::N2)) = __float2bfloat16_rn(v);
+      }
+      __syncthreads();
+    }
+    // ---- rows
+    int rowcount = 0;
+    for (int tj = 0; tj < D.ntypes && ok; ++tj) {
+      const int sel = D.sel[tj], cnt_j = D.offs[tj + 1] - D.offs[tj];
+      const int per_atom = sel * nim, total = nb * per_atom;
+      const uint32_t w1_u = net_u + tj * MD::NETB, w2_u = w1_u + MD::W1B;
+      const float *sm = small + tj * MD::NSMALL;
+      for (int base = 0; base < total + 128 && ok; base += 128) {
+        const bool flush = base >= total;
+        if (!flush) {
+          const int p = base + tid;
+          bool keep = false;
+          float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (p < total) {
+            const int slot = p / per_atom, rem = p - slot * per_atom;
+            const int sidx = nim == 1 ? rem : rem / nim, mimg = rem - sidx * nim;
+            const int idx = nbrs[(g0 + slot) * D.S + D.col[tj] + sidx] & DPB_NBR_INDEX_MASK;
+            if (idx < cnt_j) {
+              const int js = D.offs[tj] + idx;
+              const int src = perm ? perm[js] : js;
+              const float *pj = pos + (frame_base + src) * 3;
+              const float3 x = rel_coord(ri_s[slot], make_float3(pj[0], pj[1], pj[2]), L, ni, mimg);
+              RowGeom gm;
+              row_geom(x, M.rcut, gm);
+              if (gm.s != 0.f) {
+                keep = true;
+                rv = make_float4(x.x, x.y, x.z, __int_as_float((src << 3) | slot));
+              }
+            }
+          }
+          int tot;
+          const int pos_ = block_compact(keep, wcnt, &tot);
+          if (keep) rowbuf[rowcount + pos_] = rv;
+          rowcount += tot;
+          __syncthreads();
+        }
+        while (rowcount >= 128 || (flush && rowcount > 0)) {
+          const int nrows = min(rowcount, 128);
+          const bool act = tid < nrows;
+          const float4 rv = act ? rowbuf[tid] : make_float4(100.f, 100.f, 100.f, 0.f);
+          const int packed = act ? __float_as_int(rv.w) : 0;
+          const int slot = packed & 7, jsrc = packed >> 3;
+          RowGeom gm;
+          float st, R[10];
+          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
+          // ---- layer 0 with tangent: h0, d0 = dh0/ds~ -> A0, A0t
+          float h1[E1], d1[E1];
+          {
+            float h0[E0], d0[E0];
+#pragma unroll
+            for (int k = 0; k < E0; ++k) {
+              const float t = tanhf(fmaf(st, sm[k], sm[E0 + k]));
+              h0[k] = t;
+              d0[k] = (1.f - t * t) * sm[k];
+            }
+#pragma unroll
+            for (int k8 = 0; k8 < MD::K1; k8 += 8) {
+              float a_[8], b_[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                a_[u] = (k8 + u < E0) ? h0[min(k8 + u, E0 - 1)] : 0.f;
+                b_[u] = (k8 + u < E0) ? d0[min(k8 + u, E0 - 1)] : 0.f;
+              }
+              *reinterpret_cast<uint4 *>(opb + oA0 + tc::kmajor_off(tid, k8, MD::K1)) =
+                  make_uint4(tc::pack_bf16(a_[0], a_[1]), tc::pack_bf16(a_[2], a_[3]), tc::pack_bf16(a_[4], a_[5]),
+                             tc::pack_bf16(a_[6], a_[7]));
+              *reinterpret_cast<uint4 *>(opb + oA0t + tc::kmajor_off(tid, k8, MD::K1)) =
+                  make_uint4(tc::pack_bf16(b_[0], b_[1]), tc::pack_bf16(b_[2], b_[3]), tc::pack_bf16(b_[4], b_[5]),
+                             tc::pack_bf16(b_[6], b_[7]));
+            }
+            tc::fence_proxy_async();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (tid == 0) {
+              tc::fence_after_sync();
+#pragma unroll
+              for (int ks = 0; ks < MD::K1 / 16; ++ks) {
+                const uint64_t bd = tc::make_desc(w1_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128);
+                tc::mma_bf16(tbase, tc::make_desc(opb_u + oA0 + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                                                  (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
+                tc::mma_bf16(tbase + 64, tc::make_desc(opb_u + oA0t + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                                                       (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
+              }
+              tc::commit(&mbar);
+            }
+            MIX_WAIT();
+            if (!ok) break;
+            // ---- layer 1 epilogue with tangent -> A1, A1t
+#pragma unroll
+            for (int c0 = 0; c0 < MD::N1; c0 += 16) {
+              float z[16], dz[16];
+              tc::tmem_ld16(tbase + lane_off + c0, z);
+              tc::tmem_ld16(tbase + 64 + lane_off + c0, dz);
+#pragma unroll
+              for (int i = 0; i < 16; ++i)
+                if (c0 + i < E1) {
+                  const float t = tc::tanh_fast(z[i] + sm[2 * E0 + c0 + i]);
+                  h1[c0 + i] = t + h0[(c0 + i) / MD::Z1];
+                  d1[c0 + i] = (1.f - t * t) * dz[i] + d0[(c0 + i) / MD::Z1];
+                }
+            }
+          }
+#pragma unroll
+          for (int k8 = 0; k8 < MD::K2; k8 += 8) {
+            float a_[8], b_[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              a_[u] = (k8 + u < E1) ? h1[min(k8 + u, E1 - 1)] : 0.f;
+              b_[u] = (k8 + u < E1) ? d1[min(k8 + u, E1 - 1)] : 0.f;
+            }
+            *reinterpret_cast<uint4 *>(opb + oA1 + tc::kmajor_off(tid, k8, MD::K2)) =
+                make_uint4(tc::pack_bf16(a_[0], a_[1]), tc::pack_bf16(a_[2], a_[3]), tc::pack_bf16(a_[4], a_[5]),
+                           tc::pack_bf16(a_[6], a_[7]));
+            *reinterpret_cast<uint4 *>(opb + oA1t + tc::kmajor_off(tid, k8, MD::K2)) =
+                make_uint4(tc::pack_bf16(b_[0], b_[1]), tc::pack_bf16(b_[2], b_[3]), tc::pack_bf16(b_[4], b_[5]),
+                           tc::pack_bf16(b_[6], b_[7]));
+          }
+          tc::fence_proxy_async();
+          tc::fence_before_sync();
+          __syncthreads();
+          if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < MD::K2 / 16; ++ks) {
+              const uint64_t bd = tc::make_desc(w2_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128);
+              tc::mma_bf16(tbase, tc::make_desc(opb_u + oA1 + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+                                                (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
+              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + oA1t + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+                                                      (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
+            }
+            tc::commit(&mbar);
+          }
+          MIX_WAIT();
+          if (!ok) break;
+          // ---- layer 2 epilogue with tangent -> H2, H2t (K-major A of U / V)
+#pragma unroll
+          for (int c0 = 0; c0 < MD::N2; c0 += 16) {
+            float z[16], dz[16];
+            tc::tmem_ld16(tbase + lane_off + c0, z);
+            tc::tmem_ld16(tbase + 128 + lane_off + c0, dz);
+            float hh[16], dd[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              if (c0 + i < E2) {
+                const float t = tc::tanh_fast(z[i] + sm[2 * E0 + E1 + min(c0 + i, E2 - 1)]);
+                hh[i] = t + h1[min((c0 + i) / MD::Z2, E1 - 1)];
+                dd[i] = (1.f - t * t) * dz[i] + d1[min((c0 + i) / MD::Z2, E1 - 1)];
+              } else {
+                hh[i] = 0.f;
+                dd[i] = 0.f;
+              }
+            }
+#pragma unroll
+            for (int h = 0; h < 16; h += 8) {
+              *reinterpret_cast<uint4 *>(opb + oH2 + tc::kmajor_off(tid, c0 + h, MD::N2)) =
+                  make_uint4(tc::pack_bf16(hh[h], hh[h + 1]), tc::pack_bf16(hh[h + 2], hh[h + 3]),
+                             tc::pack_bf16(hh[h + 4], hh[h + 5]), tc::pack_bf16(hh[h + 6], hh[h + 7]));
+              *reinterpret_cast<uint4 *>(opb + oH2t + tc::kmajor_off(tid, c0 + h, MD::N2)) =
+                  make_uint4(tc::pack_bf16(dd[h], dd[h + 1]), tc::pack_bf16(dd[h + 2], dd[h + 3]),
+                             tc::pack_bf16(dd[h + 4], dd[h + 5]), tc::pack_bf16(dd[h + 6], dd[h + 7]));
+            }
+          }
+          tc::fence_proxy_async();
+          tc::fence_before_sync();
+          __syncthreads();
+          if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < MD::N2 / 16; ++ks) {
+              const uint64_t bd = tc::make_desc(dtb_u + tc::kmajor_off(0, 16 * ks, MD::N2), 128, (MD::N2 / 8) * 128);
+              tc::mma_bf16(tbase, tc::make_desc(opb_u + oH2 + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+                                                (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
+              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + oH2t + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+                                                      (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
+            }
+            tc::commit(&mbar);
+          }
+          MIX_WAIT();
+          if (!ok) break;
+          // ---- u, v of this row's atom slot; FP32 row adjoint
+          float u[10], v[10];
+#pragma unroll
+          for (int c = 0; c < 10; ++c) u[c] = v[c] = 0.f;
+#pragma unroll
+          for (int q = 0; q < kBlkAtoms; ++q) {
+            float uu[16], vv[16];
+            tc::tmem_ld16(tbase + lane_off + 16 * q, uu);
+            tc::tmem_ld16(tbase + 128 + lane_off + 16 * q, vv);
+            if (q == slot) {
+#pragma unroll
+              for (int c = 0; c < 10; ++c) {
+                u[c] = uu[c];
+                v[c] = vv[c];
+              }
+            }
+          }
+          tc::fence_before_sync();
+          float gst = 0.f;
+#pragma unroll
+          for (int c = 0; c < 10; ++c) gst = fmaf(R[c], v[c], gst);
+          float gx[3];
+          row_adjoint(gm, inv_std, u, gst, gx);
+          if (act) {
+            atomicAdd(&F4[frame_base + jsrc], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
+            atomicAdd(&fi_s[slot * 3 + 0], gx[0]);
+            atomicAdd(&fi_s[slot * 3 + 1], gx[1]);
+            atomicAdd(&fi_s[slot * 3 + 2], gx[2]);
+#pragma unroll
+            for (int p3 = 0; p3 < 3; ++p3)
+#pragma unroll
+              for (int q3 = 0; q3 < 3; ++q3) vir[p3 * 3 + q3] -= gm.x[p3] * gx[q3];
+          }
+          // ---- drop the processed rows, keep the carry
+          const int rem = rowcount - nrows;
+          float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (tid < rem) carry = rowbuf[nrows + tid];
+          __syncthreads();
+          if (tid < rem) rowbuf[tid] = carry;
+          rowcount = rem;
+          __syncthreads();
+        }
+      }
+    }
+    if (!ok) break;
+    __syncthreads();
+    if (tid < nb * 3) {
+      const int a = tid / 3, k = tid - a * 3;
+      const int src = perm ? perm[D.offs[ti] + a0 + a] : D.offs[ti] + a0 + a;
+      atomicAdd(reinterpret_cast<float *>(&F4[frame_base + src]) + k, fi_s[tid]);
+    }
+    __syncthreads();
+  }
+  // virial: per thread -> block (FP64) -> one atomic per component (frames
+  // of a block share f; blocks may span frames, so use the last frame only
+  // when F == 1 and the per-frame path otherwise)
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const float s = warp_sum(vir[k]);
+    if ((tid & 31) == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(err, 1);
+    tc::mbar_wait(&mbar, ph);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 9 && D.F == 1) atomicAdd(&virial[tid], vir_s[tid]);
+  if (warp == 0) tc::tmem_dealloc(tbase, 256);
+}
+
+template <int E0, int E1, int E2>
+size_t mix_bwd_smem(int ntypes) {
+  using MD = MixDims<E0, E1, E2>;
+  return (size_t)ntypes * MD::NETB + ((ntypes * MD::NSMALL * 4 + 1023) / 1024) * 1024 +
+         ((128 * MD::N2 * 2 + 1023) / 1024) * 1024 + ((2 * MD::OPA_H2 + 1023) / 1024) * 1024 + kRowCap * 16 + 1024;
+}
+
+template <int E0, int E1, int E2>
+int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+                         const float *box, const int32_t *nbrs, const float *T, const float *dG, float4 *F4,
+                         double *virial, int *err, cudaStream_t st) {
+  const int cnt = D.offs[ti + 1] - D.offs[ti];
+  if (cnt == 0) return DPB_OK;
+  const int nblk = (cnt + kBlkAtoms - 1) / kBlkAtoms * D.F;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = mix_bwd_smem<E0, E1, E2>(M.ntypes);
+  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_bwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  // frames are separate grid slices when F > 1 so that each block's virial
+  // belongs to one frame
+  if (D.F == 1) {
+    const int grid = nblk < nsm ? nblk : nsm;
+    k_mix_embed_bwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, err);
+    count_launch();
+  } else {
+    for (int f = 0; f < D.F; ++f) {
+      SysDesc Df = D;
+      Df.F = 1;
+      const int nb1 = (cnt + kBlkAtoms - 1) / kBlkAtoms;
+      const int grid = nb1 < nsm ? nb1 : nsm;
+      const size_t off = (size_t)f * D.N;
+      k_mix_embed_bwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, Df, ti, pos + off * 3, perm, box + f * 3,
+                                                            nbrs + off * D.S, T + off * 10 * M.E2,
+                                                            dG + off * M.A * M.E2, F4 + off, virial + f * 9, err);
+      count_launch();
+    }
+  }
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}
+
 // ---------------------------------------------------------------- dispatch
 template <int E0, int E1, int E2>
 int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
@@ -527,8 +952,9 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   if (rc) return rc;
   prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    rc = (M.E2 == 100) ? launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st)
-                       : launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    rc = (M.E2 == 100)
+             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, err, st)
+             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_BWD, st);
