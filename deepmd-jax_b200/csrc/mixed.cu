@@ -902,6 +902,302 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
   return DPB_OK;
 }
 
+// ---------------------------------------------------------------- fitting chain (BF16 tcgen05)
+// One CTA per 128 atoms of one centre type (thread = atom = TMEM lane).  The
+// forward layers and the adjoint down to dE/dG are GEMMs of M = 128 on the
+// tensor cores with the B operand (weights, BF16, K contiguous) streamed from
+// global memory through two shared-memory buffers, accumulating in TMEM
+// (two 256-column regions used alternately).  Epilogues run in FP32 on the
+// CUDA cores: tanh, dt-residuals, the energy dot product (FP64 frame sums) and
+// the adjoint gates; tanh values and residual sources go to a per-atom FP32
+// scratch, the BF16 activation for the next GEMM stays in shared memory.
+constexpr int kFitKC = 48;                 // K per streamed chunk (multiple of 16)
+constexpr int kFitMaxN = 256;              // N per GEMM pass (TMEM region)
+
+struct FitStream {
+  char *buf[2];
+  uint64_t *bar;      // [2]
+  uint32_t uses[2];
+};
+
+// B tile chunk: rows n in [n0, n0 + N) of a BF16 matrix with row stride ldb
+// (K contiguous), columns [k0, k0 + KC) -> K-major tile (N x KC) in dst.
+__device__ __forceinline__ void fit_load_b(char *dst, const __nv_bfloat16 *__restrict__ B, int ldb, int n0, int nvalid,
+                                           int N, int k0, int kvalid) {
+  const int nchunk8 = kFitKC / 8;
+  for (int e = threadIdx.x; e < N * nchunk8; e += blockDim.x) {
+    const int n = e / nchunk8, k8 = (e - n * nchunk8) * 8;
+    uint4 q = make_uint4(0, 0, 0, 0);
+    if (n < nvalid && k8 < kvalid) {
+      const __nv_bfloat16 *src = B + (size_t)(n0 + n) * ldb + k0 + k8;
+      if (k8 + 8 <= kvalid && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+        q = *reinterpret_cast<const uint4 *>(src);
+      } else {
+        __nv_bfloat16 t[8];
+        for (int u = 0; u < 8; ++u) t[u] = (k8 + u < kvalid) ? src[u] : __float2bfloat16_rn(0.f);
+        q = *reinterpret_cast<uint4 *>(t);
+      }
+    }
+    *reinterpret_cast<uint4 *>(dst + tc::kmajor_off(n, k8, kFitKC)) = q;
+  }
+}
+
+// A chunk from FP32 global rows (the descriptor G): 128 x KC -> K-major BF16.
+__device__ __forceinline__ void fit_load_a(char *dst, const float *__restrict__ Gm, const size_t *atom_of_row,
+                                           int nrows, int ld, int k0, int kvalid) {
+  const int nchunk8 = kFitKC / 8;
+  for (int e = threadIdx.x; e < 128 * nchunk8; e += blockDim.x) {
+    const int r = e / nchunk8, k8 = (e - r * nchunk8) * 8;
+    float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (r < nrows && k8 < kvalid) {
+      const float *src = Gm + atom_of_row[r] * ld + k0 + k8;
+      if (k8 + 8 <= kvalid) {
+        const float4 a = *reinterpret_cast<const float4 *>(src), b = *reinterpret_cast<const float4 *>(src + 4);
+        t[0] = a.x; t[1] = a.y; t[2] = a.z; t[3] = a.w; t[4] = b.x; t[5] = b.y; t[6] = b.z; t[7] = b.w;
+      } else {
+        for (int u = 0; u < 8 && k8 + u < kvalid; ++u) t[u] = src[u];
+      }
+    }
+    *reinterpret_cast<uint4 *>(dst + tc::kmajor_off(r, k8, kFitKC)) =
+        make_uint4(tc::pack_bf16(t[0], t[1]), tc::pack_bf16(t[2], t[3]), tc::pack_bf16(t[4], t[5]),
+                   tc::pack_bf16(t[6], t[7]));
+  }
+}
+
+// D[128 x N] = A[128 x K] . B^T-rows[n0 : n0 + N][k] (B row stride ldb).  A is
+// either resident (K-major tile with row length Kres) or streamed from G.
+// Returns false when a barrier wait gave up.
+__device__ bool fit_gemm(FitStream &S, uint32_t tmem_d, int N, int nvalid, int K, const __nv_bfloat16 *B, int ldb,
+                         int n0, const char *A_res, int Kres, const float *Gm, const size_t *atom_of_row, int nrows,
+                         int ldg) {
+  const int nch = (K + kFitKC - 1) / kFitKC;
+  const uint32_t idesc = tc::idesc_bf16(128, N, 0, 0);
+  const int a_bytes = A_res ? 0 : 128 * kFitKC * 2;
+  bool ok = true;
+  for (int c = 0; c < nch; ++c) {
+    const int b = c & 1;
+    if (S.uses[b] > 0) {
+      const bool w = tc::mbar_wait(&S.bar[b], (S.uses[b] - 1) & 1);
+      ok = __syncthreads_and(w && ok) != 0;
+      if (!ok) return false;
+    }
+    const int k0 = c * kFitKC, kv = min(kFitKC, K - k0);
+    char *bufb = S.buf[b];
+    if (!A_res) fit_load_a(bufb, Gm, atom_of_row, nrows, ldg, k0, kv);
+    fit_load_b(bufb + a_bytes, B, ldb, n0, nvalid, N, k0, kv);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::fence_after_sync();
+      const uint32_t bu = tc::smem_u32(bufb);
+      for (int ks = 0; ks < kFitKC / 16; ++ks) {
+        uint64_t ad;
+        if (A_res)
+          ad = tc::make_desc(tc::smem_u32(A_res) + tc::kmajor_off(0, k0 + 16 * ks, Kres), 128, (Kres / 8) * 128);
+        else
+          ad = tc::make_desc(bu + tc::kmajor_off(0, 16 * ks, kFitKC), 128, (kFitKC / 8) * 128);
+        const uint64_t bd = tc::make_desc(bu + a_bytes + tc::kmajor_off(0, 16 * ks, kFitKC), 128, (kFitKC / 8) * 128);
+        tc::mma_bf16(tmem_d, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+      }
+      tc::commit(&S.bar[b]);
+    }
+    S.uses[b]++;
+  }
+  // the accumulator is complete when the last chunk's MMAs are
+  const int bl = (nch - 1) & 1;
+  const bool w = tc::mbar_wait(&S.bar[bl], (S.uses[bl] - 1) & 1);
+  ok = __syncthreads_and(w && ok) != 0;
+  tc::fence_after_sync();
+  return ok;
+}
+
+// Store a row of FW FP32 values into the K-major BF16 activation tile.
+__device__ __forceinline__ void fit_store_act(char *HA, int row, int k8, const float (&v)[8], int FWp) {
+  *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, k8, FWp)) =
+      make_uint4(tc::pack_bf16(v[0], v[1]), tc::pack_bf16(v[2], v[3]), tc::pack_bf16(v[4], v[5]),
+                 tc::pack_bf16(v[6], v[7]));
+}
+
+template <int FW>
+__global__ void __launch_bounds__(128, 1) k_mix_fit(DevModel M, int ti, int Mrows, RowMap rm, const float *__restrict__ Gin,
+                                                   float *__restrict__ dGout, float *__restrict__ scratch,
+                                                   float *__restrict__ Eatom, double *__restrict__ energy, int N,
+                                                   int *__restrict__ err) {
+  static_assert(FW % 16 == 0 && FW <= kFitMaxN, "fit width");
+  constexpr int BUFB = 128 * kFitKC * 2 + kFitMaxN * kFitKC * 2;
+  extern __shared__ __align__(1024) char smem[];
+  char *HA = smem;                                  // 128 x FW bf16 (K-major)
+  char *bufs = HA + ((128 * FW * 2 + 1023) / 1024) * 1024;
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t tbase_s;
+  __shared__ size_t atom_s[128];
+  __shared__ double es[128];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int L = M.nfit, K0 = M.A * M.E2;
+  if (tid < 2) tc::mbar_init(&bars[tid], 1);
+  if (warp == 0) tc::tmem_alloc(&tbase_s, 512);
+  FitStream S;
+  S.buf[0] = bufs;
+  S.buf[1] = bufs + BUFB;
+  S.bar = bars;
+  S.uses[0] = S.uses[1] = 0;
+  const int r0 = blockIdx.x * 128, nrows = min(128, Mrows - r0);
+  const bool act = tid < nrows;
+  atom_s[tid] = act ? rm.atom(r0 + tid) : rm.atom(r0);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tb = tbase_s, lane_off = (uint32_t)(warp * 32) << 16;
+  const size_t me = atom_s[tid];
+  // per-atom scratch: t_l (L x FW), H_l (L x FW), gH (FW)
+  float *tl = scratch + me * (size_t)(2 * L + 1) * FW;
+  float *hl = tl + (size_t)L * FW;
+  float *gh = hl + (size_t)L * FW;
+  bool ok = true;
+  uint32_t region = 0;
+  // ---- forward
+  for (int l = 0; l < L && ok; ++l) {
+    const uint32_t td = tb + region * 256;
+    if (l == 0)
+      ok = fit_gemm(S, td, FW, FW, K0, M.fwT_bf[ti][0], K0, 0, nullptr, 0, Gin, atom_s, nrows, K0);
+    else
+      ok = fit_gemm(S, td, FW, FW, FW, M.fwT_bf[ti][l], FW, 0, HA, FW, nullptr, nullptr, 0, 0);
+    if (!ok) break;
+    const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
+    for (int c0 = 0; c0 < FW; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(td + lane_off + c0, v);
+      float hv[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int n = c0 + i;
+        const float t = tc::tanh_fast(v[i] + bias[n]);
+        float h = t;
+        if (dt) h = t * dt[n] + hl[(size_t)(l - 1) * FW + n];
+        hv[i] = h;
+        if (act) {
+          tl[(size_t)l * FW + n] = t;
+          hl[(size_t)l * FW + n] = h;
+        }
+      }
+      tc::fence_before_sync();
+      __syncthreads();  // every thread has read this chunk; HA may be overwritten after the GEMM
+      fit_store_act(HA, tid, c0, *reinterpret_cast<float(*)[8]>(hv), FW);
+      fit_store_act(HA, tid, c0 + 8, *reinterpret_cast<float(*)[8]>(hv + 8), FW);
+    }
+    region ^= 1;
+  }
+  // ---- energy and the first adjoint gate
+  double e_me = 0.0;
+  if (ok) {
+    const float *wf = M.fw[ti][L], *dtL = M.fdt[ti][L - 1];
+    float s = 0.f;
+    for (int c0 = 0; c0 < FW; c0 += 8) {
+      float g[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int n = c0 + i;
+        s = fmaf(hl[(size_t)(L - 1) * FW + n], wf[n], s);
+        const float t = tl[(size_t)(L - 1) * FW + n];
+        g[i] = wf[n] * (dtL ? dtL[n] : 1.f) * (1.f - t * t);
+      }
+      fit_store_act(HA, tid, c0, g, FW);
+    }
+    s += M.fb[ti][L][0];
+    if (act) Eatom[me] = s;
+    e_me = act ? (double)s : 0.0;
+  }
+  es[tid] = e_me;
+  __syncthreads();
+  if (tid == 0 && ok) {
+    double run = 0.0;
+    int cf = (int)(atom_s[0] / N);
+    for (int k = 0; k < nrows; ++k) {
+      const int fk = (int)(atom_s[k] / N);
+      if (fk != cf) {
+        atomicAdd(&energy[cf], run);
+        run = 0.0;
+        cf = fk;
+      }
+      run += es[k];
+    }
+    atomicAdd(&energy[cf], run);
+  }
+  // ---- adjoint: layers L-1 .. 1, gH_{l-1} = gZ_l W_l^T (+ gH_l if residual)
+  for (int l = L - 1; l >= 1 && ok; --l) {
+    const uint32_t td = tb + region * 256;
+    ok = fit_gemm(S, td, FW, FW, FW, M.fw_bf[ti][l], FW, 0, HA, FW, nullptr, nullptr, 0, 0);
+    if (!ok) break;
+    const bool res_l = M.fdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.fdt[ti][l - 1] != nullptr;
+    const float *dtm1 = M.fdt[ti][l - 1], *wf = M.fw[ti][L];
+    for (int c0 = 0; c0 < FW; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(td + lane_off + c0, v);
+      float gz[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int n = c0 + i;
+        float g = v[i];
+        if (res_l) g += (l == L - 1) ? wf[n] : gh[n];
+        const float t = tl[(size_t)(l - 1) * FW + n];
+        gz[i] = g * (res_lm1 ? dtm1[n] : 1.f) * (1.f - t * t);
+        if (act && res_lm1) gh[n] = g;  // read by the next layer's epilogue (same thread)
+      }
+      tc::fence_before_sync();
+      __syncthreads();
+      fit_store_act(HA, tid, c0, *reinterpret_cast<float(*)[8]>(gz), FW);
+      fit_store_act(HA, tid, c0 + 8, *reinterpret_cast<float(*)[8]>(gz + 8), FW);
+    }
+    region ^= 1;
+  }
+  // ---- dE/dG = gZ_0 W_0^T in column passes of 256
+  for (int n0 = 0; n0 < K0 && ok; n0 += kFitMaxN) {
+    const int nv = min(kFitMaxN, K0 - n0), Np = (nv + 15) / 16 * 16;
+    const uint32_t td = tb + region * 256;
+    ok = fit_gemm(S, td, Np, nv, FW, M.fw_bf[ti][0], FW, n0, HA, FW, nullptr, nullptr, 0, 0);
+    if (!ok) break;
+    for (int c0 = 0; c0 < Np; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(td + lane_off + c0, v);
+      if (act) {
+#pragma unroll
+        for (int i = 0; i < 16; i += 4)
+          if (c0 + i < nv)
+            *reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      }
+    }
+    tc::fence_before_sync();
+    region ^= 1;
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(err, 1);
+    tc::mbar_wait(&bars[0], 0);
+    tc::mbar_wait(&bars[1], 0);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tb, 512);
+}
+
+template <int FW>
+int launch_mix_fit(const DevModel &M, const SysDesc &D, float *G, float *dG, float *scratch, float *Eatom,
+                   double *energy, int *err, cudaStream_t st) {
+  constexpr int BUFB = 128 * kFitKC * 2 + kFitMaxN * kFitKC * 2;
+  const size_t smem = ((128 * FW * 2 + 1023) / 1024) * 1024 + 2 * BUFB;
+  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    const int cnt = D.offs[ti + 1] - D.offs[ti];
+    if (!cnt) continue;
+    const RowMap rm{cnt, D.N, D.offs[ti]};
+    const int Mrows = cnt * D.F;
+    k_mix_fit<FW><<<(Mrows + 127) / 128, 128, smem, st>>>(M, ti, Mrows, rm, G, dG, scratch, Eatom, energy, D.N, err);
+    count_launch();
+    DPB_LAUNCH_CHECK();
+  }
+  return DPB_OK;
+}
+
 // ---------------------------------------------------------------- dispatch
 template <int E0, int E1, int E2>
 int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
@@ -947,7 +1243,13 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   int rc = mixed_descriptors(M, D, pos, perm, box, nbrs, T, G, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
-  rc = fit_fp32_chain(M, D, G, Eatom, energy, w, st);
+  if (M.FW[0] == 240) {
+    rc = launch_mix_fit<240>(M, D, G, G, reinterpret_cast<float *>(w), Eatom, energy, err, st);
+  } else if (M.FW[0] == 128) {
+    rc = launch_mix_fit<128>(M, D, G, G, reinterpret_cast<float *>(w), Eatom, energy, err, st);
+  } else {
+    rc = fit_fp32_chain(M, D, G, Eatom, energy, w, st);
+  }
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_EMBED_BWD, st);

@@ -327,16 +327,18 @@ class Simulation:
             self._report_row(tic)
         self._is_initial_state = False
         NF3 = self._natoms * self._n_bead * 3
-        cap = min(self._step_chunk_size, steps) if steps else 0
-        buf_p = torch.empty((max(cap, 1), NF3), dtype=torch.float32, device="cuda")
-        buf_v = torch.empty((max(cap, 1), NF3), dtype=torch.float32, device="cuda")
+        cap = self._step_chunk_size
+        if getattr(self, "_traj_bufs", None) is None:
+            # trajectory frames of one chunk, kept across runs so captured graphs stay valid
+            self._traj_bufs = (torch.empty((cap, NF3), dtype=torch.float32, device="cuda"),
+                               torch.empty((cap, NF3), dtype=torch.float32, device="cuda"))
+        buf_p, buf_v = self._traj_bufs
         done, idx = 0, int(first)
         overflow_twice = False
         while done < steps:
             n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
             _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
-            self._run_chunk(n, buf_p[:n] if n == cap else buf_p[:n].contiguous(), buf_v[:n] if n == cap else
-                            buf_v[:n].contiguous())
+            self._run_chunk(n, buf_p[:n], buf_v[:n])
             r = self._report_struct()
             code = int(r.status)
             if code & 16:
