@@ -1,5 +1,6 @@
 // C ABI of libdpb200: model upload, workspace sizing and evaluation dispatch.
 #include "internal.cuh"
+#include "tc.cuh"
 #include <cuda_bf16.h>
 #include <cstring>
 #include <vector>
@@ -73,8 +74,9 @@ size_t mixed_workspace_per_atom(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
                cudaStream_t st);
-int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
-                      const int32_t *nbrs, float *T, float *G, int *err, cudaStream_t st);
+int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
+                          const float *box, const int32_t *nbrs, float *T, float *G, int *err, void *ws,
+                          cudaStream_t st);
 int fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Eatom, double *energy, char *w,
                    cudaStream_t st);
 }  // namespace dpb
@@ -145,6 +147,39 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
         rc = upload_bf16(m, v, &M.ew_bf[k][l]);
       }
     }
+  // shared-memory images of the embedding nets for the tensor-core kernels
+  {
+    const int K1 = (M.E0 + 15) / 16 * 16, N1 = (M.E1 + 15) / 16 * 16, K2 = N1, N2 = (M.E2 + 15) / 16 * 16;
+    const int W1B = N1 * K1 * 2, W2B = N2 * K2 * 2;
+    M.net_img_bytes = W1B + W2B;
+    M.net_small_floats = ((2 * M.E0 + M.E1 + M.E2) + 3) / 4 * 4;
+    for (int k = 0; k < nt * nt && rc == DPB_OK; ++k) {
+      std::vector<uint8_t> img(M.net_img_bytes, 0);
+      const float *W1 = d->embed_kernel[k * 3 + 1], *W2 = d->embed_kernel[k * 3 + 2];
+      for (int n = 0; n < N1; ++n)
+        for (int kk = 0; kk < K1; ++kk) {
+          const float v = (n < M.E1 && kk < M.E0) ? W1[kk * M.E1 + n] : 0.f;
+          *reinterpret_cast<__nv_bfloat16 *>(img.data() + dpb::tc::kmajor_off(n, kk, K1)) = __float2bfloat16_rn(v);
+        }
+      for (int n = 0; n < N2; ++n)
+        for (int kk = 0; kk < K2; ++kk) {
+          const float v = (n < M.E2 && kk < M.E1) ? W2[kk * M.E2 + n] : 0.f;
+          *reinterpret_cast<__nv_bfloat16 *>(img.data() + W1B + dpb::tc::kmajor_off(n, kk, K2)) =
+              __float2bfloat16_rn(v);
+        }
+      const char *dimg = nullptr;
+      rc = upload(m, reinterpret_cast<const char *>(img.data()), img.size(), &dimg);
+      M.net_img[k] = dimg;
+      std::vector<float> sm(M.net_small_floats, 0.f);
+      for (int e = 0; e < M.E0; ++e) {
+        sm[e] = d->embed_kernel[k * 3 + 0][e];
+        sm[M.E0 + e] = d->embed_bias[k * 3 + 0][e];
+      }
+      for (int e = 0; e < M.E1; ++e) sm[2 * M.E0 + e] = d->embed_bias[k * 3 + 1][e];
+      for (int e = 0; e < M.E2; ++e) sm[2 * M.E0 + M.E1 + e] = d->embed_bias[k * 3 + 2][e];
+      if (rc == DPB_OK) rc = upload(m, sm.data(), sm.size(), &M.net_small[k]);
+    }
+  }
   if (rc == DPB_OK) rc = upload(m, d->tbias, (size_t)M.E2, &M.tbias);
   const int K0 = M.A * M.E2;
   for (int t = 0; t < nt && rc == DPB_OK; ++t) {
@@ -393,9 +428,12 @@ static int descriptors_fp32(const DevModel &M, const SysDesc &D, const float *po
 extern "C" int dpb_eval_descriptors(const dpb_model *m, int precision, const float *pos, const int32_t *perm,
                                     int natoms, int nframes, const int *type_count, const float *box,
                                     const int32_t *nbrs, const int *sel, float *T, float *G, int *err,
-                                    void *stream) {
+                                    void *workspace, size_t ws_bytes, void *stream) {
   if (!m || !pos || !box || !nbrs || !T || !G || !err || !type_count || !sel || natoms <= 0 || nframes <= 0)
     return DPB_ERR_INVALID_ARG;
+  size_t need = 0;
+  dpb_eval_workspace_bytes(m, natoms, nframes, &need);
+  if (!workspace || ws_bytes < need) return DPB_ERR_WORKSPACE;
   SysDesc D;
   int rc = fill_sys(m, natoms, nframes, type_count, sel, D);
   if (rc) return rc;
@@ -403,7 +441,7 @@ extern "C" int dpb_eval_descriptors(const dpb_model *m, int precision, const flo
   if (precision == DPB_PREC_FP32) return descriptors_fp32(m->dm, D, pos, perm, box, nbrs, T, G, st);
   if (precision == DPB_PREC_MIXED) {
     if (!mixed_supported(m->dm)) return DPB_ERR_UNSUPPORTED;
-    return mixed_descriptors(m->dm, D, pos, perm, box, nbrs, T, G, err, st);
+    return mixed_descriptors_f32(m->dm, D, pos, perm, box, nbrs, T, G, err, workspace, st);
   }
   return DPB_ERR_INVALID_ARG;
 }

@@ -259,11 +259,12 @@ DPB_API int dpb_profile_read(int stage, double *ms, uint64_t *count);
 
 /* The descriptor stage alone: T (F,N,10,W) = sum_j R~^T h2 / Nnbrs and
  * G (F,N,A*W) float32, type-sorted atom order (deepmd_jax/dpmodel.py:50-78);
- * err: device int set when a tensor-core wait gave up (mixed path). */
+ * err: device int set when a tensor-core wait gave up (mixed path);
+ * workspace as for dpb_eval. */
 DPB_API int dpb_eval_descriptors(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
                                  int natoms, int nframes, const int *type_count, const float *box,
                                  const int32_t *nbrs, const int *sel, float *T, float *G, int *err,
-                                 void *stream);
+                                 void *workspace, size_t workspace_bytes, void *stream);
 
 /* Number of kernels the library launched since load (for launch accounting). */
 DPB_API uint64_t dpb_kernel_launch_count(void);

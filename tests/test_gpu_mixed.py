@@ -29,7 +29,8 @@ def _descriptors(precision, p, v, w):
     lib = dm.lib
     lib.dpb_eval_descriptors.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 2 + \
         [ctypes.c_int] * 2 + [ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.c_void_p,
-                              ctypes.POINTER(ctypes.c_int)] + [ctypes.c_void_p] * 4
+                              ctypes.POINTER(ctypes.c_int)] + [ctypes.c_void_p] * 4 + \
+        [ctypes.c_size_t, ctypes.c_void_p]
     perm, cnt = sort_by_type(w["type_idx"], 2)
     N = len(perm)
     pos = torch.tensor(np.ascontiguousarray(w["position"][None]), dtype=torch.float32, device="cuda")
@@ -40,9 +41,10 @@ def _descriptors(precision, p, v, w):
     T = torch.zeros((N, 10, W), dtype=torch.float32, device="cuda")
     Gd = torch.zeros((N, A * W), dtype=torch.float32, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws = dm.eval_workspace(N, 1)
     rc = lib.dpb_eval_descriptors(dm.handle, {"fp32": 0, "mixed": 1}[precision], _ptr(pos), _ptr(pm), N, 1,
                                   _lib.int_array(cnt), _ptr(box), _ptr(nbrs), _lib.int_array([46, 92]), _ptr(T),
-                                  _ptr(Gd), _ptr(err), _stream())
+                                  _ptr(Gd), _ptr(err), _ptr(ws), ws.numel(), _stream())
     torch.cuda.synchronize()
     assert rc == 0 and int(err.item()) == 0
     return T.cpu().numpy(), Gd.cpu().numpy()
