@@ -230,7 +230,8 @@ def gpu_arm(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         ms = s.elapsed_time(e)
-        launches = lib.dpb_kernel_launch_count() - l0
+        launches = lib.dpb_kernel_launch_count() - l0 + sim._graph_launches_replayed
+        sim._graph_launches_replayed = 0
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -254,7 +255,7 @@ def gpu_arm(args, rank, world, local_rank):
         _, _ = timed_device_steps(sim, min(args.steps, 10), graph=False)
         stages = {}
         for sid, name in enumerate(["nlist", "embed_fwd", "fit", "embed_bwd", "integrate",
-                                    "mixed_embed_fwd", "mixed_fit", "mixed_embed_bwd"]):
+                                    "mixed_embed_fwd", "mixed_fit", "mixed_embed_bwd", "mixed_dT"]):
             msr, cnt = ctypes.c_double(), ctypes.c_uint64()
             lib.dpb_profile_read(sid, ctypes.byref(msr), ctypes.byref(cnt))
             if cnt.value:
@@ -289,13 +290,20 @@ def gpu_arm(args, rank, world, local_rank):
     flop_stage = {"embed_fwd": rows * EMB_FWD_FLOP_ROW, "embed_bwd": rows * EMB_BWD_FLOP_ROW,
                   "fit": FIT_FLOP_ATOM}
     roof = None
+    traffic = {}
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
+    except Exception:
+        pass
     if dom:
         key = dom.replace("mixed_", "")
         fl = flop_stage.get(key, 0) * N
         t_ms = cand[dom][0]
         ach = fl / (t_ms / 1e3) / 1e12 if fl else 0.0
+        tr = traffic.get(dom)
         roof = {"bound": "tensor", "achieved": ach, "peak": pk_tensor, "unit": "TFLOP/s",
-                "frac": ach / pk_tensor, "traffic": None, "kernel": dom, "launch_ms": t_ms,
+                "frac": ach / pk_tensor, "traffic": tr["bytes_per_step"] if tr else None,
+                "traffic_source": tr["source"] if tr else None, "kernel": dom, "launch_ms": t_ms,
                 "algorithmic_flop_per_launch": fl, "peak_source": peak_src + " (bf16 dense, burst)"}
     line = {
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,

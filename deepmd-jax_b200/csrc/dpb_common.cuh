@@ -25,7 +25,8 @@ enum ProfId : int {
   PROF_MIXED_EMBED_FWD = 5,
   PROF_MIXED_FIT = 6,
   PROF_MIXED_EMBED_BWD = 7,
-  PROF_COUNT = 8
+  PROF_MIXED_DT = 8,
+  PROF_COUNT = 9
 };
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st);

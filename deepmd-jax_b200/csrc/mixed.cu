@@ -1248,7 +1248,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
                         : launch_mix_fit<128>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
-  prof_begin(PROF_MIXED_EMBED_BWD, st);
+  prof_begin(PROF_MIXED_DT, st);
   {
     const size_t smem = (size_t)4 * (20 * M.E2 + K0 + 20 * M.A) * 4;
     if (M.E2 == 100) {
@@ -1261,6 +1261,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
     count_launch();
     DPB_LAUNCH_CHECK();
   }
+  prof_end(PROF_MIXED_DT, st);
+  prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     rc = (M.E2 == 100)
              ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, dTb, F4, virial, err, st)

@@ -167,6 +167,8 @@ class Simulation:
         self._kT = (temperature if temperature is not None else 0.0) * TEMP_UNIT_CONVERSION
         self._use_graph = use_cuda_graph
         self._graphs = {}
+        self._graph_kernels = {}
+        self._graph_launches_replayed = 0
         nt = int(params["ntypes"])
         self._perm, self._type_count = sort_by_type(self._type_idx, nt)
         # neighbour capacity from a measurement at the initial positions (allocate_fn)
@@ -268,6 +270,7 @@ class Simulation:
             g = torch.cuda.CUDAGraph()
             side = torch.cuda.Stream()
             side.wait_stream(stream)
+            k0 = self.lib.dpb_kernel_launch_count()
             with torch.cuda.stream(side):
                 with torch.cuda.graph(g, stream=side, capture_error_mode="relaxed"):
                     rc = self.lib.dpb_md_run(self._h, n, _ptr(traj_p), _ptr(traj_v),
@@ -275,7 +278,9 @@ class Simulation:
             stream.wait_stream(side)
             _lib.check(rc, "dpb_md_run (capture)")
             self._graphs[key] = g
+            self._graph_kernels[key] = int(self.lib.dpb_kernel_launch_count() - k0)
         g.replay()
+        self._graph_launches_replayed += self._graph_kernels.get(key, 0)
 
     # ------------------------------------------------------------------ reports
     def _temperature_of(self, KE):

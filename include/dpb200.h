@@ -249,7 +249,8 @@ DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
 /* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
  * default; not for use inside graph capture).  Stage ids: 0 neighbour
  * drift/rebuild, 1 embedding forward, 2 fitting chain, 3 embedding adjoint,
- * 4 integrator, 5/6/7 the same three stages of the mixed path. */
+ * 4 integrator, 5/6/7 the same three stages of the mixed path, 8 the mixed
+ * path's dE/dT kernel. */
 DPB_API int dpb_profile_enable(int on);
 /* Diagnostics: known-answer test of the tcgen05 tensor-core path, a
  * 128x64x32 BF16 product into TMEM (variant 0: K-major operands, 1: MN-major);
