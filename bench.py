@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling case: plain MD steps (direct launches, no timing) for ncu")
     ap.add_argument("--n-side", type=int, default=N_SIDE, help="waters per box side (profiling case)")
+    ap.add_argument("--study", default="none", choices=["none", "drift", "pimd"],
+                    help="drift: NVE total-energy drift of both forms on the 98,304-atom box; "
+                         "pimd: 32-bead PILE-L throughput of both forms (1,536-atom water)")
+    ap.add_argument("--report-every", type=int, default=100, help="drift study: steps between energy samples")
     return ap.parse_args()
 
 
@@ -375,10 +379,88 @@ def ncu_case(args):
     return 0
 
 
+def _models():
+    from deepmd_jax_b200.systems import water_box, init_dp_params, nnbrs_rule
+    w0 = water_box(4, 12.42, seed=0)
+    return init_dp_params(nnbrs=nnbrs_rule(w0["position"], w0["box"], w0["type_idx"], 6.0))
+
+
+def study_drift(args):
+    """Total-energy drift of NVE on the 98,304-atom box, FP32 and mixed forms:
+    args.steps steps from the same state, the invariant sampled every
+    args.report_every steps; slope of a least-squares line in eV/atom/ps."""
+    import numpy as np
+    import torch
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import water_box
+    params, variables = _models()
+    w = water_box(N_SIDE, BOX, seed=0)
+    N = len(w["position"])
+    out = {"study": "nve_drift", "atoms": N, "dt_fs": DT, "steps": args.steps, "forms": {}}
+    for prec in ("fp32", "mixed"):
+        sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVE", DT,
+                         w["position"], initial_velocity=w["velocity"], report_interval=args.report_every,
+                         precision=prec, verbose=False)
+        t0 = time.perf_counter()
+        sim.run(args.steps, trajectory=False)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        rows = np.array([[r[0], r[4]] for r in sim.log])
+        t_ps = rows[:, 0] * DT / 1000.0
+        e = rows[:, 1] / N
+        slope = float(np.polyfit(t_ps, e, 1)[0]) if len(t_ps) > 1 else None
+        out["forms"][prec] = {"drift_eV_per_atom_per_ps": slope, "max_dev_eV_per_atom": float(np.abs(e - e[0]).max()),
+                              "E0_eV_per_atom": float(e[0]), "samples": len(e), "wall_s": wall,
+                              "status": int(sim._report_struct().status)}
+    return out
+
+
+def study_pimd(args):
+    """32-bead PILE-L PIMD (1,536-atom water, L = 24.83 A, 300 K, dt 0.25 fs):
+    all beads evaluated in one batched launch per kernel; atom-steps/s counts
+    beads x atoms, timed with CUDA events over args.steps steps (graphs)."""
+    import numpy as np
+    import torch
+    from deepmd_jax_b200 import _lib
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import water_box
+    params, variables = _models()
+    w = water_box(8, 24.83, seed=0)
+    N, P = len(w["position"]), 32
+    lib = _lib.load()
+    out = {"study": "pimd_pile_l", "atoms": N, "beads": P, "dt_fs": 0.25, "steps": args.steps, "forms": {}}
+    for prec in ("fp32", "mixed"):
+        sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.25,
+                         w["position"], temperature=300.0, n_bead=P, tau_t=100.0, seed=1,
+                         report_interval=10 ** 9, precision=prec, verbose=False)
+        for _ in range(max(args.warmup, 3)):
+            sim._run_chunk(1, None, None)
+        sim._run_chunk(CHUNK, None, None)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_full, rem = divmod(args.steps, CHUNK)
+        s.record()
+        for _ in range(n_full):
+            sim._run_chunk(CHUNK, None, None)
+        if rem:
+            sim._run_chunk(rem, None, None)
+        e.record()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e)
+        r = sim._report_struct()
+        out["forms"][prec] = {"atom_steps_per_s": N * P * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                              "ns_per_day": 1e-6 * 0.25 * 86400 * args.steps / (ms / 1e3),
+                              "status": int(r.status), "rebuilds": int(r.rebuilds)}
+    return out
+
+
 def main():
     args = parse()
     if args.ncu_case:
         return ncu_case(args)
+    if args.study != "none":
+        print(json.dumps(study_drift(args) if args.study == "drift" else study_pimd(args)))
+        return 0
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -17,6 +17,7 @@ import torch
 
 from . import _lib
 from .engine import DeviceModel, NeighborBuilder, sort_by_type, _ptr, _stream
+from .md_utils import knbr_from_counts
 from .systems import MASS_UNIT_CONVERSION, TEMP_UNIT_CONVERSION
 from .utils import load_model
 
@@ -86,12 +87,10 @@ def normal_mode_transform(n_bead, kT):
     return ring_poly_freq * np.sqrt(np.maximum(eva, 0.0)), eve
 
 
-def knbr_from_counts(max_counts, buffer_ratio):
-    """Capacity rule of the reference allocate_fn (md_utils.py:394-403);
-    returns the number of kept columns (knbr - 1) per type."""
-    k = np.asarray(max_counts, float)
-    knbr = np.where(k == 0, 1, 1 + (k * buffer_ratio + np.maximum(20 - k, 0) * max(buffer_ratio - 1.2, 0)))
-    return [max(int(x) - 1, 1) for x in knbr.astype(int)]
+def sel_from_counts(max_counts, buffer_ratio):
+    """Kept columns (knbr - 1) per type under the reference's capacity rule
+    (md_utils.py:394-403)."""
+    return [max(k - 1, 1) for k in knbr_from_counts(max_counts, buffer_ratio)]
 
 
 class Simulation:
@@ -225,7 +224,7 @@ class Simulation:
         counts = torch.empty((self._n_bead, self._natoms, len(big)), dtype=torch.int32, device="cuda")
         nb.build(p, perm=pm, counts=counts)
         mx = counts.reshape(-1, len(big)).max(0).values.cpu().numpy()
-        return knbr_from_counts(mx, self._buffer_ratio)
+        return sel_from_counts(mx, self._buffer_ratio)
 
     def _initial_velocity(self, seed):
         """Maxwell-Boltzmann momenta sqrt(m kT) N(0,1) with the mean momentum
@@ -313,18 +312,23 @@ class Simulation:
         return r
 
     # ------------------------------------------------------------------ public API
-    def run(self, steps, dump_interval=None, dump_prefix=None, dump_content="positions", dump_mode="overwrite"):
+    def run(self, steps, dump_interval=None, dump_prefix=None, dump_content="positions", dump_mode="overwrite",
+            trajectory=True):
         """Run ``steps`` steps; returns the trajectory dict of every step
-        (deepmd_jax/md.py:874-964)."""
+        (deepmd_jax/md.py:874-964).  ``trajectory=False`` keeps every frame on
+        the device (no per-step copy to the host) and returns None; the state
+        stays readable through the getters."""
         if dump_prefix is not None:
             raise NotImplementedError("XYZ dumping is outside this engine; use the returned trajectory")
         steps = int(steps)
         first = self._is_initial_state
         L = steps + int(first)
         fs = self._frame_shape()
-        traj = {"position": np.zeros((L,) + fs), "velocity": np.zeros((L,) + fs),
-                "box": np.tile(self._box, (L, 1))}
-        if first:
+        traj = None
+        if trajectory:
+            traj = {"position": np.zeros((L,) + fs), "velocity": np.zeros((L,) + fs),
+                    "box": np.tile(self._box, (L, 1))}
+        if first and trajectory:
             traj["position"][0] = self.getPosition()
             traj["velocity"][0] = self.getVelocity()
         tic_run = tic = time()
@@ -343,7 +347,10 @@ class Simulation:
         while done < steps:
             n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
             _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
-            self._run_chunk(n, buf_p[:n], buf_v[:n])
+            if trajectory:
+                self._run_chunk(n, buf_p[:n], buf_v[:n])
+            else:
+                self._run_chunk(n, None, None)
             r = self._report_struct()
             code = int(r.status)
             if code & 16:
@@ -359,6 +366,13 @@ class Simulation:
                 self._resize_capacity()
                 continue
             overflow_twice = False
+            if not trajectory:
+                done += n
+                self.step += n
+                if self.step % self.report_interval == 0 or done == steps:
+                    self._report_row(tic)
+                    tic = time()
+                continue
             pos_chunk = buf_p[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
             mom_chunk = buf_v[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
             pos_u = np.empty_like(pos_chunk)
@@ -382,7 +396,7 @@ class Simulation:
             print("# Finished %d steps in %.2f s." % (steps, elapsed))
             print("# Performance: %.3f ns/day, %.3f step/us/atom" %
                   (nsd, 1e-6 * steps * self._natoms * self._n_bead / (elapsed + 1e-6)))
-        if self._is_pimd:
+        if self._is_pimd and traj is not None:
             traj["centroid"] = np.stack([self._centroid(p) for p in traj["position"]])
         return traj
 

@@ -51,16 +51,21 @@ def shift_ortho(d, box3):
     return torch.remainder(d - box3 / 2, box3) - box3 / 2
 
 
-def _t(a, dtype):
-    return torch.as_tensor(np.asarray(a), dtype=dtype)
+def _t(a, dtype, device="cpu"):
+    return torch.as_tensor(np.asarray(a), dtype=dtype, device=device)
 
 
 class OracleModel:
     """Holds one model's parameters as torch tensors of a chosen dtype."""
 
-    def __init__(self, params, variables, dtype=torch.float64):
+    def __init__(self, params, variables, dtype=torch.float64, device="cpu"):
         self.params = params
         self.dtype = dtype
+        self.device = torch.device(device)
+
+        def _td(a, dt):
+            return _t(a, dt, self.device)
+
         v = variables["params"]
         p = params
         self.nt = int(p["ntypes"])
@@ -68,18 +73,18 @@ class OracleModel:
         self.A = int(p["axis"])
         self.ew = list(p["embed_widths"])
         self.fw = list(p["fit_widths"])
-        self.mean = _t(p["sr_mean"], dtype)
-        self.std = _t(p["sr_std"], dtype)
+        self.mean = _td(p["sr_mean"], dtype)
+        self.std = _td(p["sr_std"], dtype)
         self.nnbrs = float(p["Nnbrs"])
-        self.ebias = _t(p["Ebias"], dtype)
+        self.ebias = _td(p["Ebias"], dtype)
         self.out_norm = float(p.get("out_norm", 1.0))
         self.compressed = bool(p.get("is_compressed", False))
         self.emb = []
         for k in range(self.nt * self.nt):
             net = v["embedding_net_%d" % k]
-            self.emb.append([(_t(net["Dense_%d" % i]["kernel"], dtype), _t(net["Dense_%d" % i]["bias"], dtype))
+            self.emb.append([(_td(net["Dense_%d" % i]["kernel"], dtype), _td(net["Dense_%d" % i]["bias"], dtype))
                              for i in range(len(self.ew))])
-        self.tbias = _t(v["Tbias"], dtype)
+        self.tbias = _td(v["Tbias"], dtype)
         self.fit = []
         for t in range(self.nt):
             net = v["fitting_net_%d" % t]
@@ -87,15 +92,15 @@ class OracleModel:
             for i in range(len(self.fw) + 1):
                 d = net["Dense_%d" % i]
                 dt = net.get("dt%d" % i) if 0 < i < len(self.fw) else None
-                layers.append((_t(d["kernel"], dtype), _t(d["bias"], dtype),
-                               None if dt is None else _t(dt, dtype)))
+                layers.append((_td(d["kernel"], dtype), _td(d["bias"], dtype),
+                               None if dt is None else _td(dt, dtype)))
             self.fit.append(layers)
         self.cvar = None
         if self.compressed:
             cv = variables["compress_var"]
             self.cvar = [(float(np.asarray(cv["embedding_net_%d" % k]["srmin"])),
                           float(np.asarray(cv["embedding_net_%d" % k]["srmax"])),
-                          _t(cv["embedding_net_%d" % k]["poly_coeff"], dtype))
+                          _td(cv["embedding_net_%d" % k]["poly_coeff"], dtype))
                          for k in range(self.nt * self.nt)]
 
     # -- embedding net (utils.py:100-151) ---------------------------------
@@ -146,11 +151,12 @@ class OracleModel:
         """
         dtype = self.dtype
         N = x_groups[0].shape[0]
-        ctype = torch.repeat_interleave(torch.arange(self.nt), torch.as_tensor(type_count))
+        dev = x_groups[0].device
+        ctype = torch.repeat_interleave(torch.arange(self.nt, device=dev), torch.as_tensor(type_count, device=dev))
         mean = self.mean[ctype]
         std = self.std[ctype]
         W = self.ew[-1]
-        T = torch.zeros((N, 10, W), dtype=dtype)
+        T = torch.zeros((N, 10, W), dtype=dtype, device=dev)
         for j in range(self.nt):
             x = x_groups[j]
             valid = valid_groups[j].to(dtype)
@@ -182,7 +188,7 @@ class OracleModel:
         G2 = tensor_3to6(T3[:, :, A:2 * A], 1) + T6[:, :, A:2 * A]
         G = G + (G2[..., None] * T6[:, :, None, :]).sum(1)
         G = G.reshape(N, -1)
-        E = torch.zeros(N, dtype=dtype)
+        E = torch.zeros(N, dtype=dtype, device=dev)
         off = 0
         for i in range(self.nt):
             n_i = int(type_count[i])
@@ -210,13 +216,13 @@ def relative_coords_nlist(coord_sorted, box3, nbrs, sel, type_count):
     col = np.concatenate([[0], np.cumsum(sel)])
     xs, vs = [], []
     for j in range(len(sel)):
-        idx = torch.as_tensor(np.asarray(nbrs[:, col[j]:col[j + 1]], dtype=np.int64))
+        idx = torch.as_tensor(np.asarray(nbrs[:, col[j]:col[j + 1]], dtype=np.int64), device=coord_sorted.device)
         nj = int(type_count[j])
         valid = idx < nj
         cj = coord_sorted[offs[j]:offs[j + 1]]
         if nj == 0:
-            xs.append(torch.zeros((N, idx.shape[1], 3), dtype=coord_sorted.dtype))
-            vs.append(torch.zeros((N, idx.shape[1]), dtype=torch.bool))
+            xs.append(torch.zeros((N, idx.shape[1], 3), dtype=coord_sorted.dtype, device=coord_sorted.device))
+            vs.append(torch.zeros((N, idx.shape[1]), dtype=torch.bool, device=coord_sorted.device))
             continue
         g = cj[idx.clamp(max=nj - 1)]
         x = shift_ortho(g - coord_sorted[:, None, :], box3)
@@ -238,8 +244,8 @@ def relative_coords_lattice(coord_sorted, box3, type_count, rcut):
     for orthorhombic boxes: every atom of type j and every lattice image within
     reach is a slot; images beyond rcut carry s = 0."""
     offs = np.concatenate([[0], np.cumsum(type_count)])
-    imgs = torch.as_tensor(lattice_images(box3.detach().numpy() if torch.is_tensor(box3) else box3, rcut),
-                           dtype=coord_sorted.dtype) * box3
+    imgs = torch.as_tensor(lattice_images(box3.detach().cpu().numpy() if torch.is_tensor(box3) else box3, rcut),
+                           dtype=coord_sorted.dtype, device=coord_sorted.device) * box3
     xs, vs = [], []
     N = coord_sorted.shape[0]
     for j in range(len(type_count)):
@@ -247,7 +253,7 @@ def relative_coords_lattice(coord_sorted, box3, type_count, rcut):
         x = shift_ortho(cj[None, :, :] - coord_sorted[:, None, :], box3)    # (N, M, 3)
         x = (x[:, :, None, :] - imgs[None, None]).reshape(N, -1, 3)
         xs.append(x)
-        vs.append(torch.ones(x.shape[:2], dtype=torch.bool))
+        vs.append(torch.ones(x.shape[:2], dtype=torch.bool, device=x.device))
     return xs, vs
 
 
@@ -259,10 +265,11 @@ def energy_force(model: OracleModel, coord, box3, type_idx, nbrs=None, sel=None,
     W_ab = -sum_pairs x_a dE/dx_b (its trace is -dU/deps under a uniform
     scaling of coordinates and box, md_utils.py:139-159)."""
     dtype = model.dtype
-    coord = torch.as_tensor(np.asarray(coord), dtype=dtype).clone().requires_grad_(True)
-    box3 = torch.as_tensor(np.asarray(box3), dtype=dtype)
+    dev = model.device
+    coord = torch.as_tensor(np.asarray(coord), dtype=dtype, device=dev).clone().requires_grad_(True)
+    box3 = torch.as_tensor(np.asarray(box3), dtype=dtype, device=dev)
     perm, count = sort_by_type(type_idx, model.nt)
-    cs = coord[torch.as_tensor(perm)]
+    cs = coord[torch.as_tensor(perm, device=dev)]
     if nbrs is not None:
         xs, vs = relative_coords_nlist(cs, box3, nbrs, sel, count)
     else:
@@ -276,20 +283,21 @@ def energy_force(model: OracleModel, coord, box3, type_idx, nbrs=None, sel=None,
     F = -torch.autograd.grad(xs, coord, grad_outputs=list(gx))[0]
     Wv = None
     if virial:
-        Wv = torch.zeros((3, 3), dtype=dtype)
+        Wv = torch.zeros((3, 3), dtype=dtype, device=dev)
         for x, g, v in zip(xs, gx, vs):
             Wv = Wv - torch.einsum("nsa,nsb->ab", x.detach() * v[..., None], g)
     E_user = torch.empty_like(E_atom)
-    E_user[torch.as_tensor(perm)] = E_atom.detach()
-    return dict(energy=float(E.detach()), atom_energy=E_user.numpy(),
-                force=F.detach().numpy(), virial=None if Wv is None else Wv.numpy())
+    E_user[torch.as_tensor(perm, device=dev)] = E_atom.detach()
+    return dict(energy=float(E.detach()), atom_energy=E_user.cpu().numpy(),
+                force=F.detach().cpu().numpy(), virial=None if Wv is None else Wv.cpu().numpy())
 
 
 def energy_only(model: OracleModel, coord, box3, type_idx, nbrs=None, sel=None):
-    coord = torch.as_tensor(np.asarray(coord), dtype=model.dtype)
-    box3 = torch.as_tensor(np.asarray(box3), dtype=model.dtype)
+    dev = model.device
+    coord = torch.as_tensor(np.asarray(coord), dtype=model.dtype, device=dev)
+    box3 = torch.as_tensor(np.asarray(box3), dtype=model.dtype, device=dev)
     perm, count = sort_by_type(type_idx, model.nt)
-    cs = coord[torch.as_tensor(perm)]
+    cs = coord[torch.as_tensor(perm, device=dev)]
     if nbrs is not None:
         xs, vs = relative_coords_nlist(cs, box3, nbrs, sel, count)
     else:

@@ -1,0 +1,55 @@
+"""Host-side logic of the reference-facing API that needs no GPU: the box
+shapes evaluate() accepts and its error message (deepmd_jax/train.py:718-740),
+the neighbour capacity rule (deepmd_jax/md_utils.py:394-403) and the
+conversion between the packed list and the reference's nested nbrs_nm."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import nlist as onl
+
+
+def test_box_shapes_of_evaluate():
+    from deepmd_jax_b200.train import normalize_boxes
+    F, N = 2, 6
+    coord = np.zeros((F, N, 3))
+    t = np.zeros(N, dtype=int)
+    want = np.stack([np.diag([5.0, 5.0, 5.0])] * F)
+    for b in (np.full(F, 5.0), np.full((F, 1), 5.0), np.full((F, 3), 5.0), want.reshape(F, 9), want):
+        assert np.array_equal(normalize_boxes(coord, b, t), want)
+    for bad_coord, bad_box, bad_t in ((coord[0], np.full(F, 5.0), t), (coord, np.full(F + 1, 5.0), t),
+                                      (coord, np.full(F, 5.0), t[:-1]), (coord, np.zeros((F, 3, 2)), t)):
+        with pytest.raises(ValueError, match="Input shapes are incorrect"):
+            normalize_boxes(bad_coord, bad_box, bad_t)
+
+
+def test_non_orthorhombic_box_is_rejected():
+    from deepmd_jax_b200.dpmodel import box_diagonal
+    assert np.array_equal(box_diagonal(4.0), [4.0, 4.0, 4.0])
+    assert np.array_equal(box_diagonal(np.diag([1.0, 2.0, 3.0])), [1.0, 2.0, 3.0])
+    tri = np.diag([5.0, 5.0, 5.0])
+    tri[0, 1] = 1.0
+    with pytest.raises(NotImplementedError):
+        box_diagonal(tri)
+
+
+@pytest.mark.parametrize("ratio", [1.2, 1.25, 1.5])
+def test_capacity_rule_matches_oracle(ratio):
+    from deepmd_jax_b200.md_utils import knbr_from_counts
+    from deepmd_jax_b200.md import sel_from_counts
+    for counts in ([0, 5], [19, 20], [46, 92], [1, 300]):
+        want = [int(k) for k in onl.knbr_rule(counts, ratio)]
+        assert knbr_from_counts(counts, ratio) == want
+        assert sel_from_counts(counts, ratio) == [max(k - 1, 1) for k in want]
+
+
+def test_nested_and_packed_lists_round_trip():
+    from deepmd_jax_b200.md_utils import from_nbrs_nm, to_nbrs_nm
+    cnt, sel = [3, 5], [2, 4]
+    rng = np.random.default_rng(0)
+    packed = torch.tensor(rng.integers(0, 9, size=(8, 6)), dtype=torch.int32)
+    nested = to_nbrs_nm(packed, cnt, sel)
+    assert [tuple(a.shape) for a in nested[0]] == [(3, 2), (3, 4)]
+    assert [tuple(a.shape) for a in nested[1]] == [(5, 2), (5, 4)]
+    back, sel2 = from_nbrs_nm([[a.numpy() for a in row] for row in nested], device="cpu")
+    assert sel2 == sel and torch.equal(back, packed)
