@@ -168,6 +168,7 @@ def reference_arm(args):
     dt = time.perf_counter() - t0
     N = len(r)
     val = N * steps / dt
+    install = _reference_install_state()
     return {"metric": METRIC, "value": val, "unit": "atom-steps/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -177,7 +178,21 @@ def reference_arm(args):
                              "sample": "%d velocity-Verlet steps of the 12,288-atom water box with the FP32 "
                                        "torch restatement of the reference model (the reference is JAX and "
                                        "cannot be installed here)" % steps},
-            "e2e": {"value": val, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": val, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_install": install}
+
+
+def _reference_install_state():
+    """Why the reference itself is not the timed arm: import it from
+    baseline/_ref (installed there with --no-deps) and report the outcome."""
+    path = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(path):
+        return "baseline/_ref absent (pip install fails: dependency jax-md is a git URL, no network)"
+    code = "import sys; sys.path.insert(0, %r); import deepmd_jax" % path
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    if r.returncode == 0:
+        return "deepmd_jax imports from baseline/_ref (jax present); the port is still timed"
+    return "baseline/_ref holds deepmd_jax 0.2.1 (--no-deps); import fails: " + (r.stderr.strip().splitlines() or ["?"])[-1]
 
 
 def cpu_baseline_sample():
