@@ -138,7 +138,24 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   }
   const int ew_in[3] = {1, M.E0, M.E1}, ew_out[3] = {M.E0, M.E1, M.E2};
   int rc = DPB_OK;
-  for (int k = 0; k < nt * nt && rc == DPB_OK; ++k)
+  const bool have_mlp = d->embed_kernel != nullptr && d->embed_bias != nullptr;
+  if (d->n_grids < 0 || (d->n_grids == 0 && !have_mlp) ||
+      (d->n_grids > 0 && (!d->cmp_coeff || !d->cmp_srmin || !d->cmp_srmax))) {
+    delete m;
+    return DPB_ERR_INVALID_ARG;
+  }
+  // compressed tables: the reference's lookup runs in float32 (srmin, srmax
+  // and delta = (srmax - srmin) / Ngrids as float32 arrays, utils.py:131-134)
+  M.ngrids = d->n_grids;
+  for (int k = 0; k < nt * nt && rc == DPB_OK && M.ngrids > 0; ++k) {
+    if (!d->cmp_coeff[k]) rc = DPB_ERR_INVALID_ARG;
+    if (rc == DPB_OK) rc = upload(m, d->cmp_coeff[k], (size_t)M.ngrids * 6 * M.E2, &M.cmp_coeff[k]);
+    const float lo = (float)d->cmp_srmin[k], hi = (float)d->cmp_srmax[k];
+    volatile float span = hi - lo;  // float32 rounding, as in the reference
+    M.cmp_srmin[k] = lo;
+    M.cmp_delta[k] = span / (float)M.ngrids;
+  }
+  for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp; ++k)
     for (int l = 0; l < 3 && rc == DPB_OK; ++l) {
       rc = upload(m, d->embed_kernel[k * 3 + l], (size_t)ew_in[l] * ew_out[l], &M.ew[k][l]);
       if (rc == DPB_OK) rc = upload(m, d->embed_bias[k * 3 + l], (size_t)ew_out[l], &M.eb[k][l]);
@@ -153,7 +170,7 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
     const int W1B = N1 * K1 * 2, W2B = N2 * K2 * 2;
     M.net_img_bytes = W1B + W2B;
     M.net_small_floats = ((2 * M.E0 + M.E1 + M.E2) + 3) / 4 * 4;
-    for (int k = 0; k < nt * nt && rc == DPB_OK; ++k) {
+    for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp; ++k) {
       std::vector<uint8_t> img(M.net_img_bytes, 0);
       const float *W1 = d->embed_kernel[k * 3 + 1], *W2 = d->embed_kernel[k * 3 + 2];
       for (int n = 0; n < N1; ++n)

@@ -40,6 +40,11 @@ struct DevModel {
   const char *net_img[kMaxTypes * kMaxTypes];
   const float *net_small[kMaxTypes * kMaxTypes];
   int net_img_bytes, net_small_floats;
+  // compressed embedding (ngrids > 0): per net, poly_coeff (ngrids, 6, E2)
+  // and the float32 srmin / interval width of the reference's table lookup
+  int ngrids;
+  const float *cmp_coeff[kMaxTypes * kMaxTypes];
+  float cmp_srmin[kMaxTypes * kMaxTypes], cmp_delta[kMaxTypes * kMaxTypes];
 };
 
 // Frame/type geometry of one evaluation call.

@@ -127,12 +127,64 @@ __device__ __forceinline__ void embed_rows_fwd(const float *__restrict__ W, int 
   }
 }
 
+// ---------------------------------------------------------------- compressed embedding
+// The table lookup of the compressed embedding net (deepmd_jax/utils.py:126-151):
+// x = s~ - srmin; idx = trunc(x / delta); x0 = x - idx * delta; the gather
+// clamps idx into [0, Ngrids) while x0 keeps the unclamped idx; h[w] =
+// sum_i c[idx][i][w] x0^(5-i), evaluated here by Horner's rule.
+__device__ __forceinline__ void cmp_locate(float st, float srmin, float delta, int ng, int &idx, float &x0) {
+  const float x = __fsub_rn(st, srmin);
+  const int k = (int)__fdiv_rn(x, delta);  // truncation toward zero, like astype(int)
+  x0 = __fsub_rn(x, __fmul_rn((float)k, delta));
+  idx = k < 0 ? 0 : (k >= ng ? ng - 1 : k);
+}
+
+// One round of up to 32 compacted rows, column-parallel: lane owns columns
+// q*32 + lane; the rows' (idx, x0) and env rows are read from the row buffer
+// (st slot overwritten by x0, slot 11 by idx) and each table row is read with
+// coalesced loads.  T += R~^T h accumulates into the warp's shared T.
+template <int E2>
+__device__ __forceinline__ void embed_rows_fwd_cmp(const float *__restrict__ coeff, float srmin, float delta,
+                                                   int ng, int n, float *__restrict__ rowbuf,
+                                                   float *__restrict__ Ts, int lane) {
+  if (lane < n) {
+    int idx;
+    float x0;
+    cmp_locate(rowbuf[lane * 12], srmin, delta, ng, idx, x0);
+    rowbuf[lane * 12] = x0;
+    rowbuf[lane * 12 + 11] = __int_as_float(idx);
+  }
+  __syncwarp();
+#pragma unroll 1
+  for (int q = 0; q < (E2 + 31) / 32; ++q) {
+    const int col = q * 32 + lane;
+    if (col < E2) {
+      float Tq[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) Tq[c] = 0.f;
+      for (int r = 0; r < n; ++r) {
+        const float *rb = rowbuf + r * 12;
+        const float x0 = rb[0];
+        const float *cr = coeff + (size_t)__float_as_int(rb[11]) * 6 * E2 + col;
+        float h = __ldg(cr);
+#pragma unroll
+        for (int i = 1; i < 6; ++i) h = fmaf(h, x0, __ldg(cr + i * E2));
+#pragma unroll
+        for (int c = 0; c < 10; ++c) Tq[c] = fmaf(rb[1 + c], h, Tq[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 10; ++c) Ts[c * E2 + col] += Tq[c];
+    }
+  }
+  __syncwarp();
+}
+
 template <int E0, int E1, int E2>
 __host__ __device__ constexpr int embed_fwd_warp_floats() {
   return 64 * 12 + (32 * 33 > E0 * 32 ? 32 * 33 : E0 * 32) + E1 * 32 + 10 * E2;
 }
 
-template <int E0, int E1, int E2>
+template <int E0, int E1, int E2, bool CMP>
 __global__ void __launch_bounds__(256) k_embed_fwd(DevModel M, SysDesc D, int ti, const float *__restrict__ pos,
                                                    const int32_t *__restrict__ perm, const float *__restrict__ box,
                                                    const int32_t *__restrict__ nbrs, float *__restrict__ Tout,
@@ -141,12 +193,12 @@ __global__ void __launch_bounds__(256) k_embed_fwd(DevModel M, SysDesc D, int ti
   extern __shared__ float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   float *wsm = smem;
-  float *rowbuf = smem + M.ntypes * ED::NW + warp * embed_fwd_warp_floats<E0, E1, E2>();
+  float *rowbuf = smem + (CMP ? 0 : M.ntypes * ED::NW) + warp * embed_fwd_warp_floats<E0, E1, E2>();
   float *h2s = rowbuf + 64 * 12;  // aliases h0s
   float *h0s = h2s;
   float *h1s = h2s + (32 * 33 > E0 * 32 ? 32 * 33 : E0 * 32);
   float *Ts = h1s + E1 * 32;
-  load_nets<E0, E1, E2>(M, ti, wsm);
+  if (!CMP) load_nets<E0, E1, E2>(M, ti, wsm);
   __syncthreads();
   const int f = blockIdx.y;
   const int a = blockIdx.x * wpb + warp;
@@ -200,7 +252,11 @@ __global__ void __launch_bounds__(256) k_embed_fwd(DevModel M, SysDesc D, int ti
       nbuf += __popc(m);
       __syncwarp();
       if (nbuf >= 32) {
-        embed_rows_fwd<E0, E1, E2>(W, 32, rowbuf, h0s, h1s, h2s, Ts, lane);
+        if constexpr (CMP)
+          embed_rows_fwd_cmp<E2>(M.cmp_coeff[ti * M.ntypes + tj], M.cmp_srmin[ti * M.ntypes + tj],
+                                 M.cmp_delta[ti * M.ntypes + tj], M.ngrids, 32, rowbuf, Ts, lane);
+        else
+          embed_rows_fwd<E0, E1, E2>(W, 32, rowbuf, h0s, h1s, h2s, Ts, lane);
         const int rem = nbuf - 32;
         if (lane < rem)
           for (int c = 0; c < 12; ++c) rowbuf[lane * 12 + c] = rowbuf[(32 + lane) * 12 + c];
@@ -208,7 +264,13 @@ __global__ void __launch_bounds__(256) k_embed_fwd(DevModel M, SysDesc D, int ti
         nbuf = rem;
       }
     }
-    if (nbuf > 0) embed_rows_fwd<E0, E1, E2>(W, nbuf, rowbuf, h0s, h1s, h2s, Ts, lane);
+    if (nbuf > 0) {
+      if constexpr (CMP)
+        embed_rows_fwd_cmp<E2>(M.cmp_coeff[ti * M.ntypes + tj], M.cmp_srmin[ti * M.ntypes + tj],
+                               M.cmp_delta[ti * M.ntypes + tj], M.ngrids, nbuf, rowbuf, Ts, lane);
+      else
+        embed_rows_fwd<E0, E1, E2>(W, nbuf, rowbuf, h0s, h1s, h2s, Ts, lane);
+    }
     __syncwarp();
   }
 
@@ -352,7 +414,81 @@ __device__ __forceinline__ void embed_rows_bwd(const float *__restrict__ W, int 
   }
 }
 
-template <int E0, int E1, int E2>
+// Adjoint of one round of rows of a compressed net (row = lane): h and
+// dh/ds~ = dh/dx0 from the row's table entry (float4 loads along w), u =
+// dT.h, v = dT.dh, then the same env-row adjoint as the MLP path.
+template <int E2>
+__device__ __forceinline__ void embed_rows_bwd_cmp(const float *__restrict__ coeff, float srmin, float delta,
+                                                   int ng, int n, const float *__restrict__ rowbuf,
+                                                   const float *__restrict__ dT, float inv_std, float mean,
+                                                   int lane, float &fi0, float &fi1, float &fi2, float (&vir)[9],
+                                                   float4 *__restrict__ F4, size_t frame_base) {
+  static_assert(E2 % 4 == 0, "table width");
+  const bool act = lane < n;
+  RowGeom gm;
+  int jj = 0;
+  if (act) {
+    const float *rb = rowbuf + lane * 8;
+    gm.x[0] = rb[0]; gm.x[1] = rb[1]; gm.x[2] = rb[2];
+    gm.r = rb[3]; gm.s = rb[4]; gm.dsdr = rb[5];
+    jj = __float_as_int(rb[6]);
+  } else {
+    gm.x[0] = gm.x[1] = gm.x[2] = 0.f; gm.r = 1.f; gm.s = 0.f; gm.dsdr = 0.f;
+  }
+  const float sn = gm.s * inv_std, st = (gm.s - mean) * inv_std;
+  int idx;
+  float x0;
+  cmp_locate(st, srmin, delta, ng, idx, x0);
+  float u[10], v[10];
+#pragma unroll
+  for (int c = 0; c < 10; ++c) u[c] = v[c] = 0.f;
+  const float4 *cr = reinterpret_cast<const float4 *>(coeff + (size_t)idx * 6 * E2);
+#pragma unroll 1
+  for (int w4 = 0; w4 < E2 / 4; ++w4) {
+    float4 c[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) c[i] = __ldg(cr + i * (E2 / 4) + w4);
+    const float cc[6][4] = {{c[0].x, c[0].y, c[0].z, c[0].w}, {c[1].x, c[1].y, c[1].z, c[1].w},
+                            {c[2].x, c[2].y, c[2].z, c[2].w}, {c[3].x, c[3].y, c[3].z, c[3].w},
+                            {c[4].x, c[4].y, c[4].z, c[4].w}, {c[5].x, c[5].y, c[5].z, c[5].w}};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float h = cc[0][e], dh = 5.f * cc[0][e];
+#pragma unroll
+      for (int i = 1; i < 5; ++i) {
+        h = fmaf(h, x0, cc[i][e]);
+        dh = fmaf(dh, x0, (float)(5 - i) * cc[i][e]);
+      }
+      h = fmaf(h, x0, cc[5][e]);
+      const int col = w4 * 4 + e;
+#pragma unroll
+      for (int ch = 0; ch < 10; ++ch) {
+        const float dtc = dT[ch * E2 + col];
+        u[ch] = fmaf(dtc, h, u[ch]);
+        v[ch] = fmaf(dtc, dh, v[ch]);
+      }
+    }
+  }
+  const float inv_rp = 1.f / (gm.r + 1e-16f);
+  const float xh[3] = {gm.x[0] * inv_rp, gm.x[1] * inv_rp, gm.x[2] * inv_rp};
+  float R[10];
+  env_row(sn, xh, R);
+  float gst = 0.f;
+#pragma unroll
+  for (int c = 0; c < 10; ++c) gst = fmaf(R[c], v[c], gst);
+  float gx[3];
+  row_adjoint(gm, inv_std, u, gst, gx);
+  if (act) {
+    atomicAdd(&F4[frame_base + jj], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
+    fi0 += gx[0]; fi1 += gx[1]; fi2 += gx[2];
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+      for (int qq = 0; qq < 3; ++qq) vir[p * 3 + qq] -= gm.x[p] * gx[qq];
+  }
+}
+
+template <int E0, int E1, int E2, bool CMP>
 __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti, const float *__restrict__ pos,
                                                    const int32_t *__restrict__ perm, const float *__restrict__ box,
                                                    const int32_t *__restrict__ nbrs, const float *__restrict__ Tin,
@@ -365,13 +501,13 @@ __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti
   float *wsm = smem;
   const int r1 = (A * E2 > 64 * 8 + 2 * E1 * 32) ? A * E2 : 64 * 8 + 2 * E1 * 32;
   const int per_warp = r1 + 10 * E2 + 20 * A;
-  float *bufA = smem + M.ntypes * ED::NW + warp * per_warp;  // dG, later rows + h1/dh1 staging
+  float *bufA = smem + (CMP ? 0 : M.ntypes * ED::NW) + warp * per_warp;  // dG, later rows + h1/dh1 staging
   float *bufB = bufA + r1;                                   // X, later dT
   float *Qs = bufB + 10 * E2;                                // 10 x A
   float *dQs = Qs + 10 * A;                                  // 10 x A
   __shared__ double vsm[9];
   if (threadIdx.x < 9) vsm[threadIdx.x] = 0.0;
-  load_nets<E0, E1, E2>(M, ti, wsm);
+  if (!CMP) load_nets<E0, E1, E2>(M, ti, wsm);
   __syncthreads();
   const int f = blockIdx.y;
   const int a = blockIdx.x * wpb + warp;
@@ -487,8 +623,13 @@ __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti
         nbuf += __popc(m);
         __syncwarp();
         if (nbuf >= 32) {
-          embed_rows_bwd<E0, E1, E2>(W, 32, rowbuf, bufB, h1s, d1s, inv_std, mean, lane, fi0, fi1, fi2,
-                                     vir, F4, frame_base);
+          if constexpr (CMP)
+            embed_rows_bwd_cmp<E2>(M.cmp_coeff[ti * M.ntypes + tj], M.cmp_srmin[ti * M.ntypes + tj],
+                                   M.cmp_delta[ti * M.ntypes + tj], M.ngrids, 32, rowbuf, bufB, inv_std, mean,
+                                   lane, fi0, fi1, fi2, vir, F4, frame_base);
+          else
+            embed_rows_bwd<E0, E1, E2>(W, 32, rowbuf, bufB, h1s, d1s, inv_std, mean, lane, fi0, fi1, fi2,
+                                       vir, F4, frame_base);
           const int rem = nbuf - 32;
           if (lane < rem)
             for (int c = 0; c < 8; ++c) rowbuf[lane * 8 + c] = rowbuf[(32 + lane) * 8 + c];
@@ -496,9 +637,15 @@ __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti
           nbuf = rem;
         }
       }
-      if (nbuf > 0)
-        embed_rows_bwd<E0, E1, E2>(W, nbuf, rowbuf, bufB, h1s, d1s, inv_std, mean, lane, fi0, fi1, fi2,
-                                   vir, F4, frame_base);
+      if (nbuf > 0) {
+        if constexpr (CMP)
+          embed_rows_bwd_cmp<E2>(M.cmp_coeff[ti * M.ntypes + tj], M.cmp_srmin[ti * M.ntypes + tj],
+                                 M.cmp_delta[ti * M.ntypes + tj], M.ngrids, nbuf, rowbuf, bufB, inv_std, mean,
+                                 lane, fi0, fi1, fi2, vir, F4, frame_base);
+        else
+          embed_rows_bwd<E0, E1, E2>(W, nbuf, rowbuf, bufB, h1s, d1s, inv_std, mean, lane, fi0, fi1, fi2,
+                                     vir, F4, frame_base);
+      }
       __syncwarp();
     }
     fi0 = warp_sum(fi0); fi1 = warp_sum(fi1); fi2 = warp_sum(fi2);
@@ -702,10 +849,16 @@ int launch_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float *p
                      const float *box, const int32_t *nbrs, float *T, float *G, cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
-  size_t smem = embed_fwd_smem<E0, E1, E2>(M.ntypes);
-  cudaFuncSetAttribute(k_embed_fwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((cnt + 7) / 8, D.F);
-  k_embed_fwd<E0, E1, E2><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G);
+  if (M.ngrids > 0) {
+    size_t smem = embed_fwd_smem<E0, E1, E2>(0);
+    cudaFuncSetAttribute(k_embed_fwd<E0, E1, E2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_embed_fwd<E0, E1, E2, true><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G);
+  } else {
+    size_t smem = embed_fwd_smem<E0, E1, E2>(M.ntypes);
+    cudaFuncSetAttribute(k_embed_fwd<E0, E1, E2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_embed_fwd<E0, E1, E2, false><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G);
+  }
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
@@ -717,10 +870,16 @@ int launch_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float *p
                      double *virial, cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
-  size_t smem = embed_bwd_smem<E0, E1, E2>(M.ntypes, M.A);
-  cudaFuncSetAttribute(k_embed_bwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((cnt + 7) / 8, D.F);
-  k_embed_bwd<E0, E1, E2><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial);
+  if (M.ngrids > 0) {
+    size_t smem = embed_bwd_smem<E0, E1, E2>(0, M.A);
+    cudaFuncSetAttribute(k_embed_bwd<E0, E1, E2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_embed_bwd<E0, E1, E2, true><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial);
+  } else {
+    size_t smem = embed_bwd_smem<E0, E1, E2>(M.ntypes, M.A);
+    cudaFuncSetAttribute(k_embed_bwd<E0, E1, E2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_embed_bwd<E0, E1, E2, false><<<grid, 256, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial);
+  }
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;

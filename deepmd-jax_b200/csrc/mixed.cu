@@ -1198,6 +1198,7 @@ size_t mixed_workspace_per_atom(const DevModel &M) {
 
 int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                       const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, int *err, cudaStream_t st) {
+  if (M.ngrids > 0) return DPB_ERR_UNSUPPORTED;  // compressed nets: the FP32 table kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, Gb, err, st)
@@ -1211,6 +1212,58 @@ int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, con
 __global__ void k_bf16_to_f32(const __nv_bfloat16 *__restrict__ a, float *__restrict__ b, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = __bfloat162float(a[i]);
+}
+
+__global__ void k_f32_to_bf16(const float4 *__restrict__ a, uint2 *__restrict__ b, size_t n4) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n4) {
+    const float4 v = a[i];
+    b[i] = make_uint2(tc::pack_bf16(v.x, v.y), tc::pack_bf16(v.z, v.w));
+  }
+}
+
+template <int E0, int E1, int E2>
+int launch_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+                     const float *box, const int32_t *nbrs, float *T, float *G, cudaStream_t st);
+template <int E0, int E1, int E2>
+int launch_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+                     const float *box, const int32_t *nbrs, const float *T, const float *dG, float4 *F4,
+                     double *virial, cudaStream_t st);
+
+// Compressed embedding nets in the mixed form: the table lookup has no GEMM,
+// so the FP32 table kernels produce T and G (FP32) and take the adjoint; the
+// fitting chain runs on the tensor cores from a BF16 copy of G.
+static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
+                                 const float *box, const int32_t *nbrs, double *energy, float *Eatom, float4 *F4,
+                                 double *virial, float *T, __nv_bfloat16 *Gb, float *dG, float *scratch, int *err,
+                                 cudaStream_t st) {
+  const size_t NF = (size_t)D.N * D.F;
+  const size_t NG = NF * M.A * M.E2;  // a multiple of 8 (mixed_supported)
+  int rc;
+  prof_begin(PROF_EMBED_FWD, st);
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    rc = (M.E2 == 100) ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, st)
+                       : launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, dG, st);
+    if (rc) return rc;
+  }
+  k_f32_to_bf16<<<(unsigned)((NG / 4 + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(dG),
+                                                                   reinterpret_cast<uint2 *>(Gb), NG / 4);
+  count_launch();
+  DPB_LAUNCH_CHECK();
+  prof_end(PROF_EMBED_FWD, st);
+  prof_begin(PROF_MIXED_FIT, st);
+  rc = (M.FW[0] == 240) ? launch_mix_fit<240>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
+                        : launch_mix_fit<128>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+  prof_end(PROF_MIXED_FIT, st);
+  if (rc) return rc;
+  prof_begin(PROF_EMBED_BWD, st);
+  for (int ti = 0; ti < M.ntypes; ++ti) {
+    rc = (M.E2 == 100) ? launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st)
+                       : launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st);
+    if (rc) return rc;
+  }
+  prof_end(PROF_EMBED_BWD, st);
+  return DPB_OK;
 }
 
 // Descriptor stage alone (diagnostics): T and G as FP32; the BF16 G of the
@@ -1241,6 +1294,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   __nv_bfloat16 *dTb = (__nv_bfloat16 *)w; w += al256(NF * 10 * N2 * 2);
   float *scratch = (float *)w;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+  if (M.ngrids > 0)
+    return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
   int rc = mixed_descriptors(M, D, pos, perm, box, nbrs, T, Gb, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);

@@ -51,6 +51,10 @@ class ModelDesc(ctypes.Structure):
         ("fit_kernel", ctypes.POINTER(ctypes.c_void_p)),
         ("fit_bias", ctypes.POINTER(ctypes.c_void_p)),
         ("fit_dt", ctypes.POINTER(ctypes.c_void_p)),
+        ("n_grids", ctypes.c_int),
+        ("cmp_coeff", ctypes.POINTER(ctypes.c_void_p)),
+        ("cmp_srmin", ctypes.POINTER(ctypes.c_double)),
+        ("cmp_srmax", ctypes.POINTER(ctypes.c_double)),
     ]
 
 

@@ -54,8 +54,9 @@ class DeviceModel:
             raise NotImplementedError("only se_a energy models (no message passing / atomic / dplr)")
         if not p.get("use_2nd", True):
             raise NotImplementedError("use_2nd=False models are not supported")
-        if p.get("is_compressed", False):
-            raise NotImplementedError("compressed models: pass the uncompressed variables['params']")
+        compressed = bool(p.get("is_compressed", False))
+        if compressed and "compress_var" not in variables:
+            raise ValueError("params['is_compressed'] is set but variables has no 'compress_var'")
         self.params = p
         self.ntypes = int(p["ntypes"])
         self.rcut = float(p["rcut"])
@@ -113,6 +114,27 @@ class DeviceModel:
         d.fit_kernel = ctypes.cast(self._arrs[2], ctypes.POINTER(VP))
         d.fit_bias = ctypes.cast(self._arrs[3], ctypes.POINTER(VP))
         d.fit_dt = ctypes.cast(self._arrs[4], ctypes.POINTER(VP))
+        if compressed:
+            # piecewise quintic tables of compress_model (deepmd_jax/utils.py:250-297)
+            cv = variables["compress_var"]
+            coeff, lo, hi = [], [], []
+            for k in range(nt * nt):
+                e = cv["embedding_net_%d" % k]
+                pc = np.asarray(e["poly_coeff"])
+                if pc.ndim != 3 or pc.shape[1] != 6 or pc.shape[2] != int(ew[-1]):
+                    raise ValueError("poly_coeff of embedding_net_%d has shape %s" % (k, pc.shape))
+                coeff.append(f32(pc))
+                lo.append(float(np.asarray(e["srmin"])))
+                hi.append(float(np.asarray(e["srmax"])))
+            ngrids = {int(np.asarray(cv["embedding_net_%d" % k]["poly_coeff"]).shape[0]) for k in range(nt * nt)}
+            if len(ngrids) != 1:
+                raise NotImplementedError("embedding tables with different grid counts")
+            d.n_grids = ngrids.pop()
+            self._arrs.append((VP * len(coeff))(*coeff))
+            d.cmp_coeff = ctypes.cast(self._arrs[-1], ctypes.POINTER(VP))
+            d.cmp_srmin = f64(lo)
+            d.cmp_srmax = f64(hi)
+        self.compressed = compressed
         h = ctypes.c_void_p()
         _lib.check(self.lib.dpb_model_create(ctypes.byref(d), ctypes.byref(h)), "dpb_model_create")
         self.handle = h

@@ -87,6 +87,15 @@ typedef struct {
   const float *const *fit_kernel;   /* [ntypes*(n_fit+1)] */
   const float *const *fit_bias;     /* same */
   const float *const *fit_dt;       /* [ntypes*n_fit], NULL where the layer has no dt */
+  /* Compressed embedding (deepmd_jax/utils.py:126-151, tables made by
+   * compress_model, utils.py:250-297).  n_grids > 0 replaces every embedding
+   * net k by its piecewise quintic table: cmp_coeff[k] is poly_coeff
+   * (n_grids, 6, W) float32 row-major over [cmp_srmin[k], cmp_srmax[k]);
+   * embed_kernel / embed_bias may then be NULL.  n_grids = 0: uncompressed. */
+  int n_grids;
+  const float *const *cmp_coeff;    /* [ntypes*ntypes] or NULL */
+  const double *cmp_srmin;          /* [ntypes*ntypes] or NULL */
+  const double *cmp_srmax;          /* [ntypes*ntypes] or NULL */
 } dpb_model_desc;
 
 /* Upload the weights (FP32 and BF16 copies) to the current device.

@@ -71,6 +71,47 @@ def compressed_variant(params, variables, seed, ngrids=64):
     return params, variables
 
 
+def hermite_compressed(params, variables, ngrids=256, rmin=0.5):
+    """Attach compress_var tables built the way the reference's
+    compress_model builds them (deepmd_jax/utils.py:250-297): on each of
+    ``ngrids`` intervals of [srmin, srmax) = [(0 - mean)/std, (sr(rmin) -
+    mean)/std) of the centre type, the quintic that matches the embedding
+    net's value, first and second derivative at both ends (C2 piecewise
+    quintic), stored as poly_coeff (ngrids, 6, W) in powers x0^(5-i).
+    Values and derivatives come from the float64 oracle net and torch
+    autograd."""
+    import torch
+    from oracle import model as om
+    params = dict(params)
+    params["is_compressed"] = True
+    nt = int(params["ntypes"])
+    m = om.OracleModel(params | {"is_compressed": False}, variables, torch.float64)
+    cv = {}
+    for k in range(nt * nt):
+        i = k // nt
+        mean, std = float(params["sr_mean"][i]), float(params["sr_std"][i])
+        lo = (0.0 - mean) / std
+        hi = (float(om.sr(torch.tensor(rmin, dtype=torch.float64), float(params["rcut"]))) - mean) / std
+        x = torch.linspace(lo, hi, ngrids + 1, dtype=torch.float64).requires_grad_(True)
+        f0 = m.embed(k, x)                                  # (ngrids+1, W)
+        W = f0.shape[1]
+        f1 = torch.stack([torch.autograd.grad(f0[:, w].sum(), x, create_graph=True)[0] for w in range(W)], 1)
+        f2 = torch.stack([torch.autograd.grad(f1[:, w].sum(), x, retain_graph=True)[0] for w in range(W)], 1)
+        f0, f1, f2 = f0.detach().numpy(), f1.detach().numpy(), f2.detach().numpy()
+        h = (hi - lo) / ngrids
+        # p(t) = a0 + a1 t + ... + a5 t^5 on [0, h] with end conditions
+        M3 = np.array([[h ** 3, h ** 4, h ** 5], [3 * h ** 2, 4 * h ** 3, 5 * h ** 4], [6 * h, 12 * h ** 2, 20 * h ** 3]])
+        a0, a1, a2 = f0[:-1], f1[:-1], 0.5 * f2[:-1]
+        rhs = np.stack([f0[1:] - (a0 + a1 * h + a2 * h ** 2), f1[1:] - (a1 + 2 * a2 * h), f2[1:] - 2 * a2], 1)
+        a345 = np.einsum("ij,njw->niw", np.linalg.inv(M3), rhs)     # (ngrids, 3, W)
+        coeff = np.stack([a345[:, 2], a345[:, 1], a345[:, 0], a2, a1, a0], 1)  # x0^5 ... x0^0
+        cv["embedding_net_%d" % k] = {"srmin": np.float32(lo), "srmax": np.float32(hi),
+                                      "poly_coeff": coeff.astype(np.float32)}
+    variables = dict(variables)
+    variables["compress_var"] = cv
+    return params, variables
+
+
 def ref_energy_force(ref, params, variables, coord, box3, type_idx, nbrs_nm=None):
     dpmodel = ref["dpmodel"]
     data = ref["data"]

@@ -161,3 +161,19 @@ def test_adjoint_matches_central_differences():
     e = EnergyFunction.apply(x, model, v, box, typ)
     e.backward()
     assert np.allclose(-x.grad.numpy(), F0, rtol=0, atol=1e-6)
+
+
+def test_evaluate_compressed_model_pkl(tmp_path):
+    """A model.pkl carrying compress_var (the default output of the
+    reference's train(), deepmd_jax/train.py:31) evaluates through the
+    compressed tables: against the float64 oracle with the same tables."""
+    from deepmd_jax_b200.train import evaluate
+    from deepmd_jax_b200.utils import save_model
+    from make_golden import hermite_compressed
+    p, v = hermite_compressed(*MODELS["B"])
+    path = str(tmp_path / "model_cmp.pkl")
+    save_model(path, p, v)
+    pos, box, typ = G["A_pos"], G["A_box"], G["A_type"]
+    out = evaluate(path, pos[None], box[None], typ)
+    ref = om.energy_force(om.OracleModel(p, v, torch.float64), pos, box, typ, virial=False)
+    _close(out["energy"][0], out["force"][0], ref["energy"], ref["force"], len(typ))

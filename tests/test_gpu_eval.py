@@ -80,3 +80,50 @@ def test_nonfinite_sets_status_bit():
     pos[3, 0] = np.nan
     got = run_gpu(p, v, pos, G["A_box"], G["A_type"])
     assert got["status"] & 16
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_compressed_model_neighbour_list_path(precision):
+    """Compressed embedding tables (deepmd_jax/utils.py:126-151) on a 1,536-atom
+    box through the neighbour list, two frames; FP32 at the FP32 bars, mixed
+    (FP32 tables + BF16 fitting) at the mixed bars.  The tables are C2
+    piecewise quintics fitted to model B the way compress_model builds them;
+    the golden model C (random, discontinuous tables) pins only the float64
+    oracle, because a float32 lookup can land in the neighbouring interval
+    of a discontinuous table."""
+    from deepmd_jax_b200.systems import water_box
+    from make_golden import hermite_compressed
+    p, v = hermite_compressed(*MODELS["B"])
+    ws = [water_box(8, 24.83, seed=s) for s in (21, 22)]
+    pos = np.stack([w["position"] for w in ws])
+    got = run_gpu(p, v, pos, ws[0]["box"], ws[0]["type_idx"], precision=precision)
+    assert got["status"] == 0
+    m = om.OracleModel(p, v, torch.float64)
+    for f, w in enumerate(ws):
+        ref = om.energy_force(m, w["position"], w["box"], w["type_idx"], nbrs=got["nbrs"][f], sel=[46, 92])
+        one = dict(energy=got["energy"][f], force=got["force"][f], virial=got["virial"][f],
+                   atom_energy=got["atom_energy"][f])
+        if precision == "fp32":
+            check_close(one, ref, "cmp%d" % f)
+        else:
+            N = len(w["type_idx"])
+            rms_err = np.sqrt(((one["force"] - ref["force"]) ** 2).mean())
+            assert rms_err <= 5e-3 and rms_err <= 3e-2 * np.sqrt((ref["force"] ** 2).mean())
+            assert abs(one["energy"] - ref["energy"]) / N <= 2e-2 * np.abs(ref["atom_energy"]).mean() + 1e-6
+
+
+def test_compressed_tables_match_uncompressed_model():
+    """The compressed form of model B on the 192-atom box: FP32 kernels vs the
+    float64 oracle with the same tables, and vs the uncompressed float64
+    model (the compression error of 256 intervals is far below the bars)."""
+    from make_golden import hermite_compressed
+    pc, vc = hermite_compressed(*MODELS["B"])
+    pos, box, typ = G["A_pos"], G["A_box"], G["A_type"]
+    got = run_gpu(pc, vc, pos, box, typ)
+    assert got["status"] == 0
+    one = dict(energy=got["energy"][0], force=got["force"][0], virial=got["virial"][0],
+               atom_energy=got["atom_energy"][0])
+    check_close(one, om.energy_force(om.OracleModel(pc, vc, torch.float64), pos, box, typ), "cmp")
+    ref = om.energy_force(om.OracleModel(*MODELS["B"], torch.float64), pos, box, typ)
+    ref["energy"] = float(G["B_E"])
+    check_close(one, ref, "cmp-vs-uncompressed")

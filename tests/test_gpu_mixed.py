@@ -61,9 +61,14 @@ def test_mixed_descriptors_match_fp32(mk):
     assert np.abs(Gm - G32).max() <= 2e-2 * np.abs(G32).max()
 
 
-@pytest.mark.parametrize("key,sysk,mk", [("B", "A", "B"), ("D", "D", "B"), ("A", "A", "A")])
+@pytest.mark.parametrize("key,sysk,mk", [("B", "A", "B"), ("D", "D", "B"), ("A", "A", "A"), ("H", "A", "H")])
 def test_mixed_eval_vs_fp64(key, sysk, mk):
-    p, v = MODELS[mk]
+    """H: model B with compressed (C2 piecewise quintic) embedding tables."""
+    if mk == "H":
+        from make_golden import hermite_compressed
+        p, v = hermite_compressed(*MODELS["B"])
+    else:
+        p, v = MODELS[mk]
     pos, box, typ = G[sysk + "_pos"], G[sysk + "_box"], G[sysk + "_type"]
     got = run_gpu(p, v, pos, box, typ, precision="mixed")
     assert got["status"] == 0
