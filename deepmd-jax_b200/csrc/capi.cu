@@ -65,9 +65,9 @@ int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, cons
                      const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
 int launch_sgemm(int, int, int, const float *, int, RowMap, const float *, const Epi &, cudaStream_t);
 int launch_fit_energy(int, RowMap, int, const float *, const float *, const float *, const float *,
-                      const float *, float *, float *, double *, int, cudaStream_t);
+                      const float *, float *, float *, double *, int, const int32_t *, cudaStream_t);
 int launch_finalize(int, int, const float4 *, float *, const float *, const int32_t *, float *, double *, int,
-                    const float *, uint32_t *, cudaStream_t);
+                    const float *, const int32_t *, uint32_t *, cudaStream_t);
 // mixed path (mixed.cu)
 int mixed_supported(const DevModel &M);
 size_t mixed_workspace_per_atom(const DevModel &M);
@@ -244,13 +244,22 @@ static size_t fp32_ws_per_atom(const DevModel &M) {
   return (size_t)(10 * M.E2 + M.A * M.E2 + 2 * M.nfit * FW + 4 * FW + 1) * 4 + 16;
 }
 
+// Workspace of NF atoms with nE energy / virial rows.
+static size_t eval_ws_bytes(const DevModel &M, size_t NF, size_t nE) {
+  size_t a = al(NF * fp32_ws_per_atom(M)) + 16 * 256 + al(nE * 9 * 8);
+  size_t b = al(NF * mixed_workspace_per_atom(M)) + al(NF * 16) + al(NF * 4) + al(nE * 9 * 8) + 16 * 256;
+  return std::max(a, b);
+}
+
 extern "C" int dpb_eval_workspace_bytes(const dpb_model *m, int natoms, int nframes, size_t *bytes) {
   if (!m || !bytes || natoms <= 0 || nframes <= 0) return DPB_ERR_INVALID_ARG;
-  const size_t NF = (size_t)natoms * nframes;
-  size_t a = al(NF * fp32_ws_per_atom(m->dm)) + 16 * 256 + al((size_t)nframes * 9 * 8);
-  size_t b = al(NF * mixed_workspace_per_atom(m->dm)) + al(NF * 16) + al(NF * 4) + al((size_t)nframes * 9 * 8) +
-             16 * 256;
-  *bytes = std::max(a, b);
+  *bytes = eval_ws_bytes(m->dm, (size_t)natoms * nframes, (size_t)nframes);
+  return DPB_OK;
+}
+
+extern "C" int dpb_eval_packed_workspace_bytes(const dpb_model *m, int natoms, int nseg, size_t *bytes) {
+  if (!m || !bytes || natoms <= 0 || nseg <= 0) return DPB_ERR_INVALID_ARG;
+  *bytes = eval_ws_bytes(m->dm, (size_t)natoms, (size_t)nseg);
   return DPB_OK;
 }
 
@@ -258,6 +267,7 @@ static int fill_sys(const dpb_model *m, int natoms, int nframes, const int *type
                     SysDesc &D) {
   const int nt = m->dm.ntypes;
   D.N = natoms; D.F = nframes; D.ntypes = nt;
+  D.seg = nullptr;
   int off = 0, col = 0;
   for (int t = 0; t < nt; ++t) {
     if (type_count[t] < 0 || sel[t] < 0) return DPB_ERR_INVALID_ARG;
@@ -311,7 +321,7 @@ int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Ea
     }
     int cur = 0;
     rc = launch_fit_energy(Mrows, rm, FW, hb[L - 1], tb[L - 1], M.fw[ti][L], M.fb[ti][L], M.fdt[ti][L - 1], Eatom,
-                           gz[cur], energy, D.N, st);
+                           gz[cur], energy, D.N, D.seg, st);
     if (rc) return rc;
     for (int l = L - 1; l >= 1; --l) {
       Epi ep{};
@@ -375,29 +385,30 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
 int dpb::eval_impl(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,
                    int nframes, const int *type_count, const float *box, const int32_t *nbrs, const int *sel,
                    double *energy, float *atom_energy, float *force, double *virial, uint32_t *status,
-                   void *workspace, size_t ws_bytes, cudaStream_t st) {
+                   void *workspace, size_t ws_bytes, cudaStream_t st, const int32_t *seg, int nseg) {
   if (!m || !pos || !box || !nbrs || !energy || !force || !status || !type_count || !sel || natoms <= 0 ||
       nframes <= 0)
     return DPB_ERR_INVALID_ARG;
   if (precision != DPB_PREC_FP32 && precision != DPB_PREC_MIXED) return DPB_ERR_INVALID_ARG;
   if (natoms >= (1 << 24)) return DPB_ERR_UNSUPPORTED;
-  size_t need = 0;
-  dpb_eval_workspace_bytes(m, natoms, nframes, &need);
-  if (!workspace || ws_bytes < need) return DPB_ERR_WORKSPACE;
+  if (seg && (nframes != 1 || nseg <= 0)) return DPB_ERR_INVALID_ARG;
+  const size_t nE = seg ? (size_t)nseg : (size_t)nframes;
+  if (!workspace || ws_bytes < eval_ws_bytes(m->dm, (size_t)natoms * nframes, nE)) return DPB_ERR_WORKSPACE;
   SysDesc D;
   int rc = fill_sys(m, natoms, nframes, type_count, sel, D);
   if (rc) return rc;
+  D.seg = seg;
   const DevModel &M = m->dm;
   const size_t NF = (size_t)natoms * nframes;
   char *w = (char *)workspace;
   float4 *F4 = (float4 *)w; w += al(NF * 16);
   float *Eatom = (float *)w; w += al(NF * 4);
   double *vir = virial;
-  double *vscratch = (double *)w; w += al((size_t)nframes * 9 * 8);
+  double *vscratch = (double *)w; w += al(nE * 9 * 8);
   if (!vir) vir = vscratch;
   DPB_CUDA_TRY(cudaMemsetAsync(F4, 0, NF * 16, st));
-  DPB_CUDA_TRY(cudaMemsetAsync(energy, 0, (size_t)nframes * 8, st));
-  DPB_CUDA_TRY(cudaMemsetAsync(vir, 0, (size_t)nframes * 72, st));
+  DPB_CUDA_TRY(cudaMemsetAsync(energy, 0, nE * 8, st));
+  DPB_CUDA_TRY(cudaMemsetAsync(vir, 0, nE * 72, st));
   if (precision == DPB_PREC_FP32) {
     rc = eval_fp32(M, D, pos, perm, box, nbrs, energy, F4, Eatom, vir, w, st);
   } else {
@@ -405,7 +416,18 @@ int dpb::eval_impl(const dpb_model *m, int precision, const float *pos, const in
     rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st);
   }
   if (rc) return rc;
-  return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, nframes, pos, status, st);
+  return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, (int)nE, pos, seg, status,
+                         st);
+}
+
+extern "C" int dpb_eval_packed(const dpb_model *m, int precision, const float *pos, const int32_t *perm,
+                               int natoms, const int *type_count, const int32_t *seg, int nseg, const float *box,
+                               const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,
+                               float *force, double *virial, uint32_t *status, void *workspace, size_t ws_bytes,
+                               void *stream) {
+  if (!seg) return DPB_ERR_INVALID_ARG;
+  return dpb::eval_impl(m, precision, pos, perm, natoms, 1, type_count, box, nbrs, sel, energy, atom_energy, force,
+                        virial, status, workspace, ws_bytes, (cudaStream_t)stream, seg, nseg);
 }
 
 extern "C" int dpb_eval(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms,

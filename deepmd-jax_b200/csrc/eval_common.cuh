@@ -48,12 +48,33 @@ struct DevModel {
 };
 
 // Frame/type geometry of one evaluation call.
+// Packed (ragged) batches run as one frame (F = 1) whose atoms come from many
+// request frames: seg[k] is the request frame ("segment") of sorted atom k,
+// i.e. the row of its box and of its energy / virial; padding atoms carry
+// -(s + 1) (box of segment s, no energy).  Each segment's run of atoms of one
+// type starts at a multiple of 8 of the type block, so every 8-atom block of
+// the embedding kernels lies in one segment.  seg == NULL: ordinary frames.
 struct SysDesc {
   int N, F, ntypes, S;
   int offs[kMaxTypes + 1];
   int sel[kMaxTypes];
   int col[kMaxTypes + 1];
+  const int32_t *seg;
 };
+
+// Box row of sorted atom g (global index f * N + k) of frame f.
+__device__ __forceinline__ int box_slot(const SysDesc &D, size_t g, int f) {
+  if (!D.seg) return f;
+  const int s = D.seg[g];
+  return s >= 0 ? s : -s - 1;
+}
+
+// Energy row of sorted atom g, or -1 for a padding atom.
+__device__ __forceinline__ int energy_slot(const int32_t *seg, size_t g, int N) {
+  if (!seg) return (int)(g / N);
+  const int s = seg[g];
+  return s >= 0 ? s : -1;
+}
 
 // Rows of the fitting GEMMs are the atoms of one centre type across frames:
 // row r -> atom (r / cnt) * N + off + r % cnt.

@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(256) k_embed_fwd(DevModel M, SysDesc D, int ti
   const int i = D.offs[ti] + a;
   const size_t g = (size_t)f * D.N + i;
   const float3 ri = load_pos(pos, perm, f, i, D.N);
-  const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+  const int bs = box_slot(D, g, f);
+  const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
   const int3 ni = image_range(L, M.rcut);
   const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
   const float inv_std = M.inv_std[ti], mean = M.mean[ti];
@@ -583,7 +584,8 @@ __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti
     __syncwarp();
     // ---- rows: recompute with tangents, scatter forces
     const float3 ri = load_pos(pos, perm, f, i, D.N);
-    const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+    const int bs = box_slot(D, g, f);
+    const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
     const float inv_std = M.inv_std[ti], mean = M.mean[ti];
@@ -657,7 +659,11 @@ __global__ void __launch_bounds__(256) k_embed_bwd(DevModel M, SysDesc D, int ti
     if (lane == 0 && s != 0.f) atomicAdd(&vsm[k], (double)s);
   }
   __syncthreads();
-  if (threadIdx.x < 9) atomicAdd(&virial[f * 9 + threadIdx.x], vsm[threadIdx.x]);
+  // the block's 8 atoms share one frame (segment-aligned in packed batches)
+  if (threadIdx.x < 9) {
+    const int vs = box_slot(D, (size_t)f * D.N + D.offs[ti] + blockIdx.x * wpb, f);
+    atomicAdd(&virial[vs * 9 + threadIdx.x], vsm[threadIdx.x]);
+  }
 }
 
 // ---------------------------------------------------------------- fitting (SGEMM chain)
@@ -766,7 +772,8 @@ __global__ void __launch_bounds__(256) k_fit_energy(int Mrows, RowMap rm, int FW
                                                     const float *__restrict__ tl, const float *__restrict__ wfin,
                                                     const float *__restrict__ bfin, const float *__restrict__ dtl,
                                                     float *__restrict__ Eatom, float *__restrict__ gZ,
-                                                    double *__restrict__ energy, int N) {
+                                                    double *__restrict__ energy, int N,
+                                                    const int32_t *__restrict__ seg) {
   __shared__ double es[64];
   __shared__ int fs[64];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -788,7 +795,7 @@ __global__ void __launch_bounds__(256) k_fit_energy(int Mrows, RowMap rm, int FW
     if (lane == 0) {
       Eatom[at] = s;
       es[slot] = (double)s;
-      fs[slot] = (int)(at / N);
+      fs[slot] = energy_slot(seg, at, N);
     }
   }
   __syncthreads();
@@ -812,8 +819,9 @@ __global__ void __launch_bounds__(256) k_fit_energy(int Mrows, RowMap rm, int FW
 // in the reference's float arithmetic, make the frame's energy NaN.
 __global__ void k_finalize(int NF, int N, const float4 *__restrict__ F4, float *__restrict__ force,
                            const float *__restrict__ Eatom_sorted, const int32_t *__restrict__ perm,
-                           float *__restrict__ atom_energy, double *__restrict__ energy, int F,
-                           const float *__restrict__ pos, uint32_t *__restrict__ status) {
+                           float *__restrict__ atom_energy, double *__restrict__ energy, int nE,
+                           const float *__restrict__ pos, const int32_t *__restrict__ seg,
+                           uint32_t *__restrict__ status) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < NF) {
     const float4 v = F4[g];
@@ -821,16 +829,15 @@ __global__ void k_finalize(int NF, int N, const float4 *__restrict__ F4, float *
     force[(size_t)g * 3 + 1] = v.y;
     force[(size_t)g * 3 + 2] = v.z;
     const int f = g / N, k = g - f * N;
-    if (atom_energy) {
-      const int dst = perm ? perm[k] : k;
-      atom_energy[(size_t)f * N + dst] = Eatom_sorted[g];
-    }
-    const float *p = pos + (size_t)g * 3;
+    const int dst = perm ? perm[k] : k;
+    if (atom_energy) atom_energy[(size_t)f * N + dst] = Eatom_sorted[g];
+    const float *p = pos + ((size_t)f * N + dst) * 3;  // position of sorted atom g
     const bool bad_in = !isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2]);
     if (bad_in || !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) atomicOr(status, DPB_ST_NONFINITE);
-    if (bad_in) energy[f] = __longlong_as_double(0x7ff8000000000000LL);
+    const int e = energy_slot(seg, g, N);
+    if (bad_in && e >= 0) energy[e] = __longlong_as_double(0x7ff8000000000000LL);
   }
-  if (g < F && !isfinite(energy[g])) atomicOr(status, DPB_ST_NONFINITE);
+  if (g < nE && !isfinite(energy[g])) atomicOr(status, DPB_ST_NONFINITE);
 }
 
 // Explicit instantiation helpers used by the C ABI dispatch.
@@ -908,19 +915,20 @@ int launch_sgemm(int Mrows, int Nc, int K, const float *A, int lda, RowMap rm, c
 
 int launch_fit_energy(int Mrows, RowMap rm, int FWl, const float *H, const float *tl, const float *wfin,
                       const float *bfin, const float *dtl, float *Eatom, float *gZ, double *energy, int N,
-                      cudaStream_t st) {
+                      const int32_t *seg, cudaStream_t st) {
   if (Mrows == 0) return DPB_OK;
-  k_fit_energy<<<(Mrows + 63) / 64, 256, 0, st>>>(Mrows, rm, FWl, H, tl, wfin, bfin, dtl, Eatom, gZ, energy, N);
+  k_fit_energy<<<(Mrows + 63) / 64, 256, 0, st>>>(Mrows, rm, FWl, H, tl, wfin, bfin, dtl, Eatom, gZ, energy, N,
+                                                  seg);
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
 }
 
 int launch_finalize(int NF, int N, const float4 *F4, float *force, const float *Eatom, const int32_t *perm,
-                    float *atom_energy, double *energy, int F, const float *pos, uint32_t *status,
-                    cudaStream_t st) {
-  int n = NF > F ? NF : F;
-  k_finalize<<<(n + 255) / 256, 256, 0, st>>>(NF, N, F4, force, Eatom, perm, atom_energy, energy, F, pos,
+                    float *atom_energy, double *energy, int nE, const float *pos, const int32_t *seg,
+                    uint32_t *status, cudaStream_t st) {
+  int n = NF > nE ? NF : nE;
+  k_finalize<<<(n + 255) / 256, 256, 0, st>>>(NF, N, F4, force, Eatom, perm, atom_energy, energy, nE, pos, seg,
                                               status);
   count_launch();
   DPB_LAUNCH_CHECK();

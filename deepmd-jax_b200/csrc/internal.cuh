@@ -13,7 +13,7 @@ namespace dpb {
 int eval_impl(const dpb_model *m, int precision, const float *pos, const int32_t *perm, int natoms, int nframes,
               const int *type_count, const float *box, const int32_t *nbrs, const int *sel, double *energy,
               float *atom_energy, float *force, double *virial, uint32_t *status, void *workspace,
-              size_t ws_bytes, cudaStream_t st);
+              size_t ws_bytes, cudaStream_t st, const int32_t *seg = nullptr, int nseg = 0);
 int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
                      const int *type_count, const int *sel, const float box[3], const float *ref_box, float rc,
                      int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status, void *workspace,

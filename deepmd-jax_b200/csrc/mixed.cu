@@ -247,7 +247,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
     const int nb = min(kBlkAtoms, cnt_i - a0);
     const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
     const size_t frame_base = (size_t)f * D.N;
-    const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+    const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
+    const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
     if (tid < nb) {
@@ -608,6 +609,23 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
   float vir[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) vir[k] = 0.f;
+  // the virial goes to the frame of the blocks processed; a CTA that moves on
+  // to a block of another frame (packed batches) flushes its sum first
+  int vframe = -1;
+  auto flush_virial = [&]() {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float s = warp_sum(vir[k]);
+      if ((tid & 31) == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
+      vir[k] = 0.f;
+    }
+    __syncthreads();
+    if (tid < 9) {
+      atomicAdd(&virial[vframe * 9 + tid], vir_s[tid]);
+      vir_s[tid] = 0.0;
+    }
+    __syncthreads();
+  };
 
   const int cnt_i = D.offs[ti + 1] - D.offs[ti];
   const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
@@ -626,7 +644,12 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     const int nb = min(kBlkAtoms, cnt_i - a0);
     const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
     const size_t frame_base = (size_t)f * D.N;
-    const float3 L = make_float3(box[f * 3], box[f * 3 + 1], box[f * 3 + 2]);
+    const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
+    if (bs != vframe) {
+      if (vframe >= 0) flush_virial();
+      vframe = bs;
+    }
+    const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
     if (tid < nb) {
@@ -859,7 +882,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
   tc::cp_async_wait<0>();
   tc::fence_before_sync();
   __syncthreads();
-  if (tid < 9) atomicAdd(&virial[tid], vir_s[tid]);
+  if (tid < 9 && vframe >= 0) atomicAdd(&virial[vframe * 9 + tid], vir_s[tid]);
   if (warp == 0) tc::tmem_dealloc(tbase, 256);
 }
 
@@ -1010,7 +1033,8 @@ template <int FW>
 __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrows, RowMap rm,
                                                     const __nv_bfloat16 *__restrict__ Gb, float *__restrict__ dGout,
                                                     float *__restrict__ scratch, float *__restrict__ Eatom,
-                                                    double *__restrict__ energy, int N, int *__restrict__ err) {
+                                                    double *__restrict__ energy, int N, int *__restrict__ err,
+                                                    const int32_t *__restrict__ seg) {
   static_assert(FW % 32 == 0 || FW % 16 == 0, "fit width");
   extern __shared__ __align__(1024) char smem[];
   char *HA = smem;                                  // 128 x FW bf16 (K-major)
@@ -1094,17 +1118,17 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
   __syncthreads();
   if (tid == 0 && ok) {
     double run = 0.0;
-    int cf = (int)(atom_s[0] / N);
+    int cf = energy_slot(seg, atom_s[0], N);
     for (int k = 0; k < nrows; ++k) {
-      const int fk = (int)(atom_s[k] / N);
+      const int fk = energy_slot(seg, atom_s[k], N);
       if (fk != cf) {
-        atomicAdd(&energy[cf], run);
+        if (cf >= 0) atomicAdd(&energy[cf], run);
         run = 0.0;
         cf = fk;
       }
       run += es[k];
     }
-    atomicAdd(&energy[cf], run);
+    if (cf >= 0) atomicAdd(&energy[cf], run);
   }
   // ---- adjoint: layers L-1 .. 1, gH_{l-1} = gZ_l W_l^T (+ gH_l if residual)
   for (int l = L - 1; l >= 1 && ok; --l) {
@@ -1172,7 +1196,8 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
     if (!cnt) continue;
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
-    k_mix_fit<FW><<<(Mrows + 127) / 128, 128, smem, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err);
+    k_mix_fit<FW><<<(Mrows + 127) / 128, 128, smem, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
+                                                          D.seg);
     count_launch();
     DPB_LAUNCH_CHECK();
   }

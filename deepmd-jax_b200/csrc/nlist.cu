@@ -351,3 +351,61 @@ extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms
   return dpb::nlist_build_impl(pos, perm, natoms, nframes, ntypes, type_count, sel, box, ref_box, rc, nbrs,
                                ref_pos, counts, status, workspace, ws_bytes, nullptr, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------- packed batches
+namespace dpb {
+// Where the frames of one request land in a packed batch: frame f's type-t
+// atoms are packed rows row0[t] + f * stride[t] + m (m < count of type t), and
+// its type-t atom m is type-local index base0[t] + f * stride[t] + m of the
+// packed type block.
+struct PackMap {
+  int ntypes, S, Ns, nframes, Np;
+  int soffs[kMaxTypes + 1];
+  int col[kMaxTypes + 1];
+  int row0[kMaxTypes], base0[kMaxTypes], stride[kMaxTypes];
+};
+
+__global__ void nl_pack_kernel(const int32_t *__restrict__ src, PackMap m, int32_t *__restrict__ dst) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t per_frame = (size_t)m.Ns * m.S;
+  if (e >= per_frame * m.nframes) return;
+  const int f = (int)(e / per_frame);
+  const size_t rc = e - (size_t)f * per_frame;
+  const int r = (int)(rc / m.S), c = (int)(rc - (size_t)r * m.S);
+  int i = 0, j = 0;
+  while (i + 1 < m.ntypes && r >= m.soffs[i + 1]) ++i;
+  while (j + 1 < m.ntypes && c >= m.col[j + 1]) ++j;
+  const int v = src[e] & DPB_NBR_INDEX_MASK;
+  const int cnt_j = m.soffs[j + 1] - m.soffs[j];
+  const int out = v < cnt_j ? m.base0[j] + f * m.stride[j] + v : m.Np;
+  const size_t row = (size_t)m.row0[i] + (size_t)f * m.stride[i] + (r - m.soffs[i]);
+  dst[row * m.S + c] = out;
+}
+}  // namespace dpb
+
+extern "C" int dpb_nlist_pack(const int32_t *src, int natoms, int nframes, int ntypes, const int *type_count,
+                              const int *sel, const int *row0, const int *base0, const int *stride,
+                              int packed_natoms, int32_t *dst, void *stream) {
+  if (!src || !dst || !type_count || !sel || !row0 || !base0 || !stride || natoms <= 0 || nframes <= 0 ||
+      ntypes < 1 || ntypes > dpb::kMaxTypes || packed_natoms <= 0)
+    return DPB_ERR_INVALID_ARG;
+  dpb::PackMap m;
+  m.ntypes = ntypes; m.Ns = natoms; m.nframes = nframes; m.Np = packed_natoms;
+  int off = 0, col = 0;
+  for (int t = 0; t < ntypes; ++t) {
+    if (type_count[t] < 0 || sel[t] < 0 || stride[t] < type_count[t]) return DPB_ERR_INVALID_ARG;
+    m.soffs[t] = off; off += type_count[t];
+    m.col[t] = col; col += sel[t];
+    m.row0[t] = row0[t]; m.base0[t] = base0[t]; m.stride[t] = stride[t];
+    if (row0[t] < 0 || base0[t] < 0 || (long long)row0[t] + (long long)stride[t] * nframes > packed_natoms)
+      return DPB_ERR_INVALID_ARG;
+  }
+  if (off != natoms) return DPB_ERR_INVALID_ARG;
+  m.soffs[ntypes] = off; m.col[ntypes] = col; m.S = col;
+  const size_t n = (size_t)natoms * col * nframes;
+  if (n == 0) return DPB_OK;
+  dpb::nl_pack_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(src, m, dst);
+  dpb::count_launch();
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}

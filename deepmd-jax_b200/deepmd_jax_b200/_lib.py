@@ -22,7 +22,8 @@ PREC_MIXED = 1
 NBR_INDEX_MASK = 0x00FFFFFF
 
 EXPORTED = ["dpb_model_create", "dpb_model_destroy", "dpb_nlist_workspace_bytes", "dpb_nlist_build",
-            "dpb_eval_workspace_bytes", "dpb_eval", "dpb_eval_noalloc", "dpb_kernel_launch_count", "dpb_version"]
+            "dpb_eval_workspace_bytes", "dpb_eval", "dpb_eval_noalloc", "dpb_eval_packed_workspace_bytes",
+            "dpb_eval_packed", "dpb_nlist_pack", "dpb_kernel_launch_count", "dpb_version"]
 
 
 class DPBError(RuntimeError):
@@ -90,6 +91,14 @@ def load():
     lib.dpb_eval_noalloc.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, ctypes.c_int, c_int_p, f32p, i32p,
                                      c_int_p, f64p, f32p, f32p, f64p, vp, vp]
     lib.dpb_eval_noalloc.restype = ctypes.c_int
+    lib.dpb_eval_packed_workspace_bytes.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+    lib.dpb_eval_packed_workspace_bytes.restype = ctypes.c_int
+    lib.dpb_eval_packed.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, c_int_p, i32p, ctypes.c_int, f32p,
+                                    i32p, c_int_p, f64p, f32p, f32p, f64p, vp, vp, ctypes.c_size_t, vp]
+    lib.dpb_eval_packed.restype = ctypes.c_int
+    lib.dpb_nlist_pack.argtypes = [i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p, c_int_p, c_int_p,
+                                   c_int_p, ctypes.c_int, i32p, vp]
+    lib.dpb_nlist_pack.restype = ctypes.c_int
     lib.dpb_kernel_launch_count.argtypes = []
     lib.dpb_kernel_launch_count.restype = ctypes.c_uint64
     lib.dpb_version.argtypes = []

@@ -222,3 +222,107 @@ def sort_by_type(type_idx, ntypes):
     perm = np.argsort(type_idx, kind="stable")
     count = np.bincount(type_idx, minlength=ntypes)
     return perm, count
+
+
+def _pad8(n):
+    return (int(n) + 7) // 8 * 8
+
+
+class PackedBatch:
+    """Host layout of many request frames packed into one evaluation
+    (dpb_eval_packed / dpb_nlist_pack).
+
+    ``items`` is a list of (type_idx (N,), nframes, box (3,)); the frames of
+    one item share the atom order, the type counts and the box.  Segment
+    s numbers the frames item after item.  Packed type block t holds, item
+    after item and frame after frame, each frame's type-t atoms padded to a
+    multiple of 8; the slots (rows of the position / force buffers) are the
+    items' frames in their own atom order, then one slot per padding atom."""
+
+    def __init__(self, items, ntypes):
+        self.ntypes = ntypes
+        self.items = []
+        counts = []
+        for type_idx, nframes, box in items:
+            perm, cnt = sort_by_type(np.asarray(type_idx), ntypes)
+            counts.append((perm, cnt, int(nframes), np.asarray(box, np.float32).reshape(3)))
+        pad = np.array([[_pad8(c) for c in cnt] for _, cnt, _, _ in counts], dtype=np.int64).reshape(-1, ntypes)
+        nfr = np.array([nf for _, _, nf, _ in counts], dtype=np.int64)
+        self.type_count = [int((pad[:, t] * nfr).sum()) for t in range(ntypes)]
+        self.natoms = int(sum(self.type_count))
+        offs = np.concatenate([[0], np.cumsum(self.type_count)]).astype(np.int64)
+        perm_p = np.empty(self.natoms, dtype=np.int64)
+        seg_p = np.empty(self.natoms, dtype=np.int64)
+        self.nreal = int(sum(len(p) * nf for p, _, nf, _ in counts))
+        dummy_next = self.nreal
+        base = np.zeros(ntypes, dtype=np.int64)
+        u0, s0 = 0, 0
+        boxes = []
+        for (perm, cnt, nf, box), pd in zip(counts, pad):
+            N = len(perm)
+            soffs = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+            it = {"natoms": N, "nframes": nf, "slot0": u0, "seg0": s0, "perm": perm, "type_count": cnt,
+                  "row0": [], "base0": [], "stride": [], "box": box}
+            for t in range(ntypes):
+                p, n = int(pd[t]), int(cnt[t])
+                it["row0"].append(int(offs[t] + base[t]))
+                it["base0"].append(int(base[t]))
+                it["stride"].append(p)
+                rows = offs[t] + base[t] + np.arange(nf)[:, None] * p + np.arange(p)[None, :]   # (nf, p)
+                real = u0 + np.arange(nf)[:, None] * N + perm[soffs[t]:soffs[t + 1]][None, :]   # (nf, n)
+                nd = nf * (p - n)
+                dummies = np.arange(dummy_next, dummy_next + nd).reshape(nf, p - n)
+                dummy_next += nd
+                perm_p[rows] = np.concatenate([real, dummies], axis=1)
+                s = s0 + np.arange(nf)[:, None]
+                seg_p[rows] = np.concatenate([np.broadcast_to(s, (nf, n)), np.broadcast_to(-(s + 1), (nf, p - n))],
+                                             axis=1)
+                base[t] += nf * p
+            boxes += [box] * nf
+            self.items.append(it)
+            u0 += nf * N
+            s0 += nf
+        self.nseg = s0
+        self.perm = perm_p.astype(np.int32)
+        self.seg = seg_p.astype(np.int32)
+        self.boxes = np.asarray(boxes, np.float32).reshape(-1, 3)
+
+
+def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energy=False):
+    """One packed evaluation of every frame of ``batch`` (a PackedBatch).
+
+    slot_pos: (batch.natoms, 3) float32 CUDA, the frames' positions at their
+    slots (padding slots any finite value).  Returns energy (nseg,) f64,
+    force (natoms, 3) f32 at the slots, virial (nseg, 9) f64, status."""
+    lib = dm.lib
+    dev = slot_pos.device
+    Np, S = batch.natoms, int(sum(sel))
+    nbrs = torch.full((Np, S), Np, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    for it in batch.items:
+        N, nf = it["natoms"], it["nframes"]
+        pos = slot_pos[it["slot0"]:it["slot0"] + nf * N].view(nf, N, 3)
+        perm = torch.tensor(it["perm"].astype(np.int32), device=dev)
+        nb, _ = NeighborBuilder(N, nf, it["type_count"], sel, it["box"], rcut).build(pos, perm=perm, status=status)
+        _lib.check(lib.dpb_nlist_pack(_ptr(nb), N, nf, batch.ntypes, _lib.int_array(it["type_count"]),
+                                      _lib.int_array(sel), _lib.int_array(it["row0"]), _lib.int_array(it["base0"]),
+                                      _lib.int_array(it["stride"]), Np, _ptr(nbrs), _stream()), "dpb_nlist_pack")
+    n = ctypes.c_size_t()
+    _lib.check(lib.dpb_eval_packed_workspace_bytes(dm.handle, Np, batch.nseg, ctypes.byref(n)),
+               "dpb_eval_packed_workspace_bytes")
+    ws = torch.empty(n.value, dtype=torch.uint8, device=dev)
+    perm = torch.tensor(batch.perm, device=dev)
+    seg = torch.tensor(batch.seg, device=dev)
+    box = torch.tensor(batch.boxes, device=dev)
+    out = dict(energy=torch.empty(batch.nseg, dtype=torch.float64, device=dev),
+               force=torch.empty((Np, 3), dtype=torch.float32, device=dev),
+               virial=torch.empty((batch.nseg, 9), dtype=torch.float64, device=dev),
+               atom_energy=torch.empty(Np, dtype=torch.float32, device=dev) if atom_energy else None)
+    rc = lib.dpb_eval_packed(dm.handle, PRECISIONS[precision], _ptr(slot_pos), _ptr(perm), Np,
+                             _lib.int_array(batch.type_count), _ptr(seg), batch.nseg, _ptr(box), _ptr(nbrs),
+                             _lib.int_array(sel), _ptr(out["energy"]), _ptr(out["atom_energy"]), _ptr(out["force"]),
+                             _ptr(out["virial"]), _ptr(status), _ptr(ws), ws.numel(), _stream())
+    _lib.check(rc, "dpb_eval_packed")
+    out["status"] = status
+    out["nbrs"] = nbrs
+    return out

@@ -157,6 +157,38 @@ DPB_API int dpb_eval(const dpb_model *model, int precision, const float *pos, co
              float *force, double *virial, uint32_t *status, void *workspace,
              size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------- packed (ragged) batches
+ * Many request frames of different atom counts and boxes evaluated by ONE
+ * launch sequence (the serving loop's batch).  Replaces: the per-request
+ * jit(vmap(energy_and_force)) calls of evaluate()/test()
+ * (deepmd_jax/train.py:523-788), which compile and run one shape at a time.
+ *
+ * Layout ("segments" = request frames, s = 0..nseg-1):
+ *   - packed atoms are type-sorted: type block t holds, segment after
+ *     segment, each segment's type-t atoms padded with padding atoms to a
+ *     multiple of 8 (so every 8-atom block lies in one segment);
+ *   - seg[k] (natoms int32) = s for a real atom, -(s+1) for padding;
+ *   - perm[k] = slot of packed atom k in pos / force (a bijection on
+ *     [0, natoms)); padding atoms get their own slots (any finite position);
+ *   - box (nseg, 3) device; energy (nseg) f64; virial (nseg, 9) f64;
+ *   - nbrs (natoms, sum(sel)): type-local indices of the packed type blocks,
+ *     pad = natoms; padding atoms' rows all pad (dpb_nlist_pack fills it). */
+DPB_API int dpb_eval_packed_workspace_bytes(const dpb_model *model, int natoms, int nseg, size_t *bytes);
+DPB_API int dpb_eval_packed(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
+                            int natoms, const int *type_count, const int32_t *seg, int nseg, const float *box,
+                            const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,
+                            float *force, double *virial, uint32_t *status, void *workspace, size_t ws_bytes,
+                            void *stream);
+/* Copy the lists of `nframes` frames of one request (built by
+ * dpb_nlist_build: (nframes, natoms, sum(sel)), type-local indices, pad =
+ * natoms) into a packed list: frame f's type-t rows go to packed rows
+ * row0[t] + f*stride[t] + m and its type-j index v becomes
+ * base0[j] + f*stride[j] + v (pad -> packed_natoms).  No reference
+ * counterpart (the reference has no packed batches). */
+DPB_API int dpb_nlist_pack(const int32_t *src, int natoms, int nframes, int ntypes, const int *type_count,
+                           const int *sel, const int *row0, const int *base0, const int *stride,
+                           int packed_natoms, int32_t *dst, void *stream);
+
 /* dpb_eval without a caller workspace, for callers that cannot allocate
  * device memory (a host code that keeps the force field inside its own fixed
  * memory pool, a plugin whose process forbids foreign cudaMalloc calls, code
