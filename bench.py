@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling case: plain MD steps (direct launches, no timing) for ncu")
     ap.add_argument("--n-side", type=int, default=N_SIDE, help="waters per box side (profiling case)")
-    ap.add_argument("--study", default="none", choices=["none", "drift", "pimd"],
+    ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving study: seconds of arrivals")
+    ap.add_argument("--study", default="none", choices=["none", "drift", "pimd", "serving"],
                     help="drift: NVE total-energy drift of both forms on the 98,304-atom box; "
                          "pimd: 32-bead PILE-L throughput of both forms (1,536-atom water)")
     ap.add_argument("--report-every", type=int, default=100, help="drift study: steps between energy samples")
@@ -469,12 +470,83 @@ def study_pimd(args):
     return out
 
 
+def study_serving(args):
+    """Serving stream of the benchmark model: Poisson arrivals at 200
+    requests/s for args.serve_seconds; 98 % are evaluate() requests of 1-16
+    water frames with the atom count log-uniform in [96, 24,576] (multiples
+    of 3; waters on the first n_w sites of a ceil(n_w^(1/3))^3 lattice, box
+    12.42 (n_w / 64)^(1/3) A), 2 % are MD continuations of 100 NVT steps on
+    3,000-30,000-atom boxes; 60 GB HBM admission budget.  Both forms.
+    Latency = submit to result on the host; throughput over the whole run
+    (arrivals + drain)."""
+    import numpy as np
+    import torch
+    from deepmd_jax_b200.serving import Server
+    from deepmd_jax_b200.systems import serving_water
+    params, variables = _models()
+    rng = np.random.default_rng(0)
+    cache = {}
+
+    def water(n_w):
+        if n_w not in cache:
+            cache[n_w] = serving_water(n_w, seed=n_w)
+        return cache[n_w]
+
+    sched, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / 200.0)
+        if t > args.serve_seconds:
+            break
+        if rng.random() < 0.02:
+            n_w = int(np.exp(rng.uniform(np.log(1000), np.log(10000))))
+            sched.append((t, "md", n_w, 100))
+        else:
+            n_w = max(32, int(np.exp(rng.uniform(np.log(96), np.log(24576)))) // 3)
+            sched.append((t, "eval", n_w, int(rng.integers(1, 17))))
+    for _, _, n_w, _ in sched:
+        water(n_w)
+    out = {"study": "serving", "arrival_rate_per_s": 200, "seconds_of_arrivals": args.serve_seconds,
+           "requests": len(sched), "md_requests": sum(1 for x in sched if x[1] == "md"),
+           "hbm_budget_GB": 60, "forms": {}}
+    for prec in ("fp32", "mixed"):
+        with Server((params, variables), precision=prec, hbm_budget=60e9) as srv:
+            w = water(64)
+            srv.submit_evaluate(w["position"], w["box"], w["type_idx"]).result()   # warm-up
+            srv.completed.clear()
+            futs, atoms_eval, frames = [], 0, 0
+            t0 = time.perf_counter()
+            for ta, kind, n_w, k in sched:
+                dt = t0 + ta - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                w = water(n_w)
+                if kind == "eval":
+                    pos = w["position"][None] + 0.01 * rng.standard_normal((k,) + w["position"].shape)
+                    futs.append(srv.submit_evaluate(pos, w["box"], w["type_idx"]))
+                    atoms_eval += k * len(w["type_idx"])
+                    frames += k
+                else:
+                    futs.append(srv.submit_md(w["position"], w["box"], w["type_idx"], w["mass_per_type"], k,
+                                              routine="NVT", seed=n_w))
+            for f in futs:
+                f.result()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            lat = srv.latency_summary()
+            out["forms"][prec] = {"latency": lat, "wall_s": wall, "frames_per_s": frames / wall,
+                                  "atom_evals_per_s": atoms_eval / wall, "batches": srv.batches,
+                                  "mean_batch_atoms": float(np.mean(srv.batch_sizes)) if srv.batch_sizes else 0,
+                                  "peak_reserved_GB": srv.budget.peak / 1e9}
+    return out
+
+
 def main():
     args = parse()
     if args.ncu_case:
         return ncu_case(args)
     if args.study != "none":
-        print(json.dumps(study_drift(args) if args.study == "drift" else study_pimd(args)))
+        fn = {"drift": study_drift, "pimd": study_pimd, "serving": study_serving}[args.study]
+        print(json.dumps(fn(args)))
         return 0
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))

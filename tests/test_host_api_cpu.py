@@ -53,3 +53,35 @@ def test_nested_and_packed_lists_round_trip():
     assert [tuple(a.shape) for a in nested[1]] == [(5, 2), (5, 4)]
     back, sel2 = from_nbrs_nm([[a.numpy() for a in row] for row in nested], device="cpu")
     assert sel2 == sel and torch.equal(back, packed)
+
+
+def test_packed_batch_layout():
+    """Layout of the serving loop's packed batches: slots are a bijection,
+    each frame's type runs start at multiples of 8, padding atoms carry
+    -(s+1), and every real atom's slot holds its own type."""
+    from deepmd_jax_b200.engine import PackedBatch
+    rng = np.random.default_rng(0)
+    items = [(rng.integers(0, 2, 13), 2, [5.0, 5.0, 5.0]), (rng.integers(0, 2, 30), 1, [7.0, 7.0, 7.0]),
+             (np.array([1, 1, 1]), 3, [4.0, 4.0, 4.0])]
+    b = PackedBatch(items, 2)
+    assert sorted(b.perm.tolist()) == list(range(b.natoms))
+    assert b.nseg == 6 and b.nreal == 13 * 2 + 30 + 3 * 3
+    slot_type = np.full(b.natoms, -1)
+    for (t, nf, _), it in zip(items, b.items):
+        for f in range(nf):
+            slot_type[it["slot0"] + f * len(t):it["slot0"] + (f + 1) * len(t)] = t
+    offs = np.concatenate([[0], np.cumsum(b.type_count)])
+    for k in range(b.natoms):
+        ty = int(np.searchsorted(offs, k, side="right") - 1)
+        if b.seg[k] >= 0:
+            assert slot_type[b.perm[k]] == ty
+        else:
+            assert b.perm[k] >= b.nreal
+    for it in b.items:
+        for t in range(2):
+            assert it["stride"][t] % 8 == 0 and it["base0"][t] % 8 == 0
+            for f in range(it["nframes"]):
+                rows = it["row0"][t] + f * it["stride"][t] + np.arange(it["stride"][t])
+                n = int(it["type_count"][t])
+                assert np.all(b.seg[rows[:n]] == it["seg0"] + f)
+                assert np.all(b.seg[rows[n:]] == -(it["seg0"] + f) - 1)
