@@ -71,6 +71,7 @@ int launch_finalize(int, int, const float4 *, float *, const float *, const int3
 // mixed path (mixed.cu)
 int mixed_supported(const DevModel &M);
 size_t mixed_workspace_per_atom(const DevModel &M);
+size_t mixed_workspace_fixed(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
                cudaStream_t st);
@@ -247,7 +248,8 @@ static size_t fp32_ws_per_atom(const DevModel &M) {
 // Workspace of NF atoms with nE energy / virial rows.
 static size_t eval_ws_bytes(const DevModel &M, size_t NF, size_t nE) {
   size_t a = al(NF * fp32_ws_per_atom(M)) + 16 * 256 + al(nE * 9 * 8);
-  size_t b = al(NF * mixed_workspace_per_atom(M)) + al(NF * 16) + al(NF * 4) + al(nE * 9 * 8) + 16 * 256;
+  size_t b = al(NF * mixed_workspace_per_atom(M)) + mixed_workspace_fixed(M) + al(NF * 16) + al(NF * 4) +
+             al(nE * 9 * 8) + 16 * 256;
   return std::max(a, b);
 }
 

@@ -509,57 +509,126 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
 template <int E2, int N2>
 __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
                                                 const float *__restrict__ dG, __nv_bfloat16 *__restrict__ dTb) {
-  extern __shared__ float smf[];
+  // Warp per atom; lane owns columns w = lane + 32 j.  The atom's dE/dG rows
+  // stay in registers (D[a][j]); X = T + Tbias sits in shared memory.
+  //   dQ[c][a] = sum_w dG[a][w] X[c][w]   (per-lane partials, then a shuffle
+  //                                         reduce-scatter: lane l ends with a = l & 15)
+  //   dX[c][w] = sum_a dG[a][w] Q[c][a] + the Q -> X terms at w < 2A
+  constexpr int NJ = (E2 + 31) / 32;
+  static_assert((N2 + 31) / 32 == NJ, "padded width");
+  __shared__ float Xs[4][10 * E2];
+  __shared__ float Qs[4][160], dQs[4][160];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int A = M.A;
-  float *Xs = smf + warp * (20 * E2 + A * E2 + 20 * A);
-  float *dGs = Xs + 10 * E2, *Qs = dGs + A * E2, *dQs = Qs + 10 * A, *dXs = dQs + 10 * A;
   const size_t g = (size_t)blockIdx.x * 4 + warp;
   if (g >= (size_t)NF) return;
-  for (int e = lane; e < 10 * E2; e += 32) Xs[e] = Tin[g * 10 * E2 + e] + (e < E2 ? M.tbias[e] : 0.f);
-  for (int e = lane; e < A * E2; e += 32) dGs[e] = dG[g * (size_t)A * E2 + e];
+  const int A = M.A;  // 1..16 (checked at model creation: 2A <= 32)
+  float *X = Xs[warp], *Q = Qs[warp], *dQ = dQs[warp];
+  const float *Tg = Tin + g * 10 * E2;
+  for (int e = lane; e < 10 * E2; e += 32) X[e] = Tg[e] + (e < E2 ? M.tbias[e] : 0.f);
+  float D[16][NJ];
+  const float *Gg = dG + g * (size_t)A * E2;
+#pragma unroll
+  for (int a = 0; a < 16; ++a)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int w = lane + 32 * j;
+      D[a][j] = (a < A && w < E2) ? Gg[a * E2 + w] : 0.f;
+    }
   __syncwarp();
-  for (int e = lane; e < 10 * A; e += 32) {
-    const int c = e / A, aa = e - c * A;
-    float qv;
-    if (c < 4) {
-      qv = Xs[c * E2 + aa];
-    } else {
-      const float y1 = Xs[E2 + A + aa], y2 = Xs[2 * E2 + A + aa], y3 = Xs[3 * E2 + A + aa];
-      const int m = c - 4;
+  if (lane < 16) {  // Q[c][a] (dpmodel.py:74-78), zero for a >= A
+    const int aa = lane;
+    float q[10];
+#pragma unroll
+    for (int c = 0; c < 10; ++c) q[c] = 0.f;
+    if (aa < A) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) q[c] = X[c * E2 + aa];
+      const float y1 = X[E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
       const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
-      qv = b6[m] + Xs[c * E2 + A + aa];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) q[4 + m] = b6[m] + X[(4 + m) * E2 + A + aa];
     }
-    Qs[e] = qv;
-    float dq = 0.f;
-    for (int w = 0; w < E2; ++w) dq = fmaf(dGs[aa * E2 + w], Xs[c * E2 + w], dq);
-    dQs[e] = dq;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) Q[c * 16 + aa] = q[c];
+  }
+#pragma unroll 1
+  for (int c = 0; c < 10; ++c) {
+    float p[16];
+    float xc[NJ];
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int w = lane + 32 * j;
+      xc[j] = w < E2 ? X[c * E2 + w] : 0.f;
+    }
+#pragma unroll
+    for (int a = 0; a < 16; ++a) {
+      float v = 0.f;
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) v = fmaf(D[a][j], xc[j], v);
+      p[a] = v;
+    }
+    // reduce-scatter of the 16 partials over the 32 lanes
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const bool hi = lane & 8;
+      const float send = hi ? p[k] : p[k + 8];
+      const float keep = hi ? p[k + 8] : p[k];
+      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const bool hi = lane & 4;
+      const float send = hi ? p[k] : p[k + 4];
+      const float keep = hi ? p[k + 4] : p[k];
+      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const bool hi = lane & 2;
+      const float send = hi ? p[k] : p[k + 2];
+      const float keep = hi ? p[k + 2] : p[k];
+      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    {
+      const bool hi = lane & 1;
+      const float send = hi ? p[0] : p[1];
+      const float keep = hi ? p[1] : p[0];
+      p[0] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+    }
+    p[0] += __shfl_xor_sync(0xffffffffu, p[0], 16);
+    if (lane < 16) dQ[c * 16 + lane] = p[0];  // the sum for a = lane
   }
   __syncwarp();
-  for (int e = lane; e < 10 * E2; e += 32) {
-    const int c = e / E2, w = e - c * E2;
-    float v = 0.f;
-    for (int aa = 0; aa < A; ++aa) v = fmaf(dGs[aa * E2 + w], Qs[c * A + aa], v);
-    if (w < A && c < 4) v += dQs[c * A + w];
-    if (w >= A && w < 2 * A) {
-      const int aa = w - A;
-      if (c >= 4) {
-        v += dQs[c * A + aa];
-      } else if (c >= 1) {
-        const float y1 = Xs[E2 + w], y2 = Xs[2 * E2 + w], y3 = Xs[3 * E2 + w];
-        const float d0 = dQs[4 * A + aa], d1 = dQs[5 * A + aa], d2 = dQs[6 * A + aa], d3 = dQs[7 * A + aa],
-                    d4 = dQs[8 * A + aa], d5 = dQs[9 * A + aa];
-        if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
-        if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
-        if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
+  __nv_bfloat16 *out = dTb + g * 10 * N2;
+#pragma unroll 1
+  for (int c = 0; c < 10; ++c) {
+    float q[16];
+#pragma unroll
+    for (int a = 0; a < 16; ++a) q[a] = Q[c * 16 + a];
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int w = lane + 32 * j;
+      float v = 0.f;
+#pragma unroll
+      for (int a = 0; a < 16; ++a) v = fmaf(D[a][j], q[a], v);
+      if (j == 0) {  // w < 32: the Q -> X terms live at w < 2A <= 32
+        if (w < A && c < 4) v += dQ[c * 16 + w];
+        if (w >= A && w < 2 * A) {
+          const int aa = w - A;
+          if (c >= 4) {
+            v += dQ[c * 16 + aa];
+          } else if (c >= 1) {
+            const float y1 = X[E2 + w], y2 = X[2 * E2 + w], y3 = X[3 * E2 + w];
+            const float d0 = dQ[64 + aa], d1 = dQ[80 + aa], d2 = dQ[96 + aa], d3 = dQ[112 + aa], d4 = dQ[128 + aa],
+                        d5 = dQ[144 + aa];
+            if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
+            if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
+            if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
+          }
+        }
       }
+      if (w < N2) out[c * N2 + w] = __float2bfloat16_rn(w < E2 ? v * M.inv_nnbrs : 0.f);
     }
-    dXs[e] = v * M.inv_nnbrs;
-  }
-  __syncwarp();
-  for (int e = lane; e < 10 * N2; e += 32) {
-    const int c = e / N2, w = e - c * N2;
-    dTb[g * 10 * N2 + e] = __float2bfloat16_rn(w < E2 ? dXs[c * E2 + w] : 0.f);
   }
 }
 
@@ -1034,7 +1103,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
                                                     const __nv_bfloat16 *__restrict__ Gb, float *__restrict__ dGout,
                                                     float *__restrict__ scratch, float *__restrict__ Eatom,
                                                     double *__restrict__ energy, int N, int *__restrict__ err,
-                                                    const int32_t *__restrict__ seg) {
+                                                    const int32_t *__restrict__ seg, int tile0) {
   static_assert(FW % 32 == 0 || FW % 16 == 0, "fit width");
   extern __shared__ __align__(1024) char smem[];
   char *HA = smem;                                  // 128 x FW bf16 (K-major)
@@ -1060,9 +1129,10 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
   tc::fence_after_sync();
   const uint32_t td = tbase_s, lane_off = (uint32_t)(warp * 32) << 16;
   const size_t me = atom_s[tid];
-  float *tl = scratch + me * (size_t)(2 * L + 1) * FW;
-  float *hl = tl + (size_t)L * FW;
-  float *gh = hl + (size_t)L * FW;
+  // per-CTA scratch tile [slot][n][thread] (coalesced): slots 0..L-1 tanh
+  // values, L..2L-1 layer outputs, 2L the residual adjoint
+  float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + tid;
+#define FIT_SCR(slot, n) tile[((size_t)(slot) * FW + (n)) * 128]
   bool ok = true;
   // ---- forward
   for (int l = 0; l < L && ok; ++l) {
@@ -1075,19 +1145,25 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
     for (int c0 = 0; c0 < FW; c0 += 16) {
       uint32_t r[16];
       tc::tmem_ld16_issue(td + lane_off + c0, r);
+      float bv[16], dv[16];
+#pragma unroll
+      for (int i = 0; i < 16; i += 4) {
+        const float4 b4 = __ldg(reinterpret_cast<const float4 *>(bias + c0 + i));
+        bv[i] = b4.x; bv[i + 1] = b4.y; bv[i + 2] = b4.z; bv[i + 3] = b4.w;
+        const float4 d4 = dt ? __ldg(reinterpret_cast<const float4 *>(dt + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+      }
       tc::tmem_wait();
       float hv[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int n = c0 + i;
-        const float t = tc::tanh_fast(__uint_as_float(r[i]) + bias[n]);
+        const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
         float h = t;
-        if (dt) h = t * dt[n] + hl[(size_t)(l - 1) * FW + n];
+        if (dt) h = t * dv[i] + FIT_SCR(L + l - 1, n);
         hv[i] = h;
-        if (act) {
-          tl[(size_t)l * FW + n] = t;
-          hl[(size_t)l * FW + n] = h;
-        }
+        FIT_SCR(l, n) = t;
+        FIT_SCR(L + l, n) = h;
       }
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(hv);
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(hv + 8);
@@ -1104,9 +1180,10 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int n = c0 + i;
-        s = fmaf(hl[(size_t)(L - 1) * FW + n], wf[n], s);
-        const float t = tl[(size_t)(L - 1) * FW + n];
-        g[i] = wf[n] * (dtL ? dtL[n] : 1.f) * (1.f - t * t);
+        const float wn = __ldg(wf + n);
+        s = fmaf(FIT_SCR(2 * L - 1, n), wn, s);
+        const float t = FIT_SCR(L - 1, n);
+        g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - t * t);
       }
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(g);
     }
@@ -1139,16 +1216,25 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
     for (int c0 = 0; c0 < FW; c0 += 16) {
       uint32_t r[16];
       tc::tmem_ld16_issue(td + lane_off + c0, r);
+      float wv[16], dv[16];
+#pragma unroll
+      for (int i = 0; i < 16; i += 4) {
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wf + c0 + i));
+        wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
+        const float4 d4 =
+            res_lm1 ? __ldg(reinterpret_cast<const float4 *>(dtm1 + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+      }
       tc::tmem_wait();
       float gz[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int n = c0 + i;
         float g = __uint_as_float(r[i]);
-        if (res_l) g += (l == L - 1) ? wf[n] : gh[n];
-        const float t = tl[(size_t)(l - 1) * FW + n];
-        gz[i] = g * (res_lm1 ? dtm1[n] : 1.f) * (1.f - t * t);
-        if (act && res_lm1) gh[n] = g;
+        if (res_l) g += (l == L - 1) ? wv[i] : FIT_SCR(2 * L, n);
+        const float t = FIT_SCR(l - 1, n);
+        gz[i] = g * dv[i] * (1.f - t * t);
+        if (res_lm1) FIT_SCR(2 * L, n) = g;
       }
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(gz);
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(gz + 8);
@@ -1184,6 +1270,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(td, 256);
+#undef FIT_SCR
 }
 
 template <int FW>
@@ -1191,13 +1278,16 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
                    float *Eatom, double *energy, int *err, cudaStream_t st) {
   const size_t smem = round1k(128 * FW * 2) + 2 * (kFitBufA + kFitBufB);
   DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int tile0 = 0;  // scratch tiles of 128 rows, consecutive over the centre types
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
     if (!cnt) continue;
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
-    k_mix_fit<FW><<<(Mrows + 127) / 128, 128, smem, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
-                                                          D.seg);
+    const int ntile = (Mrows + 127) / 128;
+    k_mix_fit<FW><<<ntile, 128, smem, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err, D.seg,
+                                            tile0);
+    tile0 += ntile;
     count_launch();
     DPB_LAUNCH_CHECK();
   }
@@ -1214,6 +1304,11 @@ int mixed_supported(const DevModel &M) {
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static int n2_of(const DevModel &M) { return (M.E2 + 15) / 16 * 16; }
+
+// Fitting scratch rounds each centre type's rows up to whole 128-row tiles.
+size_t mixed_workspace_fixed(const DevModel &M) {
+  return (size_t)127 * M.ntypes * (2 * M.nfit + 1) * M.FW[0] * 4 + 1024;
+}
 
 size_t mixed_workspace_per_atom(const DevModel &M) {
   const int FW = M.FW[0], K0 = M.A * M.E2;
@@ -1330,14 +1425,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);
   {
-    const size_t smem = (size_t)4 * (20 * M.E2 + K0 + 20 * M.A) * 4;
-    if (M.E2 == 100) {
-      DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_dT<100, 112>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_mix_dT<100, 112><<<(unsigned)((NF + 3) / 4), 128, smem, st>>>(M, (int)NF, T, dG, dTb);
-    } else {
-      DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_dT<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_mix_dT<64, 64><<<(unsigned)((NF + 3) / 4), 128, smem, st>>>(M, (int)NF, T, dG, dTb);
-    }
+    if (M.E2 == 100) k_mix_dT<100, 112><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dG, dTb);
+    else k_mix_dT<64, 64><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dG, dTb);
     count_launch();
     DPB_LAUNCH_CHECK();
   }
