@@ -191,7 +191,8 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
 // ---------------------------------------------------------------- embedding forward (BF16 tcgen05)
 // Per block of 8 centre atoms of type ti: neighbour rows with s(r) != 0 are
 // compacted block-wide into 128-row tiles.  Per tile (thread = row = TMEM lane):
-//   layer 0 (1 -> E0) FP32 on CUDA cores, h0 -> A0 (bf16)
+//   layer 0 (1 -> E0) FP32 on CUDA cores (tanh.approx.f32: its ~2^-11 relative
+//           error is below the BF16 rounding of the h0 operand), h0 -> A0 (bf16)
 //   D  = A0 . W1   (tcgen05, 128 x N1)   -> h1 = tanh(D + b1) + rep(h0) -> A1
 //   D  = A1 . W2   (tcgen05, 128 x N2)   -> h2 = tanh(D + b2) + rep(h1) -> H2
 //   D3 += Rblk . H2 (tcgen05, M = 8 slots x 16 channels, K = 128 rows)
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
           __syncthreads();  // net image visible
           float h0[E0];
 #pragma unroll
-          for (int k = 0; k < E0; ++k) h0[k] = tanhf(fmaf(st, sm[k], sm[E0 + k]));
+          for (int k = 0; k < E0; ++k) h0[k] = tc::tanh_fast(fmaf(st, sm[k], sm[E0 + k]));
 #pragma unroll
           for (int k8 = 0; k8 < MD::K1; k8 += 8) {
             float t[8];
@@ -771,7 +772,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
             float h0[E0], d0[E0];
 #pragma unroll
             for (int k = 0; k < E0; ++k) {
-              const float t = tanhf(fmaf(st, sm[k], sm[E0 + k]));
+              const float t = tc::tanh_fast(fmaf(st, sm[k], sm[E0 + k]));
               h0[k] = t;
               d0[k] = (1.f - t * t) * sm[k];
             }
