@@ -107,6 +107,22 @@ FIT_FLOP_ATOM = 2 * 2 * (1600 * 240 + 2 * 240 * 240)                       # fwd
 G_FLOP_ATOM = 2 * 16 * 100 * 10 * 3                                        # G and its adjoint
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The slowest rank's time: every rank contributes its own figure and all
+    get the maximum (a no-op on one rank)."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of independent replicas: the units every rank
+    processed over the slowest rank's time."""
+    return units_per_rank * world / seconds
+
+
 def rows_within_rcut(pos_sorted, nbrs, type_count, sel, box, rcut):
     """Average number of (centre, neighbour) rows with 0 < r < rcut."""
     import torch
@@ -252,10 +268,7 @@ def gpu_arm(args, rank, world, local_rank):
         ms = s.elapsed_time(e)
         launches = lib.dpb_kernel_launch_count() - l0 + sim._graph_launches_replayed
         sim._graph_launches_replayed = 0
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), launches
+        return max_over_ranks(ms, dist), launches
 
     results = {}
     for prec in (["fp32", "mixed"] if args.precision == "mixed" else ["fp32"]):
@@ -286,7 +299,7 @@ def gpu_arm(args, rank, world, local_rank):
     head = "mixed" if "mixed" in results and "error" not in results["mixed"] else "fp32"
     R = results[head]
     K = args.steps
-    value = N * K * world / (R["ms"] / 1e3)
+    value = job_rate(N * K, world, R["ms"] / 1e3)
     # rows with s(r) != 0 (the work the kernels do; padded slots are skipped)
     sim = R["sim"]
     ptrs = None
@@ -363,11 +376,8 @@ def gpu_arm(args, rank, world, local_rank):
         torch.cuda.synchronize()
         dt_e2e = time.perf_counter() - t0
         barrier()
-        t = torch.tensor([dt_e2e], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt_e2e = float(t.item())
-        line["e2e"] = {"value": N * K * world / dt_e2e, "unit": "atom-steps/s",
+        dt_e2e = max_over_ranks(dt_e2e, dist)
+        line["e2e"] = {"value": job_rate(N * K, world, dt_e2e), "unit": "atom-steps/s",
                        "h2d_bytes_per_step": int(2 * N * 3 * 8 / K),
                        "d2h_bytes_per_step": int(2 * N * 3 * 4),
                        "api": "Simulation.setPosition + setVelocity + run(K) returning the per-step trajectory"}

@@ -17,6 +17,7 @@ import torch
 
 from . import _lib
 from .engine import DeviceModel, NeighborBuilder, sort_by_type, _ptr, _stream
+from . import dump
 from .md_utils import knbr_from_counts
 from .systems import MASS_UNIT_CONVERSION, TEMP_UNIT_CONVERSION
 from .utils import load_model
@@ -158,6 +159,12 @@ class Simulation:
         if ct is not None:
             z2i = {z: i for i, z in enumerate(ct)}
             self._type_idx = np.array([z2i[int(z)] for z in self._type_idx], dtype=np.int32)
+        if type_symbols is None and ct is not None:
+            type_symbols = [dump.SYMBOLS[int(z)] for z in ct]
+        if type_symbols is not None and len(type_symbols) < int(self._type_idx.max()) + 1:
+            raise ValueError("type_symbols has length %d but type_idx needs %d types"
+                             % (len(type_symbols), int(self._type_idx.max()) + 1))
+        self._type_symbols = list(type_symbols) if type_symbols is not None else None
         self._mass_per_type = np.asarray(mass, dtype=np.float64)
         self._mass = self._mass_per_type[self._type_idx]
         self._step_chunk_size = max(10, min(100, 100000 // (self._natoms * self._n_bead)))
@@ -318,8 +325,10 @@ class Simulation:
         (deepmd_jax/md.py:874-964).  ``trajectory=False`` keeps every frame on
         the device (no per-step copy to the host) and returns None; the state
         stays readable through the getters."""
-        if dump_prefix is not None:
-            raise NotImplementedError("XYZ dumping is outside this engine; use the returned trajectory")
+        dumps, interval = dump.prepare(self._type_idx, self._type_symbols, self._n_bead, self.report_interval,
+                                       dump_interval, dump_prefix, dump_content, dump_mode)
+        if dumps:
+            trajectory = False                  # frames stream to the files instead (md.py:907-938)
         steps = int(steps)
         first = self._is_initial_state
         L = steps + int(first)
@@ -334,6 +343,9 @@ class Simulation:
         tic_run = tic = time()
         if first:
             self._report_row(tic)
+        if dumps and first and self.step % interval == 0:
+            dump.write_frame(dumps, self.getPosition(), self.getVelocity(),
+                             self.getCentroidPosition() if self._is_pimd else None, self._box, step=self.step)
         self._is_initial_state = False
         NF3 = self._natoms * self._n_bead * 3
         cap = self._step_chunk_size
@@ -347,7 +359,7 @@ class Simulation:
         while done < steps:
             n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
             _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
-            if trajectory:
+            if trajectory or dumps:
                 self._run_chunk(n, buf_p[:n], buf_v[:n])
             else:
                 self._run_chunk(n, None, None)
@@ -366,6 +378,8 @@ class Simulation:
                 self._resize_capacity()
                 continue
             overflow_twice = False
+            if dumps:
+                self._write_dump_frames(dumps, interval, buf_p, buf_v, n)
             if not trajectory:
                 done += n
                 self.step += n
@@ -399,6 +413,28 @@ class Simulation:
         if self._is_pimd and traj is not None:
             traj["centroid"] = np.stack([self._centroid(p) for p in traj["position"]])
         return traj
+
+    def _unpack_frame(self, p_row, v_row):
+        """User-order positions and velocities of one device frame row."""
+        P, N = self._n_bead, self._natoms
+        p = p_row.view(P, N, 3).cpu().numpy().astype(np.float64)
+        m = v_row.view(P, N, 3).cpu().numpy().astype(np.float64)
+        pos, mom = np.empty_like(p), np.empty_like(m)
+        pos[:, self._perm] = p
+        mom[:, self._perm] = m
+        vel = mom / (self._mass * MASS_UNIT_CONVERSION)[None, :, None]
+        return (pos, vel) if self._is_pimd else (pos[0], vel[0])
+
+    def _write_dump_frames(self, dumps, interval, buf_p, buf_v, n):
+        """Frames of the last chunk whose step is a multiple of the dump
+        interval, copied from the device and appended to the XYZ files."""
+        for i in range(n):
+            step = self.step + i + 1
+            if step % interval:
+                continue
+            pos, vel = self._unpack_frame(buf_p[i], buf_v[i])
+            cen = self._centroid(pos) if self._is_pimd else None
+            dump.write_frame(dumps, pos, vel, cen, self._box, step=step)
 
     def _resize_capacity(self):
         pos = self.getPosition()

@@ -125,3 +125,28 @@ def test_simulation_getters_and_force_match_eval():
     assert abs(sim.getEnergy() - ref["energy"]) < 1e-4 * max(1.0, abs(ref["energy"]))
     assert np.allclose(sim.getPosition(), w["position"], atol=1e-5)
     assert np.allclose(sim.getVelocity(), w["velocity"], rtol=1e-6, atol=1e-9)
+
+
+def test_xyz_dumps_match_the_trajectory(tmp_path):
+    """run(dump_prefix=...) streams every dump_interval-th frame (step 0
+    included) to extended-XYZ files and returns None (md.py:907-964); the
+    frames equal the in-memory trajectory of the same run."""
+    from deepmd_jax_b200 import dump
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+
+    def sim():
+        return Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.5, w["position"],
+                          initial_velocity=w["velocity"], report_interval=10, type_symbols=["O", "H"],
+                          verbose=False)
+    traj = sim().run(20)
+    prefix = str(tmp_path / "run")
+    assert sim().run(20, dump_interval=5, dump_prefix=prefix, dump_content="all") is None
+    fp = dump.read_xyz(prefix + "_position.xyz")
+    fv = dump.read_xyz(prefix + "_velocity.xyz")
+    assert [f[2].split("step=")[1].split()[0] for f in fp] == ["0", "5", "10", "15", "20"]
+    for k, step in enumerate(range(0, 21, 5)):
+        assert fp[k][0][:3] == [("O" if t == 0 else "H") for t in w["type_idx"][:3]]
+        assert np.abs(fp[k][1] - traj["position"][step]).max() < 2e-5
+        assert np.abs(fv[k][1] - traj["velocity"][step]).max() < 2e-6

@@ -85,3 +85,32 @@ def test_packed_batch_layout():
                 n = int(it["type_count"][t])
                 assert np.all(b.seg[rows[:n]] == it["seg0"] + f)
                 assert np.all(b.seg[rows[n:]] == -(it["seg0"] + f) - 1)
+
+
+def test_xyz_dump_format_and_options(tmp_path):
+    """Trajectory dump files (deepmd_jax/md_utils.py:30-256): names, option
+    errors and the extended-XYZ frame text."""
+    from deepmd_jax_b200 import dump
+    prefix = str(tmp_path / "traj")
+    with pytest.raises(ValueError, match="type_symbols"):
+        dump.prepare([0, 1], None, 1, 10, dump_prefix=prefix)
+    with pytest.raises(ValueError, match="centroid"):
+        dump.prepare([0, 1], ["O", "H"], 1, 10, dump_prefix=prefix, dump_content=["centroid"])
+    with pytest.raises(ValueError, match="requires dump_prefix"):
+        dump.prepare([0, 1], ["O", "H"], 1, 10, dump_content=["velocity"])
+    assert dump.normalize_content("positions", 4) == ("position", "centroid")
+    assert dump.normalize_content("all", 1) == ("position", "velocity")
+    d, k = dump.prepare([0, 1, 1], ["O", "H"], 1, 10, dump_interval=5, dump_prefix=prefix, dump_content="all")
+    assert k == 5 and [x[1] for x in d] == [prefix + "_position.xyz", prefix + "_velocity.xyz"]
+    pos = np.array([[1.0, 2.0, 3.0], [0.5, 0.25, 0.125], [4.0, 5.0, 6.0]])
+    dump.write_frame(d, pos, 2 * pos, None, [12.42, 12.42, 12.42], step=5)
+    text = open(prefix + "_position.xyz").read().splitlines()
+    assert text[0] == "3"
+    assert text[1] == ('Lattice="12.42000000 0.00000000 0.00000000 0.00000000 12.42000000 0.00000000 0.00000000 '
+                       '0.00000000 12.42000000" Properties=species:S:1:pos:R:3 step=5 pbc="T T T"')
+    assert text[2] == "O  1.00000000 2.00000000 3.00000000"
+    frames = dump.read_xyz(prefix + "_velocity.xyz")
+    assert frames[0][0] == ["O", "H", "H"] and np.allclose(frames[0][1], 2 * pos)
+    d2, _ = dump.prepare([0, 1, 1], ["O", "H"], 2, 10, dump_prefix=prefix)
+    assert [x[1] for x in d2] == [prefix + "_position_bead0.xyz", prefix + "_position_bead1.xyz",
+                                  prefix + "_centroid.xyz"]
