@@ -17,5 +17,5 @@ int eval_impl(const dpb_model *m, int precision, const float *pos, const int32_t
 int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
                      const int *type_count, const int *sel, const float box[3], const float *ref_box, float rc,
                      int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status, void *workspace,
-                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream);
+                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream, const float *dbox = nullptr);
 }  // namespace dpb

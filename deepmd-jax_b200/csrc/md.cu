@@ -1,5 +1,6 @@
-// Device-resident MD engine: velocity Verlet (NVE), Nose-Hoover chain (NVT)
-// and ring-polymer BAOAB with the PILE-L thermostat (PIMD NVT).
+// Device-resident MD engine: velocity Verlet (NVE), Nose-Hoover chain (NVT),
+// ring-polymer BAOAB with the PILE-L thermostat (PIMD NVT) and the MTK
+// barostat with Nose-Hoover chains (NPT, orthorhombic, coupled axis groups).
 //
 // One step (the reference's scan body, deepmd_jax/md.py:763-795):
 //   1. soft neighbour update: max drift of the canonical positions since the
@@ -53,8 +54,12 @@ __global__ void k_md_begin(MdScalars *sc) {
 // pre-step state (md.py:638-640).
 __global__ void k_md_drift(const float *__restrict__ pos, const float *__restrict__ mom,
                            const float *__restrict__ ref_pos, int NF, float3 L, float3 scale, float3 RB,
-                           MdScalars *sc, uint32_t *status) {
+                           MdScalars *sc, uint32_t *status, const float *__restrict__ dbox) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dbox) {  // NPT: the current box lives on the device (single frame)
+    L = make_float3(dbox[0], dbox[1], dbox[2]);
+    scale = make_float3(__fdiv_rn(RB.x, L.x), __fdiv_rn(RB.y, L.y), __fdiv_rn(RB.z, L.z));
+  }
   float dn = 0.f;
   bool bad = false;
   if (g < NF) {
@@ -76,7 +81,23 @@ __global__ void k_md_drift(const float *__restrict__ pos, const float *__restric
   if (bad) atomicOr(status, DPB_ST_NONFINITE);
 }
 
-__global__ void k_md_decide(MdScalars *sc, float threshold) {
+// NPT (dbox != NULL): the allowed drift shrinks with the box, safe scale
+// 1.02 max(ref / box) (md.py:727-731), and status bit 1 flags a box that
+// shrank past the skin or below 2 (rcut + skin) (md.py:630-634).
+__global__ void k_md_decide(MdScalars *sc, float threshold, const float *__restrict__ dbox, float3 RB, float rc,
+                            float skin, uint32_t *status) {
+  if (dbox) {
+    const float L[3] = {dbox[0], dbox[1], dbox[2]}, R[3] = {RB.x, RB.y, RB.z};
+    float smax = 0.f, shrink = -1e30f, lmin = 1e30f, rmin = 1e30f;
+    for (int a = 0; a < 3; ++a) {
+      smax = fmaxf(smax, R[a] / L[a]);
+      shrink = fmaxf(shrink, 1.f - L[a] / R[a]);
+      lmin = fminf(lmin, L[a]);
+      rmin = fminf(rmin, R[a]);
+    }
+    threshold = ((rc + skin) - rc * (smax * 1.02f)) / 2.f - rmin * 1e-6f;
+    if (shrink > 0.8f * skin / (rc + skin) || lmin < 2.f * (rc + skin) * 1.02f) atomicOr(status, DPB_ST_BOX_SHRUNK);
+  }
   const unsigned r = __uint_as_float(sc->drift_bits) > threshold ? 1u : 0u;
   sc->rebuild = r;
   sc->nrebuild += r;
@@ -121,15 +142,14 @@ __global__ void k_vv_kick(float *__restrict__ mom, const float *__restrict__ for
 }
 
 // One MTK Nose-Hoover chain substep of length delta/2 (jax_md
-// nose_hoover_chain, wrapped by deepmd_jax/routine.py:147-158), FP64.
-// which == 1: first half step, uses chain_ke; which == 2: second half step,
-// chain_ke := KE of the current momenta first.
-__global__ void k_nhc_substep(MdScalars *sc, int L, double kT, double tau, double delta, int which) {
-  if (which == 2) sc->chain_ke = sc->ke;
+// nose_hoover_chain, wrapped by deepmd_jax/routine.py:147-158), FP64, on a
+// chain (xi, p, Q) of L links over `dof` degrees of freedom with kinetic
+// energy ke (updated); returns the momentum scale.
+__device__ double nhc_half(double *xi, double *p, double *Q, double &ke, double dof, int L, double kT, double tau,
+                           double delta) {
   // update_mass (kT fixed): Q = kT tau^2, Q0 *= DOF
-  for (int m = 0; m < L; ++m) sc->Q[m] = kT * tau * tau;
-  sc->Q[0] *= sc->dof;
-  double *p = sc->pxi, *Q = sc->Q;
+  for (int m = 0; m < L; ++m) Q[m] = kT * tau * tau;
+  Q[0] *= dof;
   const double d2 = delta / 2, d4 = d2 / 2, d8 = d4 / 2;
   const int M = L - 1;
   double G = p[M - 1] * p[M - 1] / Q[M - 1] - kT;
@@ -139,20 +159,27 @@ __global__ void k_nhc_substep(MdScalars *sc, int L, double kT, double tau, doubl
     const double sc_ = exp(-d8 * p[m + 1] / Q[m + 1]);
     p[m] = sc_ * (sc_ * p[m] + d4 * G);
   }
-  G = 2.0 * sc->chain_ke - sc->dof * kT;
+  G = 2.0 * ke - dof * kT;
   double s1 = exp(-d8 * p[1] / Q[1]);
   p[0] = s1 * (s1 * p[0] + d4 * G);
   const double scale = exp(-d2 * p[0] / Q[0]);
-  sc->chain_ke *= scale * scale;
-  for (int m = 0; m < L; ++m) sc->xi[m] += d2 * p[m] / Q[m];
-  G = 2.0 * sc->chain_ke - sc->dof * kT;
+  ke *= scale * scale;
+  for (int m = 0; m < L; ++m) xi[m] += d2 * p[m] / Q[m];
+  G = 2.0 * ke - dof * kT;
   for (int m = 0; m < M; ++m) {
     const double sm = exp(-d8 * p[m + 1] / Q[m + 1]);
     p[m] = sm * (sm * p[m] + d4 * G);
     G = p[m] * p[m] / Q[m] - kT;
   }
   p[M] += d4 * G;
-  sc->scale = scale;
+  return scale;
+}
+
+// which == 1: first half step, uses chain_ke; which == 2: second half step,
+// chain_ke := KE of the current momenta first.
+__global__ void k_nhc_substep(MdScalars *sc, int L, double kT, double tau, double delta, int which) {
+  if (which == 2) sc->chain_ke = sc->ke;
+  sc->scale = nhc_half(sc->xi, sc->pxi, sc->Q, sc->chain_ke, sc->dof, L, kT, tau, delta);
 }
 
 __global__ void k_scale_mom(float *__restrict__ mom, int n, const MdScalars *__restrict__ sc) {
@@ -163,6 +190,174 @@ __global__ void k_scale_mom(float *__restrict__ mom, int n, const MdScalars *__r
 __global__ void k_copy_frame(const float *__restrict__ src, float *__restrict__ dst, int n) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e < n) dst[e] = src[e];
+}
+
+// ---------------------------------------------------------------- NPT (MTK barostat)
+// State of the barostat (deepmd_jax/routine.py:161-456): per coupled group g
+// the log box scale Rb, its momentum Pb and mass Mb; the per-group dU/d(eps)
+// of the last force evaluation (the reference caches it between steps); the
+// per-axis sum of p^2/m and the per-axis factors of the two propagators.
+struct NptScalars {
+  int G;
+  int ngrp[3];          // axes in group g
+  int gid[3];           // group of axis a, -1 for a fixed axis
+  double ref[3];        // the integrator's reference box
+  double Rb[3], Pb[3], Mb[3];
+  double dUde[3];
+  double ke2[3];
+  double a2[3], b2[3];  // exp_iL2: p <- p a2 + F b2
+  double a1[3], b1[3];  // exp_iL1: r <- r a1 + (p / m) b1
+  double pressure;
+  double bxi[kMaxChain], bp[kMaxChain], bQ[kMaxChain];
+  double bke, bdof;
+};
+
+// sinh(x)/x by the series the reference uses (routine.py:290-292)
+__device__ __forceinline__ double sinhx_x(double x) {
+  const double x2 = x * x;
+  return 1.0 + x2 / 6.0 + x2 * x2 / 120.0 + x2 * x2 * x2 / 5040.0 + x2 * x2 * x2 * x2 / 362880.0 +
+         x2 * x2 * x2 * x2 * x2 / 39916800.0;
+}
+
+__device__ double npt_volume(const NptScalars *np) {
+  double V = 1.0;
+  for (int a = 0; a < 3; ++a) V *= np->ref[a] * (np->gid[a] >= 0 ? exp(np->Rb[np->gid[a]]) : 1.0);
+  return V;
+}
+
+// G_g = KE2_g + (n_g / N_f) KE2_total - dU/deps_g - P V n_g   (routine.py:279-286)
+__device__ void npt_box_force(const NptScalars *np, double V, double Nf, double *Gout) {
+  const double tot = np->ke2[0] + np->ke2[1] + np->ke2[2];
+  for (int g = 0; g < np->G; ++g) {
+    double k = 0.0;
+    for (int a = 0; a < 3; ++a)
+      if (np->gid[a] == g) k += np->ke2[a];
+    Gout[g] = k + (np->ngrp[g] / Nf) * tot - np->dUde[g] - np->pressure * V * np->ngrp[g];
+  }
+}
+
+// Start of a step: box masses, barostat and thermostat half steps
+// (routine.py:415-426); the thermostat scale is applied by k_npt_scale_ke2.
+__global__ void k_npt_begin(MdScalars *sc, NptScalars *np, int Lt, int Lb, double kT, double tau_t, double tau_p,
+                            double dt, int N) {
+  for (int g = 0; g < np->G; ++g) np->Mb[g] = np->ngrp[g] * (N + 1.0) * kT * tau_p * tau_p;
+  const double bs = nhc_half(np->bxi, np->bp, np->bQ, np->bke, np->bdof, Lb, kT, tau_p, dt);
+  for (int g = 0; g < np->G; ++g) np->Pb[g] *= bs;
+  sc->scale = nhc_half(sc->xi, sc->pxi, sc->Q, sc->chain_ke, sc->dof, Lt, kT, tau_t, dt);
+  np->ke2[0] = np->ke2[1] = np->ke2[2] = 0.0;
+}
+
+// Per-axis sum of p^2 / m over the atoms (FP64 block sums), optionally after
+// scaling the momenta; with ke != NULL also the kinetic energy.
+__device__ void npt_reduce3(float v0, float v1, float v2, double *out, double *ke) {
+  __shared__ float part[3][8];
+  float v[3] = {v0, v1, v2};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) v[a] = warp_sum(v[a]);
+  if ((threadIdx.x & 31) == 0)
+    for (int a = 0; a < 3; ++a) part[a][threadIdx.x >> 5] = v[a];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      for (int a = 0; a < 3; ++a) t[a] += part[a][w];
+    for (int a = 0; a < 3; ++a) atomicAdd(&out[a], t[a]);
+    if (ke) atomicAdd(ke, 0.5 * (t[0] + t[1] + t[2]));
+  }
+}
+
+// Thermostat scale of the first half step, then the per-axis sums.
+__global__ void k_npt_scale_ke2(float *__restrict__ mom, const float *__restrict__ inv_mass, int N,
+                                const MdScalars *__restrict__ sc, NptScalars *np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float k[3] = {0.f, 0.f, 0.f};
+  if (i < N) {
+    const float s = (float)sc->scale, im = inv_mass[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float p = mom[i * 3 + a] * s;
+      mom[i * 3 + a] = p;
+      k[a] = p * p * im;
+    }
+  }
+  npt_reduce3(k[0], k[1], k[2], np->ke2, nullptr);
+}
+
+// First barostat kick with the cached dU/deps, the box update and the
+// propagator factors (routine.py:383-396, 294-311).
+__global__ void k_npt_box1(NptScalars *np, float *boxd, double dt, int N) {
+  const double Nf = 3.0 * N;
+  double Ge[3];
+  npt_box_force(np, npt_volume(np), Nf, Ge);
+  double Vb[3] = {0.0, 0.0, 0.0}, tr = 0.0;
+  for (int g = 0; g < np->G; ++g) {
+    np->Pb[g] += 0.5 * dt * Ge[g];
+    Vb[g] = np->Pb[g] / np->Mb[g];
+    tr += np->ngrp[g] * Vb[g];
+  }
+  for (int a = 0; a < 3; ++a) {
+    const double va = np->gid[a] >= 0 ? Vb[np->gid[a]] : 0.0;
+    const double x = (va + tr / Nf) * (0.5 * dt), x2 = x / 2;
+    np->a2[a] = exp(-x);
+    np->b2[a] = 0.5 * dt * sinhx_x(x2) * exp(-x2);
+    const double y = va * dt, y2 = y / 2;
+    np->a1[a] = exp(y);
+    np->b1[a] = dt * exp(y2) * sinhx_x(y2);
+  }
+  for (int g = 0; g < np->G; ++g) np->Rb[g] += Vb[g] * dt;
+  for (int a = 0; a < 3; ++a)
+    boxd[a] = (float)(np->ref[a] * (np->gid[a] >= 0 ? exp(np->Rb[np->gid[a]]) : 1.0));
+  np->ke2[0] = np->ke2[1] = np->ke2[2] = 0.0;
+}
+
+// p <- exp_iL2(p, F); r <- exp_iL1(r, p / m)
+__global__ void k_npt_move(float *__restrict__ pos, float *__restrict__ mom, const float *__restrict__ force,
+                           const float *__restrict__ inv_mass, int N3, const NptScalars *__restrict__ np) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N3) return;
+  const int a = e % 3;
+  const float p = mom[e] * (float)np->a2[a] + force[e] * (float)np->b2[a];
+  mom[e] = p;
+  pos[e] = pos[e] * (float)np->a1[a] + p * inv_mass[e / 3] * (float)np->b1[a];
+}
+
+// p <- exp_iL2(p, F) with the new forces; per-axis sums and the kinetic energy.
+__global__ void k_npt_kick2(float *__restrict__ mom, const float *__restrict__ force,
+                            const float *__restrict__ inv_mass, int N, MdScalars *sc, NptScalars *np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float k[3] = {0.f, 0.f, 0.f};
+  if (i < N) {
+    const float im = inv_mass[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float p = mom[i * 3 + a] * (float)np->a2[a] + force[i * 3 + a] * (float)np->b2[a];
+      mom[i * 3 + a] = p;
+      k[a] = p * p * im;
+    }
+  }
+  npt_reduce3(k[0], k[1], k[2], np->ke2, &sc->ke);
+}
+
+// Second barostat kick with the new dU/deps, then the thermostat and
+// barostat half steps (routine.py:398-436); the thermostat scale is applied
+// by k_scale_mom.
+__global__ void k_npt_end(MdScalars *sc, NptScalars *np, const double *__restrict__ virial, int Lt, int Lb,
+                          double kT, double tau_t, double tau_p, double dt, int N) {
+  for (int g = 0; g < np->G; ++g) np->dUde[g] = 0.0;
+  for (int a = 0; a < 3; ++a)
+    if (np->gid[a] >= 0) np->dUde[np->gid[a]] -= virial[a * 3 + a];  // dU/deps_a = -W_aa
+  double Ge[3];
+  npt_box_force(np, npt_volume(np), 3.0 * N, Ge);
+  double kb = 0.0;
+  for (int g = 0; g < np->G; ++g) {
+    np->Pb[g] += 0.5 * dt * Ge[g];
+    kb += 0.5 * np->Pb[g] * np->Pb[g] / np->Mb[g];
+  }
+  np->bke = kb;
+  sc->chain_ke = sc->ke;
+  sc->scale = nhc_half(sc->xi, sc->pxi, sc->Q, sc->chain_ke, sc->dof, Lt, kT, tau_t, dt);
+  const double bs = nhc_half(np->bxi, np->bp, np->bQ, np->bke, np->bdof, Lb, kT, tau_p, dt);
+  for (int g = 0; g < np->G; ++g) np->Pb[g] *= bs;
 }
 
 // Philox4x32-10 (Salmon et al., SC'11) and Box-Muller normals; stream:
@@ -309,6 +504,8 @@ struct dpb_md {
   uint32_t *status = nullptr;
   double *energy = nullptr, *virial = nullptr;
   MdScalars *sc = nullptr;
+  NptScalars *np = nullptr, *s_np = nullptr;  // NPT barostat state and its snapshot
+  float *s_box = nullptr;
   float *C = nullptr, *freqs = nullptr, *gamma = nullptr;
   void *nl_ws = nullptr, *ev_ws = nullptr;
   size_t nl_ws_bytes = 0, ev_ws_bytes = 0;
@@ -337,7 +534,21 @@ static int md_alloc_lists(dpb_md *m) {
 extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_md **out) {
   if (!model || !d || !out || d->natoms <= 0 || d->nbeads <= 0 || !d->type_idx || !d->mass_per_type || !d->sel)
     return DPB_ERR_INVALID_ARG;
-  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_PIMD_PILE) return DPB_ERR_INVALID_ARG;
+  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_NPT_NHC) return DPB_ERR_INVALID_ARG;
+  if (d->routine == DPB_MD_NPT_NHC) {
+    if (d->nbeads != 1 || d->chain_length < 2 || d->chain_length > kMaxChain || d->chain_length_p < 2 ||
+        d->chain_length_p > kMaxChain || !(d->tau_p > 0.0))
+      return DPB_ERR_UNSUPPORTED;
+    int G = -1;
+    for (int a = 0; a < 3; ++a) {
+      if (d->couple_groups[a] < -1 || d->couple_groups[a] > 2) return DPB_ERR_INVALID_ARG;
+      G = std::max(G, d->couple_groups[a]);
+    }
+    if (G < 0) return DPB_ERR_INVALID_ARG;  // no moving axis: use NVT
+    for (int g = 0; g <= G; ++g)
+      if (d->couple_groups[0] != g && d->couple_groups[1] != g && d->couple_groups[2] != g)
+        return DPB_ERR_INVALID_ARG;  // groups must be numbered 0..G-1
+  }
   if (d->routine == DPB_MD_PIMD_PILE && (d->nbeads < 2 || d->nbeads > kMaxBeads || !d->nm_transform || !d->nm_freqs))
     return DPB_ERR_INVALID_ARG;
   if (d->routine != DPB_MD_PIMD_PILE && d->nbeads != 1) return DPB_ERR_INVALID_ARG;
@@ -383,6 +594,11 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   rc_ |= md_alloc(m, (void **)&m->s_force, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_ref, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_sc, sizeof(MdScalars));
+  if (d->routine == DPB_MD_NPT_NHC) {
+    rc_ |= md_alloc(m, (void **)&m->np, sizeof(NptScalars));
+    rc_ |= md_alloc(m, (void **)&m->s_np, sizeof(NptScalars));
+    rc_ |= md_alloc(m, (void **)&m->s_box, 12);
+  }
   rc_ |= md_alloc_lists(m);
   if (rc_) { dpb_md_destroy(m); return DPB_ERR_CUDA; }
   // masses in eV fs^2 / A^2 (md.py:24), sorted order
@@ -501,10 +717,14 @@ extern "C" int dpb_md_get_state(const dpb_md *m, double *pos, double *vel, doubl
   return rc;
 }
 
+// m->box is the neighbour list's reference box; under NPT the current box is
+// the device copy m->boxd and the list canonicalises into the reference box.
 static int md_build_list(dpb_md *m, const unsigned *gate, cudaStream_t st) {
   const float rc = m->model->dm.rcut + (float)m->d.skin;
+  const bool npt = m->d.routine == DPB_MD_NPT_NHC;
   return nlist_build_impl(m->pos, nullptr, m->N, m->P, m->ntypes, m->type_count, m->sel, m->box, nullptr, rc,
-                          m->nbrs, m->ref_pos, nullptr, m->status, m->nl_ws, m->nl_ws_bytes, gate, st);
+                          m->nbrs, m->ref_pos, nullptr, m->status, m->nl_ws, m->nl_ws_bytes, gate, st,
+                          npt ? m->boxd : nullptr);
 }
 
 static int md_forces(dpb_md *m, cudaStream_t st) {
@@ -543,6 +763,26 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
     h.scale = 1.0;
     h.twork = 0.0;
     cudaMemcpy(sc, &h, sizeof(h), cudaMemcpyHostToDevice);
+    if (m->d.routine == DPB_MD_NPT_NHC) {  // npt init_fn (routine.py:322-350)
+      NptScalars n;
+      std::memset(&n, 0, sizeof(n));
+      std::vector<double> vir(9);
+      cudaMemcpy(vir.data(), m->virial, 72, cudaMemcpyDeviceToHost);
+      n.G = 0;
+      for (int a = 0; a < 3; ++a) {
+        n.gid[a] = m->d.couple_groups[a];
+        if (n.gid[a] >= 0) { n.ngrp[n.gid[a]]++; n.G = std::max(n.G, n.gid[a] + 1); }
+        n.ref[a] = m->box[a];
+      }
+      for (int g = 0; g < n.G; ++g) n.Mb[g] = n.ngrp[g] * (m->N + 1.0) * m->kT * m->d.tau_p * m->d.tau_p;
+      for (int a = 0; a < 3; ++a)
+        if (n.gid[a] >= 0) n.dUde[n.gid[a]] -= vir[a * 3 + a];
+      n.pressure = m->d.pressure;
+      for (int k = 0; k < m->d.chain_length_p; ++k) n.bQ[k] = m->kT * m->d.tau_p * m->d.tau_p;
+      n.bdof = n.G;
+      n.bQ[0] *= n.bdof;
+      if (cudaMemcpy(m->np, &n, sizeof(n), cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+    }
   }
   return DPB_OK;
 }
@@ -555,14 +795,33 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel)
   const float dt = (float)m->d.dt;
   prof_begin(PROF_NLIST, st);
   k_md_begin<<<1, 1, 0, st>>>(sc);
-  k_md_drift<<<nb, 256, 0, st>>>(m->pos, m->mom, m->ref_pos, NF, L, make_float3(1.f, 1.f, 1.f), L, sc, m->status);
-  k_md_decide<<<1, 1, 0, st>>>(sc, m->threshold);
+  const bool npt = m->d.routine == DPB_MD_NPT_NHC;
+  k_md_drift<<<nb, 256, 0, st>>>(m->pos, m->mom, m->ref_pos, NF, L, make_float3(1.f, 1.f, 1.f), L, sc, m->status,
+                                 npt ? m->boxd : nullptr);
+  k_md_decide<<<1, 1, 0, st>>>(sc, m->threshold, npt ? m->boxd : nullptr, L, m->model->dm.rcut, (float)m->d.skin,
+                               m->status);
   count_launch(3);
   DPB_LAUNCH_CHECK();
   int rc = md_build_list(m, &sc->rebuild, st);
   if (rc) return rc;
   prof_end(PROF_NLIST, st);
-  if (m->d.routine == DPB_MD_PIMD_PILE) {
+  if (npt) {  // MTK NPT step (routine.py:403-436)
+    const int N = m->N, nbn = (N + 255) / 256;
+    const int Lt = m->d.chain_length, Lb = m->d.chain_length_p;
+    const double kT = m->kT, tt = m->d.tau_t, tp = m->d.tau_p, dtd = m->d.dt;
+    k_npt_begin<<<1, 1, 0, st>>>(sc, m->np, Lt, Lb, kT, tt, tp, dtd, N);
+    k_npt_scale_ke2<<<nbn, 256, 0, st>>>(m->mom, m->inv_mass, N, sc, m->np);
+    k_npt_box1<<<1, 1, 0, st>>>(m->np, m->boxd, dtd, N);
+    k_npt_move<<<nb3, 256, 0, st>>>(m->pos, m->mom, m->force, m->inv_mass, NF3, m->np);
+    count_launch(4);
+    DPB_LAUNCH_CHECK();
+    rc = md_forces(m, st);
+    if (rc) return rc;
+    k_npt_kick2<<<nbn, 256, 0, st>>>(m->mom, m->force, m->inv_mass, N, sc, m->np);
+    k_npt_end<<<1, 1, 0, st>>>(sc, m->np, m->virial, Lt, Lb, kT, tt, tp, dtd, N);
+    k_scale_mom<<<nb3, 256, 0, st>>>(m->mom, NF3, sc);
+    count_launch(3);
+  } else if (m->d.routine == DPB_MD_PIMD_PILE) {
     PimdParams pp;
     pp.P = m->P; pp.N = m->N; pp.dt = dt; pp.kT = (float)m->kT; pp.L = L; pp.seed = m->d.seed; pp.tag = 1u;
     k_pimd_baoa<<<(m->N * 3 + 127) / 128, 128, 0, st>>>(m->pos, m->mom, m->force, m->mass, m->C, m->freqs,
@@ -640,6 +899,21 @@ extern "C" int dpb_md_report(dpb_md *m, dpb_md_report_t *r) {
   r->chain_length = m->d.chain_length;
   r->chain_dof = h.dof;
   for (int k = 0; k < kMaxChain; ++k) { r->chain_xi[k] = h.xi[k]; r->chain_p[k] = h.pxi[k]; r->chain_Q[k] = h.Q[k]; }
+  for (int a = 0; a < 3; ++a) r->box[a] = m->box[a];
+  if (m->np) {
+    NptScalars n;
+    cudaMemcpy(&n, m->np, sizeof(n), cudaMemcpyDeviceToHost);
+    r->ngroups = n.G;
+    for (int a = 0; a < 3; ++a) r->box[a] = n.ref[a] * (n.gid[a] >= 0 ? std::exp(n.Rb[n.gid[a]]) : 1.0);
+    for (int g = 0; g < 3; ++g) {
+      r->box_position[g] = n.Rb[g];
+      r->box_momentum[g] = n.Pb[g];
+      r->box_mass[g] = n.Mb[g];
+      r->dU_deps[g] = n.dUde[g];
+    }
+    r->baro_length = m->d.chain_length_p;
+    for (int k = 0; k < kMaxChain; ++k) { r->baro_xi[k] = n.bxi[k]; r->baro_p[k] = n.bp[k]; r->baro_Q[k] = n.bQ[k]; }
+  }
   return DPB_OK;
 }
 
@@ -662,14 +936,43 @@ extern "C" int dpb_md_snapshot(dpb_md *m, int restore) {
     bad |= cudaMemcpy(m->s_force, m->force, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->s_ref, m->ref_pos, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->s_sc, m->sc, sizeof(MdScalars), k) != cudaSuccess;
+    if (m->np) {
+      bad |= cudaMemcpy(m->s_np, m->np, sizeof(NptScalars), k) != cudaSuccess;
+      bad |= cudaMemcpy(m->s_box, m->boxd, 12, k) != cudaSuccess;
+    }
   } else {
     bad |= cudaMemcpy(m->pos, m->s_pos, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->mom, m->s_mom, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->force, m->s_force, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->ref_pos, m->s_ref, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->sc, m->s_sc, sizeof(MdScalars), k) != cudaSuccess;
+    if (m->np) {
+      bad |= cudaMemcpy(m->np, m->s_np, sizeof(NptScalars), k) != cudaSuccess;
+      bad |= cudaMemcpy(m->boxd, m->s_box, 12, k) != cudaSuccess;
+    }
   }
   return bad ? DPB_ERR_CUDA : DPB_OK;
+}
+
+extern "C" int dpb_md_set_skin(dpb_md *m, double skin, void *stream) {
+  if (!m || !(skin > 0.0)) return DPB_ERR_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
+  float cur[3];
+  if (cudaMemcpy(cur, m->boxd, 12, cudaMemcpyDeviceToHost) != cudaSuccess) return DPB_ERR_CUDA;
+  m->d.skin = skin;
+  for (int a = 0; a < 3; ++a) m->box[a] = cur[a];  // the list's new reference box
+  const float rc = m->model->dm.rcut, sk = (float)skin;
+  m->threshold = ((rc + sk) - rc) / 2.f - std::min(m->box[0], std::min(m->box[1], m->box[2])) * 1e-6f;
+  size_t need = 0;
+  if (dpb_nlist_workspace_bytes(m->N, m->P, m->box, (rc + sk) * 0.999f, &need)) return DPB_ERR_INVALID_ARG;
+  if (need > m->nl_ws_bytes) {
+    cudaFree(m->nl_ws);
+    m->allocs.erase(std::remove(m->allocs.begin(), m->allocs.end(), m->nl_ws), m->allocs.end());
+    m->nl_ws = nullptr;
+    m->nl_ws_bytes = need;
+    if (md_alloc(m, &m->nl_ws, need)) return DPB_ERR_CUDA;
+  }
+  return md_build_list(m, nullptr, (cudaStream_t)stream);
 }
 
 // Resize the neighbour capacity (overflow resolution, md.py:657-668) and

@@ -52,14 +52,22 @@ __global__ void nl_zero_kernel(int *__restrict__ a, int na, int *__restrict__ b,
   if (i < nb) b[i] = 0;
 }
 
+// dbox (device, (F,3)) replaces L and scale = RB / L when the box changes on
+// the device (NPT): the reference's canonicalize(coord, box) with the current
+// box (md_utils.py:364-373).
 __global__ void nl_canon_kernel(const float *__restrict__ pos, const int32_t *__restrict__ perm,
                                 int N, int F, float3 L, float3 scale, float3 RB, int3 nc,
                                 float *__restrict__ canon, int *__restrict__ atom_cell,
-                                int *__restrict__ cell_count, const unsigned *__restrict__ gate) {
+                                int *__restrict__ cell_count, const unsigned *__restrict__ gate,
+                                const float *__restrict__ dbox) {
   if (gate && *gate == 0u) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= N * F) return;
   int f = g / N, k = g - f * N;
+  if (dbox) {
+    L = make_float3(dbox[f * 3], dbox[f * 3 + 1], dbox[f * 3 + 2]);
+    scale = make_float3(__fdiv_rn(RB.x, L.x), __fdiv_rn(RB.y, L.y), __fdiv_rn(RB.z, L.z));
+  }
   int src = perm ? perm[k] : k;
   const float *p = pos + ((size_t)f * N + src) * 3;
   const float shrink = 0.9999995f;  // float32(1 - 5e-7)
@@ -273,7 +281,7 @@ namespace dpb {
 int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
                      const int *type_count, const int *sel, const float box[3], const float *ref_box, float rc,
                      int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status, void *workspace,
-                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream) {
+                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream, const float *dbox) {
   if (!pos || natoms <= 0 || nframes <= 0 || ntypes < 1 || ntypes > kMaxTypes || !type_count || !sel ||
       !box || !nbrs || !status || rc <= 0)
     return DPB_ERR_INVALID_ARG;
@@ -326,7 +334,7 @@ int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nfra
   float3 scale = make_float3(rb[0] / box[0], rb[1] / box[1], rb[2] / box[2]);
   int nb = (int)((NF + 255) / 256);
   nl_canon_kernel<<<nb, 256, 0, stream>>>(pos, perm, natoms, nframes, L, scale, P.L, P.nc, canon, atom_cell,
-                                          cell_count, gate);
+                                          cell_count, gate, dbox);
   nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C, gate);
   nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, natoms, nframes,
                                             g.ncell, gate);
@@ -349,7 +357,8 @@ extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms
                                int32_t *counts, uint32_t *status, void *workspace, size_t ws_bytes,
                                void *stream) {
   return dpb::nlist_build_impl(pos, perm, natoms, nframes, ntypes, type_count, sel, box, ref_box, rc, nbrs,
-                               ref_pos, counts, status, workspace, ws_bytes, nullptr, (cudaStream_t)stream);
+                               ref_pos, counts, status, workspace, ws_bytes, nullptr, (cudaStream_t)stream,
+                               nullptr);
 }
 
 // ---------------------------------------------------------------- packed batches

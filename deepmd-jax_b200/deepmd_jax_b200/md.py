@@ -34,6 +34,8 @@ class MDDesc(ctypes.Structure):
         ("tau_t", ctypes.c_double), ("pimd_lambda", ctypes.c_double),
         ("nm_transform", ctypes.POINTER(ctypes.c_double)), ("nm_freqs", ctypes.POINTER(ctypes.c_double)),
         ("seed", ctypes.c_uint64), ("precision", ctypes.c_int),
+        ("pressure", ctypes.c_double), ("tau_p", ctypes.c_double), ("chain_length_p", ctypes.c_int),
+        ("couple_groups", ctypes.c_int * 3),
     ]
 
 
@@ -44,6 +46,11 @@ class MDReport(ctypes.Structure):
         ("steps", ctypes.c_uint64), ("rebuilds", ctypes.c_uint64), ("rebuild_rate", ctypes.c_double),
         ("chain_length", ctypes.c_int), ("chain_dof", ctypes.c_double),
         ("chain_xi", ctypes.c_double * 8), ("chain_p", ctypes.c_double * 8), ("chain_Q", ctypes.c_double * 8),
+        ("box", ctypes.c_double * 3), ("ngroups", ctypes.c_int),
+        ("box_position", ctypes.c_double * 3), ("box_momentum", ctypes.c_double * 3),
+        ("box_mass", ctypes.c_double * 3), ("baro_length", ctypes.c_int),
+        ("baro_xi", ctypes.c_double * 8), ("baro_p", ctypes.c_double * 8), ("baro_Q", ctypes.c_double * 8),
+        ("dU_deps", ctypes.c_double * 3),
     ]
 
 
@@ -63,10 +70,11 @@ def _declare(lib):
     lib.dpb_md_clear_status.argtypes = [vp, ctypes.c_uint32]
     lib.dpb_md_snapshot.argtypes = [vp, ctypes.c_int]
     lib.dpb_md_set_capacity.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp]
+    lib.dpb_md_set_skin.argtypes = [vp, ctypes.c_double, vp]
     lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
               "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
-              "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_device_bytes"):
+              "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes"):
         getattr(lib, f).restype = ctypes.c_int
     lib._md_declared = True
 
@@ -94,6 +102,32 @@ def sel_from_counts(max_counts, buffer_ratio):
     return [max(k - 1, 1) for k in knbr_from_counts(max_counts, buffer_ratio)]
 
 
+PRESS_UNIT_CONVERSION = 6.241509e-7  # bar -> eV / A^3 (deepmd_jax/md.py:26)
+
+
+def parse_couple_axes(couple_axes):
+    """Validated groups and the group of each axis (-1: fixed), as the
+    reference's _parse_couple_axes (deepmd_jax/routine.py:196-229)."""
+    try:
+        groups = tuple(tuple(int(a) for a in g) for g in couple_axes)
+    except TypeError:
+        raise ValueError("couple_axes must be a tuple of tuples of ints; got %r" % (couple_axes,))
+    axes = [a for g in groups for a in g]
+    if any(a not in (0, 1, 2) for a in axes):
+        raise ValueError("couple_axes axes must be in {0,1,2}; got %r" % (couple_axes,))
+    if len(set(axes)) != len(axes):
+        raise ValueError("couple_axes must be a partition (no repeats); got %r" % (couple_axes,))
+    if any(len(g) == 0 for g in groups):
+        raise ValueError("couple_axes groups must be non-empty; got %r" % (couple_axes,))
+    if len(groups) == 0:
+        raise ValueError("couple_axes must contain at least one group; use NVT instead")
+    gid = [-1, -1, -1]
+    for k, g in enumerate(groups):
+        for a in g:
+            gid[a] = k
+    return groups, gid
+
+
 class Simulation:
     """Two-step usage, as in the reference: ``sim = Simulation(...)`` then
     ``traj = sim.run(steps)``.  Extra keyword ``precision`` selects 'fp32'
@@ -116,18 +150,23 @@ class Simulation:
             params = model.params
         self._params = params
         self.model = DeviceModel(params, variables)
-        if routine not in ("NVE", "NVT"):
-            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NVT PIMD)" % routine)
+        if routine not in ("NVE", "NVT", "NPT"):
+            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT PIMD)" % routine)
         if len(model_deviation_paths) or fixed_indices is not None or remove_com_motion:
             raise NotImplementedError("model deviation / fixed atoms / COM removal are not supported")
-        if chain_steps_t != 1 or sy_steps_t != 1:
+        if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
             raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
-        if pressure is not None:
-            raise NotImplementedError("NPT is not supported")
         self._n_bead = int(n_bead)
         self._is_pimd = self._n_bead > 1
         if self._is_pimd and routine != "NVT":
             raise NotImplementedError("Path-integral MD (n_bead > 1) supports routine='NVT'.")
+        if routine == "NPT":
+            if pressure is None:
+                raise ValueError("Missing argument 'pressure' (in bar) for routine 'NPT'")
+            if temperature is None:
+                raise ValueError("Missing argument 'temperature' for routine 'NPT'")
+            self._couple_axes, self._group_ids = parse_couple_axes(couple_axes)
+        self._pressure = pressure
         pos0 = np.asarray(initial_position, dtype=np.float64)
         if self._is_pimd:
             if pos0.ndim == 2:
@@ -168,7 +207,7 @@ class Simulation:
         self._mass_per_type = np.asarray(mass, dtype=np.float64)
         self._mass = self._mass_per_type[self._type_idx]
         self._step_chunk_size = max(10, min(100, 100000 // (self._natoms * self._n_bead)))
-        self._neighbor_skin = (0.3 if neighbor_skin is None else float(neighbor_skin))
+        self._neighbor_skin = ((0.5 if routine == "NPT" else 0.3) if neighbor_skin is None else float(neighbor_skin))
         self._buffer_ratio = float(neighbor_buffer_ratio)
         self._kT = (temperature if temperature is not None else 0.0) * TEMP_UNIT_CONVERSION
         self._use_graph = use_cuda_graph
@@ -180,7 +219,13 @@ class Simulation:
         # neighbour capacity from a measurement at the initial positions (allocate_fn)
         self._sel = self._measure_capacity(pos0)
         desc = MDDesc()
-        desc.routine = 2 if self._is_pimd else (0 if routine == "NVE" else 1)
+        desc.routine = 2 if self._is_pimd else {"NVE": 0, "NVT": 1, "NPT": 3}[routine]
+        if routine == "NPT":
+            desc.pressure = float(pressure) * PRESS_UNIT_CONVERSION
+            desc.tau_p = float(tau_p)
+            desc.chain_length_p = int(chain_length_p)
+            for a in range(3):
+                desc.couple_groups[a] = int(self._group_ids[a])
         desc.natoms = self._natoms
         desc.nbeads = self._n_bead
         self._keep = [np.ascontiguousarray(self._type_idx, dtype=np.int32), np.ascontiguousarray(self._mass_per_type)]
@@ -309,6 +354,27 @@ class Simulation:
                 E += r.chain_p[k] ** 2 / (2 * r.chain_Q[k]) + kT * r.chain_xi[k]
             row.append(E)
             headers.append("Invariant")
+        elif self._routine == "NPT" and not self._is_pimd:
+            # Pressure (md_utils.py:139-159), moving box axes and the invariant (routine.py:439-456)
+            kT = self._kT
+            box = np.array(r.box)
+            V = float(np.prod(box))
+            dU_iso = -(r.virial[0] + r.virial[4] + r.virial[8])
+            row.append((self._natoms * kT - dU_iso / 3.0) / V / PRESS_UNIT_CONVERSION)
+            headers.append("Pressure")
+            for a in sorted(a for g in self._couple_axes for a in g):
+                row.append(box[a])
+                headers.append("box_" + "xyz"[a])
+            E = PE + KE + r.chain_p[0] ** 2 / (2 * r.chain_Q[0]) + r.chain_dof * kT * r.chain_xi[0]
+            for k in range(1, r.chain_length):
+                E += r.chain_p[k] ** 2 / (2 * r.chain_Q[k]) + kT * r.chain_xi[k]
+            for k in range(r.baro_length):
+                E += r.baro_p[k] ** 2 / (2 * r.baro_Q[k]) + kT * r.baro_xi[k]
+            E += self._pressure * PRESS_UNIT_CONVERSION * V
+            E += sum(r.box_momentum[g] ** 2 / (2 * r.box_mass[g]) for g in range(r.ngroups))
+            row.append(E)
+            headers.append("Invariant")
+        self.log_headers = headers + ["Time"]
         row.append(time() - tic)
         headers.append("Time")
         if self.verbose:
@@ -369,6 +435,16 @@ class Simulation:
                 print("# Warning: Nan or Inf encountered in simulation. Terminating.")
                 self._error_code = code
                 break
+            if code & 1:
+                # box shrank past the skin: a larger skin, a list on the current box, re-run (md.py:649-654)
+                _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
+                self._neighbor_skin += 0.4
+                _lib.check(self.lib.dpb_md_set_skin(self._h, self._neighbor_skin, _stream()), "dpb_md_set_skin")
+                _lib.check(self.lib.dpb_md_clear_status(self._h, ~1 & 0xFFFFFFFF), "dpb_md_clear_status")
+                self._graphs = {}
+                if self.verbose:
+                    print("# Box shrank past the skin: neighbour skin now %.2f A" % self._neighbor_skin)
+                continue
             if code & 2:
                 # reallocate (grow the buffer ratio on a repeat) and re-run the chunk (md.py:657-668,913-916)
                 _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
@@ -473,6 +549,9 @@ class Simulation:
         return self._centroid(p) if self._is_pimd else p
 
     def getBox(self):
+        """Current box (3,); under NPT the barostat's box."""
+        if self._routine == "NPT":
+            return np.array(self._report_struct().box)
         return np.array(self._box)
 
     def getEnergy(self):

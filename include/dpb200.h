@@ -209,13 +209,14 @@ DPB_API int dpb_eval_noalloc(const dpb_model *model, int precision, const float 
 #define DPB_MD_NVE 0
 #define DPB_MD_NVT_NHC 1
 #define DPB_MD_PIMD_PILE 2
+#define DPB_MD_NPT_NHC 3
 
 typedef struct dpb_md dpb_md;
 
 /* Host-side description of an MD run (deepmd_jax/md.py:61-282 constructor
  * arguments).  Units: Angstrom, fs, Dalton, Kelvin. */
 typedef struct {
-  int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE */
+  int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE, DPB_MD_NPT_NHC */
   int natoms;
   int nbeads;                  /* 1, or P ring-polymer beads for PIMD */
   const int *type_idx;         /* [natoms] user order */
@@ -232,6 +233,12 @@ typedef struct {
   const double *nm_freqs;      /* PIMD: (P) normal-mode frequencies, 1/fs */
   uint64_t seed;               /* Philox key of the stochastic steps */
   int precision;               /* DPB_PREC_* of the force evaluations */
+  /* NPT (DPB_MD_NPT_NHC: MTK barostat + Nose-Hoover chains,
+   * deepmd_jax/routine.py:161-456; orthorhombic, axes in coupled groups) */
+  double pressure;             /* target pressure, eV / A^3 */
+  double tau_p;                /* barostat time constant, fs */
+  int chain_length_p;          /* barostat chain length */
+  int couple_groups[3];        /* group of each axis (0..G-1), -1: fixed axis */
 } dpb_md_desc;
 
 typedef struct {
@@ -245,6 +252,14 @@ typedef struct {
   int chain_length;
   double chain_dof;
   double chain_xi[8], chain_p[8], chain_Q[8];
+  /* NPT: current box, per-group log box scale / momentum / mass, barostat
+   * chain, per-group dU/d(eps) of the last force evaluation */
+  double box[3];
+  int ngroups;
+  double box_position[3], box_momentum[3], box_mass[3];
+  int baro_length;
+  double baro_xi[8], baro_p[8], baro_Q[8];
+  double dU_deps[3];
 } dpb_md_report_t;
 
 typedef struct {
@@ -283,6 +298,9 @@ DPB_API int dpb_md_report(dpb_md *md, dpb_md_report_t *report);
 DPB_API int dpb_md_clear_status(dpb_md *md, uint32_t keep_bits);
 /* restore == 0: save the state (chunk start); 1: restore it (chunk re-run). */
 DPB_API int dpb_md_snapshot(dpb_md *md, int restore);
+/* New neighbour skin and a rebuild whose reference box is the current box
+ * (box-shrink resolution, status bit 1; deepmd_jax/md.py:649-654). */
+DPB_API int dpb_md_set_skin(dpb_md *md, double skin, void *stream);
 /* New neighbour capacity and a rebuild (overflow resolution, md.py:657-668). */
 DPB_API int dpb_md_set_capacity(dpb_md *md, const int *sel, void *stream);
 DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);

@@ -9,6 +9,8 @@ on the reference's hot path.
     deepmd_jax/routine.py:9-25;
   * PIMD BAOAB with exact free ring-polymer propagation and the PILE-L
     thermostat (deepmd_jax/pimd.py:22-44,92-111,114-207,210-247);
+  * MTK NPT with Nose-Hoover chains on the particles and on the box, axes in
+    coupled groups (deepmd_jax/routine.py:161-456);
   * min_image_unwrap (deepmd_jax/md_utils.py:162-169).
 
 jax_md is a third-party dependency that is absent here (unpinned git HEAD,
@@ -98,6 +100,89 @@ def nvt_step(r, p, F, m, dt, kT, chain: NHChain, force_fn):
     chain.KE = kinetic_energy(p, m)
     p = chain.substep(dt, p, kT)
     return r, p, F, extra
+
+
+def sinhx_x(x):
+    """sinh(x)/x by the series of deepmd_jax/routine.py:290-292."""
+    return 1 + x ** 2 / 6 + x ** 4 / 120 + x ** 6 / 5040 + x ** 8 / 362_880 + x ** 10 / 39_916_800
+
+
+class NPTState:
+    """MTK NPT state with coupled axis groups (deepmd_jax/routine.py:161-456):
+    log box scales Rb, momenta Pb, masses Mb per group, the cached per-group
+    dU/d(eps), a thermostat chain (DOF 3N, tau_t) and a barostat chain (DOF G,
+    tau_p).  force_fn(r, box) -> (F, (E, W)) with W the virial, whose
+    diagonal gives dU/d(eps_a) = -W_aa."""
+
+    def __init__(self, r, p, F, W, m, box, pressure, kT, tau_t, tau_p, gid, chain_t=3, chain_p=3):
+        self.r, self.p, self.F, self.m = r.copy(), p.copy(), F.copy(), m
+        self.ref = np.asarray(box, float).copy()
+        self.gid = np.asarray(gid)
+        self.G = int(self.gid.max()) + 1
+        self.ngrp = np.array([(self.gid == g).sum() for g in range(self.G)], float)
+        N = r.shape[0]
+        self.Rb = np.zeros(self.G)
+        self.Pb = np.zeros(self.G)
+        self.tau_p = tau_p
+        self.Mb = self.ngrp * (N + 1) * kT * tau_p ** 2
+        self.dUde = self.dU_deps(W)
+        self.pressure = pressure
+        self.thermo = NHChain(chain_t, 3 * N, kT, tau_t, kinetic_energy(p, m))
+        self.baro = NHChain(chain_p, self.G, kT, tau_p, 0.0)
+
+    def dU_deps(self, W):
+        out = np.zeros(self.G)
+        for a in range(3):
+            if self.gid[a] >= 0:
+                out[self.gid[a]] -= W[a, a]
+        return out
+
+    def box(self):
+        return self.ref * np.array([np.exp(self.Rb[g]) if g >= 0 else 1.0 for g in self.gid])
+
+    def box_force(self, V, Nf):
+        KE2 = (self.p ** 2 / self.m).sum(0)
+        tot = KE2.sum()
+        grp = np.array([KE2[self.gid == g].sum() for g in range(self.G)])
+        return grp + (self.ngrp / Nf) * tot - self.dUde - self.pressure * V * self.ngrp
+
+
+def npt_step(st: NPTState, dt, kT, force_fn):
+    """One apply_fn step of npt_nose_hoover (deepmd_jax/routine.py:403-436)."""
+    N = st.r.shape[0]
+    Nf = 3.0 * N
+    st.thermo.update_mass(kT)
+    st.baro.update_mass(kT)
+    st.Mb = st.ngrp * (N + 1) * kT * st.tau_p ** 2
+    st.Pb = st.baro.substep(dt, st.Pb, kT)
+    st.p = st.thermo.substep(dt, st.p, kT)
+    # inner step
+    G = st.box_force(np.prod(st.box()), Nf)
+    st.Pb = st.Pb + 0.5 * dt * G
+    Vb = st.Pb / st.Mb
+    va = np.array([Vb[g] if g >= 0 else 0.0 for g in st.gid])
+    rate = va + (st.ngrp * Vb).sum() / Nf
+    x = rate * dt / 2
+
+    def exp_iL2(p, F):
+        return p * np.exp(-x) + (dt / 2) * F * sinhx_x(x / 2) * np.exp(-x / 2)
+
+    st.p = exp_iL2(st.p, st.F)
+    st.Rb = st.Rb + Vb * dt
+    box = st.box()
+    y = va * dt
+    st.r = st.r * np.exp(y) + dt * (st.p / st.m) * np.exp(y / 2) * sinhx_x(y / 2)
+    F, (E, W) = force_fn(st.r, box)
+    st.F = F
+    st.dUde = st.dU_deps(W)
+    st.p = exp_iL2(st.p, F)
+    G = st.box_force(np.prod(box), Nf)
+    st.Pb = st.Pb + 0.5 * dt * G
+    st.thermo.KE = kinetic_energy(st.p, st.m)
+    st.baro.KE = 0.5 * float((st.Pb ** 2 / st.Mb).sum())
+    st.p = st.thermo.substep(dt, st.p, kT)
+    st.Pb = st.baro.substep(dt, st.Pb, kT)
+    return E, W
 
 
 def normal_mode_transform(n_bead, kT):
