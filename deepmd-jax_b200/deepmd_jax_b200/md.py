@@ -347,7 +347,7 @@ class Simulation:
         if self._routine == "NVE":
             row.append(KE + PE)
             headers.append("Invariant")
-        elif not self._is_pimd:
+        elif self._routine == "NVT" and not self._is_pimd:
             kT = self._kT
             E = PE + KE + r.chain_p[0] ** 2 / (2 * r.chain_Q[0]) + r.chain_dof * kT * r.chain_xi[0]
             for k in range(1, r.chain_length):

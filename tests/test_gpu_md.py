@@ -157,7 +157,9 @@ def test_npt_matches_oracle_and_conserves_invariant():
     1,536-atom box, semi-isotropic couple_axes ((0, 1), (2,)): after 10 steps
     the device run and the float64 oracle agree on positions (2e-4 A), box
     lengths (2e-6 relative) and box momenta (1e-3 relative + 1e-6 abs); the
-    NPT invariant of 40 steps stays within 1e-4 eV/atom."""
+    NPT invariant of the first 30 steps stays within 1e-5 eV/atom.  (From
+    step ~34 atoms of this random-weight model pass through one another and
+    the invariant jumps - in NVT just the same, so the window stops before.)"""
     from deepmd_jax_b200.md import Simulation, PRESS_UNIT_CONVERSION
     from deepmd_jax_b200.systems import water_box
     from oracle import nlist as onl
@@ -190,8 +192,8 @@ def test_npt_matches_oracle_and_conserves_invariant():
     assert np.allclose(np.array(r_dev.box), st.box(), rtol=2e-6, atol=0)
     assert np.allclose(np.array(r_dev.box_momentum[:2]), st.Pb, rtol=1e-3, atol=1e-6)
     assert r_dev.ngroups == 2
-    sim.run(30, trajectory=False)
+    sim.run(20, trajectory=False)
     inv = np.array([row[sim.log_headers.index("Invariant")] for row in sim.log])
     assert sim.log_headers[:5] == ["Step", "Temperature", "KE", "PE", "Pressure"]
     assert "box_x" in sim.log_headers and "box_z" in sim.log_headers
-    assert np.abs(inv - inv[0]).max() / N < 1e-4
+    assert len(inv) == 4 and np.abs(inv - inv[0]).max() / N < 1e-5
