@@ -190,7 +190,10 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
 
 // ---------------------------------------------------------------- embedding forward (BF16 tcgen05)
 // Per block of 8 centre atoms of type ti: neighbour rows with s(r) != 0 are
-// compacted block-wide into 128-row tiles.  Per tile (thread = row = TMEM lane):
+// compacted block-wide into 128-row tiles.  Two threads serve each row (TMEM
+// lane): warps w and w + 4 share lane quarter w % 4 and split the columns of
+// every layer ("halves"), so 16 warps per SM hide the latencies of the three
+// MMA round trips per tile:
 //   layer 0 (1 -> E0) FP32 on CUDA cores (tanh.approx.f32: its ~2^-11 relative
 //           error is below the BF16 rounding of the h0 operand), h0 -> A0 (bf16)
 //   D  = A0 . W1   (tcgen05, 128 x N1)   -> h1 = tanh(D + b1) + rep(h0) -> A1
@@ -201,13 +204,123 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
 // TMEM across all tiles of both neighbour types.  The block epilogue writes
 // T / Nnbrs (FP32) and the descriptor G (BF16, dpmodel.py:74-78).  Only the
 // current neighbour type's net is resident (2 CTAs per SM).
+constexpr int kFwdThreads = 256;
+constexpr int kRowCapFwd = 128 + kFwdThreads;  // one tile + the carry of a compaction round
+
+// Column split of the two halves: half 0 owns h1 columns [0, S1) and h2
+// columns [0, S2), half 1 the rest; S2 = S1 * Z2 so every residual source
+// h1[c / Z2] of a half's h2 columns is one of its own h1 columns.
 template <int E0, int E1, int E2>
-__global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D, int ti,
-                                                          const float *__restrict__ pos,
-                                                          const int32_t *__restrict__ perm,
-                                                          const float *__restrict__ box,
-                                                          const int32_t *__restrict__ nbrs, float *__restrict__ Tout,
-                                                          __nv_bfloat16 *__restrict__ Gout, int *__restrict__ err) {
+struct FwdSplit {
+  using MD = MixDims<E0, E1, E2>;
+  static constexpr int S1 = (E1 / 2) / 8 * 8;
+  static constexpr int S2 = S1 * MD::Z2;
+  static constexpr int A0C = MD::K1 / 2;                 // h0 operand columns of half 0
+  // h0 columns each half computes: its operand columns and its residual sources
+  static constexpr int H0LO1 = (S1 / MD::Z1 < A0C) ? S1 / MD::Z1 : A0C;
+  static constexpr int H0N0 = (A0C > (S1 + MD::Z1 - 1) / MD::Z1) ? A0C : (S1 + MD::Z1 - 1) / MD::Z1;
+  static constexpr int H0N1 = E0 - H0LO1;
+  static constexpr int H0MAX = H0N0 > H0N1 ? H0N0 : H0N1;
+  static constexpr int H1N1 = E1 - S1;
+  static constexpr int H1MAX = S1 > H1N1 ? S1 : H1N1;
+};
+
+// layer 0 of one half: h0 (FP32) for the half's columns and its A0 chunks
+template <int E0, int E1, int E2, int HALF>
+__device__ __forceinline__ void fwd_layer0(float st, const float *sm, int row, char *opa, float (&h0)[16]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = FwdSplit<E0, E1, E2>;
+  constexpr int lo = HALF ? SP::H0LO1 : 0, n = HALF ? SP::H0N1 : SP::H0N0;
+  static_assert(n <= 16, "h0 registers");
+#pragma unroll
+  for (int k = 0; k < n; ++k) h0[k] = tc::tanh_fast(fmaf(st, sm[lo + k], sm[E0 + lo + k]));
+  constexpr int c0 = HALF ? SP::A0C : 0, c1 = HALF ? MD::K1 : SP::A0C;
+#pragma unroll
+  for (int k8 = c0; k8 < c1; k8 += 8) {
+    float t[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = k8 + u;
+      t[u] = (c < E0) ? h0[(c - lo) < 0 ? 0 : ((c - lo) >= n ? n - 1 : (c - lo))] : 0.f;
+    }
+    *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(row, k8, MD::K1)) = pack8(t);
+  }
+}
+
+// epilogue of layer 1 for one half: h1 columns and their A1 chunks
+template <int E0, int E1, int E2, int HALF>
+__device__ __forceinline__ void fwd_epi1(uint32_t tD, uint32_t lane_off, const float *sm, int row, char *opa,
+                                         const float (&h0)[16], float (&h1)[32]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = FwdSplit<E0, E1, E2>;
+  constexpr int c0 = HALF ? SP::S1 : 0, c1 = HALF ? E1 : SP::S1;
+  constexpr int h0lo = HALF ? SP::H0LO1 : 0;
+  constexpr int g0 = c0 / 16 * 16, g1 = (c1 + 15) / 16 * 16, NG = (g1 - g0) / 16;
+  static_assert(c1 - c0 <= 32, "h1 registers");
+  uint32_t r[NG][16];
+#pragma unroll
+  for (int q = 0; q < NG; ++q) tc::tmem_ld16_issue(tD + lane_off + g0 + 16 * q, r[q]);
+  tc::tmem_wait();
+#pragma unroll
+  for (int q = 0; q < NG; ++q)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int c = g0 + 16 * q + i;
+      if (c >= c0 && c < c1)
+        h1[c - c0] = tc::tanh_fast(__uint_as_float(r[q][i]) + sm[2 * E0 + c]) + h0[c / MD::Z1 - h0lo];
+    }
+  constexpr int k0 = HALF ? SP::S1 : 0, k1 = HALF ? MD::K2 : SP::S1;
+#pragma unroll
+  for (int k8 = k0; k8 < k1; k8 += 8) {
+    float t[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = k8 + u;
+      t[u] = (c < c1) ? h1[c - c0] : 0.f;
+    }
+    *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(row, k8, MD::K2)) = pack8(t);
+  }
+}
+
+// epilogue of layer 2 for one half: h2 columns into the MN-major operand H2
+template <int E0, int E1, int E2, int HALF>
+__device__ __forceinline__ void fwd_epi2(uint32_t tD, uint32_t lane_off, const float *sm, int row, char *opa,
+                                         const float (&h1)[32]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = FwdSplit<E0, E1, E2>;
+  constexpr int c0 = HALF ? SP::S2 : 0, c1 = HALF ? MD::N2 : SP::S2;
+  constexpr int h1lo = HALF ? SP::S1 : 0, h1n = HALF ? SP::H1N1 : SP::S1;
+#pragma unroll
+  for (int g = c0 / 16 * 16; g < c1; g += 16) {
+    uint32_t r[16];
+    tc::tmem_ld16_issue(tD + lane_off + g, r);
+    tc::tmem_wait();
+#pragma unroll
+    for (int h8 = 0; h8 < 16; h8 += 8) {
+      if (g + h8 < c0 || g + h8 >= c1) continue;
+      float h2[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int col = g + h8 + i;
+        const int src = col / MD::Z2 - h1lo;
+        h2[i] = (col < E2) ? tc::tanh_fast(__uint_as_float(r[h8 + i]) + sm[2 * E0 + E1 + (col < E2 ? col : 0)]) +
+                                 h1[src < 0 ? 0 : (src >= h1n ? h1n - 1 : src)]
+                           : 0.f;
+      }
+      *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(row, g + h8, MD::N2)) = pack8(h2);
+    }
+  }
+}
+
+template <int E0, int E1, int E2>
+__global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, SysDesc D, int ti,
+                                                                  const float *__restrict__ pos,
+                                                                  const int32_t *__restrict__ perm,
+                                                                  const float *__restrict__ box,
+                                                                  const int32_t *__restrict__ nbrs,
+                                                                  float *__restrict__ Tout,
+                                                                  __nv_bfloat16 *__restrict__ Gout,
+                                                                  int *__restrict__ err) {
   using MD = MixDims<E0, E1, E2>;
   extern __shared__ __align__(1024) char smem[];
   char *netb = smem;
@@ -215,20 +328,21 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
   char *opa = reinterpret_cast<char *>(small) + round1k(MD::NSMALL * 4);
   char *rblk = opa + round1k(MD::OPA);
   float4 *rowbuf = reinterpret_cast<float4 *>(rblk + kRblkBytes);
-  __shared__ int wcnt[4];
+  __shared__ int wcnt[kFwdThreads / 32];
   __shared__ float3 ri_s[kBlkAtoms];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tbase_s;
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = tid & 127, half = tid >> 7;
 
-  for (int e = tid; e < kRblkBytes / 16; e += 128) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
+  for (int e = tid; e < kRblkBytes / 16; e += kFwdThreads) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
   if (tid == 0) tc::mbar_init(&mbar, 1);
   if (warp == 0) tc::tmem_alloc(&tbase_s, 256);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = tbase_s;
-  const uint32_t tD = tbase, tD3 = tbase + 128, lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t tD = tbase, tD3 = tbase + 128, lane_off = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t ph = 0;
   bool ok = true;
 
@@ -270,7 +384,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
-      for (int base = 0; base < total + 128 && ok; base += 128) {
+      for (int base = 0; base < total + kFwdThreads && ok; base += kFwdThreads) {
         const bool flush = base >= total;
         if (!flush)
           mix_compact_round(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm, nbrs,
@@ -281,8 +395,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
             MIX_WAIT();
             pending = false;
             if (!ok) break;
-            if (my_slot >= 0) {
-              const uint32_t o = tc::mnmajor_off(tid, 16 * my_slot, 128);
+            if (half == 0 && my_slot >= 0) {
+              const uint32_t o = tc::mnmajor_off(row, 16 * my_slot, 128);
               *reinterpret_cast<uint4 *>(rblk + o) = make_uint4(0, 0, 0, 0);
               *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(0, 0, 0, 0);
             }
@@ -292,27 +406,20 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
             mix_load_net<E0, E1, E2>(M, knet, netb, small);
             loaded_net = knet;
           }
-          const bool act = tid < nrows;
-          const float4 rv = act ? rowbuf[tid] : make_float4(100.f, 100.f, 100.f, 0.f);
+          const bool act = row < nrows;
+          const float4 rv = act ? rowbuf[row] : make_float4(100.f, 100.f, 100.f, 0.f);
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
           RowGeom gm;
           float st, R[10];
           mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
-          __syncthreads();  // net image visible
-          float h0[E0];
-#pragma unroll
-          for (int k = 0; k < E0; ++k) h0[k] = tc::tanh_fast(fmaf(st, sm[k], sm[E0 + k]));
-#pragma unroll
-          for (int k8 = 0; k8 < MD::K1; k8 += 8) {
-            float t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = (k8 + u < E0) ? h0[min(k8 + u, E0 - 1)] : 0.f;
-            *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(tid, k8, MD::K1)) = pack8(t);
-          }
+          __syncthreads();  // net image visible; rowbuf read by every thread
+          float h0[16];
+          if (half == 0) fwd_layer0<E0, E1, E2, 0>(st, sm, row, opa, h0);
+          else fwd_layer0<E0, E1, E2, 1>(st, sm, row, opa, h0);
           my_slot = slot;
-          if (act) {
-            const uint32_t o = tc::mnmajor_off(tid, 16 * slot, 128);
+          if (half == 0 && act) {
+            const uint32_t o = tc::mnmajor_off(row, 16 * slot, 128);
             *reinterpret_cast<uint4 *>(rblk + o) = pack8(R);
             *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(tc::pack_bf16(R[8], R[9]), 0u, 0u, 0u);
           }
@@ -330,27 +437,9 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
           }
           MIX_WAIT();
           if (!ok) break;
-          float h1[E1];
-          {
-            uint32_t r[MD::N1 / 16][16];
-#pragma unroll
-            for (int q = 0; q < MD::N1 / 16; ++q) tc::tmem_ld16_issue(tD + lane_off + 16 * q, r[q]);
-            tc::tmem_wait();
-#pragma unroll
-            for (int q = 0; q < MD::N1 / 16; ++q)
-#pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if (16 * q + i < E1)
-                  h1[16 * q + i] = tc::tanh_fast(__uint_as_float(r[q][i]) + sm[2 * E0 + 16 * q + i]) +
-                                   h0[(16 * q + i) / MD::Z1];
-          }
-#pragma unroll
-          for (int k8 = 0; k8 < MD::K2; k8 += 8) {
-            float t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = (k8 + u < E1) ? h1[min(k8 + u, E1 - 1)] : 0.f;
-            *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(tid, k8, MD::K2)) = pack8(t);
-          }
+          float h1[32];
+          if (half == 0) fwd_epi1<E0, E1, E2, 0>(tD, lane_off, sm, row, opa, h0, h1);
+          else fwd_epi1<E0, E1, E2, 1>(tD, lane_off, sm, row, opa, h0, h1);
           tc::fence_proxy_async();
           tc::fence_before_sync();
           __syncthreads();
@@ -365,27 +454,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
           }
           MIX_WAIT();
           if (!ok) break;
-#pragma unroll
-          for (int c0 = 0; c0 < MD::N2; c0 += 32) {
-            uint32_t r[2][16];
-            tc::tmem_ld16_issue(tD + lane_off + c0, r[0]);
-            if (c0 + 16 < MD::N2) tc::tmem_ld16_issue(tD + lane_off + c0 + 16, r[1]);
-            tc::tmem_wait();
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-              if (c0 + 16 * q >= MD::N2) break;
-              float h2[16];
-#pragma unroll
-              for (int i = 0; i < 16; ++i) {
-                const int col = c0 + 16 * q + i;
-                h2[i] = (col < E2) ? tc::tanh_fast(__uint_as_float(r[q][i]) + sm[2 * E0 + E1 + min(col, E2 - 1)]) +
-                                         h1[min(col / MD::Z2, E1 - 1)]
-                                   : 0.f;
-              }
-              *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(tid, c0 + 16 * q, MD::N2)) = pack8(h2);
-              *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(tid, c0 + 16 * q + 8, MD::N2)) = pack8(h2 + 8);
-            }
-          }
+          if (half == 0) fwd_epi2<E0, E1, E2, 0>(tD, lane_off, sm, row, opa, h1);
+          else fwd_epi2<E0, E1, E2, 1>(tD, lane_off, sm, row, opa, h1);
           tc::fence_proxy_async();
           tc::fence_before_sync();
           __syncthreads();
@@ -409,8 +479,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
       MIX_WAIT();
       pending = false;
       if (!ok) break;
-      if (my_slot >= 0) {
-        const uint32_t o = tc::mnmajor_off(tid, 16 * my_slot, 128);
+      if (half == 0 && my_slot >= 0) {
+        const uint32_t o = tc::mnmajor_off(row, 16 * my_slot, 128);
         *reinterpret_cast<uint4 *>(rblk + o) = make_uint4(0, 0, 0, 0);
         *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(0, 0, 0, 0);
       }
@@ -419,9 +489,11 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
     __syncthreads();
     float *Xs = reinterpret_cast<float *>(rblk);  // staging [slot][c][w], 8 x 10 x E2 floats
     {
-      const int slot = tid >> 4, c = tid & 15;
-#pragma unroll
-      for (int c0 = 0; c0 < MD::N2; c0 += 16) {
+      const int slot = row >> 4, c = row & 15;
+      constexpr int NG = MD::N2 / 16, NG0 = (NG + 1) / 2;  // column groups of half 0
+      const int q0 = half ? NG0 : 0, q1 = half ? NG : NG0;
+      for (int q = q0; q < q1; ++q) {
+        const int c0 = 16 * q;
         uint32_t r[16];
         if (ntile > 0) {
           tc::tmem_ld16_issue(tD3 + lane_off + c0, r);
@@ -446,7 +518,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
     tc::fence_before_sync();
     __syncthreads();
     const int A = M.A;
-    for (int idx = tid; idx < nb * A * E2; idx += 128) {
+    for (int idx = tid; idx < nb * A * E2; idx += kFwdThreads) {
       const int slot = idx / (A * E2), rem = idx - slot * A * E2, aa = rem / E2, w = rem - aa * E2;
       const float *X = Xs + slot * 10 * E2;
       const float y1 = X[1 * E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
@@ -460,7 +532,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
       Gout[(g0 + slot) * (size_t)A * E2 + aa * E2 + w] = __float2bfloat16_rn(v);
     }
     __syncthreads();
-    for (int e = tid; e < kRblkBytes / 16; e += 128) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
+    for (int e = tid; e < kRblkBytes / 16; e += kFwdThreads) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
     __syncthreads();
   }
   if (!ok) {
@@ -476,7 +548,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_fwd(DevModel M, SysDesc D,
 template <int E0, int E1, int E2>
 size_t mix_fwd_smem() {
   using MD = MixDims<E0, E1, E2>;
-  return (size_t)round1k(MD::NETB) + round1k(MD::NSMALL * 4) + round1k(MD::OPA) + kRblkBytes + kRowCap * 16;
+  return (size_t)round1k(MD::NETB) + round1k(MD::NSMALL * 4) + round1k(MD::OPA) + kRblkBytes + kRowCapFwd * 16;
 }
 
 static int num_sms() {
@@ -497,7 +569,7 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
   DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_fwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   const int grid = nblk < 2 * num_sms() ? nblk : 2 * num_sms();
-  k_mix_embed_fwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G, err);
+  k_mix_embed_fwd<E0, E1, E2><<<grid, kFwdThreads, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G, err);
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
