@@ -517,19 +517,43 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     }
     tc::fence_before_sync();
     __syncthreads();
+    // G[a][w] = sum_c Q[c][a] X[c][w] (dpmodel.py:74-78): Q of every slot is
+    // staged once (zero for a >= A), then a thread owns (slot, w) pairs, keeps
+    // X[.][w] in registers and reads Q as warp-wide broadcasts.
     const int A = M.A;
-    for (int idx = tid; idx < nb * A * E2; idx += kFwdThreads) {
-      const int slot = idx / (A * E2), rem = idx - slot * A * E2, aa = rem / E2, w = rem - aa * E2;
-      const float *X = Xs + slot * 10 * E2;
-      const float y1 = X[1 * E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
-      float v = X[aa] * X[w] + X[E2 + aa] * X[E2 + w] + X[2 * E2 + aa] * X[2 * E2 + w] + X[3 * E2 + aa] * X[3 * E2 + w];
-      v = fmaf(y1 * y1 + X[4 * E2 + A + aa], X[4 * E2 + w], v);
-      v = fmaf(y2 * y2 + X[5 * E2 + A + aa], X[5 * E2 + w], v);
-      v = fmaf(y3 * y3 + X[6 * E2 + A + aa], X[6 * E2 + w], v);
-      v = fmaf(kSqrt2 * y1 * y3 + X[7 * E2 + A + aa], X[7 * E2 + w], v);
-      v = fmaf(kSqrt2 * y2 * y1 + X[8 * E2 + A + aa], X[8 * E2 + w], v);
-      v = fmaf(kSqrt2 * y3 * y2 + X[9 * E2 + A + aa], X[9 * E2 + w], v);
-      Gout[(g0 + slot) * (size_t)A * E2 + aa * E2 + w] = __float2bfloat16_rn(v);
+    float *Qs = Xs + kBlkAtoms * 10 * E2;  // [slot][c][16]
+    for (int e = tid; e < kBlkAtoms * 160; e += kFwdThreads) {
+      const int slot = e / 160, c = (e >> 4) % 10, aa = e & 15;
+      float q = 0.f;
+      if (slot < nb && aa < A) {
+        const float *X = Xs + slot * 10 * E2;
+        if (c < 4) {
+          q = X[c * E2 + aa];
+        } else {
+          const float y1 = X[E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
+          const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
+          q = b6[c - 4] + X[c * E2 + A + aa];
+        }
+      }
+      Qs[e] = q;
+    }
+    __syncthreads();
+    constexpr int WP = (E2 + 31) / 32 * 32;  // columns per slot, whole warps
+    for (int pr = tid; pr < nb * WP; pr += kFwdThreads) {
+      const int slot = pr / WP, w = pr - slot * WP;
+      if (w < E2) {
+        float x[10];
+#pragma unroll
+        for (int c = 0; c < 10; ++c) x[c] = Xs[(slot * 10 + c) * E2 + w];
+        const float *Q = Qs + slot * 160;
+        __nv_bfloat16 *Gs = Gout + (g0 + slot) * (size_t)A * E2 + w;
+        for (int aa = 0; aa < A; ++aa) {
+          float v = 0.f;
+#pragma unroll
+          for (int c = 0; c < 10; ++c) v = fmaf(Q[c * 16 + aa], x[c], v);
+          Gs[aa * E2] = __float2bfloat16_rn(v);
+        }
+      }
     }
     __syncthreads();
     for (int e = tid; e < kRblkBytes / 16; e += kFwdThreads) reinterpret_cast<uint4 *>(rblk)[e] = make_uint4(0, 0, 0, 0);
