@@ -729,6 +729,27 @@ __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float 
   }
 }
 
+// Columns 10 S .. 10 S + 9 of an 80-column TMEM row held in registers.
+template <int S>
+__device__ __forceinline__ void slot_cols(const uint32_t (&r)[kDtN / 16][16], float (&out)[10]) {
+#pragma unroll
+  for (int c = 0; c < 10; ++c) out[c] = __uint_as_float(r[(10 * S + c) / 16][(10 * S + c) % 16]);
+}
+
+__device__ __forceinline__ void slot_cols_rt(int slot, const uint32_t (&r)[kDtN / 16][16], float (&out)[10]) {
+  static_assert(kBlkAtoms == 8, "one case per slot");
+  switch (slot) {  // a warp's rows are sorted by slot: one or two cases run per warp
+    case 0: slot_cols<0>(r, out); break;
+    case 1: slot_cols<1>(r, out); break;
+    case 2: slot_cols<2>(r, out); break;
+    case 3: slot_cols<3>(r, out); break;
+    case 4: slot_cols<4>(r, out); break;
+    case 5: slot_cols<5>(r, out); break;
+    case 6: slot_cols<6>(r, out); break;
+    default: slot_cols<7>(r, out); break;
+  }
+}
+
 // ---------------------------------------------------------------- embedding adjoint (BF16 tcgen05)
 // Per block of 8 centre atoms: the B tile DTB (N = 8 slots x 10 channels,
 // K = N2) is copied from the per-atom dE/dT rows.  The rows are recomputed
@@ -985,26 +1006,16 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
           if (!ok) break;
           // ---- u, v of this row's atom slot (columns 10 slot .. 10 slot + 9)
           float u[10], v[10];
-#pragma unroll
-          for (int c = 0; c < 10; ++c) u[c] = v[c] = 0.f;
           {
             uint32_t r[kDtN / 16][16];
 #pragma unroll
             for (int q = 0; q < kDtN / 16; ++q) tc::tmem_ld16_issue(tbase + lane_off + 16 * q, r[q]);
             tc::tmem_wait();
-#pragma unroll
-            for (int q = 0; q < kDtN / 16; ++q)
-#pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if ((16 * q + i) / 10 == slot) u[(16 * q + i) % 10] = __uint_as_float(r[q][i]);
+            slot_cols_rt(slot, r, u);
 #pragma unroll
             for (int q = 0; q < kDtN / 16; ++q) tc::tmem_ld16_issue(tbase + 128 + lane_off + 16 * q, r[q]);
             tc::tmem_wait();
-#pragma unroll
-            for (int q = 0; q < kDtN / 16; ++q)
-#pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if ((16 * q + i) / 10 == slot) v[(16 * q + i) % 10] = __uint_as_float(r[q][i]);
+            slot_cols_rt(slot, r, v);
           }
           tc::fence_before_sync();
           float gst = 0.f;
@@ -1014,13 +1025,30 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
           row_adjoint(gm, inv_std, u, gst, gx);
           if (act) {
             atomicAdd(&F4[frame_base + jsrc], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
-            atomicAdd(&fi_s[slot * 3 + 0], gx[0]);
-            atomicAdd(&fi_s[slot * 3 + 1], gx[1]);
-            atomicAdd(&fi_s[slot * 3 + 2], gx[2]);
 #pragma unroll
             for (int p3 = 0; p3 < 3; ++p3)
 #pragma unroll
               for (int q3 = 0; q3 < 3; ++q3) vir[p3 * 3 + q3] -= gm.x[p3] * gx[q3];
+          }
+          {
+            // centre-atom force: the warp's rows are sorted by slot, so a
+            // segmented suffix sum leaves each slot's total on its first lane
+            const int lane = tid & 31, key = act ? slot : -1 - lane;
+            float s0 = act ? gx[0] : 0.f, s1 = act ? gx[1] : 0.f, s2 = act ? gx[2] : 0.f;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int ko = __shfl_down_sync(0xffffffffu, key, o);
+              const float t0 = __shfl_down_sync(0xffffffffu, s0, o);
+              const float t1 = __shfl_down_sync(0xffffffffu, s1, o);
+              const float t2 = __shfl_down_sync(0xffffffffu, s2, o);
+              if (lane + o < 32 && ko == key) { s0 += t0; s1 += t1; s2 += t2; }
+            }
+            const int kp = __shfl_up_sync(0xffffffffu, key, 1);
+            if (act && (lane == 0 || kp != key)) {
+              atomicAdd(&fi_s[slot * 3 + 0], s0);
+              atomicAdd(&fi_s[slot * 3 + 1], s1);
+              atomicAdd(&fi_s[slot * 3 + 2], s2);
+            }
           }
           mix_drop_rows(rowbuf, nrows, rowcount);
         }
