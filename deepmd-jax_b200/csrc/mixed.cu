@@ -1267,9 +1267,17 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
       ok = fit_gemm(S, td, FW, FW, FW, M.fwT_bf[ti][l], FW, 0, HA, FW, nullptr, nullptr, 0, 0);
     if (!ok) break;
     const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
+    // residual sources of the current chunk, loaded one chunk ahead so the
+    // scratch reads overlap the TMEM loads and the previous chunk's math
+    float hp[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) hp[i] = dt ? FIT_SCR(L + l - 1, i) : 0.f;
     for (int c0 = 0; c0 < FW; c0 += 16) {
       uint32_t r[16];
       tc::tmem_ld16_issue(td + lane_off + c0, r);
+      float hn[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) hn[i] = (dt && c0 + 16 < FW) ? FIT_SCR(L + l - 1, c0 + 16 + i) : 0.f;
       float bv[16], dv[16];
 #pragma unroll
       for (int i = 0; i < 16; i += 4) {
@@ -1285,11 +1293,13 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
         const int n = c0 + i;
         const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
         float h = t;
-        if (dt) h = t * dv[i] + FIT_SCR(L + l - 1, n);
+        if (dt) h = t * dv[i] + hp[i];
         hv[i] = h;
         FIT_SCR(l, n) = t;
         FIT_SCR(L + l, n) = h;
       }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) hp[i] = hn[i];
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(hv);
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(hv + 8);
     }
@@ -1300,17 +1310,34 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
   if (ok) {
     const float *wf = M.fw[ti][L], *dtL = M.fdt[ti][L - 1];
     float s = 0.f;
-    for (int c0 = 0; c0 < FW; c0 += 8) {
-      float g[8];
+    float hc[16], tcur[16];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < 16; ++i) {
+      hc[i] = FIT_SCR(2 * L - 1, i);
+      tcur[i] = FIT_SCR(L - 1, i);
+    }
+    for (int c0 = 0; c0 < FW; c0 += 16) {
+      float hn[16], tn[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        hn[i] = (c0 + 16 < FW) ? FIT_SCR(2 * L - 1, c0 + 16 + i) : 0.f;
+        tn[i] = (c0 + 16 < FW) ? FIT_SCR(L - 1, c0 + 16 + i) : 0.f;
+      }
+      float g[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
         const int n = c0 + i;
         const float wn = __ldg(wf + n);
-        s = fmaf(FIT_SCR(2 * L - 1, n), wn, s);
-        const float t = FIT_SCR(L - 1, n);
-        g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - t * t);
+        s = fmaf(hc[i], wn, s);
+        g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - tcur[i] * tcur[i]);
       }
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(g);
+      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(g + 8);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        hc[i] = hn[i];
+        tcur[i] = tn[i];
+      }
     }
     s += M.fb[ti][L][0];
     if (act) Eatom[me] = s;
@@ -1338,9 +1365,22 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
     if (!ok) break;
     const bool res_l = M.fdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.fdt[ti][l - 1] != nullptr;
     const float *dtm1 = M.fdt[ti][l - 1], *wf = M.fw[ti][L];
+    const bool use_gh = res_l && l != L - 1;
+    float ghc[16], tcur[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      ghc[i] = use_gh ? FIT_SCR(2 * L, i) : 0.f;
+      tcur[i] = FIT_SCR(l - 1, i);
+    }
     for (int c0 = 0; c0 < FW; c0 += 16) {
       uint32_t r[16];
       tc::tmem_ld16_issue(td + lane_off + c0, r);
+      float ghn[16], tn[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        ghn[i] = (use_gh && c0 + 16 < FW) ? FIT_SCR(2 * L, c0 + 16 + i) : 0.f;
+        tn[i] = (c0 + 16 < FW) ? FIT_SCR(l - 1, c0 + 16 + i) : 0.f;
+      }
       float wv[16], dv[16];
 #pragma unroll
       for (int i = 0; i < 16; i += 4) {
@@ -1356,10 +1396,15 @@ __global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrow
       for (int i = 0; i < 16; ++i) {
         const int n = c0 + i;
         float g = __uint_as_float(r[i]);
-        if (res_l) g += (l == L - 1) ? wv[i] : FIT_SCR(2 * L, n);
-        const float t = FIT_SCR(l - 1, n);
+        if (res_l) g += (l == L - 1) ? wv[i] : ghc[i];
+        const float t = tcur[i];
         gz[i] = g * dv[i] * (1.f - t * t);
         if (res_lm1) FIT_SCR(2 * L, n) = g;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        ghc[i] = ghn[i];
+        tcur[i] = tn[i];
       }
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(gz);
       *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(gz + 8);
