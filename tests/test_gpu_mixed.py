@@ -82,3 +82,23 @@ def test_mixed_eval_vs_fp64(key, sysk, mk):
     assert rms_err <= 5e-3
     assert rms_err <= 3e-2 * rms_f
     assert e_err <= 2e-2 * np.abs(ref["atom_energy"]).mean() + 1e-6
+
+
+def test_mixed_default_train_widths():
+    """The reference train() default architecture (embed 32-32-64, fit 128^3,
+    axis 12; deepmd_jax/train.py:24-27) in the mixed form, against FP64."""
+    from deepmd_jax_b200.systems import water_box, init_dp_params
+    from make_golden import randomize_model
+    w = water_box(8, 24.83, seed=5)
+    p, v = randomize_model(*init_dp_params(embed_widths=(32, 32, 64), fit_widths=(128, 128, 128), axis=12,
+                                           nnbrs=90.0, seed=3), seed=4)
+    got = run_gpu(p, v, w["position"], w["box"], w["type_idx"], precision="mixed")
+    assert got["status"] == 0
+    ref = om.energy_force(om.OracleModel(p, v, torch.float64), w["position"], w["box"], w["type_idx"],
+                          nbrs=got["nbrs"][0], sel=[46, 92])
+    N = len(w["type_idx"])
+    rms_err = np.sqrt(((got["force"][0] - ref["force"]) ** 2).mean())
+    rms_f = np.sqrt((ref["force"] ** 2).mean())
+    print("mixed default widths: force rms err %.3e (rel %.3e)" % (rms_err, rms_err / rms_f))
+    assert rms_err <= 5e-3 and rms_err <= 3e-2 * rms_f
+    assert abs(got["energy"][0] - ref["energy"]) / N <= 2e-2 * np.abs(ref["atom_energy"]).mean() + 1e-6
