@@ -179,3 +179,36 @@ def test_evaluate_compressed_model_pkl(tmp_path):
     out = evaluate(path, pos[None], box[None], typ)
     ref = om.energy_force(om.OracleModel(p, v, torch.float64), pos, box, typ, virial=False)
     _close(out["energy"][0], out["force"][0], ref["energy"], ref["force"], len(typ))
+
+
+class _Atoms:
+    """The part of ase.Atoms the calculator reads (ASE is not installed)."""
+
+    def __init__(self, positions, cell):
+        self._p, self._c = np.array(positions, float), np.array(cell, float)
+
+    def copy(self):
+        return _Atoms(self._p, self._c)
+
+    def get_positions(self):
+        return self._p.copy()
+
+    def get_cell(self, complete=False):
+        return self._c.copy()
+
+
+def test_ase_calculator_energy_forces_stress(tmp_path):
+    """DPJaxCalculator (deepmd_jax/ase_calc.py:18-144): energy and forces of
+    the reference golden vectors; stress = -W / V in Voigt order against the
+    float64 oracle's virial."""
+    from deepmd_jax_b200.ase_calc import DPJaxCalculator
+    path = _pkl(tmp_path, "B")
+    pos, box, typ = G["A_pos"], G["A_box"], G["A_type"]
+    calc = DPJaxCalculator(path, type_idx=typ)
+    atoms = _Atoms(pos, np.diag(box))
+    E, F, S = calc.get_potential_energy(atoms), calc.get_forces(atoms), calc.get_stress(atoms)
+    _close(E, F, float(G["B_E"]), G["B_F"], len(typ))
+    W = om.energy_force(om.OracleModel(*MODELS["B"], torch.float64), pos, box, typ)["virial"]
+    V = float(np.prod(box))
+    ref = -np.array([W[0, 0], W[1, 1], W[2, 2], W[1, 2], W[0, 2], W[0, 1]]) / V
+    assert S.shape == (6,) and np.abs(S - ref).max() <= 2e-4 * np.abs(ref).max() + 1e-12
