@@ -104,6 +104,25 @@ static int upload_bf16(dpb_model *m, const std::vector<float> &v, const __nv_bfl
   return upload(m, b.data(), b.size(), dev);
 }
 
+// B operand chunks of the mixed fitting kernel from a row-major matrix
+// (rows x K): for pass p of br rows and K chunk k (16 wide), the chunk is
+// [half (2)][row (br)][8] BF16, rows past `rows` zero (mixed.cu, k_mix_fit).
+static int upload_fit_tiles(dpb_model *m, const std::vector<float> &a, int rows, int K, int br,
+                            const __nv_bfloat16 **dev) {
+  const int nk = K / 16, npass = (rows + br - 1) / br;
+  std::vector<float> t((size_t)npass * nk * 2 * br * 8, 0.f);
+  for (int p = 0; p < npass; ++p)
+    for (int k = 0; k < nk; ++k)
+      for (int h = 0; h < 2; ++h)
+        for (int r = 0; r < br; ++r) {
+          const int row = p * br + r;
+          if (row >= rows) continue;
+          for (int e = 0; e < 8; ++e)
+            t[((((size_t)p * nk + k) * 2 + h) * br + r) * 8 + e] = a[(size_t)row * K + k * 16 + h * 8 + e];
+        }
+  return upload_bf16(m, t, dev);
+}
+
 static bool embed_supported(const DevModel &M) {
   return (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
 }
@@ -219,6 +238,11 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
       if (rc == DPB_OK) rc = upload(m, kt.data(), kt.size(), &M.fwT[t][l]);
       if (rc == DPB_OK) rc = upload_bf16(m, kv, &M.fw_bf[t][l]);
       if (rc == DPB_OK) rc = upload_bf16(m, kt, &M.fwT_bf[t][l]);
+      if (rc == DPB_OK && l < M.nfit && mixed_supported(M)) {
+        rc = upload_fit_tiles(m, kt, outw, in, outw, &M.fit_bt[t][kFitBtFwd + l]);
+        if (rc == DPB_OK && l >= 1) rc = upload_fit_tiles(m, kv, in, outw, in, &M.fit_bt[t][kFitBtAdj + l]);
+        if (rc == DPB_OK && l == 0) rc = upload_fit_tiles(m, kv, K0, outw, 128, &M.fit_bt[t][kFitBtDg]);
+      }
       if (rc == DPB_OK && l < M.nfit) {
         const float *dt = d->fit_dt ? d->fit_dt[t * M.nfit + l] : nullptr;
         if (dt) rc = upload(m, dt, (size_t)outw, &M.fdt[t][l]);

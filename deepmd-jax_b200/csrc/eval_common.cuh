@@ -45,7 +45,14 @@ struct DevModel {
   int ngrids;
   const float *cmp_coeff[kMaxTypes * kMaxTypes];
   float cmp_srmin[kMaxTypes * kMaxTypes], cmp_delta[kMaxTypes * kMaxTypes];
+  // BF16 fitting weights pre-tiled as the B operand chunks of the mixed
+  // fitting kernel (K = 16 per chunk, [chunk][k8 (2)][row][8]): forward layer l
+  // at kFitBtFwd + l (W_l^T), adjoint layer l >= 1 at kFitBtAdj + l (W_l), and
+  // W_0 in passes of 128 rows at kFitBtDg; null when the mixed form is unsupported
+  const __nv_bfloat16 *fit_bt[kMaxTypes][2 * kMaxFitLayers + 1];
 };
+
+constexpr int kFitBtFwd = 0, kFitBtAdj = kMaxFitLayers, kFitBtDg = 2 * kMaxFitLayers;
 
 // Frame/type geometry of one evaluation call.
 // Packed (ragged) batches run as one frame (F = 1) whose atoms come from many

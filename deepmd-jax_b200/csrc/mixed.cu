@@ -1114,340 +1114,422 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
   return DPB_OK;
 }
 
-// ---------------------------------------------------------------- fitting chain (BF16 tcgen05)
+// ---------------------------------------------------------------- fitting chain (BF16 tcgen05, TMA weights)
 // One CTA per 128 atoms of one centre type (thread = atom = TMEM lane).  The
-// forward layers and the adjoint down to dE/dG are GEMMs of M = 128 on the
-// tensor cores.  B (weights, BF16, K contiguous) and, for the first layer, A
-// (the BF16 descriptor rows) are copied asynchronously (cp.async) into two
-// shared-memory chunk buffers while the previous chunk's MMAs run.
+// forward layers, the adjoint down to the first hidden layer and dE/dG are a
+// fixed sequence of M = 128 GEMMs on the tensor cores, with L hidden layers:
+//   g <  L           forward layer g        A: G rows (g = 0) or H    B: W_g^T  (out x in)
+//   L <= g < 2L - 1  adjoint layer 2L-1-g   A: gZ                     B: W_l    (in x out)
+//   g >= 2L - 1      dE/dG columns [128 p, 128 p + 128), p = g - (2L - 1), B: rows of W_0
+// Warp roles (160 threads): warps 0-3 are the epilogue, one thread per atom,
+// which also stream layer 0's G rows into the ring with cp.async; lane 0 of
+// warp 4 issues the bulk (TMA) copies of the weights and the MMAs.  Operands
+// pass through a ring of K = 16 stages (full / empty mbarriers), so the
+// weights of the next GEMM are already in flight while the epilogue of the
+// current one runs; the dE/dG passes alternate between two TMEM accumulators
+// so that the epilogue of pass p overlaps the MMAs of pass p + 1.
+// A stage holds the A chunk as [k8 (2)][row (128)][8 bf16] and the B chunk as
+// [k8 (2)][row (br)][8 bf16] (K-major core matrices, no swizzle: LBO = rows x
+// 16 B between the two K halves, SBO = 128 B between 8-row groups).  The
+// weights are stored pre-tiled in exactly this chunk layout (DevModel::fit_bt,
+// built at model creation), so a B chunk is one contiguous cp.async.bulk.
 // Epilogues run in FP32 on the CUDA cores: tanh, dt-residuals, the energy dot
-// product (FP64 frame sums) and the adjoint gates; tanh values and residual
+// product (FP64 segment sums) and the adjoint gates; tanh values and residual
 // sources go to a per-atom FP32 scratch, the BF16 activation of the next GEMM
 // stays in shared memory.  2 CTAs per SM, 256 TMEM columns each.
-constexpr int kFitKC = 32;                 // K per chunk (multiple of 16)
-constexpr int kFitMaxN = 256;              // N per GEMM pass
-constexpr int kFitBufA = 128 * kFitKC * 2;
-constexpr int kFitBufB = kFitMaxN * kFitKC * 2;
+constexpr int kFitThreads = 160;
+constexpr int kFitDgN = 128;                 // N of one dE/dG pass
+constexpr int kFitStageA = 2 * 128 * 16;     // A chunk bytes (K = 16)
 
-struct FitStream {
-  char *buf[2];
-  uint64_t *bar;      // [2]
-  uint32_t uses[2];
+template <int FW>
+struct FitCfg {
+  static constexpr int BR = FW > kFitDgN ? FW : kFitDgN;  // rows of the largest B box
+  static constexpr int STAGE = kFitStageA + 2 * BR * 16;
+  static constexpr int ST = FW > 128 ? 4 : 8;              // ring depth (2 CTAs per SM)
+  static constexpr int HAB = 128 * FW * 2;
+  static constexpr size_t SMEM = (size_t)round1k(HAB) + (size_t)ST * STAGE;
 };
 
-__device__ __forceinline__ void fit_issue_chunk(char *bufb, bool streamA, const __nv_bfloat16 *__restrict__ Gb,
-                                                const size_t *atom_of_row, int nrows, int ldg,
-                                                const __nv_bfloat16 *__restrict__ B, int ldb, int n0, int nvalid,
-                                                int N, int k0, int kvalid) {
-  constexpr int c8 = kFitKC / 8;
-  if (streamA) {
-    for (int e = threadIdx.x; e < 128 * c8; e += blockDim.x) {
-      const int r = e / c8, k8 = (e - r * c8) * 8;
-      char *dst = bufb + tc::kmajor_off(r, k8, kFitKC);
-      if (r < nrows && k8 < kvalid) tc::cp_async16(dst, Gb + atom_of_row[r] * ldg + k0 + k8);
-      else *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
-    }
+// Bounded mbarrier wait that also gives up once another role of the CTA gave
+// up (*abort), so every role leaves its loop and reaches the final barrier.
+__device__ __forceinline__ bool fit_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+  const uint32_t a = tc::smem_u32(bar);
+  for (int it = 0; it < tc::kWaitLimit; ++it) {
+    if (tc::mbar_test(a, parity)) return true;
+    if ((it & 31) == 31 && *abort) return false;
   }
-  char *bb = bufb + (streamA ? kFitBufA : 0);
-  for (int e = threadIdx.x; e < N * c8; e += blockDim.x) {
-    const int n = e / c8, k8 = (e - n * c8) * 8;
-    char *dst = bb + tc::kmajor_off(n, k8, kFitKC);
-    if (n < nvalid && k8 < kvalid) tc::cp_async16(dst, B + (size_t)(n0 + n) * ldb + k0 + k8);
-    else *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
-  }
-  tc::cp_async_commit();
+  *abort = 1;
+  return false;
 }
 
-// D[128 x N] = A[128 x K] . B-rows[n0 : n0 + N][k] (B row stride ldb).  A is
-// resident (K-major tile with row length Kres) or streamed from the BF16
-// descriptor rows.  Returns false when a barrier wait gave up.
-__device__ bool fit_gemm(FitStream &S, uint32_t tmem_d, int N, int nvalid, int K, const __nv_bfloat16 *B, int ldb,
-                         int n0, const char *A_res, int Kres, const __nv_bfloat16 *Gb, const size_t *atom_of_row,
-                         int nrows, int ldg) {
-  const int nch = (K + kFitKC - 1) / kFitKC;
-  const uint32_t idesc = tc::idesc_bf16(128, N, 0, 0);
-  const bool streamA = A_res == nullptr;
-  bool ok = true;
-  // prefetch chunk 0 (its buffer is free once the MMA that last used it is done)
-  {
-    const int b = 0;
-    if (S.uses[b] > 0) {
-      const bool w = tc::mbar_wait(&S.bar[b], (S.uses[b] - 1) & 1);
-      ok = __syncthreads_and(w && ok) != 0;
-      if (!ok) return false;
-    }
-    fit_issue_chunk(S.buf[b], streamA, Gb, atom_of_row, nrows, ldg, B, ldb, n0, nvalid, N, 0, min(kFitKC, K));
+// Epilogue -> issuer hand-over: TMEM reads done, shared-memory operand written.
+__device__ __forceinline__ void fit_signal(uint64_t *bar) {
+  tc::fence_before_sync();
+  tc::fence_proxy_async();
+  tc::mbar_arrive(bar);
+}
+
+struct FitGemm {
+  const char *src;  // pre-tiled B chunks of this GEMM, br x 32 bytes each
+  int N, nk, br, col;  // MMA N, K chunks, B rows per chunk, TMEM column
+};
+
+template <int FW>
+__device__ __forceinline__ FitGemm fit_gemm_info(const DevModel &M, int ti, int g, int L, int K0) {
+  FitGemm G;
+  if (g < L) {
+    G.src = reinterpret_cast<const char *>(M.fit_bt[ti][kFitBtFwd + g]);
+    G.N = FW; G.nk = (g == 0 ? K0 : FW) / 16; G.br = FW; G.col = 0;
+  } else if (g < 2 * L - 1) {
+    G.src = reinterpret_cast<const char *>(M.fit_bt[ti][kFitBtAdj + 2 * L - 1 - g]);
+    G.N = FW; G.nk = FW / 16; G.br = FW; G.col = 0;
+  } else {
+    const int p = g - (2 * L - 1);
+    G.nk = FW / 16; G.br = kFitDgN;
+    G.src = reinterpret_cast<const char *>(M.fit_bt[ti][kFitBtDg]) + (size_t)p * G.nk * kFitDgN * 32;
+    G.N = min(kFitDgN, K0 - kFitDgN * p);
+    G.col = kFitDgN * (p & 1);
   }
-  for (int c = 0; c < nch; ++c) {
-    const int bc = c & 1;
-    if (c + 1 < nch) {
-      const int bn = (c + 1) & 1;
-      if (S.uses[bn] > 0) {
-        const bool w = tc::mbar_wait(&S.bar[bn], (S.uses[bn] - 1) & 1);
-        ok = __syncthreads_and(w && ok) != 0;
-        if (!ok) return false;
-      }
-      const int k1 = (c + 1) * kFitKC;
-      fit_issue_chunk(S.buf[bn], streamA, Gb, atom_of_row, nrows, ldg, B, ldb, n0, nvalid, N, k1,
-                      min(kFitKC, K - k1));
-      tc::cp_async_wait<1>();
-    } else {
-      tc::cp_async_wait<0>();
-    }
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tc::fence_after_sync();
-      const int k0 = c * kFitKC;
-      const uint32_t bu = tc::smem_u32(S.buf[bc]);
-      const uint32_t bb = bu + (streamA ? kFitBufA : 0);
-#pragma unroll
-      for (int ks = 0; ks < kFitKC / 16; ++ks) {
-        uint64_t ad;
-        if (!streamA)
-          ad = tc::make_desc(tc::smem_u32(A_res) + tc::kmajor_off(0, k0 + 16 * ks, Kres), 128, (Kres / 8) * 128);
-        else
-          ad = tc::make_desc(bu + tc::kmajor_off(0, 16 * ks, kFitKC), 128, (kFitKC / 8) * 128);
-        const uint64_t bd = tc::make_desc(bb + tc::kmajor_off(0, 16 * ks, kFitKC), 128, (kFitKC / 8) * 128);
-        tc::mma_bf16(tmem_d, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-      }
-      tc::commit(&S.bar[bc]);
-    }
-    S.uses[bc]++;
-  }
-  const int bl = (nch - 1) & 1;
-  const bool w = tc::mbar_wait(&S.bar[bl], (S.uses[bl] - 1) & 1);
-  ok = __syncthreads_and(w && ok) != 0;
-  tc::fence_after_sync();
-  return ok;
+  return G;
 }
 
 template <int FW>
-__global__ void __launch_bounds__(128, 2) k_mix_fit(DevModel M, int ti, int Mrows, RowMap rm,
-                                                    const __nv_bfloat16 *__restrict__ Gb, float *__restrict__ dGout,
-                                                    float *__restrict__ scratch, float *__restrict__ Eatom,
-                                                    double *__restrict__ energy, int N, int *__restrict__ err,
-                                                    const int32_t *__restrict__ seg, int tile0) {
-  static_assert(FW % 32 == 0 || FW % 16 == 0, "fit width");
+__global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
+                                                           int Mrows, RowMap rm,
+                                                           const __nv_bfloat16 *__restrict__ Gb,
+                                                           float *__restrict__ dGout, float *__restrict__ scratch,
+                                                           float *__restrict__ Eatom, double *__restrict__ energy,
+                                                           int N, int *__restrict__ err,
+                                                           const int32_t *__restrict__ seg, int tile0) {
+  using C = FitCfg<FW>;
+  constexpr int ST = C::ST;
+  static_assert(FW % 16 == 0 && FW <= 256, "fit width");
   extern __shared__ __align__(1024) char smem[];
-  char *HA = smem;                                  // 128 x FW bf16 (K-major)
-  char *bufs = HA + round1k(128 * FW * 2);
-  __shared__ __align__(8) uint64_t bars[2];
+  char *HA = smem;                        // 128 x FW bf16, K-major (kmajor_off)
+  char *ring = smem + round1k(C::HAB);    // ST stages
+  __shared__ __align__(8) uint64_t full[ST], fullA[ST], empty[ST], accf, accfD[2], epid, accfree[2];
   __shared__ uint32_t tbase_s;
-  __shared__ size_t atom_s[128];
-  __shared__ double es[128];
+  __shared__ int abort_s;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int L = M.nfit, K0 = M.A * M.E2;
-  if (tid < 2) tc::mbar_init(&bars[tid], 1);
+  const int NG = 2 * L - 1 + (K0 + kFitDgN - 1) / kFitDgN;
+  volatile int *abort = &abort_s;
+  if (tid == 0) {
+    for (int s = 0; s < ST; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&fullA[s], 128);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(&accf, 1);
+    tc::mbar_init(&accfD[0], 1);
+    tc::mbar_init(&accfD[1], 1);
+    tc::mbar_init(&epid, 128);
+    tc::mbar_init(&accfree[0], 128);
+    tc::mbar_init(&accfree[1], 128);
+    abort_s = 0;
+    tc::fence_mbar_init();
+  }
   if (warp == 0) tc::tmem_alloc(&tbase_s, 256);
-  FitStream S;
-  S.buf[0] = bufs;
-  S.buf[1] = bufs + kFitBufA + kFitBufB;
-  S.bar = bars;
-  S.uses[0] = S.uses[1] = 0;
-  const int r0 = blockIdx.x * 128, nrows = min(128, Mrows - r0);
-  const bool act = tid < nrows;
-  atom_s[tid] = act ? rm.atom(r0 + tid) : rm.atom(r0);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t td = tbase_s, lane_off = (uint32_t)(warp * 32) << 16;
-  const size_t me = atom_s[tid];
-  // per-CTA scratch tile [slot][n][thread] (coalesced): slots 0..L-1 tanh
-  // values, L..2L-1 layer outputs, 2L the residual adjoint
-  float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + tid;
+  const uint32_t td = tbase_s;
+  const int r0 = blockIdx.x * 128, nrows = min(128, Mrows - r0);
+
+  if (warp == 4) {
+    // ================= TMA + MMA issuer (one thread)
+    if ((tid & 31) == 0) {
+      const uint32_t ring_u = tc::smem_u32(ring), ha_u = tc::smem_u32(HA);
+      int total = 0;
+      for (int g = 0; g < NG; ++g) total += fit_gemm_info<FW>(M, ti, g, L, K0).nk;
+      int p = 0, pg = 0, pk = 0;  // next chunk to load: global index, its GEMM, its K chunk
+      FitGemm pgi = fit_gemm_info<FW>(M, ti, 0, L, K0);
+      int q = 0;                  // next chunk to multiply
+      uint32_t epid_n = 0;
+      bool ok = true;
+      for (int g = 0; g < NG && ok; ++g) {
+        const FitGemm gi = fit_gemm_info<FW>(M, ti, g, L, K0);
+        if (g >= 1 && g <= 2 * L - 1) {  // A operand (and the accumulator) handed back by the epilogue
+          ok = fit_wait(&epid, epid_n & 1, abort);
+          ++epid_n;
+        } else if (g >= 2 * L + 1) {     // dE/dG pass p reuses the accumulator of pass p - 2
+          const int pp = g - (2 * L - 1);
+          ok = fit_wait(&accfree[pp & 1], ((pp >> 1) - 1) & 1, abort);
+        }
+        if (!ok) break;
+        tc::fence_after_sync();
+        const uint32_t idesc = tc::idesc_bf16(128, gi.N, 0, 0);
+        for (int k = 0; k < gi.nk; ++k, ++q) {
+          while (p < total && p < q + ST) {  // keep the ring full
+            const int s = p % ST;
+            if (p >= ST && !(ok = fit_wait(&empty[s], ((p / ST) - 1) & 1, abort))) break;
+            const uint32_t bytes = (uint32_t)pgi.br * 32u;
+            tc::mbar_arrive_expect_tx(&full[s], bytes);
+            tc::bulk_load(ring_u + s * C::STAGE + kFitStageA, pgi.src + (size_t)pk * bytes, bytes, &full[s]);
+            ++p;
+            if (++pk == pgi.nk) {
+              pk = 0;
+              if (++pg < NG) pgi = fit_gemm_info<FW>(M, ti, pg, L, K0);
+            }
+          }
+          if (!ok) break;
+          const int s = q % ST;
+          const uint32_t par = (q / ST) & 1;
+          ok = fit_wait(&full[s], par, abort) && (g != 0 || fit_wait(&fullA[s], par, abort));
+          if (!ok) break;
+          tc::fence_after_sync();
+          const uint32_t st_u = ring_u + s * C::STAGE;
+          const uint64_t ad = (g == 0) ? tc::make_desc(st_u, 128 * 16, 128)
+                                       : tc::make_desc(ha_u + tc::kmajor_off(0, 16 * k, FW), 128, (FW / 8) * 128);
+          const uint64_t bd = tc::make_desc(st_u + kFitStageA, (uint32_t)gi.br * 16, 128);
+          tc::mma_bf16(td + gi.col, ad, bd, idesc, k > 0 ? 1u : 0u);
+          tc::commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc::commit(g < 2 * L - 1 ? &accf : &accfD[(g - (2 * L - 1)) & 1]);
+      }
+      // nothing of this CTA may be in flight when it exits: loads issued but
+      // never multiplied (only after a give-up), and the last MMAs
+      for (int c = q; c < p; ++c) tc::mbar_wait(&full[c % ST], (c / ST) & 1);
+      if (q > 0) tc::mbar_wait(&empty[(q - 1) % ST], ((q - 1) / ST) & 1);
+    }
+  } else {
+    // ================= epilogue warps: thread = atom = TMEM lane
+    const int row = tid;
+    const bool act = row < nrows;
+    const size_t me = rm.atom(act ? r0 + row : r0);
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    bool ok = true;
+    // ---- layer 0's A operand: this atom's G row, ST - 1 chunks in flight
+    {
+      const int nch0 = K0 / 16;
+      const char *grow = reinterpret_cast<const char *>(Gb + me * (size_t)K0);
+      for (int c = 0; c < nch0 + ST - 1; ++c) {
+        if (c < nch0) {
+          const int s = c % ST;
+          if (c >= ST && !(ok = __all_sync(0xffffffffu, fit_wait(&empty[s], ((c / ST) - 1) & 1, abort)))) break;
+          char *dst = ring + s * C::STAGE + row * 16;
+          if (act) {
+            tc::cp_async16(dst, grow + c * 32);
+            tc::cp_async16(dst + 128 * 16, grow + c * 32 + 16);
+          } else {
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(dst + 128 * 16) = make_uint4(0, 0, 0, 0);
+          }
+        }
+        tc::cp_async_commit();
+        const int cc = c - (ST - 1);
+        if (cc >= 0) {
+          tc::cp_async_wait<ST - 1>();
+          tc::fence_proxy_async();
+          tc::mbar_arrive(&fullA[cc % ST]);
+        }
+      }
+    }
+    uint32_t accf_n = 0;
+    // per-CTA scratch tile [slot][n][thread] (coalesced): slots 0..L-1 tanh
+    // values, L..2L-1 layer outputs, 2L the residual adjoint
+    float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + row;
 #define FIT_SCR(slot, n) tile[((size_t)(slot) * FW + (n)) * 128]
-  bool ok = true;
-  // ---- forward
-  for (int l = 0; l < L && ok; ++l) {
-    if (l == 0)
-      ok = fit_gemm(S, td, FW, FW, K0, M.fwT_bf[ti][0], K0, 0, nullptr, 0, Gb, atom_s, nrows, K0);
-    else
-      ok = fit_gemm(S, td, FW, FW, FW, M.fwT_bf[ti][l], FW, 0, HA, FW, nullptr, nullptr, 0, 0);
-    if (!ok) break;
-    const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
-    // residual sources of the current chunk, loaded one chunk ahead so the
-    // scratch reads overlap the TMEM loads and the previous chunk's math
-    float hp[16];
+    // ---- forward
+    for (int l = 0; l < L && ok; ++l) {
+      ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
+      ++accf_n;
+      if (!ok) break;
+      tc::fence_after_sync();
+      const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
+      // residual sources of the current chunk, loaded one chunk ahead so the
+      // scratch reads overlap the TMEM loads and the previous chunk's math
+      float hp[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) hp[i] = dt ? FIT_SCR(L + l - 1, i) : 0.f;
-    for (int c0 = 0; c0 < FW; c0 += 16) {
-      uint32_t r[16];
-      tc::tmem_ld16_issue(td + lane_off + c0, r);
-      float hn[16];
+      for (int i = 0; i < 16; ++i) hp[i] = dt ? FIT_SCR(L + l - 1, i) : 0.f;
+      for (int c0 = 0; c0 < FW; c0 += 16) {
+        uint32_t r[16];
+        tc::tmem_ld16_issue(td + lane_off + c0, r);
+        float hn[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) hn[i] = (dt && c0 + 16 < FW) ? FIT_SCR(L + l - 1, c0 + 16 + i) : 0.f;
-      float bv[16], dv[16];
+        for (int i = 0; i < 16; ++i) hn[i] = (dt && c0 + 16 < FW) ? FIT_SCR(L + l - 1, c0 + 16 + i) : 0.f;
+        float bv[16], dv[16];
 #pragma unroll
-      for (int i = 0; i < 16; i += 4) {
-        const float4 b4 = __ldg(reinterpret_cast<const float4 *>(bias + c0 + i));
-        bv[i] = b4.x; bv[i + 1] = b4.y; bv[i + 2] = b4.z; bv[i + 3] = b4.w;
-        const float4 d4 = dt ? __ldg(reinterpret_cast<const float4 *>(dt + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
-        dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+        for (int i = 0; i < 16; i += 4) {
+          const float4 b4 = __ldg(reinterpret_cast<const float4 *>(bias + c0 + i));
+          bv[i] = b4.x; bv[i + 1] = b4.y; bv[i + 2] = b4.z; bv[i + 3] = b4.w;
+          const float4 d4 =
+              dt ? __ldg(reinterpret_cast<const float4 *>(dt + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
+          dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+        }
+        tc::tmem_wait();
+        float hv[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int n = c0 + i;
+          const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
+          float h = t;
+          if (dt) h = t * dv[i] + hp[i];
+          hv[i] = h;
+          FIT_SCR(l, n) = t;
+          FIT_SCR(L + l, n) = h;
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) hp[i] = hn[i];
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(hv);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(hv + 8);
       }
-      tc::tmem_wait();
-      float hv[16];
+      if (l < L - 1) fit_signal(&epid);
+    }
+    // ---- energy and the first adjoint gate
+    float e_me = 0.f;
+    if (ok) {
+      const float *wf = M.fw[ti][L], *dtL = M.fdt[ti][L - 1];
+      float s = 0.f;
+      float hc[16], tcur[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int n = c0 + i;
-        const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
-        float h = t;
-        if (dt) h = t * dv[i] + hp[i];
-        hv[i] = h;
-        FIT_SCR(l, n) = t;
-        FIT_SCR(L + l, n) = h;
+        hc[i] = FIT_SCR(2 * L - 1, i);
+        tcur[i] = FIT_SCR(L - 1, i);
       }
+      for (int c0 = 0; c0 < FW; c0 += 16) {
+        float hn[16], tn[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) hp[i] = hn[i];
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(hv);
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(hv + 8);
-    }
-    tc::fence_before_sync();
-  }
-  // ---- energy and the first adjoint gate
-  double e_me = 0.0;
-  if (ok) {
-    const float *wf = M.fw[ti][L], *dtL = M.fdt[ti][L - 1];
-    float s = 0.f;
-    float hc[16], tcur[16];
+        for (int i = 0; i < 16; ++i) {
+          hn[i] = (c0 + 16 < FW) ? FIT_SCR(2 * L - 1, c0 + 16 + i) : 0.f;
+          tn[i] = (c0 + 16 < FW) ? FIT_SCR(L - 1, c0 + 16 + i) : 0.f;
+        }
+        float g[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      hc[i] = FIT_SCR(2 * L - 1, i);
-      tcur[i] = FIT_SCR(L - 1, i);
+        for (int i = 0; i < 16; ++i) {
+          const int n = c0 + i;
+          const float wn = __ldg(wf + n);
+          s = fmaf(hc[i], wn, s);
+          g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - tcur[i] * tcur[i]);
+        }
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(g);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(g + 8);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          hc[i] = hn[i];
+          tcur[i] = tn[i];
+        }
+      }
+      fit_signal(&epid);
+      e_me = s + M.fb[ti][L][0];
+      if (act) Eatom[me] = e_me;
     }
-    for (int c0 = 0; c0 < FW; c0 += 16) {
-      float hn[16], tn[16];
+    {  // energy per segment (every lane of the warp takes part): rows run
+       // through the segments in order, so a warp suffix sum over equal keys
+       // leaves each run's total at its first lane
+      const int lane = row & 31;
+      const int key = (ok && act) ? energy_slot(seg, me, N) : -2;
+      double v = (ok && act) ? (double)e_me : 0.0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double o = __shfl_down_sync(0xffffffffu, v, off);
+        const int ko = __shfl_down_sync(0xffffffffu, key, off);
+        if (lane + off < 32 && ko == key) v += o;
+      }
+      const int kprev = __shfl_up_sync(0xffffffffu, key, 1);
+      if (key >= 0 && (lane == 0 || kprev != key)) atomicAdd(&energy[key], v);
+    }
+    // ---- adjoint: layers L-1 .. 1, gH_{l-1} = gZ_l W_l^T (+ gH_l if residual)
+    for (int l = L - 1; l >= 1 && ok; --l) {
+      ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
+      ++accf_n;
+      if (!ok) break;
+      tc::fence_after_sync();
+      const bool res_l = M.fdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.fdt[ti][l - 1] != nullptr;
+      const float *dtm1 = M.fdt[ti][l - 1], *wf = M.fw[ti][L];
+      const bool use_gh = res_l && l != L - 1;
+      float ghc[16], tcur[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        hn[i] = (c0 + 16 < FW) ? FIT_SCR(2 * L - 1, c0 + 16 + i) : 0.f;
-        tn[i] = (c0 + 16 < FW) ? FIT_SCR(L - 1, c0 + 16 + i) : 0.f;
+        ghc[i] = use_gh ? FIT_SCR(2 * L, i) : 0.f;
+        tcur[i] = FIT_SCR(l - 1, i);
       }
-      float g[16];
+      for (int c0 = 0; c0 < FW; c0 += 16) {
+        uint32_t r[16];
+        tc::tmem_ld16_issue(td + lane_off + c0, r);
+        float ghn[16], tn[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int n = c0 + i;
-        const float wn = __ldg(wf + n);
-        s = fmaf(hc[i], wn, s);
-        g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - tcur[i] * tcur[i]);
-      }
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(g);
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(g + 8);
+        for (int i = 0; i < 16; ++i) {
+          ghn[i] = (use_gh && c0 + 16 < FW) ? FIT_SCR(2 * L, c0 + 16 + i) : 0.f;
+          tn[i] = (c0 + 16 < FW) ? FIT_SCR(l - 1, c0 + 16 + i) : 0.f;
+        }
+        float wv[16], dv[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        hc[i] = hn[i];
-        tcur[i] = tn[i];
+        for (int i = 0; i < 16; i += 4) {
+          const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wf + c0 + i));
+          wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
+          const float4 d4 =
+              res_lm1 ? __ldg(reinterpret_cast<const float4 *>(dtm1 + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
+          dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+        }
+        tc::tmem_wait();
+        float gz[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int n = c0 + i;
+          float g = __uint_as_float(r[i]);
+          if (res_l) g += (l == L - 1) ? wv[i] : ghc[i];
+          const float t = tcur[i];
+          gz[i] = g * dv[i] * (1.f - t * t);
+          if (res_lm1) FIT_SCR(2 * L, n) = g;
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          ghc[i] = ghn[i];
+          tcur[i] = tn[i];
+        }
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(gz);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(gz + 8);
       }
+      fit_signal(&epid);
     }
-    s += M.fb[ti][L][0];
-    if (act) Eatom[me] = s;
-    e_me = act ? (double)s : 0.0;
-  }
-  es[tid] = e_me;
-  __syncthreads();
-  if (tid == 0 && ok) {
-    double run = 0.0;
-    int cf = energy_slot(seg, atom_s[0], N);
-    for (int k = 0; k < nrows; ++k) {
-      const int fk = energy_slot(seg, atom_s[k], N);
-      if (fk != cf) {
-        if (cf >= 0) atomicAdd(&energy[cf], run);
-        run = 0.0;
-        cf = fk;
+    // ---- dE/dG = gZ_0 W_0^T, 128 columns per pass from alternating accumulators
+    const int npass = (K0 + kFitDgN - 1) / kFitDgN;
+    for (int pp = 0; pp < npass && ok; ++pp) {
+      ok = __all_sync(0xffffffffu, fit_wait(&accfD[pp & 1], (pp >> 1) & 1, abort));
+      if (!ok) break;
+      tc::fence_after_sync();
+      const int n0 = kFitDgN * pp, nv = min(kFitDgN, K0 - n0);
+      const uint32_t tcol = td + lane_off + kFitDgN * (pp & 1);
+      for (int c0 = 0; c0 < nv; c0 += 32) {
+        const bool two = c0 + 16 < nv;
+        uint32_t ra[16], rb[16];
+        tc::tmem_ld16_issue(tcol + c0, ra);
+        if (two) tc::tmem_ld16_issue(tcol + c0 + 16, rb);
+        tc::tmem_wait();
+        if (act) {
+          float4 *dst = reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0);
+#pragma unroll
+          for (int i = 0; i < 16; i += 4)
+            dst[i / 4] = make_float4(__uint_as_float(ra[i]), __uint_as_float(ra[i + 1]), __uint_as_float(ra[i + 2]),
+                                     __uint_as_float(ra[i + 3]));
+          if (two) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 4)
+              dst[4 + i / 4] = make_float4(__uint_as_float(rb[i]), __uint_as_float(rb[i + 1]),
+                                           __uint_as_float(rb[i + 2]), __uint_as_float(rb[i + 3]));
+          }
+        }
       }
-      run += es[k];
+      tc::fence_before_sync();
+      tc::mbar_arrive(&accfree[pp & 1]);
     }
-    if (cf >= 0) atomicAdd(&energy[cf], run);
-  }
-  // ---- adjoint: layers L-1 .. 1, gH_{l-1} = gZ_l W_l^T (+ gH_l if residual)
-  for (int l = L - 1; l >= 1 && ok; --l) {
-    ok = fit_gemm(S, td, FW, FW, FW, M.fw_bf[ti][l], FW, 0, HA, FW, nullptr, nullptr, 0, 0);
-    if (!ok) break;
-    const bool res_l = M.fdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.fdt[ti][l - 1] != nullptr;
-    const float *dtm1 = M.fdt[ti][l - 1], *wf = M.fw[ti][L];
-    const bool use_gh = res_l && l != L - 1;
-    float ghc[16], tcur[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      ghc[i] = use_gh ? FIT_SCR(2 * L, i) : 0.f;
-      tcur[i] = FIT_SCR(l - 1, i);
-    }
-    for (int c0 = 0; c0 < FW; c0 += 16) {
-      uint32_t r[16];
-      tc::tmem_ld16_issue(td + lane_off + c0, r);
-      float ghn[16], tn[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        ghn[i] = (use_gh && c0 + 16 < FW) ? FIT_SCR(2 * L, c0 + 16 + i) : 0.f;
-        tn[i] = (c0 + 16 < FW) ? FIT_SCR(l - 1, c0 + 16 + i) : 0.f;
-      }
-      float wv[16], dv[16];
-#pragma unroll
-      for (int i = 0; i < 16; i += 4) {
-        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wf + c0 + i));
-        wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
-        const float4 d4 =
-            res_lm1 ? __ldg(reinterpret_cast<const float4 *>(dtm1 + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
-        dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
-      }
-      tc::tmem_wait();
-      float gz[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int n = c0 + i;
-        float g = __uint_as_float(r[i]);
-        if (res_l) g += (l == L - 1) ? wv[i] : ghc[i];
-        const float t = tcur[i];
-        gz[i] = g * dv[i] * (1.f - t * t);
-        if (res_lm1) FIT_SCR(2 * L, n) = g;
-      }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        ghc[i] = ghn[i];
-        tcur[i] = tn[i];
-      }
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0, FW)) = pack8(gz);
-      *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(tid, c0 + 8, FW)) = pack8(gz + 8);
-    }
-    tc::fence_before_sync();
-  }
-  // ---- dE/dG = gZ_0 W_0^T in column passes of 256
-  for (int n0 = 0; n0 < K0 && ok; n0 += kFitMaxN) {
-    const int nv = min(kFitMaxN, K0 - n0), Np = (nv + 15) / 16 * 16;
-    ok = fit_gemm(S, td, Np, nv, FW, M.fw_bf[ti][0], FW, n0, HA, FW, nullptr, nullptr, 0, 0);
-    if (!ok) break;
-    for (int c0 = 0; c0 < Np; c0 += 16) {
-      uint32_t r[16];
-      tc::tmem_ld16_issue(td + lane_off + c0, r);
-      tc::tmem_wait();
-      if (act) {
-#pragma unroll
-        for (int i = 0; i < 16; i += 4)
-          if (c0 + i < nv)
-            *reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0 + i) =
-                make_float4(__uint_as_float(r[i]), __uint_as_float(r[i + 1]), __uint_as_float(r[i + 2]),
-                            __uint_as_float(r[i + 3]));
-      }
-    }
-    tc::fence_before_sync();
-  }
-  if (!ok) {
-    if (tid == 0) atomicOr(err, 1);
-    tc::mbar_wait(&bars[0], 0);
-    tc::mbar_wait(&bars[1], 0);
+#undef FIT_SCR
   }
   tc::cp_async_wait<0>();
   tc::fence_before_sync();
   __syncthreads();
+  if (tid == 0 && abort_s) atomicOr(err, 1);
   if (warp == 0) tc::tmem_dealloc(td, 256);
-#undef FIT_SCR
 }
 
 template <int FW>
 int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, float *dG, float *scratch,
                    float *Eatom, double *energy, int *err, cudaStream_t st) {
-  const size_t smem = round1k(128 * FW * 2) + 2 * (kFitBufA + kFitBufB);
-  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  using C = FitCfg<FW>;
+  if (!M.fit_bt[0][kFitBtDg]) return DPB_ERR_UNSUPPORTED;
+  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
   int tile0 = 0;  // scratch tiles of 128 rows, consecutive over the centre types
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -1455,8 +1537,8 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
     const int ntile = (Mrows + 127) / 128;
-    k_mix_fit<FW><<<ntile, 128, smem, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err, D.seg,
-                                            tile0);
+    k_mix_fit<FW><<<ntile, kFitThreads, C::SMEM, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
+                                                        D.seg, tile0);
     tile0 += ntile;
     count_launch();
     DPB_LAUNCH_CHECK();
@@ -1467,8 +1549,9 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
 // ---------------------------------------------------------------- dispatch
 int mixed_supported(const DevModel &M) {
   const bool emb = (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
-  const bool fit = M.FW[0] == 240 || M.FW[0] == 128;
-  return emb && fit && (M.A * M.E2) % 8 == 0;
+  bool fit = M.FW[0] == 240 || M.FW[0] == 128;
+  for (int l = 1; l < M.nfit; ++l) fit = fit && M.FW[l] == M.FW[0];
+  return emb && fit && (M.A * M.E2) % 16 == 0;
 }
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -1528,7 +1611,7 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
                                  double *virial, float *T, __nv_bfloat16 *Gb, float *dG, float *scratch, int *err,
                                  cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
-  const size_t NG = NF * M.A * M.E2;  // a multiple of 8 (mixed_supported)
+  const size_t NG = NF * M.A * M.E2;  // a multiple of 16 (mixed_supported)
   int rc;
   prof_begin(PROF_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {

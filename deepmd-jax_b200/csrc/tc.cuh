@@ -147,6 +147,41 @@ __device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16
 }
 __device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// ---- mbarrier arrivals and bulk (TMA) copies
+// Makes barrier initialisation visible to the async proxy (TMA complete_tx).
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+// Arrive and add tx_bytes to the bytes the current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t tx_bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(tx_bytes)
+               : "memory");
+}
+// One poll of the phase with the given parity.
+__device__ __forceinline__ bool mbar_test(uint32_t mbar_addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar_addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bulk (TMA) copy of `bytes` contiguous bytes global -> shared, no multicast;
+// completion is signalled on mbar as tx bytes.  Both addresses 16-byte
+// aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void *src, uint32_t bytes, uint64_t *mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst_smem),
+               "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+
 // Byte offsets of the canonical layouts (see file comment).
 __host__ __device__ constexpr uint32_t kmajor_off(int r, int k, int K) {
   return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
