@@ -1121,9 +1121,10 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
 //   g <  L           forward layer g        A: G rows (g = 0) or H    B: W_g^T  (out x in)
 //   L <= g < 2L - 1  adjoint layer 2L-1-g   A: gZ                     B: W_l    (in x out)
 //   g >= 2L - 1      dE/dG columns [128 p, 128 p + 128), p = g - (2L - 1), B: rows of W_0
-// Warp roles (160 threads): warps 0-3 are the epilogue, one thread per atom,
+// Warp roles (192 threads): warps 0-3 are the epilogue, one thread per atom,
 // which also stream layer 0's G rows into the ring with cp.async; lane 0 of
-// warp 4 issues the bulk (TMA) copies of the weights and the MMAs.  Operands
+// warp 4 issues the MMAs and lane 0 of warp 5 the bulk (TMA) copies of the
+// weights, each waiting only on its own barriers so MMAs queue back to back.  Operands
 // pass through a ring of K = 16 stages (full / empty mbarriers), so the
 // weights of the next GEMM are already in flight while the epilogue of the
 // current one runs; the dE/dG passes alternate between two TMEM accumulators
@@ -1137,7 +1138,7 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
 // product (FP64 segment sums) and the adjoint gates; tanh values and residual
 // sources go to a per-atom FP32 scratch, the BF16 activation of the next GEMM
 // stays in shared memory.  2 CTAs per SM, 256 TMEM columns each.
-constexpr int kFitThreads = 160;
+constexpr int kFitThreads = 192;
 constexpr int kFitDgN = 128;                 // N of one dE/dG pass
 constexpr int kFitStageA = 2 * 128 * 16;     // A chunk bytes (K = 16)
 
@@ -1236,15 +1237,30 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   const uint32_t td = tbase_s;
   const int r0 = blockIdx.x * 128, nrows = min(128, Mrows - r0);
 
-  if (warp == 4) {
-    // ================= TMA + MMA issuer (one thread)
+  if (warp == 5) {
+    // ================= weight producer (one thread): bulk copies into free stages
+    if ((tid & 31) == 0) {
+      const uint32_t ring_u = tc::smem_u32(ring);
+      int p = 0;  // chunks issued
+      bool ok = true;
+      for (int g = 0; g < NG && ok; ++g) {
+        const FitGemm gi = fit_gemm_info<FW>(M, ti, g, L, K0);
+        const uint32_t bytes = (uint32_t)gi.br * 32u;
+        for (int k = 0; k < gi.nk; ++k, ++p) {
+          const int s = p % ST;
+          if (p >= ST && !(ok = fit_wait(&empty[s], ((p / ST) - 1) & 1, abort))) break;
+          tc::mbar_arrive_expect_tx(&full[s], bytes);
+          tc::bulk_load(ring_u + s * C::STAGE + kFitStageA, gi.src + (size_t)k * bytes, bytes, &full[s]);
+        }
+      }
+      // copies still in flight only after a give-up: the last ST issued chunks
+      for (int c = p > ST ? p - ST : 0; c < p; ++c) tc::mbar_wait(&full[c % ST], (c / ST) & 1);
+    }
+  } else if (warp == 4) {
+    // ================= MMA issuer (one thread)
     if ((tid & 31) == 0) {
       const uint32_t ring_u = tc::smem_u32(ring), ha_u = tc::smem_u32(HA);
-      int total = 0;
-      for (int g = 0; g < NG; ++g) total += fit_gemm_info<FW>(M, ti, g, L, K0).nk;
-      int p = 0, pg = 0, pk = 0;  // next chunk to load: global index, its GEMM, its K chunk
-      FitGemm pgi = fit_gemm_info<FW>(M, ti, 0, L, K0);
-      int q = 0;                  // next chunk to multiply
+      int q = 0;  // chunks multiplied
       uint32_t epid_n = 0;
       bool ok = true;
       for (int g = 0; g < NG && ok; ++g) {
@@ -1260,19 +1276,6 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         tc::fence_after_sync();
         const uint32_t idesc = tc::idesc_bf16(128, gi.N, 0, 0);
         for (int k = 0; k < gi.nk; ++k, ++q) {
-          while (p < total && p < q + ST) {  // keep the ring full
-            const int s = p % ST;
-            if (p >= ST && !(ok = fit_wait(&empty[s], ((p / ST) - 1) & 1, abort))) break;
-            const uint32_t bytes = (uint32_t)pgi.br * 32u;
-            tc::mbar_arrive_expect_tx(&full[s], bytes);
-            tc::bulk_load(ring_u + s * C::STAGE + kFitStageA, pgi.src + (size_t)pk * bytes, bytes, &full[s]);
-            ++p;
-            if (++pk == pgi.nk) {
-              pk = 0;
-              if (++pg < NG) pgi = fit_gemm_info<FW>(M, ti, pg, L, K0);
-            }
-          }
-          if (!ok) break;
           const int s = q % ST;
           const uint32_t par = (q / ST) & 1;
           ok = fit_wait(&full[s], par, abort) && (g != 0 || fit_wait(&fullA[s], par, abort));
@@ -1288,9 +1291,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         if (!ok) break;
         tc::commit(g < 2 * L - 1 ? &accf : &accfD[(g - (2 * L - 1)) & 1]);
       }
-      // nothing of this CTA may be in flight when it exits: loads issued but
-      // never multiplied (only after a give-up), and the last MMAs
-      for (int c = q; c < p; ++c) tc::mbar_wait(&full[c % ST], (c / ST) & 1);
+      // the last MMAs complete before the CTA exits
       if (q > 0) tc::mbar_wait(&empty[(q - 1) % ST], ((q - 1) / ST) & 1);
     }
   } else {
