@@ -82,7 +82,8 @@ struct MixDims {
 };
 
 constexpr int kBlkAtoms = 8;    // centre atoms per block
-constexpr int kRowCap = 256;    // compacted-row buffer (one tile + the carry of the next compaction round)
+constexpr int kBwdCpt = 4;      // compaction candidates per thread, adjoint (128 threads)
+constexpr int kRowCap = 128 + 128 * kBwdCpt;  // compacted rows: the carry (< 128) + one compaction round
 constexpr int kRblkBytes = 128 * 128 * 2;
 constexpr int kDtN = kBlkAtoms * 10;  // N of the adjoint contraction: 8 slots x 10 channels
 
@@ -109,23 +110,6 @@ __device__ __forceinline__ void mix_load_net(const DevModel &M, int k, char *net
   tc::cp_async_commit();
 }
 
-// Block-wide stream compaction of one 128-candidate round: returns this
-// thread's slot among the kept candidates; *total gets the round's count.
-__device__ __forceinline__ int block_compact(bool keep, int *wcnt, int *total) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned m = __ballot_sync(0xffffffffu, keep);
-  if (lane == 0) wcnt[warp] = __popc(m);
-  __syncthreads();
-  int off = 0, tot = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-    if (w < warp) off += wcnt[w];
-    tot += wcnt[w];
-  }
-  __syncthreads();
-  *total = tot;
-  return off + __popc(m & ((1u << lane) - 1u));
-}
-
 // Geometry of a compacted row and the 10-channel env row (FP32).
 __device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std, float mean, RowGeom &gm,
                                             float &st, float R[10]) {
@@ -137,49 +121,97 @@ __device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std
   env_row(sn, xh, R);
 }
 
-// One round of compaction: candidates (atom slot, neighbour slot, image) of
-// the block for neighbour type tj; kept rows (s(r) != 0) are appended to
-// rowbuf as (x, y, z, packed) with packed = (neighbour user index << 3) | slot.
+// One round of compaction over CPT * blockDim candidates (atom slot,
+// neighbour slot, image) of the block for neighbour type tj: thread t takes
+// the CPT consecutive candidates base + t * CPT + k, issues all of their
+// gathers (neighbour index, permutation, position) before using any, and the
+// kept rows (s(r) != 0) are appended to rowbuf in candidate order (so rows
+// stay sorted by atom slot) as (x, y, z, packed), packed = (neighbour user
+// index << 3) | slot.  The unread rows [rowstart, rowcount) of earlier rounds
+// (fewer than 128) are first moved to the front.
+template <int CPT>
 __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevModel &M, int tj, int base, int total,
                                                   int per_atom, int nim, int3 ni, float3 L, size_t g0,
                                                   size_t frame_base, const float3 *ri_s, const float *pos,
                                                   const int32_t *perm, const int32_t *nbrs, float4 *rowbuf,
-                                                  int *wcnt, int &rowcount) {
-  const int p = base + threadIdx.x;
-  bool keep = false;
-  float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (p < total) {
-    const int slot = p / per_atom, rem = p - slot * per_atom;
-    const int sidx = nim == 1 ? rem : rem / nim, mimg = rem - sidx * nim;
-    const int cnt_j = D.offs[tj + 1] - D.offs[tj];
-    const int idx = nbrs[(g0 + slot) * D.S + D.col[tj] + sidx] & DPB_NBR_INDEX_MASK;
-    if (idx < cnt_j) {
-      const int js = D.offs[tj] + idx;
-      const int src = perm ? perm[js] : js;
-      const float *pj = pos + (frame_base + src) * 3;
-      const float3 x = rel_coord(ri_s[slot], make_float3(pj[0], pj[1], pj[2]), L, ni, mimg);
+                                                  int *wcnt, int &rowstart, int &rowcount) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (rowstart > 0) {
+    const int rem = rowcount - rowstart;  // < 128 <= blockDim
+    float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tid < rem) carry = rowbuf[rowstart + tid];
+    __syncthreads();
+    if (tid < rem) rowbuf[tid] = carry;
+    rowstart = 0;
+    rowcount = rem;
+  }
+  const int cnt_j = D.offs[tj + 1] - D.offs[tj];
+  const int p0 = base + tid * CPT;
+  int idx[CPT], slotk[CPT], mimgk[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int p = p0 + k;
+    idx[k] = cnt_j;
+    slotk[k] = 0;
+    mimgk[k] = 0;
+    if (p < total) {
+      const int slot = p / per_atom, rem = p - slot * per_atom;
+      const int sidx = nim == 1 ? rem : rem / nim;
+      slotk[k] = slot;
+      mimgk[k] = rem - sidx * nim;
+      idx[k] = nbrs[(g0 + slot) * D.S + D.col[tj] + sidx] & DPB_NBR_INDEX_MASK;
+    }
+  }
+  int src[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int js = D.offs[tj] + idx[k];
+    src[k] = idx[k] < cnt_j ? (perm ? perm[js] : js) : -1;
+  }
+  float3 pj[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    pj[k] = make_float3(0.f, 0.f, 0.f);
+    if (src[k] >= 0) {
+      const float *q = pos + (frame_base + src[k]) * 3;
+      pj[k] = make_float3(q[0], q[1], q[2]);
+    }
+  }
+  float4 rv[CPT];
+  unsigned keep = 0;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    rv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (src[k] >= 0) {
+      const float3 x = rel_coord(ri_s[slotk[k]], pj[k], L, ni, mimgk[k]);
       RowGeom gm;
       row_geom(x, M.rcut, gm);
       if (gm.s != 0.f) {
-        keep = true;
-        rv = make_float4(x.x, x.y, x.z, __int_as_float((src << 3) | slot));
+        keep |= 1u << k;
+        rv[k] = make_float4(x.x, x.y, x.z, __int_as_float((src[k] << 3) | slotk[k]));
       }
     }
   }
-  int tot;
-  const int pos_ = block_compact(keep, wcnt, &tot);
-  if (keep) rowbuf[rowcount + pos_] = rv;
+  // block-wide exclusive scan of the per-thread counts
+  const int c = __popc(keep);
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wcnt[warp] = incl;
+  __syncthreads();
+  int off = 0, tot = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    if (w < warp) off += wcnt[w];
+    tot += wcnt[w];
+  }
+  int o = rowcount + off + incl - c;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k)
+    if (keep >> k & 1u) rowbuf[o++] = rv[k];
   rowcount += tot;
-  __syncthreads();
-}
-
-__device__ __forceinline__ void mix_drop_rows(float4 *rowbuf, int nrows, int &rowcount) {
-  const int rem = rowcount - nrows;
-  float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
-  if ((int)threadIdx.x < rem) carry = rowbuf[nrows + threadIdx.x];
-  __syncthreads();
-  if ((int)threadIdx.x < rem) rowbuf[threadIdx.x] = carry;
-  rowcount = rem;
   __syncthreads();
 }
 
@@ -205,7 +237,8 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
 // T / Nnbrs (FP32) and the descriptor G (BF16, dpmodel.py:74-78).  Only the
 // current neighbour type's net is resident (2 CTAs per SM).
 constexpr int kFwdThreads = 256;
-constexpr int kRowCapFwd = 128 + kFwdThreads;  // one tile + the carry of a compaction round
+constexpr int kFwdCpt = 2;  // compaction candidates per thread, forward
+constexpr int kRowCapFwd = 128 + kFwdThreads * kFwdCpt;  // the carry (< 128) + one compaction round
 
 // Column split of the two halves: half 0 owns h1 columns [0, S1) and h2
 // columns [0, S2), half 1 the rest; S2 = S1 * Z2 so every residual source
@@ -375,7 +408,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     int ntile = 0;
     bool pending = false;
     int my_slot = -1;
-    int rowcount = 0;
+    int rowstart = 0, rowcount = 0;
     // alternate the neighbour-type order between blocks so the resident net carries over
     const int tj0 = (loaded_net >= 0) ? loaded_net - ti * M.ntypes : 0;
     for (int tt = 0; tt < D.ntypes && ok; ++tt) {
@@ -384,13 +417,14 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
-      for (int base = 0; base < total + kFwdThreads && ok; base += kFwdThreads) {
+      constexpr int kStep = kFwdThreads * kFwdCpt;
+      for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
         if (!flush)
-          mix_compact_round(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm, nbrs,
-                            rowbuf, wcnt, rowcount);
-        while (rowcount >= 128 || (flush && rowcount > 0)) {
-          const int nrows = min(rowcount, 128);
+          mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm,
+                                     nbrs, rowbuf, wcnt, rowstart, rowcount);
+        while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
+          const int nrows = min(rowcount - rowstart, 128);
           if (pending) {  // previous contraction done: operands free, clear its Rblk entries
             MIX_WAIT();
             pending = false;
@@ -407,7 +441,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
             loaded_net = knet;
           }
           const bool act = row < nrows;
-          const float4 rv = act ? rowbuf[row] : make_float4(100.f, 100.f, 100.f, 0.f);
+          const float4 rv = act ? rowbuf[rowstart + row] : make_float4(100.f, 100.f, 100.f, 0.f);
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
           RowGeom gm;
           float st, R[10];
@@ -470,7 +504,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           }
           pending = true;
           ++ntile;
-          mix_drop_rows(rowbuf, nrows, rowcount);
+          rowstart += nrows;
         }
       }
     }
@@ -487,48 +521,55 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     }
     // ---- block epilogue: T (FP32) and G (BF16) from the TMEM accumulators
     __syncthreads();
-    float *Xs = reinterpret_cast<float *>(rblk);  // staging [slot][c][w], 8 x 10 x E2 floats
+    float *Xs = reinterpret_cast<float *>(rblk);  // T staging [slot][c][w], 8 x 10 x E2 floats
     {
       const int slot = row >> 4, c = row & 15;
       constexpr int NG = MD::N2 / 16, NG0 = (NG + 1) / 2;  // column groups of half 0
       const int q0 = half ? NG0 : 0, q1 = half ? NG : NG0;
-      for (int q = q0; q < q1; ++q) {
+      for (int q = q0; q < q1; q += 2) {
         const int c0 = 16 * q;
-        uint32_t r[16];
+        const bool two = q + 1 < q1;  // warp-uniform
+        uint32_t r[2][16];
         if (ntile > 0) {
-          tc::tmem_ld16_issue(tD3 + lane_off + c0, r);
+          tc::tmem_ld16_issue(tD3 + lane_off + c0, r[0]);
+          if (two) tc::tmem_ld16_issue(tD3 + lane_off + c0 + 16, r[1]);
           tc::tmem_wait();
         } else {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) r[i] = 0u;
+          for (int i = 0; i < 16; ++i) r[0][i] = r[1][i] = 0u;
         }
         if (slot < nb && c < 10) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int w = c0 + i;
-            if (w < E2) {
-              const float t = __uint_as_float(r[i]) * M.inv_nnbrs;
-              Tout[(g0 + slot) * 10 * E2 + c * E2 + w] = t;
-              Xs[(slot * 10 + c) * E2 + w] = t + (c == 0 ? M.tbias[w] : 0.f);
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int w = c0 + 16 * h + i;
+              if ((h == 0 || two) && w < E2) Xs[(slot * 10 + c) * E2 + w] = __uint_as_float(r[h][i]) * M.inv_nnbrs;
             }
-          }
         }
       }
     }
     tc::fence_before_sync();
     __syncthreads();
-    // G[a][w] = sum_c Q[c][a] X[c][w] (dpmodel.py:74-78): Q of every slot is
-    // staged once (zero for a >= A), then a thread owns (slot, w) pairs, keeps
-    // X[.][w] in registers and reads Q as warp-wide broadcasts.
+    {  // the block's T rows are contiguous in Tout and in Xs: coalesced copy
+      const int n4 = nb * 10 * E2 / 4;
+      float4 *dst = reinterpret_cast<float4 *>(Tout + g0 * 10 * E2);
+      const float4 *src = reinterpret_cast<const float4 *>(Xs);
+      for (int e = tid; e < n4; e += kFwdThreads) dst[e] = src[e];
+    }
+    // G[a][w] = sum_c Q[c][a] X[c][w] with X = T + Tbias on channel 0
+    // (dpmodel.py:74-78): Q of every slot is staged once (zero for a >= A),
+    // then a thread owns (slot, column pair) items, keeps X[.][w], X[.][w+1]
+    // in registers and reads Q as warp-wide broadcasts.
     const int A = M.A;
-    float *Qs = Xs + kBlkAtoms * 10 * E2;  // [slot][c][16]
+    float *Qs = Xs + kBlkAtoms * 10 * E2;  // [slot][c][16], past Rblk into the (idle) row buffer
     for (int e = tid; e < kBlkAtoms * 160; e += kFwdThreads) {
       const int slot = e / 160, c = (e >> 4) % 10, aa = e & 15;
       float q = 0.f;
       if (slot < nb && aa < A) {
         const float *X = Xs + slot * 10 * E2;
         if (c < 4) {
-          q = X[c * E2 + aa];
+          q = X[c * E2 + aa] + (c == 0 ? M.tbias[aa] : 0.f);
         } else {
           const float y1 = X[E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
           const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
@@ -538,20 +579,30 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       Qs[e] = q;
     }
     __syncthreads();
-    constexpr int WP = (E2 + 31) / 32 * 32;  // columns per slot, whole warps
-    for (int pr = tid; pr < nb * WP; pr += kFwdThreads) {
-      const int slot = pr / WP, w = pr - slot * WP;
+    constexpr int WP2 = (E2 / 2 + 31) / 32 * 32;  // column pairs per slot, whole warps
+    for (int pr = tid; pr < nb * WP2; pr += kFwdThreads) {
+      const int slot = pr / WP2, w = 2 * (pr - slot * WP2);
       if (w < E2) {
-        float x[10];
+        float xa[10], xb[10];
 #pragma unroll
-        for (int c = 0; c < 10; ++c) x[c] = Xs[(slot * 10 + c) * E2 + w];
+        for (int c = 0; c < 10; ++c) {
+          const float2 v = *reinterpret_cast<const float2 *>(Xs + (slot * 10 + c) * E2 + w);
+          xa[c] = v.x;
+          xb[c] = v.y;
+        }
+        xa[0] += M.tbias[w];
+        xb[0] += M.tbias[w + 1];
         const float *Q = Qs + slot * 160;
-        __nv_bfloat16 *Gs = Gout + (g0 + slot) * (size_t)A * E2 + w;
+        __nv_bfloat162 *Gs = reinterpret_cast<__nv_bfloat162 *>(Gout + (g0 + slot) * (size_t)A * E2 + w);
         for (int aa = 0; aa < A; ++aa) {
-          float v = 0.f;
+          float va = 0.f, vb = 0.f;
 #pragma unroll
-          for (int c = 0; c < 10; ++c) v = fmaf(Q[c * 16 + aa], x[c], v);
-          Gs[aa * E2] = __float2bfloat16_rn(v);
+          for (int c = 0; c < 10; ++c) {
+            const float qv = Q[c * 16 + aa];
+            va = fmaf(qv, xa[c], va);
+            vb = fmaf(qv, xb[c], vb);
+          }
+          Gs[aa * (E2 / 2)] = __floats2bfloat162_rn(va, vb);
         }
       }
     }
@@ -855,7 +906,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     }
     tc::cp_async_commit();
     __syncthreads();
-    int rowcount = 0;
+    int rowstart = 0, rowcount = 0;
     const int tj0 = (loaded_net >= 0) ? loaded_net - ti * M.ntypes : 0;
     for (int tt = 0; tt < D.ntypes && ok; ++tt) {
       const int tj = (tj0 + tt) % D.ntypes;
@@ -863,20 +914,21 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
-      for (int base = 0; base < total + 128 && ok; base += 128) {
+      constexpr int kStep = 128 * kBwdCpt;
+      for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
         if (!flush)
-          mix_compact_round(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm, nbrs,
-                            rowbuf, wcnt, rowcount);
-        while (rowcount >= 128 || (flush && rowcount > 0)) {
-          const int nrows = min(rowcount, 128);
+          mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm,
+                                     nbrs, rowbuf, wcnt, rowstart, rowcount);
+        while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
+          const int nrows = min(rowcount - rowstart, 128);
           if (loaded_net != knet) {
             __syncthreads();
             mix_load_net<E0, E1, E2>(M, knet, netb, small);
             loaded_net = knet;
           }
           const bool act = tid < nrows;
-          const float4 rv = act ? rowbuf[tid] : make_float4(100.f, 100.f, 100.f, 0.f);
+          const float4 rv = act ? rowbuf[rowstart + tid] : make_float4(100.f, 100.f, 100.f, 0.f);
           const int packed = act ? __float_as_int(rv.w) : 0;
           const int slot = packed & 7, jsrc = packed >> 3;
           RowGeom gm;
@@ -1050,7 +1102,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
               atomicAdd(&fi_s[slot * 3 + 2], s2);
             }
           }
-          mix_drop_rows(rowbuf, nrows, rowcount);
+          rowstart += nrows;
         }
       }
     }
