@@ -110,10 +110,13 @@ __device__ __forceinline__ void mix_load_net(const DevModel &M, int k, char *net
   tc::cp_async_commit();
 }
 
-// Geometry of a compacted row and the 10-channel env row (FP32).
-__device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std, float mean, RowGeom &gm,
-                                            float &st, float R[10]) {
-  row_geom(make_float3(rb.x, rb.y, rb.z), rcut, gm);
+// Geometry of a compacted row and the 10-channel env row (FP32).  raw: the
+// row holds r_j - r_i and the minimum image (utils.py:24-26) is applied here.
+__device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float rcut, float inv_std, float mean,
+                                            RowGeom &gm, float &st, float R[10]) {
+  const float3 x = raw ? make_float3(shift_ortho(rb.x, L.x), shift_ortho(rb.y, L.y), shift_ortho(rb.z, L.z))
+                       : make_float3(rb.x, rb.y, rb.z);
+  row_geom(x, rcut, gm);
   const float sn = gm.s * inv_std;
   st = (gm.s - mean) * inv_std;
   const float inv_rp = 1.f / (gm.r + 1e-16f);
@@ -125,10 +128,15 @@ __device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std
 // neighbour slot, image) of the block for neighbour type tj: thread t takes
 // the CPT consecutive candidates base + t * CPT + k, issues all of their
 // gathers (neighbour index, permutation, position) before using any, and the
-// kept rows (s(r) != 0) are appended to rowbuf in candidate order (so rows
-// stay sorted by atom slot) as (x, y, z, packed), packed = (neighbour user
-// index << 3) | slot.  The unread rows [rowstart, rowcount) of earlier rounds
-// (fewer than 128) are first moved to the front.
+// kept rows are appended to rowbuf in candidate order (so rows stay sorted by
+// atom slot) as (x, y, z, packed), packed = (neighbour user index << 3) | slot.
+// With one image per pair (nim == 1, boxes wider than 2 rcut) a row keeps the
+// raw difference r_j - r_i (mix_row_env applies the minimum image) and the
+// keep test is a nearest-image distance estimate with a 1e-3 A margin: every
+// row with s(r) != 0 is kept, and a kept row with s(r) = 0 adds exact zeros
+// (R~ = 0, ds/dr = 0).  With several images the exact displacement and s(r)
+// decide.  The unread rows [rowstart, rowcount) of earlier rounds (fewer than
+// 128) are first moved to the front.
 template <int CPT>
 __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevModel &M, int tj, int base, int total,
                                                   int per_atom, int nim, int3 ni, float3 L, size_t g0,
@@ -148,6 +156,7 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
   const int cnt_j = D.offs[tj + 1] - D.offs[tj];
   const int p0 = base + tid * CPT;
   int idx[CPT], slotk[CPT], mimgk[CPT];
+  int slot = p0 / per_atom, rem = p0 - slot * per_atom;  // advanced incrementally below
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const int p = p0 + k;
@@ -155,11 +164,14 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
     slotk[k] = 0;
     mimgk[k] = 0;
     if (p < total) {
-      const int slot = p / per_atom, rem = p - slot * per_atom;
       const int sidx = nim == 1 ? rem : rem / nim;
       slotk[k] = slot;
       mimgk[k] = rem - sidx * nim;
       idx[k] = nbrs[(g0 + slot) * D.S + D.col[tj] + sidx] & DPB_NBR_INDEX_MASK;
+    }
+    if (++rem == per_atom) {
+      rem = 0;
+      ++slot;
     }
   }
   int src[CPT];
@@ -179,16 +191,35 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
   }
   float4 rv[CPT];
   unsigned keep = 0;
+  if (nim == 1) {
+    const float3 inv_l = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
+    const float rk = M.rcut + 1e-3f, rk2 = rk * rk;
 #pragma unroll
-  for (int k = 0; k < CPT; ++k) {
-    rv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (src[k] >= 0) {
-      const float3 x = rel_coord(ri_s[slotk[k]], pj[k], L, ni, mimgk[k]);
-      RowGeom gm;
-      row_geom(x, M.rcut, gm);
-      if (gm.s != 0.f) {
-        keep |= 1u << k;
-        rv[k] = make_float4(x.x, x.y, x.z, __int_as_float((src[k] << 3) | slotk[k]));
+    for (int k = 0; k < CPT; ++k) {
+      rv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (src[k] >= 0) {
+        const float3 ri = ri_s[slotk[k]];
+        const float dx = pj[k].x - ri.x, dy = pj[k].y - ri.y, dz = pj[k].z - ri.z;
+        const float ax = fmaf(-L.x, rintf(dx * inv_l.x), dx), ay = fmaf(-L.y, rintf(dy * inv_l.y), dy),
+                    az = fmaf(-L.z, rintf(dz * inv_l.z), dz);
+        if (ax * ax + ay * ay + az * az < rk2) {
+          keep |= 1u << k;
+          rv[k] = make_float4(dx, dy, dz, __int_as_float((src[k] << 3) | slotk[k]));
+        }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      rv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (src[k] >= 0) {
+        const float3 x = rel_coord(ri_s[slotk[k]], pj[k], L, ni, mimgk[k]);
+        RowGeom gm;
+        row_geom(x, M.rcut, gm);
+        if (gm.s != 0.f) {
+          keep |= 1u << k;
+          rv[k] = make_float4(x.x, x.y, x.z, __int_as_float((src[k] << 3) | slotk[k]));
+        }
       }
     }
   }
@@ -445,7 +476,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
           RowGeom gm;
           float st, R[10];
-          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
+          mix_row_env(rv, nim == 1, L, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image visible; rowbuf read by every thread
           float h0[16];
@@ -933,7 +964,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
           const int slot = packed & 7, jsrc = packed >> 3;
           RowGeom gm;
           float st, R[10];
-          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
+          mix_row_env(rv, nim == 1, L, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image and DTB visible
           float h1[E1], d1[E1];
