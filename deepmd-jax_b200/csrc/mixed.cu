@@ -127,7 +127,8 @@ __device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float
 // One round of compaction over CPT * blockDim candidates (atom slot,
 // neighbour slot, image) of the block for neighbour type tj: thread t takes
 // the CPT consecutive candidates base + t * CPT + k, issues all of their
-// gathers (neighbour index, permutation, position) before using any, and the
+// gathers (neighbour index, then position and user index from posS) before
+// using any, and the
 // kept rows are appended to rowbuf in candidate order (so rows stay sorted by
 // atom slot) as (x, y, z, packed), packed = (neighbour user index << 3) | slot.
 // With one image per pair (nim == 1, boxes wider than 2 rcut) a row keeps the
@@ -140,8 +141,8 @@ __device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float
 template <int CPT>
 __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevModel &M, int tj, int base, int total,
                                                   int per_atom, int nim, int3 ni, float3 L, size_t g0,
-                                                  size_t frame_base, const float3 *ri_s, const float *pos,
-                                                  const int32_t *perm, const int32_t *nbrs, float4 *rowbuf,
+                                                  size_t frame_base, const float3 *ri_s,
+                                                  const float4 *__restrict__ posS, const int32_t *nbrs, float4 *rowbuf,
                                                   int *wcnt, int &rowstart, int &rowcount) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (rowstart > 0) {
@@ -175,18 +176,15 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
     }
   }
   int src[CPT];
-#pragma unroll
-  for (int k = 0; k < CPT; ++k) {
-    const int js = D.offs[tj] + idx[k];
-    src[k] = idx[k] < cnt_j ? (perm ? perm[js] : js) : -1;
-  }
   float3 pj[CPT];
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
+    src[k] = -1;
     pj[k] = make_float3(0.f, 0.f, 0.f);
-    if (src[k] >= 0) {
-      const float *q = pos + (frame_base + src[k]) * 3;
-      pj[k] = make_float3(q[0], q[1], q[2]);
+    if (idx[k] < cnt_j) {
+      const float4 q = posS[frame_base + D.offs[tj] + idx[k]];
+      pj[k] = make_float3(q.x, q.y, q.z);
+      src[k] = __float_as_int(q.w);
     }
   }
   float4 rv[CPT];
@@ -378,8 +376,7 @@ __device__ __forceinline__ void fwd_epi2(uint32_t tD, uint32_t lane_off, const f
 
 template <int E0, int E1, int E2>
 __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, SysDesc D, int ti,
-                                                                  const float *__restrict__ pos,
-                                                                  const int32_t *__restrict__ perm,
+                                                                  const float4 *__restrict__ posS,
                                                                   const float *__restrict__ box,
                                                                   const int32_t *__restrict__ nbrs,
                                                                   float *__restrict__ Tout,
@@ -431,9 +428,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
     if (tid < nb) {
-      const int src = perm ? perm[D.offs[ti] + a0 + tid] : D.offs[ti] + a0 + tid;
-      const float *p = pos + (frame_base + src) * 3;
-      ri_s[tid] = make_float3(p[0], p[1], p[2]);
+      const float4 q = posS[g0 + tid];
+      ri_s[tid] = make_float3(q.x, q.y, q.z);
     }
     __syncthreads();
     int ntile = 0;
@@ -452,8 +448,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
         if (!flush)
-          mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm,
-                                     nbrs, rowbuf, wcnt, rowstart, rowcount);
+          mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS, nbrs,
+                                     rowbuf, wcnt, rowstart, rowcount);
         while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
           const int nrows = min(rowcount - rowstart, 128);
           if (pending) {  // previous contraction done: operands free, clear its Rblk entries
@@ -665,7 +661,7 @@ static int num_sms() {
 }
 
 template <int E0, int E1, int E2>
-int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
                          const float *box, const int32_t *nbrs, float *T, __nv_bfloat16 *G, int *err,
                          cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -675,7 +671,7 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
   DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_fwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   const int grid = nblk < 2 * num_sms() ? nblk : 2 * num_sms();
-  k_mix_embed_fwd<E0, E1, E2><<<grid, kFwdThreads, smem, st>>>(M, D, ti, pos, perm, box, nbrs, T, G, err);
+  k_mix_embed_fwd<E0, E1, E2><<<grid, kFwdThreads, smem, st>>>(M, D, ti, posS, box, nbrs, T, G, err);
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
@@ -842,8 +838,7 @@ __device__ __forceinline__ void slot_cols_rt(int slot, const uint32_t (&r)[kDtN 
 // reduced into the virial.  One resident net, 2 CTAs per SM.
 template <int E0, int E1, int E2>
 __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D, int ti,
-                                                          const float *__restrict__ pos,
-                                                          const int32_t *__restrict__ perm,
+                                                          const float4 *__restrict__ posS,
                                                           const float *__restrict__ box,
                                                           const int32_t *__restrict__ nbrs,
                                                           const __nv_bfloat16 *__restrict__ dTb,
@@ -922,9 +917,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
     if (tid < nb) {
-      const int src = perm ? perm[D.offs[ti] + a0 + tid] : D.offs[ti] + a0 + tid;
-      const float *p = pos + (frame_base + src) * 3;
-      ri_s[tid] = make_float3(p[0], p[1], p[2]);
+      const float4 q = posS[g0 + tid];
+      ri_s[tid] = make_float3(q.x, q.y, q.z);
     }
     if (tid < kBlkAtoms * 3) fi_s[tid] = 0.f;
     // ---- DTB: rows n = 10 slot + c of the 8 atoms (K-major, K = N2); zero for missing atoms
@@ -949,8 +943,8 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
       for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
         if (!flush)
-          mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, pos, perm,
-                                     nbrs, rowbuf, wcnt, rowstart, rowcount);
+          mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS, nbrs,
+                                     rowbuf, wcnt, rowstart, rowcount);
         while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
           const int nrows = min(rowcount - rowstart, 128);
           if (loaded_net != knet) {
@@ -1141,7 +1135,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     __syncthreads();
     if (tid < nb * 3) {
       const int a = tid / 3, k = tid - a * 3;
-      const int src = perm ? perm[D.offs[ti] + a0 + a] : D.offs[ti] + a0 + a;
+      const int src = __float_as_int(posS[g0 + a].w);
       atomicAdd(reinterpret_cast<float *>(&F4[frame_base + src]) + k, fi_s[tid]);
     }
     tc::cp_async_wait<0>();
@@ -1171,7 +1165,7 @@ size_t mix_bwd_smem() {
 }
 
 template <int E0, int E1, int E2>
-int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
+int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
                          const float *box, const int32_t *nbrs, const __nv_bfloat16 *dTb, float4 *F4,
                          double *virial, int *err, cudaStream_t st) {
   using MD = MixDims<E0, E1, E2>;
@@ -1188,7 +1182,7 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
     const int nb1 = (cnt + kBlkAtoms - 1) / kBlkAtoms;
     const int grid = nb1 < 2 * nsm ? nb1 : 2 * nsm;
     const size_t off = (size_t)f * D.N;
-    k_mix_embed_bwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, Df, ti, pos + off * 3, perm, box + f * 3,
+    k_mix_embed_bwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, Df, ti, posS + off, box + f * 3,
                                                           nbrs + off * D.S, dTb + off * 10 * MD::N2, F4 + off,
                                                           virial + f * 9, err);
     count_launch();
@@ -1649,17 +1643,41 @@ size_t mixed_workspace_fixed(const DevModel &M) {
 
 size_t mixed_workspace_per_atom(const DevModel &M) {
   const int FW = M.FW[0], K0 = M.A * M.E2;
-  return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 +
+  return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 + 16 +
          (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
 }
 
-int mixed_descriptors(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+// Positions in type-sorted order with each atom's frame-local user index:
+// posS[f N + k] = (r of atom perm[k] of frame f, perm[k]) - one 16-byte
+// gather per neighbour in the mixed embedding kernels.
+__global__ void k_pos_sorted(size_t NF, int N, const float *__restrict__ pos, const int32_t *__restrict__ perm,
+                             float4 *__restrict__ posS) {
+  const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < NF) {
+    const size_t f = g / N;
+    const int k = (int)(g - f * N);
+    const int src = perm ? perm[k] : k;
+    const float *p = pos + (f * N + src) * 3;
+    posS[g] = make_float4(p[0], p[1], p[2], __int_as_float(src));
+  }
+}
+
+static int launch_pos_sorted(const SysDesc &D, const float *pos, const int32_t *perm, float4 *posS,
+                             cudaStream_t st) {
+  const size_t NF = (size_t)D.N * D.F;
+  k_pos_sorted<<<(unsigned)((NF + 255) / 256), 256, 0, st>>>(NF, D.N, pos, perm, posS);
+  count_launch();
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}
+
+int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, const float *box,
                       const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, int *err, cudaStream_t st) {
   if (M.ngrids > 0) return DPB_ERR_UNSUPPORTED;  // compressed nets: the FP32 table kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, Gb, err, st)
-                           : launch_mix_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, Gb, err, st);
+    int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, posS, box, nbrs, T, Gb, err, st)
+                           : launch_mix_embed_fwd<32, 32, 64>(M, D, ti, posS, box, nbrs, T, Gb, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_FWD, st);
@@ -1730,7 +1748,10 @@ int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos,
                           cudaStream_t st) {
   const size_t NG = (size_t)D.N * D.F * M.A * M.E2;
   __nv_bfloat16 *Gb = reinterpret_cast<__nv_bfloat16 *>(ws);
-  int rc = mixed_descriptors(M, D, pos, perm, box, nbrs, T, Gb, err, st);
+  float4 *posS = reinterpret_cast<float4 *>(static_cast<char *>(ws) + al256(NG * 2));
+  int rc = launch_pos_sorted(D, pos, perm, posS, st);
+  if (rc) return rc;
+  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, err, st);
   if (rc) return rc;
   k_bf16_to_f32<<<(unsigned)((NG + 255) / 256), 256, 0, st>>>(Gb, G, NG);
   count_launch();
@@ -1749,11 +1770,14 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   __nv_bfloat16 *Gb = (__nv_bfloat16 *)w; w += al256(NF * K0 * 2);
   float *dG = (float *)w; w += al256(NF * K0 * 4);
   __nv_bfloat16 *dTb = (__nv_bfloat16 *)w; w += al256(NF * 10 * N2 * 2);
+  float4 *posS = (float4 *)w; w += al256(NF * 16);
   float *scratch = (float *)w;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
   if (M.ngrids > 0)
     return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
-  int rc = mixed_descriptors(M, D, pos, perm, box, nbrs, T, Gb, err, st);
+  int rc = launch_pos_sorted(D, pos, perm, posS, st);
+  if (rc) return rc;
+  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
   rc = (M.FW[0] == 240) ? launch_mix_fit<240>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
@@ -1771,8 +1795,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     rc = (M.E2 == 100)
-             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, dTb, F4, virial, err, st)
-             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, dTb, F4, virial, err, st);
+             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, posS, box, nbrs, dTb, F4, virial, err, st)
+             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, posS, box, nbrs, dTb, F4, virial, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_BWD, st);
