@@ -110,6 +110,13 @@ __device__ __forceinline__ void mix_load_net(const DevModel &M, int k, char *net
   tc::cp_async_commit();
 }
 
+// L2 prefetch of [base, base + bytes), one line per thread and step (the
+// persistent CTAs issue it for their next block while working on this one).
+__device__ __forceinline__ void prefetch_range_l2(const void *base, size_t bytes) {
+  const char *b = static_cast<const char *>(base);
+  for (size_t o = (size_t)threadIdx.x * 128; o < bytes; o += (size_t)blockDim.x * 128) tc::prefetch_l2(b + o);
+}
+
 // Geometry of a compacted row and the 10-channel env row (FP32).  raw: the
 // row holds r_j - r_i and the minimum image (utils.py:24-26) is applied here.
 __device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float rcut, float inv_std, float mean,
@@ -423,6 +430,11 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     const int nb = min(kBlkAtoms, cnt_i - a0);
     const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
     const size_t frame_base = (size_t)f * D.N;
+    if (blk + (int)gridDim.x < nblk) {  // the next block's neighbour rows
+      const int bn = blk + gridDim.x, fn = bn / nbpf, an = (bn - fn * nbpf) * kBlkAtoms;
+      const size_t gn = (size_t)fn * D.N + D.offs[ti] + an;
+      prefetch_range_l2(nbrs + gn * D.S, (size_t)min(kBlkAtoms, cnt_i - an) * D.S * 4);
+    }
     const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
     const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
@@ -908,6 +920,13 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     const int nb = min(kBlkAtoms, cnt_i - a0);
     const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
     const size_t frame_base = (size_t)f * D.N;
+    if (blk + (int)gridDim.x < nblk) {  // the next block's neighbour rows and dE/dT rows
+      const int bn = blk + gridDim.x, fn = bn / nbpf, an = (bn - fn * nbpf) * kBlkAtoms;
+      const size_t gn = (size_t)fn * D.N + D.offs[ti] + an;
+      const int nbn = min(kBlkAtoms, cnt_i - an);
+      prefetch_range_l2(nbrs + gn * D.S, (size_t)nbn * D.S * 4);
+      prefetch_range_l2(dTb + gn * 10 * MD::N2, (size_t)nbn * 10 * MD::N2 * 2);
+    }
     const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
     if (bs != vframe) {
       if (vframe >= 0) flush_virial();

@@ -182,6 +182,11 @@ __device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void *src, ui
                : "memory");
 }
 
+// Hint: bring the global line holding p into L2.
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Byte offsets of the canonical layouts (see file comment).
 __host__ __device__ constexpr uint32_t kmajor_off(int r, int k, int K) {
   return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
