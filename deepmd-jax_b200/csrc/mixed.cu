@@ -690,36 +690,64 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
 }
 
 // ---------------------------------------------------------------- dE/dT (SIMT, warp per atom)
-// Adjoint of the descriptor (dpmodel.py:74-78): from dE/dG (FP32, from the
+// Adjoint of the descriptor (dpmodel.py:74-78): from dE/dG (BF16, from the
 // fitting chain) and T, dE/dT / Nnbrs as BF16 rows [atom][c][w] (w padded to
 // N2 with zeros), the B operand rows of the tensor-core adjoint.
 template <int E2, int N2>
 __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
-                                                const float *__restrict__ dG, __nv_bfloat16 *__restrict__ dTb) {
-  // Warp per atom; lane owns columns w = lane + 32 j.  The atom's dE/dG rows
-  // stay in registers (D[a][j]); X = T + Tbias sits in shared memory.
+                                                const __nv_bfloat16 *__restrict__ dG,
+                                                __nv_bfloat16 *__restrict__ dTb) {
+  // Warp per atom; lane owns the column pairs w = 2 lane + 64 j (+0, +1).
+  // The atom's dE/dG rows stay in registers (D[a][2j + h]); X = T + Tbias
+  // sits in shared memory.
   //   dQ[c][a] = sum_w dG[a][w] X[c][w]   (per-lane partials, then a shuffle
   //                                         reduce-scatter: lane l ends with a = l & 15)
   //   dX[c][w] = sum_a dG[a][w] Q[c][a] + the Q -> X terms at w < 2A
-  constexpr int NJ = (E2 + 31) / 32;
-  static_assert((N2 + 31) / 32 == NJ, "padded width");
-  __shared__ float Xs[4][10 * E2];
+  constexpr int NJ = (E2 + 63) / 64;
+  static_assert(N2 <= 64 * NJ && E2 % 2 == 0, "padded width");
+  __shared__ __align__(16) float Xs[4][10 * E2];
   __shared__ float Qs[4][160], dQs[4][160];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t g = (size_t)blockIdx.x * 4 + warp;
   if (g >= (size_t)NF) return;
   const int A = M.A;  // 1..16 (checked at model creation: 2A <= 32)
   float *X = Xs[warp], *Q = Qs[warp], *dQ = dQs[warp];
-  const float *Tg = Tin + g * 10 * E2;
-  for (int e = lane; e < 10 * E2; e += 32) X[e] = Tg[e] + (e < E2 ? M.tbias[e] : 0.f);
-  float D[16][NJ];
-  const float *Gg = dG + g * (size_t)A * E2;
+  {  // X = T + Tbias: every lane issues all of its float4 loads before the first use
+    static_assert(E2 % 4 == 0, "float4 rows");
+    constexpr int N4 = 10 * E2 / 4, K4 = (N4 + 31) / 32;
+    const float4 *Tg4 = reinterpret_cast<const float4 *>(Tin + g * 10 * E2);
+    float4 tv[K4];
+#pragma unroll
+    for (int k = 0; k < K4; ++k) {
+      const int e4 = lane + 32 * k;
+      tv[k] = e4 < N4 ? Tg4[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < K4; ++k) {
+      const int e4 = lane + 32 * k, e = 4 * e4;
+      if (e4 < N4) {
+        float4 v = tv[k];
+        if (e < E2) {
+          v.x += M.tbias[e];
+          v.y += M.tbias[e + 1];
+          v.z += M.tbias[e + 2];
+          v.w += M.tbias[e + 3];
+        }
+        reinterpret_cast<float4 *>(X)[e4] = v;
+      }
+    }
+  }
+  float D[16][2 * NJ];
+  const __nv_bfloat162 *Gg = reinterpret_cast<const __nv_bfloat162 *>(dG + g * (size_t)A * E2);
 #pragma unroll
   for (int a = 0; a < 16; ++a)
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
-      const int w = lane + 32 * j;
-      D[a][j] = (a < A && w < E2) ? Gg[a * E2 + w] : 0.f;
+      const int w = 2 * lane + 64 * j;
+      float2 v = make_float2(0.f, 0.f);
+      if (a < A && w < E2) v = __bfloat1622float2(Gg[(a * E2 + w) / 2]);
+      D[a][2 * j] = v.x;
+      D[a][2 * j + 1] = v.y;
     }
   __syncwarp();
   if (lane < 16) {  // Q[c][a] (dpmodel.py:74-78), zero for a >= A
@@ -741,17 +769,19 @@ __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float 
 #pragma unroll 1
   for (int c = 0; c < 10; ++c) {
     float p[16];
-    float xc[NJ];
+    float xc[2 * NJ];
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
-      const int w = lane + 32 * j;
-      xc[j] = w < E2 ? X[c * E2 + w] : 0.f;
+      const int w = 2 * lane + 64 * j;
+      const float2 x2 = w < E2 ? *reinterpret_cast<const float2 *>(X + c * E2 + w) : make_float2(0.f, 0.f);
+      xc[2 * j] = x2.x;
+      xc[2 * j + 1] = x2.y;
     }
 #pragma unroll
     for (int a = 0; a < 16; ++a) {
       float v = 0.f;
 #pragma unroll
-      for (int j = 0; j < NJ; ++j) v = fmaf(D[a][j], xc[j], v);
+      for (int k = 0; k < 2 * NJ; ++k) v = fmaf(D[a][k], xc[k], v);
       p[a] = v;
     }
     // reduce-scatter of the 16 partials over the 32 lanes
@@ -794,27 +824,33 @@ __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float 
     for (int a = 0; a < 16; ++a) q[a] = Q[c * 16 + a];
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
-      const int w = lane + 32 * j;
-      float v = 0.f;
+      const int w = 2 * lane + 64 * j;
+      float v2[2];
 #pragma unroll
-      for (int a = 0; a < 16; ++a) v = fmaf(D[a][j], q[a], v);
-      if (j == 0) {  // w < 32: the Q -> X terms live at w < 2A <= 32
-        if (w < A && c < 4) v += dQ[c * 16 + w];
-        if (w >= A && w < 2 * A) {
-          const int aa = w - A;
-          if (c >= 4) {
-            v += dQ[c * 16 + aa];
-          } else if (c >= 1) {
-            const float y1 = X[E2 + w], y2 = X[2 * E2 + w], y3 = X[3 * E2 + w];
-            const float d0 = dQ[64 + aa], d1 = dQ[80 + aa], d2 = dQ[96 + aa], d3 = dQ[112 + aa], d4 = dQ[128 + aa],
-                        d5 = dQ[144 + aa];
-            if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
-            if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
-            if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
+      for (int h = 0; h < 2; ++h) {
+        const int ww = w + h;
+        float v = 0.f;
+#pragma unroll
+        for (int a = 0; a < 16; ++a) v = fmaf(D[a][2 * j + h], q[a], v);
+        if (j == 0) {  // the Q -> X terms live at w < 2A <= 32
+          if (ww < A && c < 4) v += dQ[c * 16 + ww];
+          if (ww >= A && ww < 2 * A) {
+            const int aa = ww - A;
+            if (c >= 4) {
+              v += dQ[c * 16 + aa];
+            } else if (c >= 1) {
+              const float y1 = X[E2 + ww], y2 = X[2 * E2 + ww], y3 = X[3 * E2 + ww];
+              const float d0 = dQ[64 + aa], d1 = dQ[80 + aa], d2 = dQ[96 + aa], d3 = dQ[112 + aa],
+                          d4 = dQ[128 + aa], d5 = dQ[144 + aa];
+              if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
+              if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
+              if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
+            }
           }
         }
+        v2[h] = ww < E2 ? v * M.inv_nnbrs : 0.f;
       }
-      if (w < N2) out[c * N2 + w] = __float2bfloat16_rn(w < E2 ? v * M.inv_nnbrs : 0.f);
+      if (w < N2) *reinterpret_cast<__nv_bfloat162 *>(out + c * N2 + w) = __floats2bfloat162_rn(v2[0], v2[1]);
     }
   }
 }
@@ -1290,11 +1326,11 @@ __device__ __forceinline__ FitGemm fit_gemm_info(const DevModel &M, int ti, int 
   return G;
 }
 
-template <int FW>
+template <int FW, typename DGT>
 __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
                                                            int Mrows, RowMap rm,
                                                            const __nv_bfloat16 *__restrict__ Gb,
-                                                           float *__restrict__ dGout, float *__restrict__ scratch,
+                                                           DGT *__restrict__ dGout, float *__restrict__ scratch,
                                                            float *__restrict__ Eatom, double *__restrict__ energy,
                                                            int N, int *__restrict__ err,
                                                            const int32_t *__restrict__ seg, int tile0) {
@@ -1596,16 +1632,32 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         if (two) tc::tmem_ld16_issue(tcol + c0 + 16, rb);
         tc::tmem_wait();
         if (act) {
-          float4 *dst = reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0);
-#pragma unroll
-          for (int i = 0; i < 16; i += 4)
-            dst[i / 4] = make_float4(__uint_as_float(ra[i]), __uint_as_float(ra[i + 1]), __uint_as_float(ra[i + 2]),
-                                     __uint_as_float(ra[i + 3]));
-          if (two) {
+          if constexpr (sizeof(DGT) == 4) {  // FP32 (for the FP32 embedding adjoint)
+            float4 *dst = reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0);
 #pragma unroll
             for (int i = 0; i < 16; i += 4)
-              dst[4 + i / 4] = make_float4(__uint_as_float(rb[i]), __uint_as_float(rb[i + 1]),
-                                           __uint_as_float(rb[i + 2]), __uint_as_float(rb[i + 3]));
+              dst[i / 4] = make_float4(__uint_as_float(ra[i]), __uint_as_float(ra[i + 1]),
+                                       __uint_as_float(ra[i + 2]), __uint_as_float(ra[i + 3]));
+            if (two) {
+#pragma unroll
+              for (int i = 0; i < 16; i += 4)
+                dst[4 + i / 4] = make_float4(__uint_as_float(rb[i]), __uint_as_float(rb[i + 1]),
+                                             __uint_as_float(rb[i + 2]), __uint_as_float(rb[i + 3]));
+            }
+          } else {  // BF16
+            float fa[16], fb[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              fa[i] = __uint_as_float(ra[i]);
+              fb[i] = __uint_as_float(rb[i]);
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(dGout + me * K0 + n0 + c0);
+            dst[0] = pack8(fa);
+            dst[1] = pack8(fa + 8);
+            if (two) {
+              dst[2] = pack8(fb);
+              dst[3] = pack8(fb + 8);
+            }
           }
         }
       }
@@ -1621,12 +1673,12 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   if (warp == 0) tc::tmem_dealloc(td, 256);
 }
 
-template <int FW>
-int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, float *dG, float *scratch,
+template <int FW, typename DGT>
+int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, DGT *dG, float *scratch,
                    float *Eatom, double *energy, int *err, cudaStream_t st) {
   using C = FitCfg<FW>;
   if (!M.fit_bt[0][kFitBtDg]) return DPB_ERR_UNSUPPORTED;
-  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW, DGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
   int tile0 = 0;  // scratch tiles of 128 rows, consecutive over the centre types
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -1634,7 +1686,7 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
     const int ntile = (Mrows + 127) / 128;
-    k_mix_fit<FW><<<ntile, kFitThreads, C::SMEM, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
+    k_mix_fit<FW, DGT><<<ntile, kFitThreads, C::SMEM, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
                                                         D.seg, tile0);
     tile0 += ntile;
     count_launch();
@@ -1746,8 +1798,8 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
   DPB_LAUNCH_CHECK();
   prof_end(PROF_EMBED_FWD, st);
   prof_begin(PROF_MIXED_FIT, st);
-  rc = (M.FW[0] == 240) ? launch_mix_fit<240>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
-                        : launch_mix_fit<128>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+  rc = (M.FW[0] == 240) ? launch_mix_fit<240, float>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
+                        : launch_mix_fit<128, float>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_EMBED_BWD, st);
@@ -1799,14 +1851,15 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
-  rc = (M.FW[0] == 240) ? launch_mix_fit<240>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
-                        : launch_mix_fit<128>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+  __nv_bfloat16 *dGb = reinterpret_cast<__nv_bfloat16 *>(dG);  // dE/dG in BF16 (the dE/dT input)
+  rc = (M.FW[0] == 240) ? launch_mix_fit<240, __nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st)
+                        : launch_mix_fit<128, __nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);
   {
-    if (M.E2 == 100) k_mix_dT<100, 112><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dG, dTb);
-    else k_mix_dT<64, 64><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dG, dTb);
+    if (M.E2 == 100) k_mix_dT<100, 112><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dGb, dTb);
+    else k_mix_dT<64, 64><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dGb, dTb);
     count_launch();
     DPB_LAUNCH_CHECK();
   }
