@@ -1460,16 +1460,22 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       }
     }
     uint32_t accf_n = 0;
-    // per-CTA scratch tile [slot][n][thread] (coalesced): slots 0..L-1 tanh
-    // values, L..2L-1 layer outputs, 2L the residual adjoint
+    // per-CTA scratch tile [slot][n][thread] (coalesced): slots 0..L-2 tanh
+    // values, L..2L-2 layer outputs (hidden layers below the last), 2L the
+    // residual adjoint
     float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + row;
 #define FIT_SCR(slot, n) tile[((size_t)(slot) * FW + (n)) * 128]
-    // ---- forward
+    // ---- forward; the last layer's epilogue also forms the atom energy and
+    // the first adjoint gate g = w_out dt (1 - t^2), the A operand of adjoint
+    // layer L-1 (its t and h never go to the scratch)
+    const float *wf = M.fw[ti][L];
+    float e_sum = 0.f;
     for (int l = 0; l < L && ok; ++l) {
       ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
       ++accf_n;
       if (!ok) break;
       tc::fence_after_sync();
+      const bool last = l == L - 1;
       const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
       // residual sources of the current chunk, loaded one chunk ahead so the
       // scratch reads overlap the TMEM loads and the previous chunk's math
@@ -1482,7 +1488,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         float hn[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) hn[i] = (dt && c0 + 16 < FW) ? FIT_SCR(L + l - 1, c0 + 16 + i) : 0.f;
-        float bv[16], dv[16];
+        float bv[16], dv[16], wv[16];
 #pragma unroll
         for (int i = 0; i < 16; i += 4) {
           const float4 b4 = __ldg(reinterpret_cast<const float4 *>(bias + c0 + i));
@@ -1490,6 +1496,8 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           const float4 d4 =
               dt ? __ldg(reinterpret_cast<const float4 *>(dt + c0 + i)) : make_float4(1.f, 1.f, 1.f, 1.f);
           dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
+          const float4 w4 = last ? __ldg(reinterpret_cast<const float4 *>(wf + c0 + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+          wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
         }
         tc::tmem_wait();
         float hv[16];
@@ -1499,53 +1507,25 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
           float h = t;
           if (dt) h = t * dv[i] + hp[i];
-          hv[i] = h;
-          FIT_SCR(l, n) = t;
-          FIT_SCR(L + l, n) = h;
+          if (!last) {
+            hv[i] = h;
+            FIT_SCR(l, n) = t;
+            FIT_SCR(L + l, n) = h;
+          } else {
+            e_sum = fmaf(h, wv[i], e_sum);
+            hv[i] = wv[i] * dv[i] * (1.f - t * t);
+          }
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) hp[i] = hn[i];
         *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(hv);
         *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(hv + 8);
       }
-      if (l < L - 1) fit_signal(&epid);
+      fit_signal(&epid);
     }
-    // ---- energy and the first adjoint gate
     float e_me = 0.f;
     if (ok) {
-      const float *wf = M.fw[ti][L], *dtL = M.fdt[ti][L - 1];
-      float s = 0.f;
-      float hc[16], tcur[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        hc[i] = FIT_SCR(2 * L - 1, i);
-        tcur[i] = FIT_SCR(L - 1, i);
-      }
-      for (int c0 = 0; c0 < FW; c0 += 16) {
-        float hn[16], tn[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          hn[i] = (c0 + 16 < FW) ? FIT_SCR(2 * L - 1, c0 + 16 + i) : 0.f;
-          tn[i] = (c0 + 16 < FW) ? FIT_SCR(L - 1, c0 + 16 + i) : 0.f;
-        }
-        float g[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int n = c0 + i;
-          const float wn = __ldg(wf + n);
-          s = fmaf(hc[i], wn, s);
-          g[i] = wn * (dtL ? __ldg(dtL + n) : 1.f) * (1.f - tcur[i] * tcur[i]);
-        }
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(g);
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(g + 8);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          hc[i] = hn[i];
-          tcur[i] = tn[i];
-        }
-      }
-      fit_signal(&epid);
-      e_me = s + M.fb[ti][L][0];
+      e_me = e_sum + M.fb[ti][L][0];
       if (act) Eatom[me] = e_me;
     }
     {  // energy per segment (every lane of the warp takes part): rows run
