@@ -117,16 +117,57 @@ __device__ __forceinline__ void prefetch_range_l2(const void *base, size_t bytes
   for (size_t o = (size_t)threadIdx.x * 128; o < bytes; o += (size_t)blockDim.x * 128) tc::prefetch_l2(b + o);
 }
 
-// Geometry of a compacted row and the 10-channel env row (FP32).  raw: the
-// row holds r_j - r_i and the minimum image (utils.py:24-26) is applied here.
-__device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float rcut, float inv_std, float mean,
-                                            RowGeom &gm, float &st, float R[10]) {
-  const float3 x = raw ? make_float3(shift_ortho(rb.x, L.x), shift_ortho(rb.y, L.y), shift_ortho(rb.z, L.z))
-                       : make_float3(rb.x, rb.y, rb.z);
-  row_geom(x, rcut, gm);
+// Row geometry of the mixed form: the guarded norm, s(r) of utils.py:29-32
+// and ds/dr as in row_geom, with fast reciprocals (a few ulp; the BF16 GEMMs
+// downstream round far more).
+__device__ __forceinline__ void row_geom_mixed(float3 x, float rcut, RowGeom &g) {
+  g.x[0] = x.x; g.x[1] = x.y; g.x[2] = x.z;
+  const float gx = fabsf(x.x) > 1e-15f ? x.x : 1e-15f;
+  const float gy = fabsf(x.y) > 1e-15f ? x.y : 1e-15f;
+  const float gz = fabsf(x.z) > 1e-15f ? x.z : 1e-15f;
+  const float r = sqrtf(gx * gx + gy * gy + gz * gz);
+  g.r = r;
+  const float t = __fdividef(r, rcut);
+  const float poly = 1.f - 3.f * t * t + 2.f * t * t * t;
+  const float den = r + 1e-15f, inv_den = __fdividef(1.f, den);
+  const bool in = (r > 1e-14f) && (t < 1.f);
+  g.s = in ? poly * inv_den : 0.f;
+  const float dpoly = __fdividef(-6.f * t + 6.f * t * t, rcut);
+  g.dsdr = in ? (dpoly * den - poly) * inv_den * inv_den : 0.f;
+}
+
+// Adjoint of the row (row_adjoint) with fast reciprocals, for the mixed form.
+__device__ __forceinline__ void row_adjoint_mixed(const RowGeom &g, float inv_std, const float gR[10], float gst,
+                                                  float gx[3]) {
+  const float inv_rp = __fdividef(1.f, g.r + 1e-16f);
+  const float xh0 = g.x[0] * inv_rp, xh1 = g.x[1] * inv_rp, xh2 = g.x[2] * inv_rp;
+  const float sn = g.s * inv_std;
+  const float g_sn = gR[0] + kSqrt3 * (gR[1] * xh0 + gR[2] * xh1 + gR[3] * xh2) +
+                     3.f * (gR[4] * (xh0 * xh0 - (1.f / 3.f)) + gR[5] * (xh1 * xh1 - (1.f / 3.f)) +
+                            gR[6] * (xh2 * xh2 - (1.f / 3.f))) +
+                     3.f * kSqrt2 * (gR[7] * xh0 * xh2 + gR[8] * xh1 * xh0 + gR[9] * xh2 * xh1);
+  const float gh0 = sn * (kSqrt3 * gR[1] + 6.f * gR[4] * xh0 + 3.f * kSqrt2 * (gR[7] * xh2 + gR[8] * xh1));
+  const float gh1 = sn * (kSqrt3 * gR[2] + 6.f * gR[5] * xh1 + 3.f * kSqrt2 * (gR[8] * xh0 + gR[9] * xh2));
+  const float gh2 = sn * (kSqrt3 * gR[3] + 6.f * gR[6] * xh2 + 3.f * kSqrt2 * (gR[7] * xh0 + gR[9] * xh1));
+  const float g_s = (g_sn + gst) * inv_std;
+  const float g_r = g_s * g.dsdr - (gh0 * g.x[0] + gh1 * g.x[1] + gh2 * g.x[2]) * inv_rp * inv_rp;
+  const float inv_r = __fdividef(1.f, g.r);
+  const float d0 = fabsf(g.x[0]) > 1e-15f ? g.x[0] * inv_r : 0.f;
+  const float d1 = fabsf(g.x[1]) > 1e-15f ? g.x[1] * inv_r : 0.f;
+  const float d2 = fabsf(g.x[2]) > 1e-15f ? g.x[2] * inv_r : 0.f;
+  gx[0] = gh0 * inv_rp + g_r * d0;
+  gx[1] = gh1 * inv_rp + g_r * d1;
+  gx[2] = gh2 * inv_rp + g_r * d2;
+}
+
+// Geometry of a compacted row (its relative coordinate) and the 10-channel
+// env row (FP32).
+__device__ __forceinline__ void mix_row_env(float4 rb, float rcut, float inv_std, float mean, RowGeom &gm, float &st,
+                                            float R[10]) {
+  row_geom_mixed(make_float3(rb.x, rb.y, rb.z), rcut, gm);
   const float sn = gm.s * inv_std;
   st = (gm.s - mean) * inv_std;
-  const float inv_rp = 1.f / (gm.r + 1e-16f);
+  const float inv_rp = __fdividef(1.f, gm.r + 1e-16f);
   const float xh[3] = {gm.x[0] * inv_rp, gm.x[1] * inv_rp, gm.x[2] * inv_rp};
   env_row(sn, xh, R);
 }
@@ -138,12 +179,13 @@ __device__ __forceinline__ void mix_row_env(float4 rb, bool raw, float3 L, float
 // using any, and the
 // kept rows are appended to rowbuf in candidate order (so rows stay sorted by
 // atom slot) as (x, y, z, packed), packed = (neighbour user index << 3) | slot.
-// With one image per pair (nim == 1, boxes wider than 2 rcut) a row keeps the
-// raw difference r_j - r_i (mix_row_env applies the minimum image) and the
-// keep test is a nearest-image distance estimate with a 1e-3 A margin: every
-// row with s(r) != 0 is kept, and a kept row with s(r) = 0 adds exact zeros
-// (R~ = 0, ds/dr = 0).  With several images the exact displacement and s(r)
-// decide.  The unread rows [rowstart, rowcount) of earlier rounds (fewer than
+// With one image per pair (nim == 1, boxes wider than 2 rcut) the row's
+// displacement is the nearest image d - L rint(d / L), which equals the
+// reference's (d - L/2) mod L - L/2 (utils.py:24-26) up to rounding (the mixed
+// form is held to a tolerance, not to bits), and the keep test is |x| <
+// rcut + 1e-3 A: every row with s(r) != 0 is kept, and a kept row with
+// s(r) = 0 adds exact zeros (R~ = 0, ds/dr = 0).  With several images the
+// reference's displacement and s(r) decide.  The unread rows [rowstart, rowcount) of earlier rounds (fewer than
 // 128) are first moved to the front.
 template <int CPT>
 __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevModel &M, int tj, int base, int total,
@@ -209,7 +251,7 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
                     az = fmaf(-L.z, rintf(dz * inv_l.z), dz);
         if (ax * ax + ay * ay + az * az < rk2) {
           keep |= 1u << k;
-          rv[k] = make_float4(dx, dy, dz, __int_as_float((src[k] << 3) | slotk[k]));
+          rv[k] = make_float4(ax, ay, az, __int_as_float((src[k] << 3) | slotk[k]));
         }
       }
     }
@@ -484,7 +526,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
           RowGeom gm;
           float st, R[10];
-          mix_row_env(rv, nim == 1, L, M.rcut, inv_std, mean, gm, st, R);
+          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image visible; rowbuf read by every thread
           float h0[16];
@@ -1013,7 +1055,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
           const int slot = packed & 7, jsrc = packed >> 3;
           RowGeom gm;
           float st, R[10];
-          mix_row_env(rv, nim == 1, L, M.rcut, inv_std, mean, gm, st, R);
+          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image and DTB visible
           float h1[E1], d1[E1];
@@ -1154,7 +1196,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 #pragma unroll
           for (int c = 0; c < 10; ++c) gst = fmaf(R[c], v[c], gst);
           float gx[3];
-          row_adjoint(gm, inv_std, u, gst, gx);
+          row_adjoint_mixed(gm, inv_std, u, gst, gx);
           if (act) {
             atomicAdd(&F4[frame_base + jsrc], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
 #pragma unroll
