@@ -402,23 +402,28 @@ __device__ __forceinline__ void fwd_epi2(uint32_t tD, uint32_t lane_off, const f
   constexpr int c0 = HALF ? SP::S2 : 0, c1 = HALF ? MD::N2 : SP::S2;
   constexpr int h1lo = HALF ? SP::S1 : 0, h1n = HALF ? SP::H1N1 : SP::S1;
 #pragma unroll
-  for (int g = c0 / 16 * 16; g < c1; g += 16) {
-    uint32_t r[16];
-    tc::tmem_ld16_issue(tD + lane_off + g, r);
+  for (int gg = c0 / 16 * 16; gg < c1; gg += 32) {
+    uint32_t r[2][16];
+    tc::tmem_ld16_issue(tD + lane_off + gg, r[0]);
+    if (gg + 16 < c1) tc::tmem_ld16_issue(tD + lane_off + gg + 16, r[1]);
     tc::tmem_wait();
 #pragma unroll
-    for (int h8 = 0; h8 < 16; h8 += 8) {
-      if (g + h8 < c0 || g + h8 >= c1) continue;
-      float h2[8];
+    for (int q = 0; q < 2; ++q) {
+      const int g = gg + 16 * q;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int col = g + h8 + i;
-        const int src = col / MD::Z2 - h1lo;
-        h2[i] = (col < E2) ? tc::tanh_fast(__uint_as_float(r[h8 + i]) + sm[2 * E0 + E1 + (col < E2 ? col : 0)]) +
-                                 h1[src < 0 ? 0 : (src >= h1n ? h1n - 1 : src)]
-                           : 0.f;
+      for (int h8 = 0; h8 < 16; h8 += 8) {
+        if (g + h8 < c0 || g + h8 >= c1) continue;
+        float h2[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int col = g + h8 + i;
+          const int src = col / MD::Z2 - h1lo;
+          h2[i] = (col < E2) ? tc::tanh_fast(__uint_as_float(r[q][h8 + i]) + sm[2 * E0 + E1 + (col < E2 ? col : 0)]) +
+                                   h1[src < 0 ? 0 : (src >= h1n ? h1n - 1 : src)]
+                             : 0.f;
+        }
+        *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(row, g + h8, MD::N2)) = pack8(h2);
       }
-      *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(row, g + h8, MD::N2)) = pack8(h2);
     }
   }
 }
