@@ -44,9 +44,14 @@ void prof_end(int id, cudaStream_t st);
   } while (0)
 
 // jnp.mod / jnp.remainder: fmod, then add y where the remainder's sign differs
-// from y's (y > 0 here).
+// from y's (y > 0 here).  fmod itself is only evaluated outside (-y, 2y):
+// inside, fmod(x, y) is x for |x| < y and x - y for y <= x < 2y (an exact
+// difference, Sterbenz), so the result is bit-identical for every x.
 __device__ __forceinline__ float jmod(float x, float y) {
-  float r = fmodf(x, y);
+  float r;
+  if (x > -y && x < y) r = x;
+  else if (x >= y && x < 2.f * y) r = x - y;
+  else r = fmodf(x, y);
   return (r != 0.f && r < 0.f) ? r + y : r;
 }
 

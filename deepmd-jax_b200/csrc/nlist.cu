@@ -8,10 +8,14 @@
 // indices in ascending order, type-local, padded with N, and flags overflow
 // when more than sel_j exist.
 //
-// Layout: cells are binned per frame; a warp owns one centre atom, walks the
-// 27 (or fewer, for 2-cell or 1-cell axes) neighbouring cells, appends hits
-// per type into shared memory with ballots, then ranks the hits (indices are
-// distinct, so rank = number of smaller hits) and writes the sorted prefix.
+// Layout: cells are binned per frame and each cell slot also holds its
+// atom's canonical position and index as one float4 (cell order), so a
+// candidate is one coalesced 16-byte load.  A warp owns one centre atom,
+// centres taken in cell order so that the warps of a block share their
+// neighbourhood in L1; it walks the 27 (or fewer, for 2-cell or 1-cell axes)
+// neighbouring cells, appends hits per type into shared memory with ballots,
+// then ranks the hits (indices are distinct, so rank = number of smaller
+// hits) and writes the sorted prefix into the centre's own row.
 #include "dpb_common.cuh"
 #include <algorithm>
 #include <cmath>
@@ -113,7 +117,8 @@ __global__ void nl_scan_kernel(const int *__restrict__ in, int *__restrict__ out
 }
 
 __global__ void nl_scatter_kernel(const int *__restrict__ atom_cell, const int *__restrict__ cell_start,
-                                  int *__restrict__ cursor, int *__restrict__ cell_atoms, int N, int F,
+                                  int *__restrict__ cursor, int *__restrict__ cell_atoms,
+                                  const float *__restrict__ canon, float4 *__restrict__ cell_pos, int N, int F,
                                   int ncell, const unsigned *__restrict__ gate) {
   if (gate && *gate == 0u) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -121,7 +126,10 @@ __global__ void nl_scatter_kernel(const int *__restrict__ atom_cell, const int *
   int f = g / N;
   int c = f * ncell + atom_cell[g];
   int slot = atomicAdd(&cursor[c], 1);
-  cell_atoms[cell_start[c] + slot] = g - f * N;  // frame-local sorted index
+  const int q = cell_start[c] + slot;
+  cell_atoms[q] = g - f * N;  // frame-local sorted index
+  cell_pos[q] = make_float4(canon[(size_t)g * 3], canon[(size_t)g * 3 + 1], canon[(size_t)g * 3 + 2],
+                            __int_as_float(g - f * N));
 }
 
 struct NlParams {
@@ -169,6 +177,7 @@ __device__ __forceinline__ bool pair_hit(float3 ci, float3 cj, float3 L, float r
 __global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float *__restrict__ canon,
                                                         const int *__restrict__ cell_start,
                                                         const int *__restrict__ cell_atoms,
+                                                        const float4 *__restrict__ cell_pos,
                                                         int32_t *__restrict__ nbrs,
                                                         int32_t *__restrict__ counts,
                                                         uint32_t *__restrict__ status,
@@ -179,9 +188,10 @@ __global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float 
   const int wpb = blockDim.x >> 5;
   int *cnt = smem + warp * kMaxTypes;
   int *lists = smem + wpb * kMaxTypes + warp * P.ntypes * P.cap;
-  int g = blockIdx.x * wpb + warp;
-  if (g >= P.N * P.F) return;
-  const int f = g / P.N, i = g - f * P.N;
+  const int gc = blockIdx.x * wpb + warp;  // position in cell order
+  if (gc >= P.N * P.F) return;
+  const int f = gc / P.N, i = cell_atoms[gc];  // frame-local sorted index of the centre
+  const int g = f * P.N + i;
   const float *cf = canon + (size_t)f * P.N * 3;
   float3 ci = make_float3(cf[i * 3], cf[i * 3 + 1], cf[i * 3 + 2]);
   if (lane < kMaxTypes) cnt[lane] = 0;
@@ -209,9 +219,9 @@ __global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float 
             bool hit = false;
             int j = 0, t = 0;
             if (q < e) {
-              j = cell_atoms[q];
-              float3 cj = make_float3(cf[j * 3], cf[j * 3 + 1], cf[j * 3 + 2]);
-              hit = (j != i) && pair_hit(ci, cj, P.L, P.rc2);
+              const float4 v = cell_pos[q];
+              j = __float_as_int(v.w);
+              hit = (j != i) && pair_hit(ci, make_float3(v.x, v.y, v.z), P.L, P.rc2);
               t = type_of(j, P.offs, P.ntypes);
             }
             append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
@@ -273,7 +283,8 @@ extern "C" int dpb_nlist_workspace_bytes(int natoms, int nframes, const float bo
   if (!bytes || natoms <= 0 || nframes <= 0 || !box || rc <= 0) return DPB_ERR_INVALID_ARG;
   NlGrid g = make_grid(box, rc);
   size_t NF = (size_t)natoms * nframes, C = (size_t)g.ncell * nframes;
-  *bytes = align_up(C * 4) * 2 + align_up((C + 1) * 4) + align_up(NF * 4) * 2 + align_up(NF * 12);
+  *bytes = align_up(C * 4) * 2 + align_up((C + 1) * 4) + align_up(NF * 4) * 2 + align_up(NF * 16) +
+           align_up(NF * 12);
   return DPB_OK;
 }
 
@@ -327,6 +338,7 @@ int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nfra
   int *cell_start = (int *)w; w += align_up((C + 1) * 4);
   int *atom_cell = (int *)w; w += align_up(NF * 4);
   int *cell_atoms = (int *)w; w += align_up(NF * 4);
+  float4 *cell_pos = (float4 *)w; w += align_up(NF * 16);
   float *canon = ref_pos ? ref_pos : (float *)w;
 
   nl_zero_kernel<<<(int)((C + 255) / 256), 256, 0, stream>>>(cell_count, (int)C, cursor, (int)C, gate);
@@ -336,15 +348,15 @@ int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nfra
   nl_canon_kernel<<<nb, 256, 0, stream>>>(pos, perm, natoms, nframes, L, scale, P.L, P.nc, canon, atom_cell,
                                           cell_count, gate, dbox);
   nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C, gate);
-  nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, natoms, nframes,
-                                            g.ncell, gate);
+  nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, canon, cell_pos, natoms,
+                                            nframes, g.ncell, gate);
   const int threads = 256, wpb = threads / 32;
   size_t smem = (size_t)wpb * kMaxTypes * 4 + (size_t)wpb * ntypes * cap * 4;
   if (smem > 48 * 1024) {
     DPB_CUDA_TRY(cudaFuncSetAttribute(nl_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   nl_search_kernel<<<(int)((NF + wpb - 1) / wpb), threads, smem, stream>>>(P, canon, cell_start, cell_atoms,
-                                                                           nbrs, counts, status, gate);
+                                                                           cell_pos, nbrs, counts, status, gate);
   count_launch(5);
   DPB_LAUNCH_CHECK();
   return DPB_OK;
