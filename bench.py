@@ -379,7 +379,7 @@ def gpu_arm(args, rank, world, local_rank):
         dt_e2e = max_over_ranks(dt_e2e, dist)
         line["e2e"] = {"value": job_rate(N * K, world, dt_e2e), "unit": "atom-steps/s",
                        "h2d_bytes_per_step": int(2 * N * 3 * 8 / K),
-                       "d2h_bytes_per_step": int(2 * N * 3 * 4),
+                       "d2h_bytes_per_step": int(2 * N * 3 * 8),  # user-order float64 positions + velocities
                        "api": "Simulation.setPosition + setVelocity + run(K) returning the per-step trajectory"}
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_sample()

@@ -416,19 +416,27 @@ class Simulation:
         NF3 = self._natoms * self._n_bead * 3
         cap = self._step_chunk_size
         if getattr(self, "_traj_bufs", None) is None:
-            # trajectory frames of one chunk, kept across runs so captured graphs stay valid
-            self._traj_bufs = (torch.empty((cap, NF3), dtype=torch.float32, device="cuda"),
-                               torch.empty((cap, NF3), dtype=torch.float32, device="cuda"))
-        buf_p, buf_v = self._traj_bufs
+            # two sets of trajectory frames of one chunk (chunk k is copied out
+            # while chunk k + 1 runs), kept across runs so captured graphs stay valid
+            self._traj_bufs = [(torch.empty((cap, NF3), dtype=torch.float32, device="cuda"),
+                                torch.empty((cap, NF3), dtype=torch.float32, device="cuda")) for _ in range(2)]
+        buf_p, buf_v = self._traj_bufs[0]
+        which = 0
+        pending = None  # an accepted chunk whose frames are still on the device
         done, idx = 0, int(first)
         overflow_twice = False
         while done < steps:
             n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
             _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
+            if trajectory:
+                buf_p, buf_v = self._traj_bufs[which]
             if trajectory or dumps:
                 self._run_chunk(n, buf_p[:n], buf_v[:n])
             else:
                 self._run_chunk(n, None, None)
+            if pending is not None:  # the previous chunk's frames leave while this one runs
+                self._copy_out(pending, traj)
+                pending = None
             r = self._report_struct()
             code = int(r.status)
             if code & 16:
@@ -463,23 +471,18 @@ class Simulation:
                     self._report_row(tic)
                     tic = time()
                 continue
-            pos_chunk = buf_p[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
-            mom_chunk = buf_v[:n].view(n, self._n_bead, self._natoms, 3).cpu().numpy()
-            pos_u = np.empty_like(pos_chunk)
-            mom_u = np.empty_like(mom_chunk)
-            pos_u[:, :, self._perm] = pos_chunk
-            mom_u[:, :, self._perm] = mom_chunk
-            vel_u = mom_u / (self._mass * MASS_UNIT_CONVERSION)[None, None, :, None]
-            if not self._is_pimd:
-                pos_u, vel_u = pos_u[:, 0], vel_u[:, 0]
-            traj["position"][idx:idx + n] = pos_u
-            traj["velocity"][idx:idx + n] = vel_u
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream())
+            pending = (buf_p, buf_v, n, idx, ev)
+            which ^= 1
             idx += n
             done += n
             self.step += n
             if self.step % self.report_interval == 0 or done == steps:
                 self._report_row(tic)
                 tic = time()
+        if pending is not None:
+            self._copy_out(pending, traj)
         elapsed = time() - tic_run
         if self.verbose:
             nsd = 1e-6 * steps * self._dt * (86400 / max(elapsed, 1e-9))
@@ -489,6 +492,33 @@ class Simulation:
         if self._is_pimd and traj is not None:
             traj["centroid"] = np.stack([self._centroid(p) for p in traj["position"]])
         return traj
+
+    def _copy_out(self, pending, traj):
+        """Frames of one accepted chunk into the host trajectory: user order
+        and velocities = momenta / (m * unit) in float64, formed on the device
+        on a side stream (the next chunk keeps the main stream busy), then
+        copied into traj[idx:idx + n].  Same values as un-permuting and
+        dividing on the host: float32 -> float64 is exact and IEEE division is
+        correctly rounded on both."""
+        buf_p, buf_v, n, idx, ev = pending
+        P, N = self._n_bead, self._natoms
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream()
+            inv = np.empty_like(self._perm)
+            inv[self._perm] = np.arange(len(self._perm))
+            self._inv_perm_dev = torch.tensor(inv.astype(np.int64), device="cuda")
+            self._mass_unit_dev = torch.tensor(self._mass * MASS_UNIT_CONVERSION, dtype=torch.float64, device="cuda")
+        cs = self._copy_stream
+        with torch.cuda.stream(cs):
+            cs.wait_event(ev)
+            pos = buf_p[:n].view(n, P, N, 3).index_select(2, self._inv_perm_dev).double()
+            vel = buf_v[:n].view(n, P, N, 3).index_select(2, self._inv_perm_dev).double()
+            vel = vel / self._mass_unit_dev[None, None, :, None]
+            if not self._is_pimd:
+                pos, vel = pos[:, 0], vel[:, 0]
+            torch.from_numpy(traj["position"][idx:idx + n]).copy_(pos)
+            torch.from_numpy(traj["velocity"][idx:idx + n]).copy_(vel)
+        cs.synchronize()
 
     def _unpack_frame(self, p_row, v_row):
         """User-order positions and velocities of one device frame row."""
