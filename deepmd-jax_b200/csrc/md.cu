@@ -210,6 +210,11 @@ struct NptScalars {
   double pressure;
   double bxi[kMaxChain], bp[kMaxChain], bQ[kMaxChain];
   double bke, bdof;
+  // NPT-PIMD: centroid drift e^y - 1 per axis, the internal-mode virial
+  // sum(r - r_centroid) . f per axis of the last evaluation, barostat work
+  double e1m1[3];
+  double intvir[3];
+  double btwork;
 };
 
 // sinh(x)/x by the series the reference uses (routine.py:290-292)
@@ -483,6 +488,284 @@ __global__ void k_pimd_baoa(float *__restrict__ pos, float *__restrict__ mom, co
   if ((threadIdx.x & 31) == 0 && dke != 0.f) atomicAdd(&sc->twork, (double)dke);
 }
 
+// ---------------------------------------------------------------- NPT-PIMD
+// deepmd_jax/pimd.py:255-518: Parrinello-Rahman on the centroid mode only,
+// internal modes propagated exactly, PILE-L on the beads and a Langevin
+// barostat on the box momenta; the barostat is driven by the centroid
+// momenta and the centroid-virial dU/d(eps).  Per step: k_nptp_begin (half
+// box kick, propagator factors, half box update), k_nptp_a (B, A, O),
+// k_nptp_mid (box Langevin, half box update), k_nptp_b (A, unwrap), forces,
+// k_nptp_c (internal virial, B, centroid p^2/m), k_nptp_end (dU/d(eps), half
+// box kick).  All beads share the box (every row of boxd).
+
+// Box of the current log scales into all P rows of boxd.
+__device__ void nptp_set_box(const NptScalars *np, float *boxd, int P) {
+  for (int a = 0; a < 3; ++a) {
+    const float L = (float)(np->ref[a] * (np->gid[a] >= 0 ? exp(np->Rb[np->gid[a]]) : 1.0));
+    for (int b = 0; b < P; ++b) boxd[b * 3 + a] = L;
+  }
+}
+
+// Factors of the centroid kick exp_iL2_pimd (pimd.py:375-383) and of the
+// half-step centroid drift exp_iL1_centroid_pimd (pimd.py:385-398) from the
+// current box momenta.
+__device__ void nptp_factors(NptScalars *np, double h, double Nf) {
+  double Vb[3] = {0.0, 0.0, 0.0}, tr = 0.0;
+  for (int g = 0; g < np->G; ++g) {
+    Vb[g] = np->Pb[g] / np->Mb[g];
+    tr += np->ngrp[g] * Vb[g];
+  }
+  for (int a = 0; a < 3; ++a) {
+    const double va = np->gid[a] >= 0 ? Vb[np->gid[a]] : 0.0;
+    const double x = (va + tr / Nf) * h;
+    np->a2[a] = exp(-x);
+    np->b2[a] = h * sinhx_x(x / 2) * exp(-x / 2);
+    const double y = va * h;
+    np->e1m1[a] = expm1(y);
+    np->b1[a] = h * exp(y / 2) * sinhx_x(y / 2);
+  }
+}
+
+__global__ void k_nptp_begin(NptScalars *np, float *boxd, int P, double dt, int N) {
+  const double h = 0.5 * dt, Nf = 3.0 * N;
+  double Ge[3];
+  npt_box_force(np, npt_volume(np), Nf, Ge);
+  for (int g = 0; g < np->G; ++g) np->Pb[g] += h * Ge[g];
+  nptp_factors(np, h, Nf);
+  for (int g = 0; g < np->G; ++g) np->Rb[g] += h * np->Pb[g] / np->Mb[g];
+  nptp_set_box(np, boxd, P);
+}
+
+// Langevin barostat (pimd.py:486-491; normals of tag 2, element g), second
+// half box update, factors for the second drift and the last kick.
+__global__ void k_nptp_mid(const MdScalars *sc, NptScalars *np, float *boxd, int P, double dt, double kT,
+                           double gamma_box, unsigned long long seed, int N) {
+  const double h = 0.5 * dt;
+  const double c1 = exp(-gamma_box * dt), c2 = sqrt(fmax(kT * (1.0 - c1 * c1), 0.0));
+  double dw = 0.0;
+  for (int g = 0; g < np->G; ++g) {
+    const double old = np->Pb[g];
+    np->Pb[g] = c1 * old + c2 * sqrt(np->Mb[g]) * (double)philox_normal(seed, (unsigned)sc->step, 2u, (unsigned)g);
+    dw += 0.5 * (np->Pb[g] * np->Pb[g] - old * old) / np->Mb[g];
+  }
+  np->btwork += dw;
+  for (int g = 0; g < np->G; ++g) np->Rb[g] += h * np->Pb[g] / np->Mb[g];
+  nptp_set_box(np, boxd, P);
+  nptp_factors(np, h, 3.0 * N);
+  for (int a = 0; a < 3; ++a) np->ke2[a] = np->intvir[a] = 0.0;
+}
+
+// dU/d(eps_g) = (sum_b sum_{a in g} -W_b,aa + sum_{a in g} internal_a) / P
+// (pimd.py:332-350), then (kick) the last half box kick.
+__global__ void k_nptp_end(NptScalars *np, const double *__restrict__ virial, int P, double dt, int N, int kick) {
+  for (int g = 0; g < np->G; ++g) np->dUde[g] = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    if (np->gid[a] < 0) continue;
+    double w = 0.0;
+    for (int b = 0; b < P; ++b) w -= virial[b * 9 + a * 3 + a];
+    np->dUde[np->gid[a]] += (w + np->intvir[a]) / P;
+  }
+  if (kick) {
+    double Ge[3];
+    npt_box_force(np, npt_volume(np), 3.0 * N, Ge);
+    for (int g = 0; g < np->G; ++g) np->Pb[g] += 0.5 * dt * Ge[g];
+  }
+  for (int a = 0; a < 3; ++a) np->intvir[a] = 0.0;
+}
+
+// Beads of one column unwrapped onto bead 0's image (pimd.py:210-226).
+__device__ __forceinline__ void ring_unwrap(const float *R, float *U, int P, float Lc) {
+  for (int b = 0; b < P; ++b) {
+    const float d = R[b] - R[0];
+    U[b] = R[0] + (d - Lc * rintf(d / Lc));
+  }
+}
+
+// exp_iL2_pimd of one column: centroid p_c e^-x + h F_c sinh(x/2)/(x/2) e^(-x/2),
+// internal modes p - p_c + h (F - F_c).
+__device__ __forceinline__ void nptp_kick(float *Pm, const float *F, int P, float a2, float b2, float h) {
+  float pc = 0.f, fc = 0.f;
+  for (int b = 0; b < P; ++b) {
+    pc += Pm[b];
+    fc += F[b];
+  }
+  pc /= (float)P;
+  fc /= (float)P;
+  const float pcn = pc * a2 + fc * b2;
+  for (int b = 0; b < P; ++b) Pm[b] = pcn + (Pm[b] - pc) + h * (F[b] - fc);
+}
+
+// Centroid drift: every bead moves by r_c (e^y - 1) + b1 v_c.
+__device__ __forceinline__ void nptp_drift(float *R, const float *Pm, float m, int P, float Lc, float e1m1,
+                                           float b1) {
+  float U[kMaxBeads];
+  ring_unwrap(R, U, P, Lc);
+  float rc = 0.f, pc = 0.f;
+  for (int b = 0; b < P; ++b) {
+    rc += U[b];
+    pc += Pm[b];
+  }
+  rc /= (float)P;
+  const float d = rc * e1m1 + b1 * (pc / (float)P) / m;
+  for (int b = 0; b < P; ++b) R[b] += d;
+}
+
+// Exact free propagation of the internal ring-polymer modes for h; the
+// centroid normal mode stays (pimd.py:400-415).  C[b][k] in shared memory.
+__device__ __forceinline__ void nptp_ring(float *R, float *Pm, float m, int P, float Lc, const float *C,
+                                          const float *__restrict__ freqs, float h) {
+  float U[kMaxBeads], Q[kMaxBeads], Pn[kMaxBeads];
+  ring_unwrap(R, U, P, Lc);
+  for (int k = 0; k < P; ++k) {
+    float q = 0.f, pn = 0.f;
+    for (int b = 0; b < P; ++b) {
+      q = fmaf(C[b * P + k], U[b], q);
+      pn = fmaf(C[b * P + k], Pm[b], pn);
+    }
+    Q[k] = q;
+    Pn[k] = pn;
+  }
+  for (int k = 1; k < P; ++k) {
+    const float w = freqs[k];
+    float sn, cs;
+    sincosf(w * h, &sn, &cs);
+    const float q = Q[k] * cs + Pn[k] * sn / (m * w);
+    const float pn = Pn[k] * cs - m * w * Q[k] * sn;
+    Q[k] = q;
+    Pn[k] = pn;
+  }
+  for (int b = 0; b < P; ++b) {
+    float r = 0.f, pv = 0.f;
+    for (int k = 0; k < P; ++k) {
+      r = fmaf(C[b * P + k], Q[k], r);
+      pv = fmaf(C[b * P + k], Pn[k], pv);
+    }
+    R[b] = r;
+    Pm[b] = pv;
+  }
+}
+
+// B (centroid Parrinello-Rahman kick), A (centroid drift + internal ring,
+// first box), O (PILE-L, the stream of k_pimd_baoa) of one column.
+__global__ void k_nptp_a(float *__restrict__ pos, float *__restrict__ mom, const float *__restrict__ force,
+                         float *__restrict__ prev, const float *__restrict__ mass, const float *__restrict__ Cg,
+                         const float *__restrict__ freqs, const float *__restrict__ gamma, PimdParams pp,
+                         const NptScalars *__restrict__ np, const float *__restrict__ boxd, MdScalars *sc) {
+  __shared__ float C[kMaxBeads * kMaxBeads];
+  const int P = pp.P;
+  for (int e = threadIdx.x; e < P * P; e += blockDim.x) C[e] = Cg[e];
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N3 = pp.N * 3;
+  float dke = 0.f;
+  if (col < N3) {
+    const int atom = col / 3, comp = col - atom * 3;
+    const float Lc = boxd[comp], m = mass[atom], h = 0.5f * pp.dt;
+    float R[kMaxBeads], Pm[kMaxBeads], F[kMaxBeads], Pn[kMaxBeads];
+    for (int b = 0; b < P; ++b) {
+      R[b] = pos[(size_t)b * N3 + col];
+      prev[(size_t)b * N3 + col] = R[b];
+      Pm[b] = mom[(size_t)b * N3 + col];
+      F[b] = force[(size_t)b * N3 + col];
+    }
+    nptp_kick(Pm, F, P, (float)np->a2[comp], (float)np->b2[comp], h);
+    nptp_drift(R, Pm, m, P, Lc, (float)np->e1m1[comp], (float)np->b1[comp]);
+    nptp_ring(R, Pm, m, P, Lc, C, freqs, h);
+    // O: PILE-L in normal modes (pimd.py:471-479)
+    for (int k = 0; k < P; ++k) {
+      float pn = 0.f;
+      for (int b = 0; b < P; ++b) pn = fmaf(C[b * P + k], Pm[b], pn);
+      const float c1 = expf(-gamma[k] * pp.dt);
+      const float c2 = sqrtf(fmaxf(pp.kT * P * (1.f - c1 * c1), 0.f));
+      Pn[k] = c1 * pn + c2 * sqrtf(m) * philox_normal(pp.seed, (unsigned)sc->step, pp.tag, (unsigned)(k * N3 + col));
+    }
+    for (int b = 0; b < P; ++b) {
+      float pv = 0.f;
+      for (int k = 0; k < P; ++k) pv = fmaf(C[b * P + k], Pn[k], pv);
+      dke += 0.5f * (pv * pv - Pm[b] * Pm[b]) / m;
+      pos[(size_t)b * N3 + col] = R[b];
+      mom[(size_t)b * N3 + col] = pv;
+    }
+  }
+  dke = warp_sum(dke);
+  if ((threadIdx.x & 31) == 0 && dke != 0.f) atomicAdd(&sc->twork, (double)dke);
+}
+
+// A (centroid drift + internal ring, second box), then the per-bead
+// min_image_unwrap against the step's initial positions (md.py:785).
+__global__ void k_nptp_b(float *__restrict__ pos, float *__restrict__ mom, const float *__restrict__ prev,
+                         const float *__restrict__ mass, const float *__restrict__ Cg, const float *__restrict__ freqs,
+                         PimdParams pp, const NptScalars *__restrict__ np, const float *__restrict__ boxd) {
+  __shared__ float C[kMaxBeads * kMaxBeads];
+  const int P = pp.P;
+  for (int e = threadIdx.x; e < P * P; e += blockDim.x) C[e] = Cg[e];
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N3 = pp.N * 3;
+  if (col >= N3) return;
+  const int atom = col / 3, comp = col - atom * 3;
+  const float Lc = boxd[comp], m = mass[atom], h = 0.5f * pp.dt;
+  float R[kMaxBeads], Pm[kMaxBeads];
+  for (int b = 0; b < P; ++b) {
+    R[b] = pos[(size_t)b * N3 + col];
+    Pm[b] = mom[(size_t)b * N3 + col];
+  }
+  nptp_drift(R, Pm, m, P, Lc, (float)np->e1m1[comp], (float)np->b1[comp]);
+  nptp_ring(R, Pm, m, P, Lc, C, freqs, h);
+  for (int b = 0; b < P; ++b) {
+    const float r0 = prev[(size_t)b * N3 + col];
+    pos[(size_t)b * N3 + col] = r0 + (jmod(R[b] - r0 + 0.5f * Lc, Lc) - 0.5f * Lc);
+    mom[(size_t)b * N3 + col] = Pm[b];
+  }
+}
+
+// Internal-mode virial sum_b (r_b - r_c) f_b per axis (pimd.py:344-349),
+// then (kick) the last centroid kick, the centroid p_c^2 / m per axis and
+// (ke) the kinetic energy of all beads.
+__global__ void k_nptp_c(const float *__restrict__ pos, float *__restrict__ mom, const float *__restrict__ force,
+                         const float *__restrict__ mass, PimdParams pp, NptScalars *np,
+                         const float *__restrict__ boxd, MdScalars *sc, int kick, int ke) {
+  const int P = pp.P;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N3 = pp.N * 3;
+  float iv[3] = {0.f, 0.f, 0.f}, k2[3] = {0.f, 0.f, 0.f}, kin = 0.f;
+  if (col < N3) {
+    const int atom = col / 3, comp = col - atom * 3;
+    const float Lc = boxd[comp], m = mass[atom];
+    float R[kMaxBeads], U[kMaxBeads], Pm[kMaxBeads], F[kMaxBeads];
+    for (int b = 0; b < P; ++b) {
+      R[b] = pos[(size_t)b * N3 + col];
+      Pm[b] = mom[(size_t)b * N3 + col];
+      F[b] = force[(size_t)b * N3 + col];
+    }
+    ring_unwrap(R, U, P, Lc);
+    float rc = 0.f;
+    for (int b = 0; b < P; ++b) rc += U[b];
+    rc /= (float)P;
+    float v = 0.f;
+    for (int b = 0; b < P; ++b) v = fmaf(U[b] - rc, F[b], v);
+    iv[comp] = v;
+    if (kick) {
+      nptp_kick(Pm, F, P, (float)np->a2[comp], (float)np->b2[comp], 0.5f * pp.dt);
+      for (int b = 0; b < P; ++b) mom[(size_t)b * N3 + col] = Pm[b];
+    }
+    float pc = 0.f;
+    for (int b = 0; b < P; ++b) {
+      pc += Pm[b];
+      kin += 0.5f * Pm[b] * Pm[b] / m;
+    }
+    pc /= (float)P;
+    k2[comp] = pc * pc / m;
+  }
+  npt_reduce3(iv[0], iv[1], iv[2], np->intvir, nullptr);
+  __syncthreads();
+  npt_reduce3(k2[0], k2[1], k2[2], np->ke2, nullptr);
+  if (ke) {
+    kin = warp_sum(kin);
+    if ((threadIdx.x & 31) == 0 && kin != 0.f) atomicAdd(&sc->ke, (double)kin);
+  }
+}
+
 }  // namespace dpb
 
 using namespace dpb;
@@ -506,6 +789,7 @@ struct dpb_md {
   MdScalars *sc = nullptr;
   NptScalars *np = nullptr, *s_np = nullptr;  // NPT barostat state and its snapshot
   float *s_box = nullptr;
+  float *prev = nullptr;  // NPT-PIMD: positions at the start of the step
   float *C = nullptr, *freqs = nullptr, *gamma = nullptr;
   void *nl_ws = nullptr, *ev_ws = nullptr;
   size_t nl_ws_bytes = 0, ev_ws_bytes = 0;
@@ -534,11 +818,14 @@ static int md_alloc_lists(dpb_md *m) {
 extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_md **out) {
   if (!model || !d || !out || d->natoms <= 0 || d->nbeads <= 0 || !d->type_idx || !d->mass_per_type || !d->sel)
     return DPB_ERR_INVALID_ARG;
-  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_NPT_NHC) return DPB_ERR_INVALID_ARG;
-  if (d->routine == DPB_MD_NPT_NHC) {
-    if (d->nbeads != 1 || d->chain_length < 2 || d->chain_length > kMaxChain || d->chain_length_p < 2 ||
-        d->chain_length_p > kMaxChain || !(d->tau_p > 0.0))
-      return DPB_ERR_UNSUPPORTED;
+  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_NPT_PIMD) return DPB_ERR_INVALID_ARG;
+  const bool has_box = d->routine == DPB_MD_NPT_NHC || d->routine == DPB_MD_NPT_PIMD;
+  const bool pimd = d->routine == DPB_MD_PIMD_PILE || d->routine == DPB_MD_NPT_PIMD;
+  if (d->routine == DPB_MD_NPT_NHC && (d->nbeads != 1 || d->chain_length < 2 || d->chain_length > kMaxChain ||
+                                       d->chain_length_p < 2 || d->chain_length_p > kMaxChain))
+    return DPB_ERR_UNSUPPORTED;
+  if (has_box) {
+    if (!(d->tau_p > 0.0)) return DPB_ERR_UNSUPPORTED;
     int G = -1;
     for (int a = 0; a < 3; ++a) {
       if (d->couple_groups[a] < -1 || d->couple_groups[a] > 2) return DPB_ERR_INVALID_ARG;
@@ -549,9 +836,9 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
       if (d->couple_groups[0] != g && d->couple_groups[1] != g && d->couple_groups[2] != g)
         return DPB_ERR_INVALID_ARG;  // groups must be numbered 0..G-1
   }
-  if (d->routine == DPB_MD_PIMD_PILE && (d->nbeads < 2 || d->nbeads > kMaxBeads || !d->nm_transform || !d->nm_freqs))
+  if (pimd && (d->nbeads < 2 || d->nbeads > kMaxBeads || !d->nm_transform || !d->nm_freqs))
     return DPB_ERR_INVALID_ARG;
-  if (d->routine != DPB_MD_PIMD_PILE && d->nbeads != 1) return DPB_ERR_INVALID_ARG;
+  if (!pimd && d->nbeads != 1) return DPB_ERR_INVALID_ARG;
   if (d->routine == DPB_MD_NVT_NHC && (d->chain_length < 2 || d->chain_length > kMaxChain))
     return DPB_ERR_UNSUPPORTED;
   *out = nullptr;
@@ -594,11 +881,12 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   rc_ |= md_alloc(m, (void **)&m->s_force, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_ref, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_sc, sizeof(MdScalars));
-  if (d->routine == DPB_MD_NPT_NHC) {
+  if (has_box) {
     rc_ |= md_alloc(m, (void **)&m->np, sizeof(NptScalars));
     rc_ |= md_alloc(m, (void **)&m->s_np, sizeof(NptScalars));
-    rc_ |= md_alloc(m, (void **)&m->s_box, 12);
+    rc_ |= md_alloc(m, (void **)&m->s_box, (size_t)m->P * 12);
   }
+  if (d->routine == DPB_MD_NPT_PIMD) rc_ |= md_alloc(m, (void **)&m->prev, NF * 12);
   rc_ |= md_alloc_lists(m);
   if (rc_) { dpb_md_destroy(m); return DPB_ERR_CUDA; }
   // masses in eV fs^2 / A^2 (md.py:24), sorted order
@@ -621,7 +909,7 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   s0.dof = 3.0 * (double)N;
   cudaMemcpy(m->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice);
   cudaMemset(m->status, 0, 4);
-  if (d->routine == DPB_MD_PIMD_PILE) {
+  if (pimd) {
     const int P = m->P;
     std::vector<float> C(P * P), fr(P), ga(P);
     for (int i = 0; i < P * P; ++i) C[i] = (float)d->nm_transform[i];
@@ -721,7 +1009,7 @@ extern "C" int dpb_md_get_state(const dpb_md *m, double *pos, double *vel, doubl
 // the device copy m->boxd and the list canonicalises into the reference box.
 static int md_build_list(dpb_md *m, const unsigned *gate, cudaStream_t st) {
   const float rc = m->model->dm.rcut + (float)m->d.skin;
-  const bool npt = m->d.routine == DPB_MD_NPT_NHC;
+  const bool npt = m->np != nullptr;  // the box lives on the device
   return nlist_build_impl(m->pos, nullptr, m->N, m->P, m->ntypes, m->type_count, m->sel, m->box, nullptr, rc,
                           m->nbrs, m->ref_pos, nullptr, m->status, m->nl_ws, m->nl_ws_bytes, gate, st,
                           npt ? m->boxd : nullptr);
@@ -763,7 +1051,7 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
     h.scale = 1.0;
     h.twork = 0.0;
     cudaMemcpy(sc, &h, sizeof(h), cudaMemcpyHostToDevice);
-    if (m->d.routine == DPB_MD_NPT_NHC) {  // npt init_fn (routine.py:322-350)
+    if (m->np) {  // npt init_fn (routine.py:322-350; NPT-PIMD: pimd.py:417-441)
       NptScalars n;
       std::memset(&n, 0, sizeof(n));
       std::vector<double> vir(9);
@@ -782,6 +1070,18 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
       n.bdof = n.G;
       n.bQ[0] *= n.bdof;
       if (cudaMemcpy(m->np, &n, sizeof(n), cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+      if (m->d.routine == DPB_MD_NPT_PIMD) {
+        // centroid-virial dU/d(eps) and centroid p^2/m of the initial state
+        PimdParams pp;
+        pp.P = m->P; pp.N = m->N; pp.dt = (float)m->d.dt; pp.kT = (float)m->kT;
+        pp.L = make_float3(m->box[0], m->box[1], m->box[2]); pp.seed = m->d.seed; pp.tag = 1u;
+        k_nptp_c<<<(m->N * 3 + 127) / 128, 128, 0, st>>>(m->pos, m->mom, m->force, m->mass, pp, m->np, m->boxd, sc,
+                                                           0, 0);
+        k_nptp_end<<<1, 1, 0, st>>>(m->np, m->virial, m->P, m->d.dt, m->N, 0);
+        count_launch(2);
+        DPB_LAUNCH_CHECK();
+        if (cudaStreamSynchronize(st) != cudaSuccess) return DPB_ERR_CUDA;
+      }
     }
   }
   return DPB_OK;
@@ -795,7 +1095,7 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel)
   const float dt = (float)m->d.dt;
   prof_begin(PROF_NLIST, st);
   k_md_begin<<<1, 1, 0, st>>>(sc);
-  const bool npt = m->d.routine == DPB_MD_NPT_NHC;
+  const bool npt = m->np != nullptr;  // the box lives on the device
   k_md_drift<<<nb, 256, 0, st>>>(m->pos, m->mom, m->ref_pos, NF, L, make_float3(1.f, 1.f, 1.f), L, sc, m->status,
                                  npt ? m->boxd : nullptr);
   k_md_decide<<<1, 1, 0, st>>>(sc, m->threshold, npt ? m->boxd : nullptr, L, m->model->dm.rcut, (float)m->d.skin,
@@ -805,7 +1105,7 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel)
   int rc = md_build_list(m, &sc->rebuild, st);
   if (rc) return rc;
   prof_end(PROF_NLIST, st);
-  if (npt) {  // MTK NPT step (routine.py:403-436)
+  if (m->d.routine == DPB_MD_NPT_NHC) {  // MTK NPT step (routine.py:403-436)
     const int N = m->N, nbn = (N + 255) / 256;
     const int Lt = m->d.chain_length, Lb = m->d.chain_length_p;
     const double kT = m->kT, tt = m->d.tau_t, tp = m->d.tau_p, dtd = m->d.dt;
@@ -821,6 +1121,23 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel)
     k_npt_end<<<1, 1, 0, st>>>(sc, m->np, m->virial, Lt, Lb, kT, tt, tp, dtd, N);
     k_scale_mom<<<nb3, 256, 0, st>>>(m->mom, NF3, sc);
     count_launch(3);
+  } else if (m->d.routine == DPB_MD_NPT_PIMD) {  // pimd.py:443-516
+    PimdParams pp;
+    pp.P = m->P; pp.N = m->N; pp.dt = dt; pp.kT = (float)m->kT; pp.L = L; pp.seed = m->d.seed; pp.tag = 1u;
+    const int nc = (m->N * 3 + 127) / 128;
+    const double dtd = m->d.dt;
+    k_nptp_begin<<<1, 1, 0, st>>>(m->np, m->boxd, m->P, dtd, m->N);
+    k_nptp_a<<<nc, 128, 0, st>>>(m->pos, m->mom, m->force, m->prev, m->mass, m->C, m->freqs, m->gamma, pp, m->np,
+                                 m->boxd, sc);
+    k_nptp_mid<<<1, 1, 0, st>>>(sc, m->np, m->boxd, m->P, dtd, m->kT, 1.0 / m->d.tau_p, m->d.seed, m->N);
+    k_nptp_b<<<nc, 128, 0, st>>>(m->pos, m->mom, m->prev, m->mass, m->C, m->freqs, pp, m->np, m->boxd);
+    count_launch(4);
+    DPB_LAUNCH_CHECK();
+    rc = md_forces(m, st);
+    if (rc) return rc;
+    k_nptp_c<<<nc, 128, 0, st>>>(m->pos, m->mom, m->force, m->mass, pp, m->np, m->boxd, sc, 1, 1);
+    k_nptp_end<<<1, 1, 0, st>>>(m->np, m->virial, m->P, dtd, m->N, 1);
+    count_launch(2);
   } else if (m->d.routine == DPB_MD_PIMD_PILE) {
     PimdParams pp;
     pp.P = m->P; pp.N = m->N; pp.dt = dt; pp.kT = (float)m->kT; pp.L = L; pp.seed = m->d.seed; pp.tag = 1u;
@@ -912,6 +1229,7 @@ extern "C" int dpb_md_report(dpb_md *m, dpb_md_report_t *r) {
       r->dU_deps[g] = n.dUde[g];
     }
     r->baro_length = m->d.chain_length_p;
+    r->box_thermostat_work = n.btwork;
     for (int k = 0; k < kMaxChain; ++k) { r->baro_xi[k] = n.bxi[k]; r->baro_p[k] = n.bp[k]; r->baro_Q[k] = n.bQ[k]; }
   }
   return DPB_OK;
@@ -938,7 +1256,7 @@ extern "C" int dpb_md_snapshot(dpb_md *m, int restore) {
     bad |= cudaMemcpy(m->s_sc, m->sc, sizeof(MdScalars), k) != cudaSuccess;
     if (m->np) {
       bad |= cudaMemcpy(m->s_np, m->np, sizeof(NptScalars), k) != cudaSuccess;
-      bad |= cudaMemcpy(m->s_box, m->boxd, 12, k) != cudaSuccess;
+      bad |= cudaMemcpy(m->s_box, m->boxd, (size_t)m->P * 12, k) != cudaSuccess;
     }
   } else {
     bad |= cudaMemcpy(m->pos, m->s_pos, n, k) != cudaSuccess;
@@ -948,7 +1266,7 @@ extern "C" int dpb_md_snapshot(dpb_md *m, int restore) {
     bad |= cudaMemcpy(m->sc, m->s_sc, sizeof(MdScalars), k) != cudaSuccess;
     if (m->np) {
       bad |= cudaMemcpy(m->np, m->s_np, sizeof(NptScalars), k) != cudaSuccess;
-      bad |= cudaMemcpy(m->boxd, m->s_box, 12, k) != cudaSuccess;
+      bad |= cudaMemcpy(m->boxd, m->s_box, (size_t)m->P * 12, k) != cudaSuccess;
     }
   }
   return bad ? DPB_ERR_CUDA : DPB_OK;

@@ -50,7 +50,7 @@ class MDReport(ctypes.Structure):
         ("box_position", ctypes.c_double * 3), ("box_momentum", ctypes.c_double * 3),
         ("box_mass", ctypes.c_double * 3), ("baro_length", ctypes.c_int),
         ("baro_xi", ctypes.c_double * 8), ("baro_p", ctypes.c_double * 8), ("baro_Q", ctypes.c_double * 8),
-        ("dU_deps", ctypes.c_double * 3),
+        ("dU_deps", ctypes.c_double * 3), ("box_thermostat_work", ctypes.c_double),
     ]
 
 
@@ -151,15 +151,15 @@ class Simulation:
         self._params = params
         self.model = DeviceModel(params, variables)
         if routine not in ("NVE", "NVT", "NPT"):
-            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT PIMD)" % routine)
+            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT / NPT PIMD)" % routine)
         if len(model_deviation_paths) or fixed_indices is not None or remove_com_motion:
             raise NotImplementedError("model deviation / fixed atoms / COM removal are not supported")
         if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
             raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
         self._n_bead = int(n_bead)
         self._is_pimd = self._n_bead > 1
-        if self._is_pimd and routine != "NVT":
-            raise NotImplementedError("Path-integral MD (n_bead > 1) supports routine='NVT'.")
+        if self._is_pimd and routine not in ("NVT", "NPT"):
+            raise NotImplementedError("Path-integral MD (n_bead > 1) supports routine='NVT' or 'NPT'.")
         if routine == "NPT":
             if pressure is None:
                 raise ValueError("Missing argument 'pressure' (in bar) for routine 'NPT'")
@@ -219,7 +219,9 @@ class Simulation:
         # neighbour capacity from a measurement at the initial positions (allocate_fn)
         self._sel = self._measure_capacity(pos0)
         desc = MDDesc()
-        desc.routine = 2 if self._is_pimd else {"NVE": 0, "NVT": 1, "NPT": 3}[routine]
+        # NVT PIMD: PILE-L (pimd.py:114-207); NPT PIMD: Langevin barostat (pimd.py:255-518)
+        desc.routine = ({"NVT": 2, "NPT": 4}[routine] if self._is_pimd
+                        else {"NVE": 0, "NVT": 1, "NPT": 3}[routine])
         if routine == "NPT":
             desc.pressure = float(pressure) * PRESS_UNIT_CONVERSION
             desc.tau_p = float(tau_p)
@@ -262,7 +264,7 @@ class Simulation:
         self._is_initial_state = True
         self._error_code = 0
         if verbose:
-            label = "NVT PIMD run" if self._is_pimd else ("%s run" % routine)
+            label = ("%s PIMD run" % routine) if self._is_pimd else ("%s run" % routine)
             print("# Initialized %s with %d atoms" % (label, self._natoms))
 
     # ------------------------------------------------------------------ helpers
@@ -374,6 +376,17 @@ class Simulation:
             E += sum(r.box_momentum[g] ** 2 / (2 * r.box_mass[g]) for g in range(r.ngroups))
             row.append(E)
             headers.append("Invariant")
+        elif self._routine == "NPT":
+            # PIMD: the pressure of the bead-averaged potential (md_utils.py:139-159,
+            # md.py:524) and the moving box axes (md.py:525-531)
+            box = np.array(r.box)
+            V = float(np.prod(box))
+            dU_iso = -(r.virial[0] + r.virial[4] + r.virial[8]) / self._n_bead
+            row.append((self._natoms * self._kT - dU_iso / 3.0) / V / PRESS_UNIT_CONVERSION)
+            headers.append("Pressure")
+            for a in sorted(a for g in self._couple_axes for a in g):
+                row.append(box[a])
+                headers.append("box_" + "xyz"[a])
         self.log_headers = headers + ["Time"]
         row.append(time() - tic)
         headers.append("Time")

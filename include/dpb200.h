@@ -210,13 +210,16 @@ DPB_API int dpb_eval_noalloc(const dpb_model *model, int precision, const float 
 #define DPB_MD_NVT_NHC 1
 #define DPB_MD_PIMD_PILE 2
 #define DPB_MD_NPT_NHC 3
+#define DPB_MD_NPT_PIMD 4  /* NPT path-integral MD: Parrinello-Rahman on the centroid
+                              mode, PILE-L, Langevin barostat (deepmd_jax/pimd.py:255-518) */
 
 typedef struct dpb_md dpb_md;
 
 /* Host-side description of an MD run (deepmd_jax/md.py:61-282 constructor
  * arguments).  Units: Angstrom, fs, Dalton, Kelvin. */
 typedef struct {
-  int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE, DPB_MD_NPT_NHC */
+  int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE, DPB_MD_NPT_NHC,
+                                  DPB_MD_NPT_PIMD */
   int natoms;
   int nbeads;                  /* 1, or P ring-polymer beads for PIMD */
   const int *type_idx;         /* [natoms] user order */
@@ -234,7 +237,9 @@ typedef struct {
   uint64_t seed;               /* Philox key of the stochastic steps */
   int precision;               /* DPB_PREC_* of the force evaluations */
   /* NPT (DPB_MD_NPT_NHC: MTK barostat + Nose-Hoover chains,
-   * deepmd_jax/routine.py:161-456; orthorhombic, axes in coupled groups) */
+   * deepmd_jax/routine.py:161-456; DPB_MD_NPT_PIMD: Langevin barostat with
+   * friction 1/tau_p on the centroid, pimd.py:255-518; orthorhombic, axes in
+   * coupled groups) */
   double pressure;             /* target pressure, eV / A^3 */
   double tau_p;                /* barostat time constant, fs */
   int chain_length_p;          /* barostat chain length */
@@ -259,7 +264,8 @@ typedef struct {
   double box_position[3], box_momentum[3], box_mass[3];
   int baro_length;
   double baro_xi[8], baro_p[8], baro_Q[8];
-  double dU_deps[3];
+  double dU_deps[3];           /* NPT-PIMD: the centroid-virial derivative */
+  double box_thermostat_work;  /* NPT-PIMD: Langevin barostat cumulative work */
 } dpb_md_report_t;
 
 typedef struct {

@@ -11,6 +11,9 @@ on the reference's hot path.
     thermostat (deepmd_jax/pimd.py:22-44,92-111,114-207,210-247);
   * MTK NPT with Nose-Hoover chains on the particles and on the box, axes in
     coupled groups (deepmd_jax/routine.py:161-456);
+  * NPT-PIMD: Parrinello-Rahman on the centroid mode, exact internal ring
+    steps, PILE-L and a Langevin barostat, centroid-virial strain
+    derivative (deepmd_jax/pimd.py:255-518);
   * min_image_unwrap (deepmd_jax/md_utils.py:162-169).
 
 jax_md is a third-party dependency that is absent here (unpinned git HEAD,
@@ -249,3 +252,116 @@ def pimd_step(R, P, F, m, dt, kT, C, w, gamma, box3, noise, force_fn):
 
 def min_image_unwrap(prev, cur, box3):
     return prev + np.remainder(cur - prev + box3 / 2, box3) - box3 / 2
+
+
+def centroid_drift(R, P, m, box3, va, h):
+    """Parrinello-Rahman drift of the centroid mode only (pimd.py:385-398):
+    every bead moves by dR_c = R_c (e^x - 1) + h v_c e^(x/2) sinh(x/2)/(x/2),
+    x = va h, with R_c the centroid of the beads unwrapped onto bead 0."""
+    x = va * h
+    Rc = unwrap_across_beads(R, box3).mean(0)
+    vc = (P / m).mean(0)
+    dRc = Rc * np.expm1(x) + h * vc * np.exp(x / 2) * sinhx_x(x / 2)
+    return R + dRc[None]
+
+
+def internal_ring_step(R, P, m, C, w, h, box3):
+    """Exact free propagation of the non-centroid ring-polymer modes only
+    (pimd.py:400-415); the centroid normal mode is left as it is."""
+    R = unwrap_across_beads(R, box3)
+    Q = np.tensordot(C.T, R, axes=(1, 0))
+    Pn = np.tensordot(C.T, P, axes=(1, 0))
+    w = w[:, None, None]
+    c, s = np.cos(w * h), np.sin(w * h)
+    sw = np.where(w == 0, 1.0, w)
+    Qn, Pm = Q.copy(), Pn.copy()
+    Qn[1:] = Q[1:] * c[1:] + Pn[1:] * s[1:] / (m * sw[1:])
+    Pm[1:] = Pn[1:] * c[1:] - m * sw[1:] * Q[1:] * s[1:]
+    return np.tensordot(C, Qn, axes=(1, 0)), np.tensordot(C, Pm, axes=(1, 0))
+
+
+class NPTPIMDState:
+    """NPT-PIMD state (pimd.py:253-296, init_fn 417-441): beads R, P, F
+    (P, N, 3); log box scales Rb, momenta Pb, masses Mb = n_g (N + 1) kT
+    tau_p^2 per coupled group; the cached centroid-virial dU/d(eps) per group;
+    thermostat and box-thermostat work.  force_fn(R, box) -> (F, W_beads)
+    with W_beads (P, 3, 3) the per-bead virials W = -sum r (x) f of the
+    per-bead energies (their sum is n_bead times the bead-averaged energy)."""
+
+    def __init__(self, R, P, F, W_beads, m, box, pressure, kT, tau_p, gid):
+        self.R, self.P, self.F, self.m = R.copy(), P.copy(), F.copy(), m
+        self.ref = np.asarray(box, float).copy()
+        self.gid = np.asarray(gid)
+        self.G = int(self.gid.max()) + 1
+        self.ngrp = np.array([(self.gid == g).sum() for g in range(self.G)], float)
+        N = R.shape[1]
+        self.Rb = np.zeros(self.G)
+        self.Pb = np.zeros(self.G)
+        self.Mb = self.ngrp * (N + 1) * kT * tau_p ** 2
+        self.pressure = pressure
+        self.twork = 0.0
+        self.btwork = 0.0
+        self.dUde = self.centroid_dU_deps(R, F, W_beads, self.box())
+
+    def box(self):
+        return self.ref * np.array([np.exp(self.Rb[g]) if g >= 0 else 1.0 for g in self.gid])
+
+    def axis_rate(self):
+        vb = self.Pb / self.Mb
+        return np.array([vb[g] if g >= 0 else 0.0 for g in self.gid]), float((self.ngrp * vb).sum())
+
+    def centroid_dU_deps(self, R, F, W_beads, box3):
+        """(dU/d eps_g + the internal-mode virial) / n_bead (pimd.py:332-350)."""
+        nb = R.shape[0]
+        Ruw = unwrap_across_beads(R, box3)
+        internal = ((Ruw - Ruw.mean(0)) * F).sum((0, 1))
+        out = np.zeros(self.G)
+        for a in range(3):
+            if self.gid[a] >= 0:
+                out[self.gid[a]] += -W_beads[:, a, a].sum() + internal[a]
+        return out / nb
+
+    def box_force(self, V, Nf):
+        """Box-momentum driver from the centroid momenta (pimd.py:366-373)."""
+        KE2 = (self.P.mean(0) ** 2 / self.m).sum(0)
+        tot = KE2.sum()
+        grp = np.array([KE2[self.gid == g].sum() for g in range(self.G)])
+        return grp + (self.ngrp / Nf) * tot - self.dUde - self.pressure * V * self.ngrp
+
+
+def npt_pimd_step(st: NPTPIMDState, dt, kT, C, w, gamma, gamma_box, noise, noise_box, force_fn):
+    """One step_fn of npt_langevin_pimd (pimd.py:443-516); noise (P, N, 3)
+    and noise_box (G,) ~ N(0, 1).  Returns the per-bead virials."""
+    N = st.R.shape[1]
+    Nf = 3.0 * N
+    h = dt / 2
+
+    def kick(P, F):  # exp_iL2_pimd (pimd.py:375-383)
+        va, tr = st.axis_rate()
+        x = (va + tr / Nf) * h
+        Pc, Fc = P.mean(0), F.mean(0)
+        Pc_new = Pc * np.exp(-x) + h * Fc * sinhx_x(x / 2) * np.exp(-x / 2)
+        return Pc_new[None] + (P - Pc[None]) + h * (F - Fc[None])
+
+    st.Pb = st.Pb + h * st.box_force(np.prod(st.box()), Nf)
+    st.P = kick(st.P, st.F)
+    st.Rb = st.Rb + h * st.Pb / st.Mb
+    box = st.box()
+    st.R = centroid_drift(st.R, st.P, st.m, box, st.axis_rate()[0], h)
+    st.R, st.P = internal_ring_step(st.R, st.P, st.m, C, w, h, box)
+    st.P, dke = pile_l_step(st.P, st.m, C, gamma, dt, kT, noise)
+    st.twork += dke
+    c1 = np.exp(-gamma_box * dt)
+    c2 = np.sqrt(max(kT * (1.0 - c1 ** 2), 0.0))
+    Pb_old = st.Pb
+    st.Pb = c1 * st.Pb + c2 * np.sqrt(st.Mb) * noise_box
+    st.btwork += 0.5 * float(((st.Pb ** 2 - Pb_old ** 2) / st.Mb).sum())
+    st.Rb = st.Rb + h * st.Pb / st.Mb
+    box = st.box()
+    st.R = centroid_drift(st.R, st.P, st.m, box, st.axis_rate()[0], h)
+    st.R, st.P = internal_ring_step(st.R, st.P, st.m, C, w, h, box)
+    st.F, W = force_fn(st.R, box)
+    st.dUde = st.centroid_dU_deps(st.R, st.F, W, box)
+    st.P = kick(st.P, st.F)
+    st.Pb = st.Pb + h * st.box_force(np.prod(box), Nf)
+    return W

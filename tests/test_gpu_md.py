@@ -197,3 +197,68 @@ def test_npt_matches_oracle_and_conserves_invariant():
     assert sim.log_headers[:5] == ["Step", "Temperature", "KE", "PE", "Pressure"]
     assert "box_x" in sim.log_headers and "box_z" in sim.log_headers
     assert len(inv) == 4 and np.abs(inv - inv[0]).max() / N < 1e-5
+
+
+def test_npt_pimd_matches_oracle_with_shared_noise():
+    """NPT path-integral MD (deepmd_jax/pimd.py:255-518: Parrinello-Rahman on
+    the centroid mode, exact internal ring steps, PILE-L, Langevin barostat,
+    centroid-virial dU/d(eps)) on the 1,536-atom box with 4 beads and
+    semi-isotropic couple_axes ((0, 1), (2,)), driven by the same Philox
+    noise as the float64 oracle: after 3 steps of dt = 0.25 fs positions
+    agree within 5e-4 A, box lengths within 2e-6 relative, box momenta,
+    dU/d(eps) and both work accumulators within 1e-3 relative."""
+    from deepmd_jax_b200.md import Simulation, PRESS_UNIT_CONVERSION
+    from deepmd_jax_b200.systems import water_box
+    from oracle import nlist as onl
+    p, v = golden_models()["B"]
+    w = water_box(8, 24.83, seed=3)
+    N, P, seed, tau_t, tau_p = len(w["type_idx"]), 4, 4321, 100.0, 200.0
+    rng = np.random.default_rng(5)
+    pos = w["position"][None] + rng.normal(scale=0.02, size=(P, N, 3))
+    vel = np.broadcast_to(w["velocity"], (P, N, 3)).copy()
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NPT", 0.25, pos,
+                     initial_velocity=vel, temperature=300.0, pressure=1000.0, tau_t=tau_t, tau_p=tau_p,
+                     couple_axes=((0, 1), (2,)), n_bead=P, seed=seed, report_interval=10, verbose=False)
+    traj = sim.run(3)
+    r_dev = sim._report_struct()
+    assert int(r_dev.status) == 0
+
+    m64 = om.OracleModel(p, v, torch.float64, device="cuda")
+    cnt = np.bincount(w["type_idx"], minlength=2)
+
+    def force_fn(R, box):
+        F, W = [], []
+        for b in range(P):
+            c = onl.canonicalize(R[b], box, w["type_idx"])
+            nb, _, _ = onl.typed_nlist(c, np.asarray(box, np.float32), onl.cutoff_sq(6.2), cnt, [80, 160])
+            o = om.energy_force(m64, R[b], box, w["type_idx"], nbrs=nb, sel=[80, 160])
+            F.append(o["force"])
+            W.append(o["virial"])
+        return np.stack(F), np.stack(W)
+
+    kT = 300.0 * KB
+    freqs, C = oi.normal_mode_transform(P, kT)
+    gamma = 2.0 * freqs
+    gamma[0] = 1.0 / tau_t
+    mass = (w["mass"] * MU)[:, None]
+    perm = np.argsort(w["type_idx"], kind="stable")
+    F, W = force_fn(pos, w["box"])
+    st = oi.NPTPIMDState(pos, vel * mass, F, W, mass, w["box"], 1000.0 * PRESS_UNIT_CONVERSION, kT, tau_p,
+                         gid=[0, 0, 1])
+    for step in range(1, 4):
+        ns = philox.normals(P * N * 3, seed, step, 1).reshape(P, N, 3)
+        noise = np.empty_like(ns)
+        noise[:, perm] = ns                       # device draws in type-sorted atom order
+        nbox = philox.normals(st.G, seed, step, 2)
+        prev = st.R.copy()
+        oi.npt_pimd_step(st, 0.25, kT, C, freqs, gamma, 1.0 / tau_p, noise, nbox, force_fn)
+        st.R = oi.min_image_unwrap(prev, st.R, st.box())
+    assert np.abs(traj["position"][-1] - st.R).max() < 5e-4
+    assert np.allclose(np.array(r_dev.box), st.box(), rtol=2e-6, atol=0)
+    assert np.allclose(np.array(r_dev.box_momentum[:2]), st.Pb, rtol=1e-3, atol=1e-3)
+    assert np.allclose(np.array(r_dev.dU_deps[:2]), st.dUde, rtol=1e-3, atol=1e-3)
+    assert abs(r_dev.thermostat_work - st.twork) < 1e-3 * abs(st.twork) + 1e-4
+    assert abs(r_dev.box_thermostat_work - st.btwork) < 1e-3 * abs(st.btwork) + 1e-6
+    sim.run(2, trajectory=False)
+    assert sim.log_headers[:5] == ["Step", "Temperature", "KE", "PE", "Pressure"]
+    assert "box_x" in sim.log_headers and "box_z" in sim.log_headers
