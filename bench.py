@@ -449,7 +449,9 @@ def study_drift(args):
 def study_pimd(args):
     """32-bead PILE-L PIMD (1,536-atom water, L = 24.83 A, 300 K, dt 0.25 fs):
     all beads evaluated in one batched launch per kernel; atom-steps/s counts
-    beads x atoms, timed with CUDA events over args.steps steps (graphs)."""
+    beads x atoms, timed with CUDA events over args.steps steps (graphs).
+    NVT in both forms, then NPT PIMD (1 bar, Langevin barostat tau_p 1 ps,
+    isotropic) in the mixed form."""
     import numpy as np
     import torch
     from deepmd_jax_b200 import _lib
@@ -460,10 +462,11 @@ def study_pimd(args):
     N, P = len(w["position"]), 32
     lib = _lib.load()
     out = {"study": "pimd_pile_l", "atoms": N, "beads": P, "dt_fs": 0.25, "steps": args.steps, "forms": {}}
-    for prec in ("fp32", "mixed"):
-        sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.25,
+    for prec, routine in (("fp32", "NVT"), ("mixed", "NVT"), ("mixed", "NPT")):
+        kw = dict(pressure=1.0, tau_p=1000.0) if routine == "NPT" else {}
+        sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], routine, 0.25,
                          w["position"], temperature=300.0, n_bead=P, tau_t=100.0, seed=1,
-                         report_interval=10 ** 9, precision=prec, verbose=False)
+                         report_interval=10 ** 9, precision=prec, verbose=False, **kw)
         for _ in range(max(args.warmup, 3)):
             sim._run_chunk(1, None, None)
         sim._run_chunk(CHUNK, None, None)
@@ -479,7 +482,8 @@ def study_pimd(args):
         torch.cuda.synchronize()
         ms = s.elapsed_time(e)
         r = sim._report_struct()
-        out["forms"][prec] = {"atom_steps_per_s": N * P * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+        key = prec if routine == "NVT" else "mixed_npt"
+        out["forms"][key] = {"atom_steps_per_s": N * P * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
                               "ns_per_day": 1e-6 * 0.25 * 86400 * args.steps / (ms / 1e3),
                               "status": int(r.status), "rebuilds": int(r.rebuilds)}
     return out
