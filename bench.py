@@ -295,6 +295,7 @@ def gpu_arm(args, rank, world, local_rank):
                 stages[name] = (msr.value / cnt.value, cnt.value)
         lib.dpb_profile_enable(0)
         results[prec] = dict(ms=ms, launches=launches, clocks=clk.summary(), stages=stages, sim=sim,
+                             launch_shapes=sim.launch_shapes,
                              status=int(r.status), rebuilds=int(r.rebuilds), steps=int(r.steps))
     head = "mixed" if "mixed" in results and "error" not in results["mixed"] else "fp32"
     R = results[head]
@@ -353,7 +354,7 @@ def gpu_arm(args, rank, world, local_rank):
         "roofline": roof,
         "forms": {p: {"atom_steps_per_s": N * K * world / (v["ms"] / 1e3), "ms_per_step": v["ms"] / K,
                       "stage_ms": {k: s[0] for k, s in v["stages"].items()}, "status": v["status"],
-                      "rebuilds": v["rebuilds"]} if "error" not in v else v
+                      "rebuilds": v["rebuilds"], "launch_shapes": v["launch_shapes"]} if "error" not in v else v
                   for p, v in results.items()},
     }
     if "mixed" in line["forms"] and "fp32" in line["forms"] and "error" not in results.get("mixed", {"error": 1}):
@@ -401,7 +402,8 @@ def ncu_case(args):
     n = args.n_side
     w = water_box(n, BOX * n / N_SIDE, seed=0)
     sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVE", DT, w["position"],
-                     initial_velocity=w["velocity"], precision=args.precision, use_cuda_graph=False, verbose=False)
+                     initial_velocity=w["velocity"], precision=args.precision, use_cuda_graph=False, verbose=False,
+                     autotune=False)
     sim._run_chunk(args.warmup + args.steps, None, None)
     torch.cuda.synchronize()
     r = sim._report_struct()

@@ -74,7 +74,7 @@ size_t mixed_workspace_per_atom(const DevModel &M);
 size_t mixed_workspace_fixed(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
-               cudaStream_t st);
+               cudaStream_t st, int dT_warps);
 int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                           const float *box, const int32_t *nbrs, float *T, float *G, int *err, void *ws,
                           cudaStream_t st);
@@ -439,12 +439,25 @@ int dpb::eval_impl(const dpb_model *m, int precision, const float *pos, const in
     rc = eval_fp32(M, D, pos, perm, box, nbrs, energy, F4, Eatom, vir, w, st);
   } else {
     if (!mixed_supported(M)) return DPB_ERR_UNSUPPORTED;
-    rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st);
+    rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st, m->dT_warps);
   }
   if (rc) return rc;
   return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, (int)nE, pos, seg, status,
                          st);
 }
+
+namespace dpb {
+// The dE/dT part of the mixed evaluation's workspace sits after the pieces
+// eval_impl carves first (forces, atom energies, virial rows).
+int eval_tune_dT(const dpb_model *m, int natoms, int nframes, void *workspace, cudaStream_t st, int *best) {
+  const size_t NF = (size_t)natoms * nframes;
+  char *w = (char *)workspace;
+  w += al(NF * 16);
+  w += al(NF * 4);
+  w += al((size_t)nframes * 9 * 8);
+  return mixed_tune_dT(m->dm, NF, w, st, best);
+}
+}  // namespace dpb
 
 extern "C" int dpb_eval_packed(const dpb_model *m, int precision, const float *pos, const int32_t *perm,
                                int natoms, const int *type_count, const int32_t *seg, int nseg, const float *box,

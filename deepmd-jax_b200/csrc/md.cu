@@ -790,6 +790,7 @@ struct dpb_md {
   NptScalars *np = nullptr, *s_np = nullptr;  // NPT barostat state and its snapshot
   float *s_box = nullptr;
   float *prev = nullptr;  // NPT-PIMD: positions at the start of the step
+  int nl_warps = 8;       // centres (warps) per block of the neighbour search (dpb_md_autotune)
   float *C = nullptr, *freqs = nullptr, *gamma = nullptr;
   void *nl_ws = nullptr, *ev_ws = nullptr;
   size_t nl_ws_bytes = 0, ev_ws_bytes = 0;
@@ -1012,7 +1013,7 @@ static int md_build_list(dpb_md *m, const unsigned *gate, cudaStream_t st) {
   const bool npt = m->np != nullptr;  // the box lives on the device
   return nlist_build_impl(m->pos, nullptr, m->N, m->P, m->ntypes, m->type_count, m->sel, m->box, nullptr, rc,
                           m->nbrs, m->ref_pos, nullptr, m->status, m->nl_ws, m->nl_ws_bytes, gate, st,
-                          npt ? m->boxd : nullptr);
+                          npt ? m->boxd : nullptr, m->nl_warps);
 }
 
 static int md_forces(dpb_md *m, cudaStream_t st) {
@@ -1302,6 +1303,52 @@ extern "C" int dpb_md_set_capacity(dpb_md *m, const int *sel, void *stream) {
   int rc = md_alloc_lists(m);
   if (rc) return rc;
   return md_build_list(m, nullptr, (cudaStream_t)stream);
+}
+
+// Launch-shape autotuner: each candidate runs on this engine's current state
+// (a warm-up, then timed repetitions with CUDA events on the stream) and the
+// fastest is kept; shapes never change results.  Ends with the list and
+// forces of the current positions, like dpb_md_init.
+extern "C" int dpb_md_autotune(dpb_md *m, int *nl_warps, int *dT_warps, void *stream) {
+  if (!m) return DPB_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t a, b;
+  DPB_CUDA_TRY(cudaEventCreate(&a));
+  DPB_CUDA_TRY(cudaEventCreate(&b));
+  const int cand[3] = {4, 8, 16};
+  int best = m->nl_warps, rc = DPB_OK;
+  float tbest = 1e30f;
+  for (int c = 0; c < 3 && !rc; ++c) {
+    m->nl_warps = cand[c];
+    int r = md_build_list(m, nullptr, st);
+    if (r == DPB_ERR_UNSUPPORTED) continue;  // hit lists of this many warps do not fit in shared memory
+    cudaEventRecord(a, st);
+    for (int k = 0; k < 3 && !r; ++k) r = md_build_list(m, nullptr, st);
+    cudaEventRecord(b, st);
+    if (!r && cudaEventSynchronize(b) != cudaSuccess) r = DPB_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (r) rc = r;
+    else if (ms < tbest) { tbest = ms; best = cand[c]; }
+  }
+  m->nl_warps = best;
+  int bestT = m->model->dT_warps;
+  if (!rc && m->d.precision == DPB_PREC_MIXED) {
+    rc = md_forces(m, st);
+    if (!rc) {
+      const int r = eval_tune_dT(m->model, m->N, m->P, m->ev_ws, st, &bestT);
+      if (r && r != DPB_ERR_UNSUPPORTED) rc = r;  // compressed nets have no mixed dE/dT
+      if (!r) m->model->dT_warps = bestT;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (!rc) rc = md_build_list(m, nullptr, st);
+  if (!rc) rc = md_forces(m, st);
+  if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = DPB_ERR_CUDA;
+  if (nl_warps) *nl_warps = m->nl_warps;
+  if (dT_warps) *dT_warps = m->model->dT_warps;
+  return rc;
 }
 
 extern "C" int dpb_md_device_pointers(dpb_md *m, dpb_md_pointers_t *p) {

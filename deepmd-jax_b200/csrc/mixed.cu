@@ -740,8 +740,8 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
 // Adjoint of the descriptor (dpmodel.py:74-78): from dE/dG (BF16, from the
 // fitting chain) and T, dE/dT / Nnbrs as BF16 rows [atom][c][w] (w padded to
 // N2 with zeros), the B operand rows of the tensor-core adjoint.
-template <int E2, int N2>
-__global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
+template <int E2, int N2, int W>
+__global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
                                                 const __nv_bfloat16 *__restrict__ dG,
                                                 __nv_bfloat16 *__restrict__ dTb) {
   // Warp per atom; lane owns the column pairs w = 2 lane + 64 j (+0, +1).
@@ -752,10 +752,10 @@ __global__ void __launch_bounds__(128) k_mix_dT(DevModel M, int NF, const float 
   //   dX[c][w] = sum_a dG[a][w] Q[c][a] + the Q -> X terms at w < 2A
   constexpr int NJ = (E2 + 63) / 64;
   static_assert(N2 <= 64 * NJ && E2 % 2 == 0, "padded width");
-  __shared__ __align__(16) float Xs[4][10 * E2];
-  __shared__ float Qs[4][160], dQs[4][160];
+  __shared__ __align__(16) float Xs[W][10 * E2];
+  __shared__ float Qs[W][160], dQs[W][160];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t g = (size_t)blockIdx.x * 4 + warp;
+  const size_t g = (size_t)blockIdx.x * W + warp;
   if (g >= (size_t)NF) return;
   const int A = M.A;  // 1..16 (checked at model creation: 2A <= 32)
   float *X = Xs[warp], *Q = Qs[warp], *dQ = dQs[warp];
@@ -1745,6 +1745,27 @@ size_t mixed_workspace_per_atom(const DevModel &M) {
          (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
 }
 
+// dE/dT with W atoms (warps) per block, W in {2, 4, 8} (launch shape only).
+template <int W>
+static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb,
+                            __nv_bfloat16 *dTb, cudaStream_t st) {
+  const unsigned grid = (unsigned)((NF + W - 1) / W);
+  if (M.E2 == 100) k_mix_dT<100, 112, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTb);
+  else k_mix_dT<64, 64, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTb);
+  count_launch();
+}
+
+static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb, __nv_bfloat16 *dTb,
+                         int warps, cudaStream_t st) {
+  switch (warps) {
+    case 2: launch_mix_dT_w<2>(M, NF, T, dGb, dTb, st); break;
+    case 8: launch_mix_dT_w<8>(M, NF, T, dGb, dTb, st); break;
+    default: launch_mix_dT_w<4>(M, NF, T, dGb, dTb, st); break;
+  }
+  DPB_LAUNCH_CHECK();
+  return DPB_OK;
+}
+
 // Positions in type-sorted order with each atom's frame-local user index:
 // posS[f N + k] = (r of atom perm[k] of frame f, perm[k]) - one 16-byte
 // gather per neighbour in the mixed embedding kernels.
@@ -1857,19 +1878,66 @@ int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos,
   return DPB_OK;
 }
 
-int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
-               const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
-               cudaStream_t st) {
-  const size_t NF = (size_t)D.N * D.F;
+// Workspace layout of mixed_eval.
+struct MixedWs {
+  int *err;
+  float *T;
+  __nv_bfloat16 *Gb;
+  float *dG;
+  __nv_bfloat16 *dTb;
+  float4 *posS;
+  float *scratch;
+};
+
+static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
   const int K0 = M.A * M.E2, N2 = n2_of(M);
   char *w = (char *)ws;
-  int *err = (int *)w; w += 256;
-  float *T = (float *)w; w += al256(NF * 10 * M.E2 * 4);
-  __nv_bfloat16 *Gb = (__nv_bfloat16 *)w; w += al256(NF * K0 * 2);
-  float *dG = (float *)w; w += al256(NF * K0 * 4);
-  __nv_bfloat16 *dTb = (__nv_bfloat16 *)w; w += al256(NF * 10 * N2 * 2);
-  float4 *posS = (float4 *)w; w += al256(NF * 16);
-  float *scratch = (float *)w;
+  MixedWs o;
+  o.err = (int *)w; w += 256;
+  o.T = (float *)w; w += al256(NF * 10 * M.E2 * 4);
+  o.Gb = (__nv_bfloat16 *)w; w += al256(NF * K0 * 2);
+  o.dG = (float *)w; w += al256(NF * K0 * 4);
+  o.dTb = (__nv_bfloat16 *)w; w += al256(NF * 10 * N2 * 2);
+  o.posS = (float4 *)w; w += al256(NF * 16);
+  o.scratch = (float *)w;
+  return o;
+}
+
+int mixed_tune_dT(const DevModel &M, size_t NF, void *ws, cudaStream_t st, int *best) {
+  if (M.ngrids > 0 || !best) return DPB_ERR_UNSUPPORTED;  // compressed nets take the FP32 adjoint
+  const MixedWs w = mixed_ws(M, NF, ws);
+  const __nv_bfloat16 *dGb = reinterpret_cast<const __nv_bfloat16 *>(w.dG);
+  cudaEvent_t a, b;
+  DPB_CUDA_TRY(cudaEventCreate(&a));
+  DPB_CUDA_TRY(cudaEventCreate(&b));
+  const int cand[3] = {2, 4, 8};
+  float tbest = 1e30f;
+  *best = 4;
+  int rc = DPB_OK;
+  for (int c = 0; c < 3 && !rc; ++c) {
+    rc = launch_mix_dT(M, NF, w.T, dGb, w.dTb, cand[c], st);  // warm-up (idempotent: dTb from dG, T)
+    cudaEventRecord(a, st);
+    for (int r = 0; r < 5 && !rc; ++r) rc = launch_mix_dT(M, NF, w.T, dGb, w.dTb, cand[c], st);
+    cudaEventRecord(b, st);
+    if (cudaEventSynchronize(b) != cudaSuccess) rc = DPB_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (!rc && ms < tbest) { tbest = ms; *best = cand[c]; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
+               const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
+               cudaStream_t st, int dT_warps) {
+  const size_t NF = (size_t)D.N * D.F;
+  const MixedWs mw = mixed_ws(M, NF, ws);
+  int *err = mw.err;
+  float *T = mw.T, *dG = mw.dG, *scratch = mw.scratch;
+  __nv_bfloat16 *Gb = mw.Gb, *dTb = mw.dTb;
+  float4 *posS = mw.posS;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
   if (M.ngrids > 0)
     return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
@@ -1884,12 +1952,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);
-  {
-    if (M.E2 == 100) k_mix_dT<100, 112><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dGb, dTb);
-    else k_mix_dT<64, 64><<<(unsigned)((NF + 3) / 4), 128, 0, st>>>(M, (int)NF, T, dGb, dTb);
-    count_launch();
-    DPB_LAUNCH_CHECK();
-  }
+  rc = launch_mix_dT(M, NF, T, dGb, dTb, dT_warps, st);
+  if (rc) return rc;
   prof_end(PROF_MIXED_DT, st);
   prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {

@@ -174,7 +174,7 @@ __device__ __forceinline__ bool pair_hit(float3 ci, float3 cj, float3 L, float r
   return d2 < rc2;
 }
 
-__global__ void __launch_bounds__(256) nl_search_kernel(NlParams P, const float *__restrict__ canon,
+__global__ void __launch_bounds__(512) nl_search_kernel(NlParams P, const float *__restrict__ canon,
                                                         const int *__restrict__ cell_start,
                                                         const int *__restrict__ cell_atoms,
                                                         const float4 *__restrict__ cell_pos,
@@ -292,7 +292,8 @@ namespace dpb {
 int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nframes, int ntypes,
                      const int *type_count, const int *sel, const float box[3], const float *ref_box, float rc,
                      int32_t *nbrs, float *ref_pos, int32_t *counts, uint32_t *status, void *workspace,
-                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream, const float *dbox) {
+                     size_t ws_bytes, const unsigned *gate, cudaStream_t stream, const float *dbox,
+                     int nl_warps) {
   if (!pos || natoms <= 0 || nframes <= 0 || ntypes < 1 || ntypes > kMaxTypes || !type_count || !sel ||
       !box || !nbrs || !status || rc <= 0)
     return DPB_ERR_INVALID_ARG;
@@ -350,8 +351,10 @@ int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nfra
   nl_scan_kernel<<<1, 1024, 0, stream>>>(cell_count, cell_start, (int)C, gate);
   nl_scatter_kernel<<<nb, 256, 0, stream>>>(atom_cell, cell_start, cursor, cell_atoms, canon, cell_pos, natoms,
                                             nframes, g.ncell, gate);
-  const int threads = 256, wpb = threads / 32;
+  if (nl_warps != 4 && nl_warps != 8 && nl_warps != 16) return DPB_ERR_INVALID_ARG;
+  const int wpb = nl_warps, threads = 32 * wpb;  // centres (warps) per block
   size_t smem = (size_t)wpb * kMaxTypes * 4 + (size_t)wpb * ntypes * cap * 4;
+  if (smem > 200 * 1024) return DPB_ERR_UNSUPPORTED;  // hit lists of this many warps do not fit
   if (smem > 48 * 1024) {
     DPB_CUDA_TRY(cudaFuncSetAttribute(nl_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
@@ -370,7 +373,7 @@ extern "C" int dpb_nlist_build(const float *pos, const int32_t *perm, int natoms
                                void *stream) {
   return dpb::nlist_build_impl(pos, perm, natoms, nframes, ntypes, type_count, sel, box, ref_box, rc, nbrs,
                                ref_pos, counts, status, workspace, ws_bytes, nullptr, (cudaStream_t)stream,
-                               nullptr);
+                               nullptr, 8);
 }
 
 // ---------------------------------------------------------------- packed batches

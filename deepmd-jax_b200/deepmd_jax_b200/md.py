@@ -72,9 +72,11 @@ def _declare(lib):
     lib.dpb_md_set_capacity.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp]
     lib.dpb_md_set_skin.argtypes = [vp, ctypes.c_double, vp]
     lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    lib.dpb_md_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
               "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
-              "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes"):
+              "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes",
+              "dpb_md_autotune"):
         getattr(lib, f).restype = ctypes.c_int
     lib._md_declared = True
 
@@ -131,7 +133,10 @@ def parse_couple_axes(couple_axes):
 class Simulation:
     """Two-step usage, as in the reference: ``sim = Simulation(...)`` then
     ``traj = sim.run(steps)``.  Extra keyword ``precision`` selects 'fp32'
-    (default, the reference's float32) or 'mixed' (BF16 tensor-core GEMMs)."""
+    (default, the reference's float32) or 'mixed' (BF16 tensor-core GEMMs);
+    ``autotune`` (default: on from 10,000 atom-beads) lets the library time
+    its launch-shape candidates on this system once, before any graph is
+    captured (``launch_shapes`` holds the choice)."""
 
     def __init__(self, model_path, box, type_idx, mass, routine, dt, initial_position, initial_velocity=None,
                  report_interval=200, temperature=None, pressure=None, debug=False, seed=0,
@@ -139,7 +144,7 @@ class Simulation:
                  neighbor_buffer_ratio=1.2, remove_com_motion=False, tau_t=100., tau_p=1000., chain_length_t=3,
                  chain_length_p=3, chain_steps_t=1, chain_steps_p=1, sy_steps_t=1, sy_steps_p=1,
                  fixed_indices=None, couple_axes=((0, 1, 2),), n_bead=1, type_symbols=None, pimd_lambda=1.0,
-                 pimd_print_invariant=False, precision="fp32", use_cuda_graph=True, verbose=True):
+                 pimd_print_invariant=False, precision="fp32", use_cuda_graph=True, verbose=True, autotune=None):
         self.lib = _lib.load()
         _declare(self.lib)
         self.verbose = verbose
@@ -261,6 +266,14 @@ class Simulation:
             vel = self._initial_velocity(seed)
         self._set_vel(vel)
         _lib.check(self.lib.dpb_md_init(self._h, 1, _stream()), "dpb_md_init")
+        # launch shapes from the library's autotuner (default: systems of 10,000
+        # atom-beads or more, where its few timed launches are negligible)
+        self.launch_shapes = None
+        if autotune if autotune is not None else self._natoms * self._n_bead >= 10000:
+            nlw, dtw = ctypes.c_int(), ctypes.c_int()
+            _lib.check(self.lib.dpb_md_autotune(self._h, ctypes.byref(nlw), ctypes.byref(dtw), _stream()),
+                       "dpb_md_autotune")
+            self.launch_shapes = {"nlist_warps_per_block": nlw.value, "dT_atoms_per_block": dtw.value}
         self._is_initial_state = True
         self._error_code = 0
         if verbose:

@@ -310,6 +310,15 @@ DPB_API int dpb_md_set_skin(dpb_md *md, double skin, void *stream);
 /* New neighbour capacity and a rebuild (overflow resolution, md.py:657-668). */
 DPB_API int dpb_md_set_capacity(dpb_md *md, const int *sel, void *stream);
 DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
+/* Launch-shape autotuner (no counterpart in the reference, which leaves
+ * launch shapes to XLA): times the neighbour search at 4 / 8 / 16 centres
+ * per block and, for the mixed form, dE/dT at 2 / 4 / 8 atoms per block on
+ * this engine's current state and keeps the fastest (*nl_warps, *dT_warps
+ * report the choice; the dE/dT choice is stored on the model).  Results do
+ * not depend on the shapes.  Call after dpb_md_init and before capturing
+ * dpb_md_run into a graph; ends with the list and forces of the current
+ * positions. */
+DPB_API int dpb_md_autotune(dpb_md *md, int *nl_warps, int *dT_warps, void *stream);
 
 /* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
  * default; not for use inside graph capture).  Stage ids: 0 neighbour

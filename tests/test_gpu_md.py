@@ -262,3 +262,29 @@ def test_npt_pimd_matches_oracle_with_shared_noise():
     sim.run(2, trajectory=False)
     assert sim.log_headers[:5] == ["Step", "Temperature", "KE", "PE", "Pressure"]
     assert "box_x" in sim.log_headers and "box_z" in sim.log_headers
+
+
+def test_autotuned_launch_shapes_leave_results_unchanged():
+    """The launch-shape autotuner (dpb_md_autotune) picks candidates only and
+    results do not depend on them: 12,288-atom water, mixed form, forces of
+    the initial state and positions after 5 steps with and without tuning
+    agree within the float-atomic summation noise (1e-5 relative, 1e-6 A)."""
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import water_box
+    p, v = golden_models()["B"]
+    w = water_box(16, 49.66, seed=0)
+    out = {}
+    for tune in (False, True):
+        sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.5, w["position"],
+                         initial_velocity=w["velocity"], precision="mixed", verbose=False, autotune=tune)
+        if tune:
+            assert sim.launch_shapes["nlist_warps_per_block"] in (4, 8, 16)
+            assert sim.launch_shapes["dT_atoms_per_block"] in (2, 4, 8)
+        else:
+            assert sim.launch_shapes is None
+        F0 = sim.getForce()
+        sim.run(5, trajectory=False)
+        out[tune] = (F0, sim.getPosition())
+    F_ref, F_tuned = out[False][0], out[True][0]
+    assert np.abs(F_tuned - F_ref).max() <= 1e-5 * np.abs(F_ref).max()
+    assert np.abs(out[True][1] - out[False][1]).max() < 1e-6
