@@ -26,6 +26,7 @@ namespace dpb {
 
 constexpr int kMaxChain = 8;
 constexpr int kMaxBeads = 64;
+constexpr int kBoxHist = 1024;  // steps of box history kept per dpb_md_run call (NPT)
 
 struct MdScalars {
   unsigned drift_bits;
@@ -791,6 +792,7 @@ struct dpb_md {
   float *s_box = nullptr;
   float *prev = nullptr;  // NPT-PIMD: positions at the start of the step
   int nl_warps = 8;       // centres (warps) per block of the neighbour search (dpb_md_autotune)
+  float *box_hist = nullptr;  // NPT: box after each step of the last dpb_md_run (kBoxHist rows)
   float *C = nullptr, *freqs = nullptr, *gamma = nullptr;
   void *nl_ws = nullptr, *ev_ws = nullptr;
   size_t nl_ws_bytes = 0, ev_ws_bytes = 0;
@@ -888,6 +890,7 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
     rc_ |= md_alloc(m, (void **)&m->s_box, (size_t)m->P * 12);
   }
   if (d->routine == DPB_MD_NPT_PIMD) rc_ |= md_alloc(m, (void **)&m->prev, NF * 12);
+  if (has_box) rc_ |= md_alloc(m, (void **)&m->box_hist, (size_t)kBoxHist * 12);
   rc_ |= md_alloc_lists(m);
   if (rc_) { dpb_md_destroy(m); return DPB_ERR_CUDA; }
   // masses in eV fs^2 / A^2 (md.py:24), sorted order
@@ -1088,7 +1091,7 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
   return DPB_OK;
 }
 
-static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel) {
+static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel, int k) {
   const int NF = m->N * m->P, NF3 = NF * 3;
   const int nb = (NF + 255) / 256, nb3 = (NF3 + 255) / 256;
   MdScalars *sc = m->sc;
@@ -1173,6 +1176,10 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel)
     k_copy_frame<<<nb3, 256, 0, st>>>(m->pos, traj_pos, NF3);
     count_launch();
   }
+  if (m->box_hist && k < kBoxHist) {  // the box of this step (md.py:784-803 emits it per step)
+    k_copy_frame<<<1, 32, 0, st>>>(m->boxd, m->box_hist + (size_t)k * 3, 3);
+    count_launch();
+  }
   if (traj_vel) {
     k_copy_frame<<<nb3, 256, 0, st>>>(m->mom, traj_vel, NF3);
     count_launch();
@@ -1186,7 +1193,7 @@ extern "C" int dpb_md_run(dpb_md *m, int nsteps, float *traj_pos, float *traj_mo
   cudaStream_t st = (cudaStream_t)stream;
   const size_t frame = (size_t)m->N * m->P * 3;
   for (int k = 0; k < nsteps; ++k) {
-    int rc = md_step(m, st, traj_pos ? traj_pos + k * frame : nullptr, traj_mom ? traj_mom + k * frame : nullptr);
+    int rc = md_step(m, st, traj_pos ? traj_pos + k * frame : nullptr, traj_mom ? traj_mom + k * frame : nullptr, k);
     if (rc) return rc;
   }
   return DPB_OK;
@@ -1303,6 +1310,21 @@ extern "C" int dpb_md_set_capacity(dpb_md *m, const int *sel, void *stream) {
   int rc = md_alloc_lists(m);
   if (rc) return rc;
   return md_build_list(m, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int dpb_md_box_history(dpb_md *m, int nsteps, double *out) {
+  if (!m || !out || nsteps < 0 || nsteps > kBoxHist) return DPB_ERR_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
+  std::vector<float> h((size_t)nsteps * 3);
+  if (m->box_hist) {
+    if (nsteps && cudaMemcpy(h.data(), m->box_hist, h.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return DPB_ERR_CUDA;
+  } else {
+    for (int k = 0; k < nsteps; ++k)
+      for (int a = 0; a < 3; ++a) h[(size_t)k * 3 + a] = m->box[a];
+  }
+  for (size_t e = 0; e < h.size(); ++e) out[e] = h[e];
+  return DPB_OK;
 }
 
 // Launch-shape autotuner: each candidate runs on this engine's current state

@@ -73,10 +73,11 @@ def _declare(lib):
     lib.dpb_md_set_skin.argtypes = [vp, ctypes.c_double, vp]
     lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     lib.dpb_md_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp]
+    lib.dpb_md_box_history.argtypes = [vp, ctypes.c_int, d64]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
               "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
               "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes",
-              "dpb_md_autotune"):
+              "dpb_md_autotune", "dpb_md_box_history"):
         getattr(lib, f).restype = ctypes.c_int
     lib._md_declared = True
 
@@ -437,7 +438,7 @@ class Simulation:
             self._report_row(tic)
         if dumps and first and self.step % interval == 0:
             dump.write_frame(dumps, self.getPosition(), self.getVelocity(),
-                             self.getCentroidPosition() if self._is_pimd else None, self._box, step=self.step)
+                             self.getCentroidPosition() if self._is_pimd else None, self.getBox(), step=self.step)
         self._is_initial_state = False
         NF3 = self._natoms * self._n_bead * 3
         cap = self._step_chunk_size
@@ -488,8 +489,9 @@ class Simulation:
                 self._resize_capacity()
                 continue
             overflow_twice = False
+            boxes = self._box_history(n)
             if dumps:
-                self._write_dump_frames(dumps, interval, buf_p, buf_v, n)
+                self._write_dump_frames(dumps, interval, buf_p, buf_v, n, boxes)
             if not trajectory:
                 done += n
                 self.step += n
@@ -497,6 +499,7 @@ class Simulation:
                     self._report_row(tic)
                     tic = time()
                 continue
+            traj["box"][idx:idx + n] = boxes
             ev = torch.cuda.Event()
             ev.record(torch.cuda.current_stream())
             pending = (buf_p, buf_v, n, idx, ev)
@@ -516,7 +519,7 @@ class Simulation:
             print("# Performance: %.3f ns/day, %.3f step/us/atom" %
                   (nsd, 1e-6 * steps * self._natoms * self._n_bead / (elapsed + 1e-6)))
         if self._is_pimd and traj is not None:
-            traj["centroid"] = np.stack([self._centroid(p) for p in traj["position"]])
+            traj["centroid"] = np.stack([self._centroid(p, b) for p, b in zip(traj["position"], traj["box"])])
         return traj
 
     def _copy_out(self, pending, traj):
@@ -557,16 +560,26 @@ class Simulation:
         vel = mom / (self._mass * MASS_UNIT_CONVERSION)[None, :, None]
         return (pos, vel) if self._is_pimd else (pos[0], vel[0])
 
-    def _write_dump_frames(self, dumps, interval, buf_p, buf_v, n):
+    def _write_dump_frames(self, dumps, interval, buf_p, buf_v, n, boxes):
         """Frames of the last chunk whose step is a multiple of the dump
-        interval, copied from the device and appended to the XYZ files."""
+        interval, copied from the device and appended to the XYZ files with
+        the box of their step."""
         for i in range(n):
             step = self.step + i + 1
             if step % interval:
                 continue
             pos, vel = self._unpack_frame(buf_p[i], buf_v[i])
-            cen = self._centroid(pos) if self._is_pimd else None
-            dump.write_frame(dumps, pos, vel, cen, self._box, step=step)
+            cen = self._centroid(pos, boxes[i]) if self._is_pimd else None
+            dump.write_frame(dumps, pos, vel, cen, boxes[i], step=step)
+
+    def _box_history(self, n):
+        """(n, 3) box after each step of the last chunk (md.py:784-803): the
+        barostat's boxes under NPT, else the fixed box."""
+        if self._routine != "NPT":
+            return np.tile(self._box, (n, 1))
+        out = np.empty(n * 3)
+        _lib.check(self.lib.dpb_md_box_history(self._h, n, _dptr(out)), "dpb_md_box_history")
+        return out.reshape(n, 3)
 
     def _resize_capacity(self):
         pos = self.getPosition()
@@ -578,10 +591,11 @@ class Simulation:
         if self.verbose:
             print("# Neighborlist reallocated with size %s" % (self._sel,))
 
-    def _centroid(self, R):
+    def _centroid(self, R, box=None):
+        box = self._box if box is None else np.asarray(box)
         ref = R[0:1]
         d = R - ref
-        d = d - self._box * np.round(d / self._box)
+        d = d - box * np.round(d / box)
         return (ref + d).mean(0)
 
     def _state(self):
@@ -602,7 +616,7 @@ class Simulation:
 
     def getCentroidPosition(self):
         p = self.getPosition()
-        return self._centroid(p) if self._is_pimd else p
+        return self._centroid(p, self.getBox()) if self._is_pimd else p
 
     def getBox(self):
         """Current box (3,); under NPT the barostat's box."""

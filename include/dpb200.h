@@ -319,6 +319,10 @@ DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
  * dpb_md_run into a graph; ends with the list and forces of the current
  * positions. */
 DPB_API int dpb_md_autotune(dpb_md *md, int *nl_warps, int *dT_warps, void *stream);
+/* Box (3 per step, Angstrom) after each of the first nsteps (<= 1024) steps
+ * of the last dpb_md_run call: the per-step box of the reference's scan
+ * output (deepmd_jax/md.py:784-803, 938); constant except under NPT. */
+DPB_API int dpb_md_box_history(dpb_md *md, int nsteps, double *out);
 
 /* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
  * default; not for use inside graph capture).  Stage ids: 0 neighbour

@@ -222,6 +222,9 @@ def test_npt_pimd_matches_oracle_with_shared_noise():
     traj = sim.run(3)
     r_dev = sim._report_struct()
     assert int(r_dev.status) == 0
+    # the trajectory carries the box of every step (md.py:784-803)
+    assert traj["box"].shape == (4, 3) and np.allclose(traj["box"][0], w["box"])
+    assert np.allclose(traj["box"][-1], np.array(r_dev.box), rtol=1e-6) and traj["box"][-1, 0] != traj["box"][0, 0]
 
     m64 = om.OracleModel(p, v, torch.float64, device="cuda")
     cnt = np.bincount(w["type_idx"], minlength=2)
