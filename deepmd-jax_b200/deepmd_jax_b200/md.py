@@ -645,6 +645,39 @@ class Simulation:
     def setVelocity(self, velocity):
         self._set_vel(velocity)
 
+    def setRandomVelocity(self, temperature, remove_com_motion=True, seed=None):
+        """Maxwell-Boltzmann velocities at temperature (K), each bead at
+        n_bead kT (deepmd_jax/md.py:1033-1047); numpy's generator stands in
+        for jax.random."""
+        if seed is None:
+            seed = np.random.randint(1, 1000000)
+        kT = temperature * TEMP_UNIT_CONVERSION
+        m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
+        vel = np.random.default_rng(seed).normal(size=self._frame_shape()) * np.sqrt(kT * self._n_bead / m)
+        self.setVelocity(vel)
+        if remove_com_motion:
+            self.remove_com_motion()
+
+    def remove_com_motion(self):
+        """Remove the centre-of-mass velocity (deepmd_jax/md.py:744-757; under
+        PIMD over all beads and atoms)."""
+        vel = self.getVelocity()
+        m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
+        if self._is_pimd:
+            vel = vel - (vel * m).sum(axis=(0, 1)) / (m.sum() * self._n_bead)
+        else:
+            vel = vel - (vel * m).sum(0) / m.sum()
+        self.setVelocity(vel)
+
+    def getPressure(self):
+        """Pressure (bar) of the current state: (N kT - dU/d(eps) / 3) / V with
+        dU/d(eps) of the (bead-averaged) potential, -trace of the virial
+        (md_utils.py:139-159, md.py:1082-1090)."""
+        r = self._report_struct()
+        V = float(np.prod(self.getBox()))
+        dU = -(r.virial[0] + r.virial[4] + r.virial[8]) / self._n_bead
+        return (self._natoms * self._kT - dU / 3.0) / V / PRESS_UNIT_CONVERSION
+
     def __del__(self):
         try:
             self._graphs = {}

@@ -291,3 +291,30 @@ def test_autotuned_launch_shapes_leave_results_unchanged():
     F_ref, F_tuned = out[False][0], out[True][0]
     assert np.abs(F_tuned - F_ref).max() <= 1e-5 * np.abs(F_ref).max()
     assert np.abs(out[True][1] - out[False][1]).max() < 1e-6
+
+
+def test_random_velocity_com_and_pressure_getters():
+    """setRandomVelocity (Maxwell-Boltzmann, centre-of-mass motion removed),
+    remove_com_motion under PIMD, and getPressure from the device virial
+    (deepmd_jax/md.py:744-757, 1033-1047, 1082-1090)."""
+    from deepmd_jax_b200.md import Simulation, PRESS_UNIT_CONVERSION
+    p, v = golden_models()["B"]
+    w = _system()
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.5, w["position"],
+                     temperature=300.0, verbose=False)
+    sim.setRandomVelocity(300.0, seed=7)
+    vel = sim.getVelocity()
+    m = (w["mass"] * MU)[:, None]
+    assert np.abs((vel * m).sum(0)).max() < 1e-6 * np.abs(vel * m).sum()
+    T = (m * vel ** 2).sum() / (3 * len(m)) / KB
+    assert 200.0 < T < 400.0
+    W = sim.getVirial()
+    V = float(np.prod(w["box"]))
+    expect = (len(m) * 300.0 * KB + np.trace(W) / 3.0) / V / PRESS_UNIT_CONVERSION
+    assert abs(sim.getPressure() - expect) <= 1e-9 * max(1.0, abs(expect))
+    pimd = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.25, w["position"],
+                      temperature=300.0, n_bead=4, verbose=False)
+    pimd.setRandomVelocity(300.0, seed=3)
+    pv = pimd.getVelocity()
+    assert pv.shape == (4, len(m), 3)
+    assert np.abs((pv * m[None]).sum(axis=(0, 1))).max() < 1e-6 * np.abs(pv * m[None]).sum()
