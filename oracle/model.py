@@ -278,9 +278,12 @@ def energy_force(model: OracleModel, coord, box3, type_idx, nbrs=None, sel=None,
     # energy as a function of the relative coordinates; chain to coord below
     E_atom, _ = model.atomic_energy(xs_leaf, vs, count)
     E = E_atom.sum()
-    gx = torch.autograd.grad(E, xs_leaf)
+    # a type block with no atoms (or no pair slots) does not enter E: zero gradient
+    gx = torch.autograd.grad(E, xs_leaf, allow_unused=True)
+    gx = [torch.zeros_like(x) if g is None else g for g, x in zip(gx, xs_leaf)]
     # dE/dcoord = sum over slots of gx * dx/dcoord  (x = shift(c_j - c_i))
-    F = -torch.autograd.grad(xs, coord, grad_outputs=list(gx))[0]
+    gc = torch.autograd.grad(xs, coord, grad_outputs=list(gx), allow_unused=True)[0]
+    F = -(torch.zeros_like(coord) if gc is None else gc)
     Wv = None
     if virial:
         Wv = torch.zeros((3, 3), dtype=dtype, device=dev)

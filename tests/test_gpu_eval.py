@@ -127,3 +127,36 @@ def test_compressed_tables_match_uncompressed_model():
     ref = om.energy_force(om.OracleModel(*MODELS["B"], torch.float64), pos, box, typ)
     ref["energy"] = float(G["B_E"])
     check_close(one, ref, "cmp-vs-uncompressed")
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_empty_type_block_and_isolated_atoms(precision):
+    """Edge cases of the evaluation in both forms: a box of oxygen only (the
+    H type block of the two-type model is empty) against the FP64 oracle,
+    and atoms with no neighbour within rcut (every environment empty):
+    forces and virial exactly zero, each atom's energy the fitting net of a
+    zero descriptor of its type."""
+    from deepmd_jax_b200.systems import water_box
+    p, v = MODELS["B"]
+    m = om.OracleModel(p, v, torch.float64)
+    w = water_box(8, 24.83, seed=21)
+    oxy = w["type_idx"] == 0
+    pos, typ = w["position"][oxy], w["type_idx"][oxy]
+    got = run_gpu(p, v, pos, w["box"], typ, precision=precision)
+    assert got["status"] == 0
+    ref = om.energy_force(m, pos, w["box"], typ, nbrs=got["nbrs"][0], sel=[46, 92])
+    if precision == "fp32":
+        check_close(dict(energy=got["energy"][0], force=got["force"][0], virial=got["virial"][0],
+                         atom_energy=got["atom_energy"][0]), ref, "O only")
+    else:  # BF16 GEMMs: the tolerances of the mixed form
+        rms = np.sqrt(((got["force"][0] - ref["force"]) ** 2).mean() / (ref["force"] ** 2).mean())
+        assert rms <= 3e-2, rms
+        assert abs(got["energy"][0] - ref["energy"]) <= 2e-2 * np.abs(ref["atom_energy"]).sum()
+    pos2 = np.array([[1.0, 1.0, 1.0], [10.0, 10.0, 10.0], [20.0, 20.0, 1.0], [1.0, 20.0, 12.0]])
+    typ2 = np.array([0, 1, 1, 0])
+    got2 = run_gpu(p, v, pos2, w["box"], typ2, precision=precision)
+    ref2 = om.energy_force(m, pos2, w["box"], typ2)
+    assert got2["status"] == 0
+    assert np.all(got2["force"] == 0.0) and np.all(got2["virial"] == 0.0)
+    tol = 2e-6 if precision == "fp32" else 2e-2
+    assert np.abs(got2["atom_energy"][0] - ref2["atom_energy"]).max() <= tol * np.abs(ref2["atom_energy"]).max()
