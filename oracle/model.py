@@ -282,7 +282,9 @@ def energy_force(model: OracleModel, coord, box3, type_idx, nbrs=None, sel=None,
     gx = torch.autograd.grad(E, xs_leaf, allow_unused=True)
     gx = [torch.zeros_like(x) if g is None else g for g, x in zip(gx, xs_leaf)]
     # dE/dcoord = sum over slots of gx * dx/dcoord  (x = shift(c_j - c_i))
-    gc = torch.autograd.grad(xs, coord, grad_outputs=list(gx), allow_unused=True)[0]
+    used = [(x, g) for x, g in zip(xs, gx) if x.requires_grad]  # empty blocks carry no graph
+    gc = (torch.autograd.grad([x for x, _ in used], coord, grad_outputs=[g for _, g in used], allow_unused=True)[0]
+          if used else None)
     F = -(torch.zeros_like(coord) if gc is None else gc)
     Wv = None
     if virial:
