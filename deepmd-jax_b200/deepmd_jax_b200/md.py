@@ -641,6 +641,13 @@ class Simulation:
             raise ValueError("Position must have the same shape as the initial position.")
         self._set_pos(pos)
         _lib.check(self.lib.dpb_md_init(self._h, 0, _stream()), "dpb_md_init")
+        if int(self._report_struct().status) & 2:
+            # the list overflowed its capacity at the new positions: re-measure
+            # the capacity and recompute the forces on the full list, as the
+            # reference's _keep_nbr_or_lattice_up_to_date / _resolve_error_code
+            # do before its force call (md.py:1010-1015)
+            self._resize_capacity()
+            _lib.check(self.lib.dpb_md_init(self._h, 0, _stream()), "dpb_md_init")
 
     def setVelocity(self, velocity):
         self._set_vel(velocity)

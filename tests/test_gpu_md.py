@@ -318,3 +318,30 @@ def test_random_velocity_com_and_pressure_getters():
     pv = pimd.getVelocity()
     assert pv.shape == (4, len(m), 3)
     assert np.abs((pv * m[None]).sum(axis=(0, 1))).max() < 1e-6 * np.abs(pv * m[None]).sum()
+
+
+def test_neighbour_overflow_on_set_position_regrows_capacity():
+    """Neighbour-list overflow when positions are replaced (status bit 2;
+    the reference's setPosition refreshes the list and reallocates before its
+    force call, md.py:985-1015, 657-668): the engine is sized on the water
+    box, then set to a configuration squeezed to 70 % about the box centre
+    (about 3x the neighbour density).  The capacity is re-measured, the
+    forces recomputed on the full list, and the trajectory equals that of an
+    engine built at the dense configuration (float-atomic noise only)."""
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+    c = w["box"] / 2
+    dense = c + 0.7 * (w["position"] - c)
+    kw = dict(initial_velocity=w["velocity"], report_interval=10, verbose=False, autotune=False)
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.25, w["position"], **kw)
+    sel0 = list(sim._sel)
+    sim.setPosition(dense)
+    sim.setVelocity(w["velocity"])
+    sim.run(5, trajectory=False)
+    assert int(sim._report_struct().status) == 0
+    assert all(a > b for a, b in zip(sim._sel, sel0))      # the capacity grew
+    ref = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.25, dense, **kw)
+    ref.run(5, trajectory=False)
+    assert list(ref._sel) == list(sim._sel)
+    assert np.abs(sim.getPosition() - ref.getPosition()).max() < 1e-5
