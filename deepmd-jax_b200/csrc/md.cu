@@ -41,12 +41,62 @@ struct MdScalars {
   double chain_ke;   // Nose-Hoover chain kinetic_energy field
   double dof;
   double xi[kMaxChain], pxi[kMaxChain], Q[kMaxChain];
+  double com[4];     // centre-of-mass removal: sum of momenta (3), total mass
 };
 
 // ---------------------------------------------------------------- kernels
 __global__ void k_md_begin(MdScalars *sc) {
   sc->drift_bits = 0u;
   sc->ke = 0.0;
+  sc->com[0] = sc->com[1] = sc->com[2] = sc->com[3] = 0.0;
+}
+
+// Centre-of-mass removal (md.py:793-796, every atom mobile):
+// v <- v - sum(m v) / sum(m), i.e. p_i <- p_i - m_i sum(p) / sum(m).
+// k_com_sum: FP64 block sums of the momenta and masses.
+__global__ void k_com_sum(const float *__restrict__ mom, const float *__restrict__ mass, int N, MdScalars *sc) {
+  __shared__ double part[4][8];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i < N) {
+    v[0] = mom[i * 3];
+    v[1] = mom[i * 3 + 1];
+    v[2] = mom[i * 3 + 2];
+    v[3] = mass[i];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 4; ++k) part[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 4; ++k) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[k][w];
+      atomicAdd(&sc->com[k], t);
+    }
+    if (blockIdx.x == 0) sc->ke = 0.0;  // recomputed from the new momenta by k_com_sub
+  }
+}
+
+// k_com_sub: the subtraction and the kinetic energy of the new momenta.
+__global__ void k_com_sub(float *__restrict__ mom, const float *__restrict__ mass, const float *__restrict__ inv_mass,
+                          int N, MdScalars *sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float ke = 0.f;
+  if (i < N) {
+    const double f = (double)mass[i] / sc->com[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float p = (float)(mom[i * 3 + k] - f * sc->com[k]);
+      mom[i * 3 + k] = p;
+      ke += 0.5f * p * p * inv_mass[i];
+    }
+  }
+  ke = warp_sum(ke);
+  if ((threadIdx.x & 31) == 0 && ke != 0.f) atomicAdd(&sc->ke, (double)ke);
 }
 
 // Drift of canonical positions since the last rebuild, reference
@@ -841,6 +891,7 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   }
   if (pimd && (d->nbeads < 2 || d->nbeads > kMaxBeads || !d->nm_transform || !d->nm_freqs))
     return DPB_ERR_INVALID_ARG;
+  if (pimd && d->remove_com_motion) return DPB_ERR_UNSUPPORTED;  // as the reference (md.py:150-151)
   if (!pimd && d->nbeads != 1) return DPB_ERR_INVALID_ARG;
   if (d->routine == DPB_MD_NVT_NHC && (d->chain_length < 2 || d->chain_length > kMaxChain))
     return DPB_ERR_UNSUPPORTED;
@@ -1171,6 +1222,11 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel,
       k_scale_mom<<<nb3, 256, 0, st>>>(m->mom, NF3, sc);
       count_launch(2);
     }
+  }
+  if (m->d.remove_com_motion) {  // after the step, before the frame is emitted (md.py:793-796)
+    k_com_sum<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->N, sc);
+    k_com_sub<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->inv_mass, m->N, sc);
+    count_launch(2);
   }
   if (traj_pos) {
     k_copy_frame<<<nb3, 256, 0, st>>>(m->pos, traj_pos, NF3);

@@ -35,7 +35,7 @@ class MDDesc(ctypes.Structure):
         ("nm_transform", ctypes.POINTER(ctypes.c_double)), ("nm_freqs", ctypes.POINTER(ctypes.c_double)),
         ("seed", ctypes.c_uint64), ("precision", ctypes.c_int),
         ("pressure", ctypes.c_double), ("tau_p", ctypes.c_double), ("chain_length_p", ctypes.c_int),
-        ("couple_groups", ctypes.c_int * 3),
+        ("couple_groups", ctypes.c_int * 3), ("remove_com_motion", ctypes.c_int),
     ]
 
 
@@ -158,8 +158,11 @@ class Simulation:
         self.model = DeviceModel(params, variables)
         if routine not in ("NVE", "NVT", "NPT"):
             raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT / NPT PIMD)" % routine)
-        if len(model_deviation_paths) or fixed_indices is not None or remove_com_motion:
-            raise NotImplementedError("model deviation / fixed atoms / COM removal are not supported")
+        if len(model_deviation_paths) or fixed_indices is not None:
+            raise NotImplementedError("model deviation / fixed atoms are not supported")
+        if remove_com_motion and int(n_bead) > 1:
+            raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
+        self._remove_com = bool(remove_com_motion)
         if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
             raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
         self._n_bead = int(n_bead)
@@ -236,6 +239,7 @@ class Simulation:
                 desc.couple_groups[a] = int(self._group_ids[a])
         desc.natoms = self._natoms
         desc.nbeads = self._n_bead
+        desc.remove_com_motion = int(self._remove_com)
         self._keep = [np.ascontiguousarray(self._type_idx, dtype=np.int32), np.ascontiguousarray(self._mass_per_type)]
         desc.type_idx = self._keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         desc.mass_per_type = _dptr(self._keep[1])

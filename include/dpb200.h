@@ -244,6 +244,8 @@ typedef struct {
   double tau_p;                /* barostat time constant, fs */
   int chain_length_p;          /* barostat chain length */
   int couple_groups[3];        /* group of each axis (0..G-1), -1: fixed axis */
+  int remove_com_motion;       /* 1: subtract the centre-of-mass velocity after every step
+                                  (md.py:793-796; not with PIMD) */
 } dpb_md_desc;
 
 typedef struct {
