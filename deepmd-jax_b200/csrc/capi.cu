@@ -383,7 +383,7 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
                      const float *box, const int32_t *nbrs, double *energy, float4 *F4, float *Eatom,
                      double *virial, char *w, cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
-  const int E2 = M.E2, A = M.A, K0 = A * E2, FW = M.FW[0], L = M.nfit;
+  const int E2 = M.E2, A = M.A, K0 = A * E2;
   float *T = (float *)w; w += al(NF * 10 * E2 * 4);
   float *G = (float *)w; w += al(NF * K0 * 4);  // G, later dE/dG
   int rc;

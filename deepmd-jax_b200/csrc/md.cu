@@ -51,14 +51,17 @@ __global__ void k_md_begin(MdScalars *sc) {
   sc->com[0] = sc->com[1] = sc->com[2] = sc->com[3] = 0.0;
 }
 
-// Centre-of-mass removal (md.py:793-796, every atom mobile):
-// v <- v - sum(m v) / sum(m), i.e. p_i <- p_i - m_i sum(p) / sum(m).
-// k_com_sum: FP64 block sums of the momenta and masses.
-__global__ void k_com_sum(const float *__restrict__ mom, const float *__restrict__ mass, int N, MdScalars *sc) {
+// Centre-of-mass removal (md.py:793-796): V = sum(mob m v) / sum(mob m) over
+// the mobile atoms, v <- v - V for every atom (md.py:788-789), after the
+// fixed atoms' momenta were masked (routine.py:130-134); mobile == NULL:
+// every atom mobile.  k_com_sum: FP64 block sums of the mobile momenta and
+// masses.
+__global__ void k_com_sum(const float *__restrict__ mom, const float *__restrict__ mass,
+                          const float *__restrict__ mobile, int N, MdScalars *sc) {
   __shared__ double part[4][8];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  if (i < N) {
+  if (i < N && (!mobile || mobile[i] != 0.f)) {
     v[0] = mom[i * 3];
     v[1] = mom[i * 3 + 1];
     v[2] = mom[i * 3 + 2];
@@ -83,20 +86,29 @@ __global__ void k_com_sum(const float *__restrict__ mom, const float *__restrict
 
 // k_com_sub: the subtraction and the kinetic energy of the new momenta.
 __global__ void k_com_sub(float *__restrict__ mom, const float *__restrict__ mass, const float *__restrict__ inv_mass,
-                          int N, MdScalars *sc) {
+                          const float *__restrict__ mobile, int N, MdScalars *sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float ke = 0.f;
   if (i < N) {
     const double f = (double)mass[i] / sc->com[3];
+    const bool mob = !mobile || mobile[i] != 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const float p = (float)(mom[i * 3 + k] - f * sc->com[k]);
+      const float p = (float)((mob ? (double)mom[i * 3 + k] : 0.0) - f * sc->com[k]);
       mom[i * 3 + k] = p;
       ke += 0.5f * p * p * inv_mass[i];
     }
   }
   ke = warp_sum(ke);
   if ((threadIdx.x & 31) == 0 && ke != 0.f) atomicAdd(&sc->ke, (double)ke);
+}
+
+// Fixed atoms: zero force rows, the gradient that the stop_gradient on their
+// coordinates removes (md.py:428-430); the mobile atoms' forces keep every
+// term, including those through fixed neighbours.
+__global__ void k_mask_rows(float *__restrict__ force, const float *__restrict__ mobile, int N) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < N * 3 && mobile[e / 3] == 0.f) force[e] = 0.f;
 }
 
 // Drift of canonical positions since the last rebuild, reference
@@ -231,6 +243,7 @@ __device__ double nhc_half(double *xi, double *p, double *Q, double &ke, double 
 __global__ void k_nhc_substep(MdScalars *sc, int L, double kT, double tau, double delta, int which) {
   if (which == 2) sc->chain_ke = sc->ke;
   sc->scale = nhc_half(sc->xi, sc->pxi, sc->Q, sc->chain_ke, sc->dof, L, kT, tau, delta);
+  if (which == 2) sc->ke = sc->chain_ke;  // the kinetic energy of the scaled momenta
 }
 
 __global__ void k_scale_mom(float *__restrict__ mom, int n, const MdScalars *__restrict__ sc) {
@@ -412,6 +425,7 @@ __global__ void k_npt_end(MdScalars *sc, NptScalars *np, const double *__restric
   np->bke = kb;
   sc->chain_ke = sc->ke;
   sc->scale = nhc_half(sc->xi, sc->pxi, sc->Q, sc->chain_ke, sc->dof, Lt, kT, tau_t, dt);
+  sc->ke = sc->chain_ke;  // the kinetic energy of the momenta after k_scale_mom
   const double bs = nhc_half(np->bxi, np->bp, np->bQ, np->bke, np->bdof, Lb, kT, tau_p, dt);
   for (int g = 0; g < np->G; ++g) np->Pb[g] *= bs;
 }
@@ -843,6 +857,10 @@ struct dpb_md {
   float *prev = nullptr;  // NPT-PIMD: positions at the start of the step
   int nl_warps = 8;       // centres (warps) per block of the neighbour search (dpb_md_autotune)
   float *box_hist = nullptr;  // NPT: box after each step of the last dpb_md_run (kBoxHist rows)
+  float *mobile = nullptr;      // fixed atoms: 1 mobile / 0 fixed per sorted atom (NULL: none fixed)
+  float *shift_inv_mass = nullptr;  // fixed atoms: 1/m of mobile atoms, 0 for fixed (the masked shift)
+  int n_mobile = 0;
+  std::vector<float> mobile_sorted;  // host copy of `mobile`
   float *C = nullptr, *freqs = nullptr, *gamma = nullptr;
   void *nl_ws = nullptr, *ev_ws = nullptr;
   size_t nl_ws_bytes = 0, ev_ws_bytes = 0;
@@ -895,6 +913,18 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   if (!pimd && d->nbeads != 1) return DPB_ERR_INVALID_ARG;
   if (d->routine == DPB_MD_NVT_NHC && (d->chain_length < 2 || d->chain_length > kMaxChain))
     return DPB_ERR_UNSUPPORTED;
+  if (d->n_fixed < 0 || (d->n_fixed > 0 && !d->fixed_indices)) return DPB_ERR_INVALID_ARG;
+  if (d->n_fixed > 0 && d->routine != DPB_MD_NVE && d->routine != DPB_MD_NVT_NHC)
+    return DPB_ERR_UNSUPPORTED;  // fixed atoms: NVE and NVT (md.py:146-147,228-229)
+  std::vector<char> fixed(d->natoms, 0);
+  for (int k = 0; k < d->n_fixed; ++k) {
+    const int a = d->fixed_indices[k];
+    if (a < 0 || a >= d->natoms) return DPB_ERR_INVALID_ARG;
+    fixed[a] = 1;
+  }
+  int n_mobile = 0;
+  for (char c : fixed) n_mobile += c ? 0 : 1;
+  if (n_mobile == 0) return DPB_ERR_INVALID_ARG;  // no degree of freedom left
   *out = nullptr;
   dpb_md *m = new dpb_md();
   m->model = model;
@@ -954,6 +984,21 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   m->mass_sorted = ms;
   cudaMemcpy(m->mass, ms.data(), N * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(m->inv_mass, im.data(), N * 4, cudaMemcpyHostToDevice);
+  m->n_mobile = n_mobile;
+  if (n_mobile < m->N) {  // fixed atoms: the mask and the masked shift, sorted order
+    std::vector<float> mob(N), sim(N);
+    for (size_t k = 0; k < N; ++k) {
+      mob[k] = fixed[m->perm[k]] ? 0.f : 1.f;
+      sim[k] = im[k] * mob[k];
+    }
+    if (md_alloc(m, (void **)&m->mobile, N * 4) || md_alloc(m, (void **)&m->shift_inv_mass, N * 4)) {
+      dpb_md_destroy(m);
+      return DPB_ERR_CUDA;
+    }
+    cudaMemcpy(m->mobile, mob.data(), N * 4, cudaMemcpyHostToDevice);
+    m->mobile_sorted = mob;
+    cudaMemcpy(m->shift_inv_mass, sim.data(), N * 4, cudaMemcpyHostToDevice);
+  }
   std::vector<float> bx(3 * m->P);
   for (int b = 0; b < m->P; ++b)
     for (int k = 0; k < 3; ++k) bx[b * 3 + k] = m->box[k];
@@ -961,7 +1006,7 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   MdScalars s0;
   std::memset(&s0, 0, sizeof(s0));
   s0.scale = 1.0;
-  s0.dof = 3.0 * (double)N;
+  s0.dof = 3.0 * (double)n_mobile;
   cudaMemcpy(m->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice);
   cudaMemset(m->status, 0, 4);
   if (pimd) {
@@ -1018,6 +1063,8 @@ static int md_upload(dpb_md *m, const double *host, float *dev, bool momentum) {
       for (int c = 0; c < 3; ++c) {
         double v = host[((size_t)b * N + u) * 3 + c];
         if (momentum) v *= m->mass_sorted[k];
+        // setVelocity masks the fixed atoms' momenta (md.py:1029-1030)
+        if (momentum && m->mobile && m->mobile_sorted[k] == 0.f) v = 0.0;
         buf[((size_t)b * N + k) * 3 + c] = (float)v;
       }
     }
@@ -1071,8 +1118,14 @@ static int md_build_list(dpb_md *m, const unsigned *gate, cudaStream_t st) {
 }
 
 static int md_forces(dpb_md *m, cudaStream_t st) {
-  return eval_impl(m->model, m->d.precision, m->pos, nullptr, m->N, m->P, m->type_count, m->boxd, m->nbrs, m->sel,
-                   m->energy, nullptr, m->force, m->virial, m->status, m->ev_ws, m->ev_ws_bytes, st);
+  int rc = eval_impl(m->model, m->d.precision, m->pos, nullptr, m->N, m->P, m->type_count, m->boxd, m->nbrs, m->sel,
+                     m->energy, nullptr, m->force, m->virial, m->status, m->ev_ws, m->ev_ws_bytes, st);
+  if (!rc && m->mobile) {
+    k_mask_rows<<<(m->N * 3 + 255) / 256, 256, 0, st>>>(m->force, m->mobile, m->N);
+    count_launch();
+    DPB_LAUNCH_CHECK();
+  }
+  return rc;
 }
 
 extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
@@ -1096,7 +1149,7 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
     MdScalars h;
     cudaMemcpy(&h, sc, sizeof(h), cudaMemcpyDeviceToHost);
     h.chain_ke = h.ke;
-    h.dof = 3.0 * (double)m->N;
+    h.dof = 3.0 * (double)m->n_mobile;  // routine.py:119-127: DOF 3 n_mobile, Q0 = kT tau^2 DOF
     for (int k = 0; k < kMaxChain; ++k) {
       h.xi[k] = 0.0;
       h.pxi[k] = 0.0;
@@ -1210,7 +1263,8 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel,
       k_nhc_substep<<<1, 1, 0, st>>>(sc, m->d.chain_length, m->kT, m->d.tau_t, m->d.dt, 1);
       count_launch();
     }
-    k_vv_kick_drift<<<nb3, 256, 0, st>>>(m->pos, m->mom, m->force, m->inv_mass, m->N, NF, dt, sc, nvt ? 1 : 0);
+    k_vv_kick_drift<<<nb3, 256, 0, st>>>(m->pos, m->mom, m->force, m->mobile ? m->shift_inv_mass : m->inv_mass,
+                                         m->N, NF, dt, sc, nvt ? 1 : 0);
     count_launch();
     DPB_LAUNCH_CHECK();
     rc = md_forces(m, st);
@@ -1224,8 +1278,8 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel,
     }
   }
   if (m->d.remove_com_motion) {  // after the step, before the frame is emitted (md.py:793-796)
-    k_com_sum<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->N, sc);
-    k_com_sub<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->inv_mass, m->N, sc);
+    k_com_sum<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->mobile, m->N, sc);
+    k_com_sub<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->inv_mass, m->mobile, m->N, sc);
     count_launch(2);
   }
   if (traj_pos) {

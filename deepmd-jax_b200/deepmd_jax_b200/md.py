@@ -36,6 +36,7 @@ class MDDesc(ctypes.Structure):
         ("seed", ctypes.c_uint64), ("precision", ctypes.c_int),
         ("pressure", ctypes.c_double), ("tau_p", ctypes.c_double), ("chain_length_p", ctypes.c_int),
         ("couple_groups", ctypes.c_int * 3), ("remove_com_motion", ctypes.c_int),
+        ("fixed_indices", ctypes.POINTER(ctypes.c_int)), ("n_fixed", ctypes.c_int),
     ]
 
 
@@ -158,8 +159,12 @@ class Simulation:
         self.model = DeviceModel(params, variables)
         if routine not in ("NVE", "NVT", "NPT"):
             raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT / NPT PIMD)" % routine)
-        if len(model_deviation_paths) or fixed_indices is not None:
-            raise NotImplementedError("model deviation / fixed atoms are not supported")
+        if len(model_deviation_paths):
+            raise NotImplementedError("model deviation is not supported")
+        if fixed_indices is not None and int(n_bead) > 1:
+            raise NotImplementedError("fixed_indices is not supported with n_bead > 1.")
+        if fixed_indices is not None and routine not in ("NVE", "NVT"):
+            raise NotImplementedError("Fixing atoms currently limited to NVE and NVT routines.")
         if remove_com_motion and int(n_bead) > 1:
             raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
         self._remove_com = bool(remove_com_motion)
@@ -240,6 +245,15 @@ class Simulation:
         desc.natoms = self._natoms
         desc.nbeads = self._n_bead
         desc.remove_com_motion = int(self._remove_com)
+        # fixed atoms (md.py:221-236): a mobile mask; the engine masks shifts,
+        # forces and momenta and gives the chain 3 n_mobile degrees of freedom
+        self._mobile = None
+        if fixed_indices is not None:
+            self._mobile = np.ones(self._natoms, dtype=bool)
+            self._mobile[np.asarray(fixed_indices, dtype=np.int64)] = False
+            self._fixed_arr = np.ascontiguousarray(np.flatnonzero(~self._mobile), dtype=np.int32)
+            desc.fixed_indices = self._fixed_arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            desc.n_fixed = len(self._fixed_arr)
         self._keep = [np.ascontiguousarray(self._type_idx, dtype=np.int32), np.ascontiguousarray(self._mass_per_type)]
         desc.type_idx = self._keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         desc.mass_per_type = _dptr(self._keep[1])
@@ -354,14 +368,13 @@ class Simulation:
         self._graph_launches_replayed += self._graph_kernels.get(key, 0)
 
     # ------------------------------------------------------------------ reports
-    def _temperature_of(self, KE):
-        return 2 * KE / (3 * self._natoms * self._n_bead) / TEMP_UNIT_CONVERSION / self._n_bead * self._n_bead
-
     def _report_row(self, tic):
         r = self._report_struct()
         KE = r.kinetic_energy / self._n_bead ** 2 if self._is_pimd else r.kinetic_energy
         PE = r.potential_energy / self._n_bead
         T = 2 * r.kinetic_energy / (3 * self._natoms * self._n_bead) / TEMP_UNIT_CONVERSION / self._n_bead
+        if self._mobile is not None:  # md.py:478: temperature over the mobile degrees of freedom
+            T *= self._natoms / int(self._mobile.sum())
         row = [self.step, T, KE, PE]
         headers = ["Step", "Temperature", "KE", "PE"]
         if self._routine == "NVE":
@@ -676,8 +689,9 @@ class Simulation:
         m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
         if self._is_pimd:
             vel = vel - (vel * m).sum(axis=(0, 1)) / (m.sum() * self._n_bead)
-        else:
-            vel = vel - (vel * m).sum(0) / m.sum()
+        else:  # over the mobile atoms (md.py:755-756); setVelocity masks the fixed ones
+            mm = m * self._mobile[:, None] if self._mobile is not None else m
+            vel = vel - (vel * mm).sum(0) / mm.sum()
         self.setVelocity(vel)
 
     def getPressure(self):

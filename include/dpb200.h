@@ -246,6 +246,12 @@ typedef struct {
   int couple_groups[3];        /* group of each axis (0..G-1), -1: fixed axis */
   int remove_com_motion;       /* 1: subtract the centre-of-mass velocity after every step
                                   (md.py:793-796; not with PIMD) */
+  /* Fixed atoms (md.py:221-236, routine.py:110-136; NVE and NVT only):
+   * user indices of atoms that never move.  Their forces read zero (the
+   * stop_gradient of md.py:428-430), their momenta are masked, the chain
+   * has 3 (N - n_fixed) degrees of freedom.  NULL / 0: every atom mobile. */
+  const int32_t *fixed_indices;
+  int n_fixed;
 } dpb_md_desc;
 
 typedef struct {

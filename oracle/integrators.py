@@ -5,8 +5,8 @@ on the reference's hot path.
     deepmd_jax/routine.py:139-144);
   * Martyna-Tuckerman-Klein Nose-Hoover chain (jax_md.simulate.nvt_nose_hoover
     and nose_hoover_chain, wrapped by deepmd_jax/routine.py:147-158), chain
-    masses Q = kT tau^2 (Q0 *= DOF), DOF = 3N; invariant per
-    deepmd_jax/routine.py:9-25;
+    masses Q = kT tau^2 (Q0 *= DOF), DOF = 3N (3 n_mobile with fixed atoms,
+    deepmd_jax/routine.py:110-136); invariant per deepmd_jax/routine.py:9-25;
   * PIMD BAOAB with exact free ring-polymer propagation and the PILE-L
     thermostat (deepmd_jax/pimd.py:22-44,92-111,114-207,210-247);
   * MTK NPT with Nose-Hoover chains on the particles and on the box, axes in
@@ -35,13 +35,33 @@ def kinetic_energy(p, m):
     return 0.5 * float((p * p / m).sum())
 
 
-def vv_step(r, p, F, m, dt, force_fn):
-    """One velocity-Verlet step; returns (r, p, F, extra) with extra from force_fn."""
+def vv_step(r, p, F, m, dt, force_fn, mobile=None):
+    """One velocity-Verlet step; returns (r, p, F, extra) with extra from force_fn.
+    mobile (N,) bool: fixed atoms keep their positions (the masked shift of
+    deepmd_jax/md.py:231-234); force_fn must then be fixed_atom_forces(...)
+    and the caller masks the momenta after the step (mask_momenta)."""
     p = p + 0.5 * dt * F
-    r = r + dt * p / m
+    dr = dt * p / m
+    r = r + (dr if mobile is None else dr * mobile[:, None])
     F, extra = force_fn(r)
     p = p + 0.5 * dt * F
     return r, p, F, extra
+
+
+def mask_momenta(p, mobile):
+    """with_fixed_atoms (deepmd_jax/routine.py:130-134): the fixed atoms'
+    momenta are zeroed after every step of the wrapped integrator."""
+    return p if mobile is None else p * mobile[:, None]
+
+
+def fixed_atom_forces(force_fn, mobile):
+    """Forces with the fixed atoms' coordinates under stop_gradient
+    (deepmd_jax/md.py:428-430): their rows are zero, the mobile rows keep
+    every term."""
+    def f(r):
+        F, extra = force_fn(r)
+        return F * mobile[:, None], extra
+    return f
 
 
 class NHChain:
@@ -96,13 +116,16 @@ class NHChain:
         return E
 
 
-def nvt_step(r, p, F, m, dt, kT, chain: NHChain, force_fn):
+def nvt_step(r, p, F, m, dt, kT, chain: NHChain, force_fn, mobile=None):
+    """One Nose-Hoover NVT step; with mobile, the chain's dof must be
+    3 n_mobile (deepmd_jax/routine.py:115-132) and the momenta are masked
+    after the step."""
     chain.update_mass(kT)
     p = chain.substep(dt, p, kT)
-    r, p, F, extra = vv_step(r, p, F, m, dt, force_fn)
+    r, p, F, extra = vv_step(r, p, F, m, dt, force_fn, mobile)
     chain.KE = kinetic_energy(p, m)
     p = chain.substep(dt, p, kT)
-    return r, p, F, extra
+    return r, mask_momenta(p, mobile), F, extra
 
 
 def sinhx_x(x):

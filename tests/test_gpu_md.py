@@ -373,3 +373,68 @@ def test_nve_with_com_motion_removed_matches_oracle():
     assert np.abs(traj["velocity"][-1] - vel).max() < 2e-4 * np.abs(vel).max()
     P = (traj["velocity"][-1] * mass).sum(0)
     assert np.abs(P).max() < 1e-5 * np.abs(traj["velocity"][-1] * mass).sum()
+
+
+def test_fixed_atoms_nvt_with_com_removal_and_nve_match_oracle():
+    """fixed_indices (md.py:221-236, routine.py:110-136): fixed atoms never
+    move (bitwise), their forces read zero (md.py:428-430), the chain has
+    3 n_mobile degrees of freedom, the temperature is scaled by
+    N / n_mobile (md.py:478), and the centre-of-mass velocity comes from the
+    mobile atoms only while it is subtracted from every atom (md.py:788-789).
+    NVT with remove_com_motion for 10 steps and NVE for 10 steps against the
+    float64 oracle; the NVT report's KE is that of the final (scaled)
+    momenta."""
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+    N = len(w["type_idx"])
+    fixed = np.array(sorted(set(range(0, N, 7)) | set(range(40, 52))))
+    mob = np.ones(N, dtype=bool)
+    mob[fixed] = False
+    m = om.OracleModel(p, v, torch.float64)
+    fn = oi.fixed_atom_forces(_oracle_forces(m, w), mob)
+    mass = (w["mass"] * MU)[:, None]
+    kT = 300.0 * KB
+    vel0 = w["velocity"] + np.array([1e-3, -2e-3, 5e-4])
+
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.5, w["position"],
+                     initial_velocity=vel0, temperature=300.0, tau_t=100.0, remove_com_motion=True,
+                     fixed_indices=list(fixed), report_interval=10, verbose=False)
+    pos32 = w["position"].astype(np.float32).astype(np.float64)
+    assert np.all(sim.getForce()[fixed] == 0.0) and np.all(sim.getVelocity()[fixed] == 0.0)
+    traj = sim.run(10)
+    r_dev = sim._report_struct()
+    assert r_dev.chain_dof == 3 * mob.sum()
+    r, pm = w["position"].copy(), oi.mask_momenta(vel0 * mass, mob)
+    F, _ = fn(r)
+    chain = oi.NHChain(3, 3 * int(mob.sum()), kT, 100.0, oi.kinetic_energy(pm, mass))
+    for _ in range(10):
+        r, pm, F, _ = oi.nvt_step(r, pm, F, mass, 0.5, kT, chain, fn, mob)
+        V = (pm * mob[:, None]).sum(0) / (mass[:, 0] * mob).sum()
+        pm = pm - mass * V
+    assert np.array_equal(traj["position"][:, fixed], np.broadcast_to(pos32[fixed], traj["position"][:, fixed].shape))
+    assert np.abs(traj["position"][-1] - r).max() < 2e-4
+    vel = pm / mass
+    assert np.abs(traj["velocity"][-1] - vel).max() < 2e-4 * np.abs(vel).max()
+    assert np.allclose(np.array(r_dev.chain_xi[:3]), chain.xi, rtol=1e-3, atol=1e-9)
+    assert np.allclose(np.array(r_dev.chain_p[:3]), chain.p, rtol=1e-3, atol=1e-7)
+    assert np.all(sim.getForce()[fixed] == 0.0)
+    ke = oi.kinetic_energy(pm, mass)
+    assert abs(sim.log[-1][2] - ke) <= 1e-4 * ke
+    assert abs(sim.log[-1][1] - 2 * ke / (3 * mob.sum()) / KB) <= 1e-4 * sim.log[-1][1]
+
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.5, w["position"],
+                     initial_velocity=w["velocity"], fixed_indices=list(fixed), report_interval=10, verbose=False)
+    traj = sim.run(10)
+    r, pm = w["position"].copy(), oi.mask_momenta(w["velocity"] * mass, mob)
+    F, _ = fn(r)
+    for _ in range(10):
+        r, pm, F, _ = oi.vv_step(r, pm, F, mass, 0.5, fn, mob)
+        pm = oi.mask_momenta(pm, mob)
+    assert np.array_equal(traj["position"][-1][fixed], pos32[fixed])
+    assert np.all(traj["velocity"][-1][fixed] == 0.0)
+    assert np.abs(traj["position"][-1] - r).max() < 2e-4
+    assert np.abs(traj["velocity"][-1] - pm / mass).max() < 2e-4 * np.abs(pm / mass).max()
+    with pytest.raises(NotImplementedError):
+        Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NPT", 0.5, w["position"],
+                   temperature=300.0, pressure=1.0, fixed_indices=[0], verbose=False)
