@@ -1,5 +1,5 @@
-"""``evaluate()`` with the reference's signature and results
-(deepmd_jax/train.py:703-788), evaluated by libdpb200 on the GPU.
+"""``evaluate()`` and ``test()`` with the reference's signatures and results
+(deepmd_jax/train.py:703-788 and 523-701), evaluated by libdpb200 on the GPU.
 
 The reference writes the frames to a temporary dataset and runs ``test()``
 (train.py:523-701), a ``jit(vmap(energy_and_force))`` over ``batch_size``
@@ -9,6 +9,8 @@ every periodic image within rcut is summed, as on the lattice path
 (deepmd_jax/utils.py:66-78).  Training is not part of this library.
 """
 from __future__ import annotations
+
+from glob import glob
 
 import numpy as np
 import torch
@@ -92,6 +94,12 @@ def evaluate(model_path, coord, box, type_idx, batch_size=1, precision="fp32"):
     _require_cuda()
     model, dm = _device_model(model_path)
     type_idx = _map_chemical_types(model.params, type_idx)
+    return _evaluate_frames(model, dm, coord, box, type_idx, batch_size, precision)
+
+
+def _evaluate_frames(model, dm, coord, box, type_idx, batch_size, precision):
+    """Energies and forces of frames (F, N, 3) in boxes (F, 3, 3) with model
+    type indices type_idx (N,), batch_size frames per dpb_eval call."""
     off = box - np.einsum("fii->fi", box)[:, :, None] * np.eye(3)
     if np.any(off):
         raise NotImplementedError("non-orthorhombic boxes are not supported by the B200 kernels")
@@ -113,3 +121,82 @@ def evaluate(model_path, coord, box, type_idx, batch_size=1, precision="fp32"):
         energy[a:b] = out["energy"].cpu().numpy()
         force[a:b] = out["force"].cpu().numpy()
     return {"energy": energy, "force": force}
+
+
+def _flatten_paths(paths):
+    for p in paths:
+        if isinstance(p, (list, tuple)):
+            yield from _flatten_paths(p)
+        else:
+            yield p
+
+
+def load_dp_data(data_path):
+    """The energy labels of DeepMD-format directories, one entry per
+    directory: type.raw and set.*/{coord,box,energy,force}.npy concatenated
+    over the sorted sets (deepmd_jax/data.py:22-70,190-200).  type.raw holds
+    model type indices.  Extended-XYZ files need ase (data.py:285-345),
+    which this library does not use: NotImplementedError."""
+    paths = [data_path] if isinstance(data_path, str) else list(_flatten_paths(data_path))
+    leaves = []
+    for p in paths:
+        if isinstance(p, str) and p.lower().endswith((".xyz", ".extxyz")):
+            raise NotImplementedError("extxyz datasets are not supported; convert them to DeepMD directories")
+        type_idx = np.atleast_1d(np.genfromtxt(p + "/type.raw").astype(int))
+        sets = sorted(glob(p + "/set.*/"))
+        if not sets:
+            raise FileNotFoundError("no set.*/ directory under %r" % p)
+        data = {l: np.concatenate([np.load(s + l + ".npy") for s in sets]) for l in ("coord", "box", "energy", "force")}
+        nf = len(data["coord"])
+        for l, v in data.items():
+            assert v.shape[0] == nf, f"{l}.npy has {v.shape[0]} frames, expected {nf}"
+        leaves.append({"type_idx": type_idx,
+                       "coord": data["coord"].reshape(nf, -1, 3),
+                       "box": data["box"].reshape(-1, 3, 3),
+                       "energy": data["energy"].reshape(-1),
+                       "force": data["force"].reshape(nf, -1, 3)})
+    return leaves
+
+
+def error_metrics(results):
+    """RMSE / MAE / l1_mixed of energy per atom and of force components over
+    test results (deepmd_jax/train.py:629-690): dE = (E_pred - E_true) / N;
+    force RMSE and MAE over all components; l1_mixed force = the mean over
+    atoms of each atom's RMS component error."""
+    e_sq = e_abs = f_sq = f_abs = f_l1 = 0.0
+    e_n = f_n = f_atoms = 0
+    for r in results:
+        n = len(r["type_idx"])
+        dE = (r["predicted_energy"] - r["true_energy"]) / n
+        e_sq += dE * dE
+        e_abs += abs(dE)
+        e_n += 1
+        dF = np.asarray(r["predicted_force"], dtype=np.float64) - np.asarray(r["true_force"], dtype=np.float64)
+        f_sq += float((dF ** 2).sum())
+        f_abs += float(np.abs(dF).sum())
+        f_n += dF.size
+        f_l1 += float(np.sqrt((dF ** 2).mean(-1)).sum())
+        f_atoms += dF.shape[0]
+    return {"rmse": {"energy": float(np.sqrt(e_sq / e_n)), "force": float(np.sqrt(f_sq / f_n))},
+            "mae": {"energy": float(e_abs / e_n), "force": float(f_abs / f_n)},
+            "l1_mixed": {"energy": float(e_abs / e_n), "force": float(f_l1 / f_atoms)}}
+
+
+def test(model_path, data_path, batch_size=1, precision="fp32"):
+    """Errors of an energy model on labelled DeepMD-format data
+    (deepmd_jax/train.py:523-701): returns (error_metrics, test_results),
+    the results one dict per frame in dataset order with 'box' (3, 3),
+    'type_idx', 'predicted_energy', 'true_energy', 'predicted_force',
+    'true_force'.  Frames run batch_size at a time through dpb_eval."""
+    _require_cuda()
+    model, dm = _device_model(model_path)
+    results = []
+    for leaf in load_dp_data(data_path):
+        pred = _evaluate_frames(model, dm, leaf["coord"], np.asarray(leaf["box"], dtype=np.float64),
+                                leaf["type_idx"], batch_size, precision)
+        for i in range(len(leaf["energy"])):
+            results.append({"box": np.asarray(leaf["box"][i]).copy(), "type_idx": leaf["type_idx"].copy(),
+                            "predicted_energy": float(pred["energy"][i]), "true_energy": float(leaf["energy"][i]),
+                            "predicted_force": pred["force"][i].copy(),
+                            "true_force": np.asarray(leaf["force"][i]).copy()})
+    return error_metrics(results), results

@@ -212,3 +212,45 @@ def test_ase_calculator_energy_forces_stress(tmp_path):
     V = float(np.prod(box))
     ref = -np.array([W[0, 0], W[1, 1], W[2, 2], W[1, 2], W[0, 2], W[0, 1]]) / V
     assert S.shape == (6,) and np.abs(S - ref).max() <= 2e-4 * np.abs(ref).max() + 1e-12
+
+
+def test_test_on_dp_directories_matches_golden_and_metrics(tmp_path):
+    """test() (deepmd_jax/train.py:523-701) on three DeepMD-format
+    directories (the 192-, 1,536- and 96-atom golden systems of model B, two
+    sets each, the second set a rigid translation), labels = golden values
+    plus known offsets: predictions match the golden vectors and the
+    metrics are those of the offsets."""
+    from deepmd_jax_b200.train import test as dp_test
+    path = _pkl(tmp_path, "B")
+    rng = np.random.default_rng(3)
+    expect = []
+    dirs = []
+    for sysk, key in (("A", "B"), ("D", "D"), ("E", "E")):
+        pos, box, typ = G[sysk + "_pos"], G[sysk + "_box"], G[sysk + "_type"]
+        root = tmp_path / ("data_" + sysk)
+        (root).mkdir()
+        (root / "type.raw").write_text("\n".join(str(int(t)) for t in typ))
+        for k, shift in enumerate((0.0, 0.41)):
+            d = root / ("set.%03d" % k)
+            d.mkdir()
+            dE = rng.normal()
+            dF = rng.normal(scale=0.1, size=pos.shape)
+            np.save(d / "coord.npy", (pos + shift).reshape(1, -1))
+            np.save(d / "box.npy", np.diag(box).reshape(1, 9))
+            np.save(d / "energy.npy", np.array([float(G[key + "_E"]) + dE]))
+            np.save(d / "force.npy", (G[key + "_F"] + dF).reshape(1, -1))
+            expect.append((float(G[key + "_E"]), G[key + "_F"], dE, dF, len(typ)))
+        dirs.append(str(root))
+    metrics, results = dp_test(path, dirs, batch_size=2)
+    assert len(results) == 6
+    e_err, f_err = [], []
+    for r, (E, F, dE, dF, n) in zip(results, expect):
+        _close(r["predicted_energy"], r["predicted_force"], E, F, n)
+        assert np.isclose(r["true_energy"], E + dE) and r["box"].shape == (3, 3)
+        e_err.append((r["predicted_energy"] - r["true_energy"]) / n)
+        f_err.append((r["predicted_force"] - r["true_force"]).reshape(-1))
+    e_err, f_err = np.array(e_err), np.concatenate(f_err)
+    assert np.isclose(metrics["rmse"]["energy"], np.sqrt((e_err ** 2).mean()))
+    assert np.isclose(metrics["rmse"]["force"], np.sqrt((f_err ** 2).mean()), rtol=1e-5)
+    # the metrics are those of the planted offsets to the FP32 error
+    assert abs(metrics["rmse"]["energy"] - np.sqrt(np.mean([(x[2] / x[4]) ** 2 for x in expect]))) < 1e-4

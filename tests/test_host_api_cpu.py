@@ -114,3 +114,56 @@ def test_xyz_dump_format_and_options(tmp_path):
     d2, _ = dump.prepare([0, 1, 1], ["O", "H"], 2, 10, dump_prefix=prefix)
     assert [x[1] for x in d2] == [prefix + "_position_bead0.xyz", prefix + "_position_bead1.xyz",
                                   prefix + "_centroid.xyz"]
+
+
+def _write_dp_dir(root, type_idx, sets):
+    """A DeepMD-format directory: type.raw and set.NNN/{coord,box,energy,force}.npy."""
+    root.mkdir(parents=True, exist_ok=True)
+    (root / "type.raw").write_text("\n".join(str(int(t)) for t in type_idx))
+    for k, frames in enumerate(sets):
+        d = root / ("set.%03d" % k)
+        d.mkdir()
+        for name, arr in frames.items():
+            np.save(d / (name + ".npy"), arr.reshape(arr.shape[0], -1) if arr.ndim > 1 else arr)
+
+
+def test_dp_loader_and_error_metrics(tmp_path):
+    """test()'s data side (deepmd_jax/data.py:190-200, train.py:629-690):
+    two directories (two compositions), sets concatenated in sorted order,
+    and the metric formulas checked on hand-made predictions."""
+    from deepmd_jax_b200.train import error_metrics, load_dp_data
+    rng = np.random.default_rng(0)
+
+    def frames(nf, n):
+        return {"coord": rng.normal(size=(nf, n, 3)), "box": np.tile(np.eye(3) * 9.0, (nf, 1, 1)),
+                "energy": rng.normal(size=nf), "force": rng.normal(size=(nf, n, 3))}
+    a_sets = [frames(2, 5), frames(3, 5)]
+    b_sets = [frames(1, 4)]
+    _write_dp_dir(tmp_path / "a", [0, 1, 1, 0, 1], a_sets)
+    _write_dp_dir(tmp_path / "b", [1, 0, 0, 1], b_sets)
+    leaves = load_dp_data([str(tmp_path / "a"), [str(tmp_path / "b")]])
+    assert [len(l["energy"]) for l in leaves] == [5, 1]
+    assert np.array_equal(leaves[0]["type_idx"], [0, 1, 1, 0, 1])
+    assert np.allclose(leaves[0]["coord"], np.concatenate([s["coord"] for s in a_sets]))
+    assert leaves[0]["box"].shape == (5, 3, 3) and leaves[1]["force"].shape == (1, 4, 3)
+    with pytest.raises(NotImplementedError):
+        load_dp_data(str(tmp_path / "x.extxyz"))
+
+    results, dE, dF = [], [], []
+    for leaf in leaves:
+        for i in range(len(leaf["energy"])):
+            pe = leaf["energy"][i] + rng.normal()
+            pf = leaf["force"][i] + rng.normal(size=leaf["force"][i].shape)
+            results.append({"type_idx": leaf["type_idx"], "predicted_energy": pe, "true_energy": leaf["energy"][i],
+                            "predicted_force": pf, "true_force": leaf["force"][i]})
+            dE.append((pe - leaf["energy"][i]) / len(leaf["type_idx"]))
+            dF.append(pf - leaf["force"][i])
+    m = error_metrics(results)
+    dE = np.array(dE)
+    allF = np.concatenate([d.reshape(-1) for d in dF])
+    per_atom = np.concatenate([np.sqrt((d ** 2).mean(-1)) for d in dF])
+    assert np.isclose(m["rmse"]["energy"], np.sqrt((dE ** 2).mean()))
+    assert np.isclose(m["mae"]["energy"], np.abs(dE).mean()) and np.isclose(m["l1_mixed"]["energy"], np.abs(dE).mean())
+    assert np.isclose(m["rmse"]["force"], np.sqrt((allF ** 2).mean()))
+    assert np.isclose(m["mae"]["force"], np.abs(allF).mean())
+    assert np.isclose(m["l1_mixed"]["force"], per_atom.mean())
