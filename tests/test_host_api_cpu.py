@@ -167,3 +167,26 @@ def test_dp_loader_and_error_metrics(tmp_path):
     assert np.isclose(m["rmse"]["force"], np.sqrt((allF ** 2).mean()))
     assert np.isclose(m["mae"]["force"], np.abs(allF).mean())
     assert np.isclose(m["l1_mixed"]["force"], per_atom.mean())
+
+
+def test_periodic_replicate():
+    """utils.periodic_replicate (deepmd_jax/utils.py:299-327): copies along
+    x, then y, then z, each axis's copies outermost; scalar, (3,) and (3, 3)
+    boxes; tiled types, forces and velocities."""
+    from deepmd_jax_b200.utils import periodic_replicate
+    rng = np.random.default_rng(1)
+    c = rng.uniform(0, 3, size=(4, 3))
+    t = np.array([0, 1, 1, 0])
+    f = rng.normal(size=(4, 3))
+    out = periodic_replicate([2, 1, 3], c, [3.0, 4.0, 5.0], type_idx=t, force=f, velocity=f * 2)
+    assert np.array_equal(out[1], [6.0, 4.0, 15.0])
+    want = np.array([c[a] + np.array([ix * 3.0, 0.0, iz * 5.0])
+                     for iz in range(3) for ix in range(2) for a in range(4)])
+    assert np.allclose(out[0], want)
+    assert np.array_equal(out[2], np.tile(t, 6)) and np.array_equal(out[3], np.concatenate([f] * 6))
+    assert np.array_equal(out[4], np.concatenate([2 * f] * 6))
+    c2, b2 = periodic_replicate(2, c, 3.0)
+    assert np.array_equal(b2, [6.0, 6.0, 6.0]) and c2.shape == (32, 3)
+    c3, b3 = periodic_replicate(2, c, np.diag([3.0, 4.0, 5.0]))
+    assert np.array_equal(b3, np.diag([6.0, 8.0, 10.0]))
+    assert np.allclose(c3[-1], c[-1] + [3.0, 4.0, 5.0])
