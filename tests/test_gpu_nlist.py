@@ -74,3 +74,43 @@ def test_nlist_frames_batch():
         c = onl.canonicalize(w["position"], w["box"], w["type_idx"])
         want, _, _ = onl.typed_nlist(c, w["box"].astype(np.float32), onl.cutoff_sq(6.3), cnt, [46, 92])
         assert np.array_equal(got[f], want)
+
+
+def test_nlist_full_size_sampled_rows_bit_exact():
+    """The 98,304-atom box of the MD benchmark (32,768 waters, L = 99.3 A):
+    300 sampled centre rows (and the first and last atom of each type block)
+    bit-exact against the oracle's float32 distance test over all atoms, and
+    on every row the size-independent layout: each type block ascending,
+    then padded with the block's type count."""
+    w = water_box(32, 99.3, seed=3)
+    sel = [46, 92]
+    got, counts, status, ref_pos, cnt = gpu_nlist(w, sel, 6.3)
+    assert (status & 2 != 0) == bool((counts[0] > np.asarray(sel)[None, :]).any())
+    c = onl.canonicalize(w["position"], w["box"], w["type_idx"])
+    assert np.array_equal(ref_pos[0], c)
+    N = len(c)
+    rng = np.random.default_rng(0)
+    rows = np.unique(np.concatenate([rng.choice(N, 300, replace=False), [0, cnt[0] - 1, cnt[0], N - 1]]))
+    L = w["box"].astype(np.float32)
+    rc2 = onl.cutoff_sq(6.3)
+    offs = np.concatenate([[0], np.cumsum(cnt)])
+    col = np.concatenate([[0], np.cumsum(sel)])
+    for i in rows:
+        d2 = onl.pair_d2(c[i][None, :], c, L)
+        m = d2 < rc2
+        m[i] = False
+        s = np.nonzero(m)[0]
+        for j in range(2):
+            nb = s[(s >= offs[j]) & (s < offs[j + 1])] - offs[j]
+            assert counts[0][i, j] == len(nb)
+            want = np.full(sel[j], cnt[j], dtype=np.int32)
+            k = min(len(nb), sel[j])
+            want[:k] = nb[:k]
+            assert np.array_equal(got[0][i, col[j]:col[j + 1]], want), (i, j)
+    for j in range(2):
+        blk = got[0][:, col[j]:col[j + 1]].astype(np.int64)
+        valid = blk < cnt[j]
+        assert np.array_equal(valid.sum(1), np.minimum(counts[0][:, j], sel[j]))
+        assert (valid[:, :-1] | ~valid[:, 1:]).all()           # pads only after the neighbours
+        d = np.diff(blk, axis=1)
+        assert ((d > 0) | ~valid[:, 1:]).all()                  # strictly ascending neighbours
