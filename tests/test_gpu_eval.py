@@ -160,3 +160,38 @@ def test_empty_type_block_and_isolated_atoms(precision):
     assert np.all(got2["force"] == 0.0) and np.all(got2["virial"] == 0.0)
     tol = 2e-6 if precision == "fp32" else 2e-2
     assert np.abs(got2["atom_energy"][0] - ref2["atom_energy"]).max() <= tol * np.abs(ref2["atom_energy"]).max()
+
+
+def test_full_size_invariants_fp32_and_mixed():
+    """The 98,304-atom benchmark box (32,768 waters, L = 99.3 A), benchmark
+    model architecture: properties that hold at any size.  Two frames, the
+    second a rigid translation by (0.37, -1.2, 2.9) A: energies within
+    2e-6 x sum|E_atom| and forces within 2e-4 x max|F| of each other (FP32);
+    the total force vanishes (<= 1e-5 x sum|F|); the energy is the sum of
+    the atom energies; the virial is symmetric (<= 1e-4 x max|W|).  The
+    mixed form against FP32 on the same lists: force RMS difference
+    <= 5e-3 eV/A and <= 3e-2 x force RMS."""
+    from deepmd_jax_b200.systems import init_dp_params, water_box
+    from make_golden import randomize_model
+    p, v = randomize_model(*init_dp_params(nnbrs=90.0, seed=0), seed=1)
+    w = water_box(32, 99.3, seed=5)
+    pos = np.stack([w["position"], w["position"] + np.array([0.37, -1.2, 2.9])])
+    sel = (60, 120)
+    r32 = run_gpu(p, v, pos, w["box"], w["type_idx"], sel=sel)
+    assert r32["status"] == 0
+    eabs = np.abs(r32["atom_energy"][0]).sum()
+    assert abs(r32["energy"][0] - r32["energy"][1]) <= 2e-6 * eabs
+    fmax = np.abs(r32["force"][0]).max()
+    assert np.abs(r32["force"][0] - r32["force"][1]).max() <= 2e-4 * fmax
+    for f in range(2):
+        F = r32["force"][f].astype(np.float64)
+        assert np.abs(F.sum(0)).max() <= 1e-5 * np.abs(F).sum()
+        assert abs(r32["energy"][f] - r32["atom_energy"][f].sum()) <= 1e-6 * eabs
+        W = r32["virial"][f]
+        assert np.abs(W - W.T).max() <= 1e-4 * np.abs(W).max()
+    rmx = run_gpu(p, v, pos, w["box"], w["type_idx"], sel=sel, precision="mixed")
+    assert rmx["status"] == 0
+    for f in range(2):
+        d = rmx["force"][f] - r32["force"][f]
+        rms_d = np.sqrt((d ** 2).mean())
+        assert rms_d <= 5e-3 and rms_d <= 3e-2 * np.sqrt((r32["force"][f] ** 2).mean()), rms_d

@@ -81,7 +81,7 @@ def test_nlist_full_size_sampled_rows_bit_exact():
     300 sampled centre rows (and the first and last atom of each type block)
     bit-exact against the oracle's float32 distance test over all atoms, and
     on every row the size-independent layout: each type block ascending,
-    then padded with the block's type count."""
+    then padded with N."""
     w = water_box(32, 99.3, seed=3)
     sel = [46, 92]
     got, counts, status, ref_pos, cnt = gpu_nlist(w, sel, 6.3)
@@ -103,13 +103,14 @@ def test_nlist_full_size_sampled_rows_bit_exact():
         for j in range(2):
             nb = s[(s >= offs[j]) & (s < offs[j + 1])] - offs[j]
             assert counts[0][i, j] == len(nb)
-            want = np.full(sel[j], cnt[j], dtype=np.int32)
+            want = np.full(sel[j], N, dtype=np.int32)  # pad N (md_utils.py:444-452)
             k = min(len(nb), sel[j])
             want[:k] = nb[:k]
             assert np.array_equal(got[0][i, col[j]:col[j + 1]], want), (i, j)
     for j in range(2):
         blk = got[0][:, col[j]:col[j + 1]].astype(np.int64)
         valid = blk < cnt[j]
+        assert (valid | (blk == N)).all()
         assert np.array_equal(valid.sum(1), np.minimum(counts[0][:, j], sel[j]))
         assert (valid[:, :-1] | ~valid[:, 1:]).all()           # pads only after the neighbours
         d = np.diff(blk, axis=1)
