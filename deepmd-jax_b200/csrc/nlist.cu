@@ -18,6 +18,7 @@
 // hits) and writes the sorted prefix into the centre's own row.
 #include "dpb_common.cuh"
 #include <algorithm>
+#include <climits>
 #include <cmath>
 
 namespace dpb {
@@ -144,24 +145,47 @@ struct NlParams {
   int3 nimg;
 };
 
-// Append the hits of one 32-candidate round into the per-type lists.
-__device__ __forceinline__ void append_hits(bool hit, int t, int key, int ntypes, int cap, int *cnt,
+// Append the hits of one 32-candidate round into the per-type lists; the
+// per-type counts are warp-uniform registers.  Hits past cap are dropped
+// (that count is flagged as an overflow), in traversal order.
+__device__ __forceinline__ void append_hits(bool hit, int t, int key, int ntypes, int cap, int (&cnt)[kMaxTypes],
                                             int *lists) {
-  unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+  const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
 #pragma unroll
   for (int tt = 0; tt < kMaxTypes; ++tt) {
     if (tt >= ntypes) break;
-    unsigned m = __ballot_sync(0xffffffffu, hit && t == tt);
-    if (m == 0u) continue;
-    int base = cnt[tt];
-    if (hit && t == tt) {
-      int p = base + __popc(m & lt);
+    const bool mine = hit && t == tt;
+    const unsigned m = __ballot_sync(0xffffffffu, mine);
+    if (mine) {
+      const int p = cnt[tt] + __popc(m & lt);
       if (p < cap) lists[tt * cap + p] = key;
     }
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) cnt[tt] = base + __popc(m);
-    __syncwarp();
+    cnt[tt] += __popc(m);
   }
+}
+
+// Rank of each of a lane's KPL keys (lane, lane + 32, ...) among the nn
+// distinct keys of a hit list padded with INT_MAX to nn4 (a multiple of 4),
+// read four at a time; the keys with rank < sel go to out[rank] - off.
+template <int KPL>
+__device__ __forceinline__ void rank_write(const int *__restrict__ L_, int nn, int nn4, int sel, int off,
+                                           int32_t *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  int key[KPL], rank[KPL];
+#pragma unroll
+  for (int k = 0; k < KPL; ++k) {
+    key[k] = lane + 32 * k < nn ? L_[lane + 32 * k] : INT_MAX;
+    rank[k] = 0;
+  }
+  for (int e2 = 0; e2 < nn4; e2 += 4) {
+    const int4 v = *reinterpret_cast<const int4 *>(L_ + e2);
+#pragma unroll
+    for (int k = 0; k < KPL; ++k)
+      rank[k] += (v.x < key[k]) + (v.y < key[k]) + (v.z < key[k]) + (v.w < key[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < KPL; ++k)
+    if (lane + 32 * k < nn && rank[k] < sel) out[rank[k]] = key[k] - off;
 }
 
 __device__ __forceinline__ bool pair_hit(float3 ci, float3 cj, float3 L, float rc2) {
@@ -174,28 +198,28 @@ __device__ __forceinline__ bool pair_hit(float3 ci, float3 cj, float3 L, float r
   return d2 < rc2;
 }
 
-__global__ void __launch_bounds__(512) nl_search_kernel(NlParams P, const float *__restrict__ canon,
-                                                        const int *__restrict__ cell_start,
-                                                        const int *__restrict__ cell_atoms,
-                                                        const float4 *__restrict__ cell_pos,
-                                                        int32_t *__restrict__ nbrs,
-                                                        int32_t *__restrict__ counts,
-                                                        uint32_t *__restrict__ status,
-                                                        const unsigned *__restrict__ gate) {
+// 40 registers: 48 resident warps per SM at every launch shape (128-512
+// threads), with nothing spilled.
+__global__ void __maxnreg__(40) nl_search_kernel(NlParams P, const float *__restrict__ canon,
+                                                 const int *__restrict__ cell_start,
+                                                 const int *__restrict__ cell_atoms,
+                                                 const float4 *__restrict__ cell_pos,
+                                                 int32_t *__restrict__ nbrs,
+                                                 int32_t *__restrict__ counts,
+                                                 uint32_t *__restrict__ status,
+                                                 const unsigned *__restrict__ gate) {
   if (gate && *gate == 0u) return;
-  extern __shared__ int smem[];
+  extern __shared__ __align__(16) int smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
-  int *cnt = smem + warp * kMaxTypes;
-  int *lists = smem + wpb * kMaxTypes + warp * P.ntypes * P.cap;
+  int *lists = smem + warp * P.ntypes * P.cap;
   const int gc = blockIdx.x * wpb + warp;  // position in cell order
   if (gc >= P.N * P.F) return;
   const int f = gc / P.N, i = cell_atoms[gc];  // frame-local sorted index of the centre
   const int g = f * P.N + i;
   const float *cf = canon + (size_t)f * P.N * 3;
   float3 ci = make_float3(cf[i * 3], cf[i * 3 + 1], cf[i * 3 + 2]);
-  if (lane < kMaxTypes) cnt[lane] = 0;
-  __syncwarp();
+  int cnt[kMaxTypes] = {0, 0, 0, 0};
 
   if (!P.image_mode) {
     const int ncell = P.nc.x * P.nc.y * P.nc.z;
@@ -206,27 +230,54 @@ __global__ void __launch_bounds__(512) nl_search_kernel(NlParams P, const float 
     int lox = P.nc.x >= 3 ? -1 : 0, hix = P.nc.x >= 2 ? 1 : 0;
     int loy = P.nc.y >= 3 ? -1 : 0, hiy = P.nc.y >= 2 ? 1 : 0;
     int loz = P.nc.z >= 3 ? -1 : 0, hiz = P.nc.z >= 2 ? 1 : 0;
-    for (int ox = lox; ox <= hix; ++ox)
-      for (int oy = loy; oy <= hiy; ++oy)
-        for (int oz = loz; oz <= hiz; ++oz) {
-          int cx = (ix + ox + P.nc.x) % P.nc.x;
-          int cy = (iy + oy + P.nc.y) % P.nc.y;
-          int cz = (iz + oz + P.nc.z) % P.nc.z;
-          int c = (cx * P.nc.y + cy) * P.nc.z + cz;
-          int b = cs[c], e = cs[c + 1];
-          for (int base = b; base < e; base += 32) {
-            int q = base + lane;
-            bool hit = false;
-            int j = 0, t = 0;
-            if (q < e) {
-              const float4 v = cell_pos[q];
-              j = __float_as_int(v.w);
-              hit = (j != i) && pair_hit(ci, make_float3(v.x, v.y, v.z), P.L, P.rc2);
-              t = type_of(j, P.offs, P.ntypes);
-            }
-            append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
+    // candidates of [b, e) of cell order, 32 per round
+    auto scan = [&](int b, int e) {
+      for (int base = b; base < e; base += 32) {
+        const int q = base + lane;
+        bool hit = false;
+        int j = 0, t = 0;
+        if (q < e) {
+          const float4 v = cell_pos[q];
+          j = __float_as_int(v.w);
+          hit = (j != i) && pair_hit(ci, make_float3(v.x, v.y, v.z), P.L, P.rc2);
+          t = type_of(j, P.offs, P.ntypes);
+        }
+        append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
+      }
+    };
+    // ix + o lies in [-1, nc], so one conditional add or subtract is the
+    // periodic wrap.  With three or more cells along z the cells iz-1..iz+1
+    // of a row are one range of cell order, or two where the row wraps, so
+    // a round takes 32 candidates of the row rather than of one cell (the
+    // visiting order only matters past cap hits, already an overflow).
+    for (int ox = lox; ox <= hix; ++ox) {
+      int cx = ix + ox;
+      cx += cx < 0 ? P.nc.x : 0;
+      cx -= cx >= P.nc.x ? P.nc.x : 0;
+      for (int oy = loy; oy <= hiy; ++oy) {
+        int cy = iy + oy;
+        cy += cy < 0 ? P.nc.y : 0;
+        cy -= cy >= P.nc.y ? P.nc.y : 0;
+        const int cxy = (cx * P.nc.y + cy) * P.nc.z, nz = P.nc.z;
+        if (nz >= 3) {
+          if (iz >= 1 && iz <= nz - 2) {
+            scan(cs[cxy + iz - 1], cs[cxy + iz + 2]);
+          } else if (iz == 0) {
+            scan(cs[cxy], cs[cxy + 2]);
+            scan(cs[cxy + nz - 1], cs[cxy + nz]);
+          } else {
+            scan(cs[cxy + nz - 2], cs[cxy + nz]);
+            scan(cs[cxy], cs[cxy + 1]);
+          }
+        } else {
+          for (int oz = loz; oz <= hiz; ++oz) {
+            int cz = iz + oz;
+            cz -= cz >= nz ? nz : 0;
+            scan(cs[cxy + cz], cs[cxy + cz + 1]);
           }
         }
+      }
+    }
   } else {
     // small box: j is listed once if any periodic image lies within rc
     const int nx = 2 * P.nimg.x + 1, ny = 2 * P.nimg.y + 1, nz = 2 * P.nimg.z + 1;
@@ -250,24 +301,33 @@ __global__ void __launch_bounds__(512) nl_search_kernel(NlParams P, const float 
       append_hits(hit, t, j, P.ntypes, P.cap, cnt, lists);
     }
   }
-  __syncwarp();
   // rank-sort each type's hits and write the sel_t smallest
   const int S = P.col[P.ntypes];
   int32_t *out = nbrs + (size_t)g * S;
   bool ovf = false;
+#pragma unroll 1
   for (int t = 0; t < P.ntypes; ++t) {
-    int n = cnt[t];
+    const int n = t == 0 ? cnt[0] : t == 1 ? cnt[1] : t == 2 ? cnt[2] : cnt[3];
     if (counts && lane == 0) counts[(size_t)g * P.ntypes + t] = n;
     ovf |= (n > P.sel[t]) || (n > P.cap);
-    int nn = min(n, P.cap);
-    const int *L_ = lists + t * P.cap;
-    for (int e = lane; e < nn; e += 32) {
-      int key = L_[e];
-      int rank = 0;
-      for (int e2 = 0; e2 < nn; ++e2) rank += (L_[e2] < key);
-      if (rank < P.sel[t]) out[P.col[t] + rank] = key - P.offs[t];
-    }
-    for (int e = nn + lane; e < P.sel[t]; e += 32) out[P.col[t] + e] = P.N;
+    const int nn = min(n, P.cap), nn4 = (nn + 3) & ~3;  // cap is a multiple of 4
+    int *L_ = lists + t * P.cap;
+    if (lane < nn4 - nn) L_[nn + lane] = INT_MAX;
+    __syncwarp();
+    int32_t *o = out + P.col[t];
+    const int sel = P.sel[t], off = P.offs[t];
+    if (nn <= 32) rank_write<1>(L_, nn, nn4, sel, off, o);
+    else if (nn <= 64) rank_write<2>(L_, nn, nn4, sel, off, o);
+    else if (nn <= 96) rank_write<3>(L_, nn, nn4, sel, off, o);
+    else if (nn <= 128) rank_write<4>(L_, nn, nn4, sel, off, o);
+    else  // long lists (large sel): one key per lane at a time, few registers
+      for (int e = lane; e < nn; e += 32) {
+        const int key = L_[e];
+        int rank = 0;
+        for (int e2 = 0; e2 < nn; ++e2) rank += (L_[e2] < key);
+        if (rank < sel) o[rank] = key - off;
+      }
+    for (int e = nn + lane; e < sel; e += 32) o[e] = P.N;
   }
   if (ovf && lane == 0) atomicOr(status, DPB_ST_NLIST_OVERFLOW);
 }
@@ -353,7 +413,7 @@ int nlist_build_impl(const float *pos, const int32_t *perm, int natoms, int nfra
                                             nframes, g.ncell, gate);
   if (nl_warps != 4 && nl_warps != 8 && nl_warps != 16) return DPB_ERR_INVALID_ARG;
   const int wpb = nl_warps, threads = 32 * wpb;  // centres (warps) per block
-  size_t smem = (size_t)wpb * kMaxTypes * 4 + (size_t)wpb * ntypes * cap * 4;
+  size_t smem = (size_t)wpb * ntypes * cap * 4;
   if (smem > 200 * 1024) return DPB_ERR_UNSUPPORTED;  // hit lists of this many warps do not fit
   if (smem > 48 * 1024) {
     DPB_CUDA_TRY(cudaFuncSetAttribute(nl_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
