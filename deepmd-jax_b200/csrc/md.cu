@@ -1437,6 +1437,35 @@ extern "C" int dpb_md_box_history(dpb_md *m, int nsteps, double *out) {
   return DPB_OK;
 }
 
+extern "C" int dpb_md_eval_model(dpb_md *m, const dpb_model *model, double *energy, double *force) {
+  if (!m || !model || !energy || !force) return DPB_ERR_INVALID_ARG;
+  if (m->P != 1 || model->dm.ntypes != m->ntypes) return DPB_ERR_UNSUPPORTED;
+  size_t wsb = 0;
+  int rc = dpb_eval_workspace_bytes(model, m->N, 1, &wsb);
+  if (rc) return rc;
+  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
+  const size_t N3 = (size_t)m->N * 3;
+  char *buf = nullptr;
+  const size_t off_f = 0, off_e = (N3 * 4 + 255) & ~(size_t)255, off_v = off_e + 256, off_s = off_v + 256,
+               off_w = off_s + 256;
+  if (cudaMalloc((void **)&buf, off_w + wsb) != cudaSuccess) return DPB_ERR_CUDA;
+  float *F = (float *)(buf + off_f);
+  double *E = (double *)(buf + off_e), *W = (double *)(buf + off_v);
+  uint32_t *stat = (uint32_t *)(buf + off_s);
+  cudaMemset(stat, 0, 4);
+  rc = eval_impl(model, m->d.precision, m->pos, nullptr, m->N, 1, m->type_count, m->boxd, m->nbrs, m->sel, E,
+                 nullptr, F, W, stat, buf + off_w, wsb, nullptr);
+  if (!rc && m->mobile) k_mask_rows<<<(m->N * 3 + 255) / 256, 256>>>(F, m->mobile, m->N);
+  if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = DPB_ERR_CUDA;
+  uint32_t hs = 0;
+  if (!rc && cudaMemcpy(energy, E, 8, cudaMemcpyDeviceToHost) != cudaSuccess) rc = DPB_ERR_CUDA;
+  if (!rc && cudaMemcpy(&hs, stat, 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = DPB_ERR_CUDA;
+  if (!rc) rc = md_download(m, F, force, false);
+  cudaFree(buf);
+  if (!rc && (hs & DPB_ST_NONFINITE)) rc = DPB_ERR_CUDA;
+  return rc;
+}
+
 // Launch-shape autotuner: each candidate runs on this engine's current state
 // (a warm-up, then timed repetitions with CUDA events on the stream) and the
 // fastest is kept; shapes never change results.  Ends with the list and

@@ -2,10 +2,12 @@
 
 Mirrors deepmd_jax/md.py:48-1091 (constructor arguments, run(), getters and
 setters, report rows, error-code handling and chunked re-runs) for the
-routines on the hot path: 'NVE' (velocity Verlet), 'NVT' (Nose-Hoover chain)
-and 'NVT' with n_bead > 1 (ring-polymer BAOAB with PILE-L).  All device work
-runs in libdpb200.so through dpb_md_*; a chunk of steps is captured once into
-a CUDA graph and replayed.
+routines 'NVE' (velocity Verlet), 'NVT' (Nose-Hoover chain), 'NPT' (MTK
+barostat, coupled axes) and, with n_bead > 1, 'NVT' / 'NPT' path-integral MD
+(ring-polymer BAOAB with PILE-L; Langevin barostat), with centre-of-mass
+removal, fixed atoms and the Model_Devi reporter.  All device work runs in
+libdpb200.so through dpb_md_*; a chunk of steps is captured once into a CUDA
+graph and replayed.
 """
 from __future__ import annotations
 
@@ -75,10 +77,11 @@ def _declare(lib):
     lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     lib.dpb_md_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp]
     lib.dpb_md_box_history.argtypes = [vp, ctypes.c_int, d64]
+    lib.dpb_md_eval_model.argtypes = [vp, vp, d64, d64]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
               "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
               "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes",
-              "dpb_md_autotune", "dpb_md_box_history"):
+              "dpb_md_autotune", "dpb_md_box_history", "dpb_md_eval_model"):
         getattr(lib, f).restype = ctypes.c_int
     lib._md_declared = True
 
@@ -159,8 +162,21 @@ class Simulation:
         self.model = DeviceModel(params, variables)
         if routine not in ("NVE", "NVT", "NPT"):
             raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT / NPT PIMD)" % routine)
-        if len(model_deviation_paths):
-            raise NotImplementedError("model deviation is not supported")
+        if len(model_deviation_paths) and int(n_bead) > 1:
+            raise NotImplementedError("model_deviation_paths is not supported with n_bead > 1.")
+        # models of the Model_Devi reporter (md.py:299-302,559-567): paths, or
+        # (params, variables) pairs
+        self._dev_models = []
+        for mp in model_deviation_paths:
+            if isinstance(mp, (tuple, list)):
+                dp, dv = mp
+            else:
+                dm_, dv = load_model(mp)
+                dp = dm_.params
+            if int(dp["ntypes"]) != int(params["ntypes"]):
+                raise ValueError("deviation model has %d types, the simulated model %d"
+                                 % (int(dp["ntypes"]), int(params["ntypes"])))
+            self._dev_models.append(DeviceModel(dp, dv))
         if fixed_indices is not None and int(n_bead) > 1:
             raise NotImplementedError("fixed_indices is not supported with n_bead > 1.")
         if fixed_indices is not None and routine not in ("NVE", "NVT"):
@@ -418,6 +434,9 @@ class Simulation:
             for a in sorted(a for g in self._couple_axes for a in g):
                 row.append(box[a])
                 headers.append("box_" + "xyz"[a])
+        if self._dev_models:  # md.py:559-567: max over atoms and axes of the std over models
+            row.append(self.model_deviation())
+            headers.append("Model_Devi")
         self.log_headers = headers + ["Time"]
         row.append(time() - tic)
         headers.append("Time")
@@ -693,6 +712,25 @@ class Simulation:
             mm = m * self._mobile[:, None] if self._mobile is not None else m
             vel = vel - (vel * mm).sum(0) / mm.sum()
         self.setVelocity(vel)
+
+    def _deviation_forces(self):
+        """Forces (n_models, N, 3) of the deviation models on the current
+        positions, box and neighbour list."""
+        out = []
+        for dm in self._dev_models:
+            e = np.zeros(1)
+            f = np.zeros(self._natoms * 3)
+            _lib.check(self.lib.dpb_md_eval_model(self._h, dm.handle, _dptr(e), _dptr(f)), "dpb_md_eval_model")
+            out.append(f.reshape(self._natoms, 3))
+        return np.stack(out)
+
+    def model_deviation(self):
+        """Model_Devi of the current state (deepmd_jax/md.py:559-567): the
+        largest, over atoms and axes, standard deviation of the deviation
+        models' forces."""
+        if not self._dev_models:
+            raise ValueError("no model_deviation_paths were given")
+        return float(self._deviation_forces().std(axis=0).max())
 
     def getPressure(self):
         """Pressure (bar) of the current state: (N kT - dU/d(eps) / 3) / V with

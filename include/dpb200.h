@@ -331,6 +331,12 @@ DPB_API int dpb_md_autotune(dpb_md *md, int *nl_warps, int *dT_warps, void *stre
  * of the last dpb_md_run call: the per-step box of the reference's scan
  * output (deepmd_jax/md.py:784-803, 938); constant except under NPT. */
 DPB_API int dpb_md_box_history(dpb_md *md, int nsteps, double *out);
+/* Energy (host, one value) and forces (host, natoms x 3, user order) of
+ * another model on the engine's current positions, box and neighbour list,
+ * in the engine's precision, fixed atoms' forces zero: one force set of the
+ * reference's Model_Devi reporter (deepmd_jax/md.py:299-302,559-567).
+ * Synchronous; allocates and frees its scratch; not with beads. */
+DPB_API int dpb_md_eval_model(dpb_md *md, const dpb_model *model, double *energy, double *force);
 
 /* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
  * default; not for use inside graph capture).  Stage ids: 0 neighbour

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 import torch
 
+from gpu_helpers import run_gpu
 from make_golden import golden_models
 from oracle import integrators as oi
 from oracle import model as om
@@ -438,3 +439,30 @@ def test_fixed_atoms_nvt_with_com_removal_and_nve_match_oracle():
     with pytest.raises(NotImplementedError):
         Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NPT", 0.5, w["position"],
                    temperature=300.0, pressure=1.0, fixed_indices=[0], verbose=False)
+
+
+def test_model_deviation_reporter_matches_separate_evaluations():
+    """model_deviation_paths (md.py:299-302,559-567): at each report the
+    forces of every deviation model on the current positions and neighbour
+    list; Model_Devi = max over atoms and axes of their standard deviation
+    over models.  Checked against separate FP32 evaluations of the three
+    models on the final positions (relative 1e-4)."""
+    from deepmd_jax_b200.md import Simulation
+    from make_golden import hermite_compressed
+    models = golden_models()
+    p, v = models["B"]
+    devs = [models["B"], models["A"], hermite_compressed(*models["B"])]
+    w = _system()
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.5, w["position"],
+                     initial_velocity=w["velocity"], temperature=300.0, model_deviation_paths=devs,
+                     report_interval=10, verbose=False)
+    sim.run(10)
+    assert sim.log_headers[-2] == "Model_Devi"
+    pos = sim.getPosition()
+    F = np.stack([run_gpu(dp, dv, pos, w["box"], w["type_idx"])["force"][0] for dp, dv in devs])
+    want = F.std(axis=0).max()
+    assert abs(sim.log[-1][-2] - want) <= 1e-4 * want
+    assert abs(sim.model_deviation() - sim.log[-1][-2]) <= 1e-5 * want  # float atomics: last bits may differ
+    with pytest.raises(NotImplementedError):
+        Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.5, w["position"],
+                   temperature=300.0, n_bead=2, model_deviation_paths=devs[:1], verbose=False)
