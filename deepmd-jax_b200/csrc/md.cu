@@ -85,13 +85,15 @@ __global__ void k_com_sum(const float *__restrict__ mom, const float *__restrict
 }
 
 // k_com_sub: the subtraction and the kinetic energy of the new momenta.
+// mask_fixed: the NVE / NVT wrapper zeroes the fixed atoms' momenta after the
+// step (routine.py:130-134); the Langevin step keeps them (routine.py:46-107).
 __global__ void k_com_sub(float *__restrict__ mom, const float *__restrict__ mass, const float *__restrict__ inv_mass,
-                          const float *__restrict__ mobile, int N, MdScalars *sc) {
+                          const float *__restrict__ mobile, int mask_fixed, int N, MdScalars *sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float ke = 0.f;
   if (i < N) {
     const double f = (double)mass[i] / sc->com[3];
-    const bool mob = !mobile || mobile[i] != 0.f;
+    const bool mob = !mobile || !mask_fixed || mobile[i] != 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const float p = (float)((mob ? (double)mom[i * 3 + k] : 0.0) - f * sc->com[k]);
@@ -455,6 +457,34 @@ __device__ __forceinline__ float philox_normal(unsigned long long seed, unsigned
   float sn, cs;
   sincospif(2.f * u2, &sn, &cs);
   return (k & 1u) ? r * sn : r * cs;
+}
+
+// BAOAB Langevin up to the force evaluation (routine.py:81-103): B (dt/2
+// kick), A (dt/2 drift), O (p = c1 p + c2 sqrt(m) xi, xi zero on fixed atoms,
+// the kinetic-energy change added to the thermostat work), A.  Noise: Philox
+// stream (seed, step, tag 3), element atom * 3 + component in sorted order.
+// shift_im is 1/m with fixed atoms at 0 (the masked shift, md.py:231-234).
+__global__ void k_lan_baoa(float *__restrict__ pos, float *__restrict__ mom, const float *__restrict__ force,
+                           const float *__restrict__ mass, const float *__restrict__ inv_mass,
+                           const float *__restrict__ shift_im, const float *__restrict__ mobile, int N, float dt,
+                           float c1, float c2, unsigned long long seed, MdScalars *sc) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  float dw = 0.f;
+  if (e < N * 3) {
+    const int atom = e / 3;
+    const float sim = shift_im[atom];
+    const float p = mom[e] + 0.5f * dt * force[e];
+    float r = pos[e] + 0.5f * dt * p * sim;
+    float xi = philox_normal(seed, (unsigned)sc->step, 3u, (unsigned)e);
+    if (mobile) xi *= mobile[atom];
+    const float pn = c1 * p + c2 * sqrtf(mass[atom]) * xi;
+    dw = 0.5f * (pn * pn - p * p) * inv_mass[atom];
+    r += 0.5f * dt * pn * sim;
+    pos[e] = r;
+    mom[e] = pn;
+  }
+  dw = warp_sum(dw);
+  if ((threadIdx.x & 31) == 0 && dw != 0.f) atomicAdd(&sc->twork, (double)dw);
 }
 
 struct PimdParams {
@@ -889,7 +919,8 @@ static int md_alloc_lists(dpb_md *m) {
 extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_md **out) {
   if (!model || !d || !out || d->natoms <= 0 || d->nbeads <= 0 || !d->type_idx || !d->mass_per_type || !d->sel)
     return DPB_ERR_INVALID_ARG;
-  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_NPT_PIMD) return DPB_ERR_INVALID_ARG;
+  if (d->routine < DPB_MD_NVE || d->routine > DPB_MD_NVT_LANGEVIN) return DPB_ERR_INVALID_ARG;
+  if (d->routine == DPB_MD_NVT_LANGEVIN && !(d->tau_t > 0.0)) return DPB_ERR_UNSUPPORTED;
   const bool has_box = d->routine == DPB_MD_NPT_NHC || d->routine == DPB_MD_NPT_PIMD;
   const bool pimd = d->routine == DPB_MD_PIMD_PILE || d->routine == DPB_MD_NPT_PIMD;
   if (d->routine == DPB_MD_NPT_NHC && (d->nbeads != 1 || d->chain_length < 2 || d->chain_length > kMaxChain ||
@@ -914,8 +945,9 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   if (d->routine == DPB_MD_NVT_NHC && (d->chain_length < 2 || d->chain_length > kMaxChain))
     return DPB_ERR_UNSUPPORTED;
   if (d->n_fixed < 0 || (d->n_fixed > 0 && !d->fixed_indices)) return DPB_ERR_INVALID_ARG;
-  if (d->n_fixed > 0 && d->routine != DPB_MD_NVE && d->routine != DPB_MD_NVT_NHC)
-    return DPB_ERR_UNSUPPORTED;  // fixed atoms: NVE and NVT (md.py:146-147,228-229)
+  if (d->n_fixed > 0 && d->routine != DPB_MD_NVE && d->routine != DPB_MD_NVT_NHC &&
+      d->routine != DPB_MD_NVT_LANGEVIN)
+    return DPB_ERR_UNSUPPORTED;  // fixed atoms: NVE, NVT, NVT Langevin (md.py:146-147,228-229)
   std::vector<char> fixed(d->natoms, 0);
   for (int k = 0; k < d->n_fixed; ++k) {
     const int a = d->fixed_indices[k];
@@ -1246,6 +1278,18 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel,
     k_nptp_c<<<nc, 128, 0, st>>>(m->pos, m->mom, m->force, m->mass, pp, m->np, m->boxd, sc, 1, 1);
     k_nptp_end<<<1, 1, 0, st>>>(m->np, m->virial, m->P, dtd, m->N, 1);
     count_launch(2);
+  } else if (m->d.routine == DPB_MD_NVT_LANGEVIN) {  // routine.py:81-103
+    const double c1 = std::exp(-m->d.dt / m->d.tau_t);
+    const double c2 = std::sqrt(std::max(m->kT * (1.0 - c1 * c1), 0.0));
+    k_lan_baoa<<<nb3, 256, 0, st>>>(m->pos, m->mom, m->force, m->mass, m->inv_mass,
+                                    m->mobile ? m->shift_inv_mass : m->inv_mass, m->mobile, m->N, dt, (float)c1,
+                                    (float)c2, m->d.seed, sc);
+    count_launch();
+    DPB_LAUNCH_CHECK();
+    rc = md_forces(m, st);
+    if (rc) return rc;
+    k_vv_kick<<<nb3, 256, 0, st>>>(m->mom, m->force, m->inv_mass, m->N, NF, dt, sc);
+    count_launch();
   } else if (m->d.routine == DPB_MD_PIMD_PILE) {
     PimdParams pp;
     pp.P = m->P; pp.N = m->N; pp.dt = dt; pp.kT = (float)m->kT; pp.L = L; pp.seed = m->d.seed; pp.tag = 1u;
@@ -1279,7 +1323,8 @@ static int md_step(dpb_md *m, cudaStream_t st, float *traj_pos, float *traj_vel,
   }
   if (m->d.remove_com_motion) {  // after the step, before the frame is emitted (md.py:793-796)
     k_com_sum<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->mobile, m->N, sc);
-    k_com_sub<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->inv_mass, m->mobile, m->N, sc);
+    k_com_sub<<<(m->N + 255) / 256, 256, 0, st>>>(m->mom, m->mass, m->inv_mass, m->mobile,
+                                                  m->d.routine != DPB_MD_NVT_LANGEVIN, m->N, sc);
     count_launch(2);
   }
   if (traj_pos) {

@@ -2,7 +2,8 @@
 
 Mirrors deepmd_jax/md.py:48-1091 (constructor arguments, run(), getters and
 setters, report rows, error-code handling and chunked re-runs) for the
-routines 'NVE' (velocity Verlet), 'NVT' (Nose-Hoover chain), 'NPT' (MTK
+routines 'NVE' (velocity Verlet), 'NVT' (Nose-Hoover chain), 'NVT_langevin'
+(BAOAB Langevin), 'NPT' (MTK
 barostat, coupled axes) and, with n_bead > 1, 'NVT' / 'NPT' path-integral MD
 (ring-polymer BAOAB with PILE-L; Langevin barostat), with centre-of-mass
 removal, fixed atoms and the Model_Devi reporter.  All device work runs in
@@ -160,8 +161,8 @@ class Simulation:
             params = model.params
         self._params = params
         self.model = DeviceModel(params, variables)
-        if routine not in ("NVE", "NVT", "NPT"):
-            raise NotImplementedError("routine %r is outside this engine (NVE, NVT, NPT, NVT / NPT PIMD)" % routine)
+        if routine not in ("NVE", "NVT", "NVT_langevin", "NPT"):
+            raise NotImplementedError("routine currently limited to 'NVE', 'NVT', 'NVT_langevin', 'NPT'")
         if len(model_deviation_paths) and int(n_bead) > 1:
             raise NotImplementedError("model_deviation_paths is not supported with n_bead > 1.")
         # models of the Model_Devi reporter (md.py:299-302,559-567): paths, or
@@ -179,8 +180,8 @@ class Simulation:
             self._dev_models.append(DeviceModel(dp, dv))
         if fixed_indices is not None and int(n_bead) > 1:
             raise NotImplementedError("fixed_indices is not supported with n_bead > 1.")
-        if fixed_indices is not None and routine not in ("NVE", "NVT"):
-            raise NotImplementedError("Fixing atoms currently limited to NVE and NVT routines.")
+        if fixed_indices is not None and routine not in ("NVE", "NVT", "NVT_langevin"):
+            raise NotImplementedError("Fixing atoms currently limited to NVE, NVT, and NVT_langevin routines.")
         if remove_com_motion and int(n_bead) > 1:
             raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
         self._remove_com = bool(remove_com_motion)
@@ -250,8 +251,9 @@ class Simulation:
         self._sel = self._measure_capacity(pos0)
         desc = MDDesc()
         # NVT PIMD: PILE-L (pimd.py:114-207); NPT PIMD: Langevin barostat (pimd.py:255-518)
+        # NVT_langevin: BAOAB with friction 1/tau_t (routine.py:46-107, md.py:352-356)
         desc.routine = ({"NVT": 2, "NPT": 4}[routine] if self._is_pimd
-                        else {"NVE": 0, "NVT": 1, "NPT": 3}[routine])
+                        else {"NVE": 0, "NVT": 1, "NPT": 3, "NVT_langevin": 5}[routine])
         if routine == "NPT":
             desc.pressure = float(pressure) * PRESS_UNIT_CONVERSION
             desc.tau_p = float(tau_p)
@@ -395,6 +397,9 @@ class Simulation:
         headers = ["Step", "Temperature", "KE", "PE"]
         if self._routine == "NVE":
             row.append(KE + PE)
+            headers.append("Invariant")
+        elif self._routine == "NVT_langevin":  # md.py:506-511: KE + PE - thermostat work
+            row.append(KE + PE - r.thermostat_work)
             headers.append("Invariant")
         elif self._routine == "NVT" and not self._is_pimd:
             kT = self._kT

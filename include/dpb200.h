@@ -212,6 +212,8 @@ DPB_API int dpb_eval_noalloc(const dpb_model *model, int precision, const float 
 #define DPB_MD_NPT_NHC 3
 #define DPB_MD_NPT_PIMD 4  /* NPT path-integral MD: Parrinello-Rahman on the centroid
                               mode, PILE-L, Langevin barostat (deepmd_jax/pimd.py:255-518) */
+#define DPB_MD_NVT_LANGEVIN 5  /* BAOAB Langevin, friction 1/tau_t, with the thermostat
+                                  work (deepmd_jax/routine.py:46-107, md.py:352-356) */
 
 typedef struct dpb_md dpb_md;
 
@@ -219,7 +221,7 @@ typedef struct dpb_md dpb_md;
  * arguments).  Units: Angstrom, fs, Dalton, Kelvin. */
 typedef struct {
   int routine;                 /* DPB_MD_NVE, DPB_MD_NVT_NHC, DPB_MD_PIMD_PILE, DPB_MD_NPT_NHC,
-                                  DPB_MD_NPT_PIMD */
+                                  DPB_MD_NPT_PIMD, DPB_MD_NVT_LANGEVIN */
   int natoms;
   int nbeads;                  /* 1, or P ring-polymer beads for PIMD */
   const int *type_idx;         /* [natoms] user order */
@@ -230,7 +232,7 @@ typedef struct {
   double dt;                   /* fs */
   double temperature;          /* K (NVT / PIMD) */
   int chain_length;            /* Nose-Hoover chain length (3) */
-  double tau_t;                /* fs: NHC tau; PIMD centroid friction 1/tau_t */
+  double tau_t;                /* fs: NHC tau; Langevin and PIMD centroid friction 1/tau_t */
   double pimd_lambda;          /* PILE internal-mode damping scale */
   const double *nm_transform;  /* PIMD: (P,P) C, primitive <- normal mode */
   const double *nm_freqs;      /* PIMD: (P) normal-mode frequencies, 1/fs */
@@ -246,7 +248,7 @@ typedef struct {
   int couple_groups[3];        /* group of each axis (0..G-1), -1: fixed axis */
   int remove_com_motion;       /* 1: subtract the centre-of-mass velocity after every step
                                   (md.py:793-796; not with PIMD) */
-  /* Fixed atoms (md.py:221-236, routine.py:110-136; NVE and NVT only):
+  /* Fixed atoms (md.py:221-236, routine.py:110-136; NVE, NVT and NVT Langevin):
    * user indices of atoms that never move.  Their forces read zero (the
    * stop_gradient of md.py:428-430), their momenta are masked, the chain
    * has 3 (N - n_fixed) degrees of freedom.  NULL / 0: every atom mobile. */

@@ -7,6 +7,7 @@ on the reference's hot path.
     and nose_hoover_chain, wrapped by deepmd_jax/routine.py:147-158), chain
     masses Q = kT tau^2 (Q0 *= DOF), DOF = 3N (3 n_mobile with fixed atoms,
     deepmd_jax/routine.py:110-136); invariant per deepmd_jax/routine.py:9-25;
+  * BAOAB Langevin with the thermostat work (deepmd_jax/routine.py:46-107);
   * PIMD BAOAB with exact free ring-polymer propagation and the PILE-L
     thermostat (deepmd_jax/pimd.py:22-44,92-111,114-207,210-247);
   * MTK NPT with Nose-Hoover chains on the particles and on the box, axes in
@@ -126,6 +127,25 @@ def nvt_step(r, p, F, m, dt, kT, chain: NHChain, force_fn, mobile=None):
     chain.KE = kinetic_energy(p, m)
     p = chain.substep(dt, p, kT)
     return r, mask_momenta(p, mobile), F, extra
+
+
+def langevin_step(r, p, F, m, dt, kT, gamma, noise, force_fn, mobile=None):
+    """One BAOAB Langevin step (deepmd_jax/routine.py:81-103): B, A, O with
+    c1 = exp(-gamma dt), c2 = sqrt(kT (1 - c1^2)) and the noise zeroed on
+    fixed atoms, A, force, B.  Returns (r, p, F, extra, dW) with dW the
+    kinetic-energy change of the O step (the thermostat work)."""
+    mob = None if mobile is None else mobile[:, None]
+    p = p + 0.5 * dt * F
+    r = r + 0.5 * dt * p / m * (1 if mob is None else mob)
+    c1 = np.exp(-gamma * dt)
+    c2 = np.sqrt(max(kT * (1.0 - c1 ** 2), 0.0))
+    xi = noise if mob is None else noise * mob
+    pn = c1 * p + c2 * np.sqrt(m) * xi
+    dW = 0.5 * float(((pn ** 2 - p ** 2) / m).sum())
+    r = r + 0.5 * dt * pn / m * (1 if mob is None else mob)
+    F, extra = force_fn(r)
+    pn = pn + 0.5 * dt * F
+    return r, pn, F, extra, dW
 
 
 def sinhx_x(x):

@@ -466,3 +466,49 @@ def test_model_deviation_reporter_matches_separate_evaluations():
     with pytest.raises(NotImplementedError):
         Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.5, w["position"],
                    temperature=300.0, n_bead=2, model_deviation_paths=devs[:1], verbose=False)
+
+
+def test_langevin_matches_oracle_with_shared_noise():
+    """routine='NVT_langevin' (routine.py:46-107, md.py:352-356): BAOAB with
+    friction 1/tau_t, noise from the same Philox stream (tag 3) in the
+    oracle; 10 steps with fixed atoms and centre-of-mass removal (the
+    Langevin step keeps the fixed atoms' momenta, md.py:788-789); positions,
+    velocities and the thermostat work against the float64 oracle, and the
+    Invariant KE + PE - work reported."""
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+    N = len(w["type_idx"])
+    fixed = np.arange(0, N, 9)
+    mob = np.ones(N, dtype=bool)
+    mob[fixed] = False
+    seed = 11
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT_langevin", 0.5, w["position"],
+                     initial_velocity=w["velocity"], temperature=300.0, tau_t=50.0, seed=seed,
+                     fixed_indices=list(fixed), remove_com_motion=True, report_interval=10, verbose=False)
+    traj = sim.run(10)
+    assert sim.log_headers[:5] == ["Step", "Temperature", "KE", "PE", "Invariant"]
+    r_dev = sim._report_struct()
+    m = om.OracleModel(p, v, torch.float64)
+    fn = oi.fixed_atom_forces(_oracle_forces(m, w), mob)
+    mass = (w["mass"] * MU)[:, None]
+    kT = 300.0 * KB
+    perm = np.argsort(w["type_idx"], kind="stable")
+    r, pm = w["position"].copy(), oi.mask_momenta(w["velocity"] * mass, mob)
+    F, _ = fn(r)
+    work = 0.0
+    for step in range(1, 11):
+        ns = philox.normals(N * 3, seed, step, 3).reshape(N, 3)
+        noise = np.empty_like(ns)
+        noise[perm] = ns                          # device draws in type-sorted atom order
+        r, pm, F, _, dW = oi.langevin_step(r, pm, F, mass, 0.5, kT, 1.0 / 50.0, noise, fn, mob)
+        work += dW
+        V = (pm * mob[:, None]).sum(0) / (mass[:, 0] * mob).sum()
+        pm = pm - mass * V
+    assert np.abs(traj["position"][-1] - r).max() < 2e-4
+    vel = pm / mass
+    assert np.abs(traj["velocity"][-1] - vel).max() < 2e-4 * np.abs(vel).max()
+    assert abs(r_dev.thermostat_work - work) <= 2e-3 * abs(work) + 1e-4
+    ke = oi.kinetic_energy(pm, mass)
+    assert abs(sim.log[-1][4] - (sim.log[-1][2] + sim.log[-1][3] - r_dev.thermostat_work)) <= 1e-9
+    assert abs(sim.log[-1][2] - ke) <= 1e-4 * ke
