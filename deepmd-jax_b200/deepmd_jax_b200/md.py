@@ -185,6 +185,7 @@ class Simulation:
         if remove_com_motion and int(n_bead) > 1:
             raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
         self._remove_com = bool(remove_com_motion)
+        self._pimd_print_invariant = bool(pimd_print_invariant) and int(n_bead) > 1
         if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
             raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
         self._n_bead = int(n_bead)
@@ -439,6 +440,12 @@ class Simulation:
             for a in sorted(a for g in self._couple_axes for a in g):
                 row.append(box[a])
                 headers.append("box_" + "xyz"[a])
+            if self._pimd_print_invariant:
+                row.append(self._pimd_invariant(r))
+                headers.append("Invariant")
+        elif self._routine == "NVT" and self._pimd_print_invariant:
+            row.append(self._pimd_invariant(r))
+            headers.append("Invariant")
         if self._dev_models:  # md.py:559-567: max over atoms and axes of the std over models
             row.append(self.model_deviation())
             headers.append("Model_Devi")
@@ -451,6 +458,28 @@ class Simulation:
             print("%-8d " % row[0] + " ".join("%-12.3f" % v for v in row[1:]))
         self.log.append(row)
         return r
+
+    def _pimd_invariant(self, r):
+        """Ring-polymer invariant (deepmd_jax/md.py:512-557): (KE + sum of
+        the bead energies + spring energy - thermostat work) / P, plus under
+        NPT the box kinetic energy, P_target V and minus the box thermostat
+        work.  Spring energy 0.5 m omega_P^2 sum (R_b - R_{b-1})^2 over beads
+        unwrapped onto bead 0's image (pimd.py:82-89,210-227), omega_P = P kT
+        / hbar; float64 on the host from the engine's state."""
+        P = self._n_bead
+        box = np.array(r.box) if self._routine == "NPT" else np.asarray(self._box, dtype=np.float64)
+        R = self.getPosition()
+        d = R - R[0:1]
+        R = R[0:1] + (d - box * np.round(d / box))
+        dR = R - np.roll(R, 1, axis=0)
+        m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
+        omega_P = P * self._kT / HBAR
+        spring = 0.5 * omega_P ** 2 * float((m * dR ** 2).sum())
+        inv = (r.kinetic_energy + r.potential_energy + spring - r.thermostat_work) / P
+        if self._routine == "NPT":
+            inv += sum(0.5 * r.box_momentum[g] ** 2 / r.box_mass[g] for g in range(r.ngroups))
+            inv += self._pressure * PRESS_UNIT_CONVERSION * float(np.prod(box)) - r.box_thermostat_work
+        return inv
 
     # ------------------------------------------------------------------ public API
     def run(self, steps, dump_interval=None, dump_prefix=None, dump_content="positions", dump_mode="overwrite",

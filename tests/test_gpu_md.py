@@ -512,3 +512,33 @@ def test_langevin_matches_oracle_with_shared_noise():
     ke = oi.kinetic_energy(pm, mass)
     assert abs(sim.log[-1][4] - (sim.log[-1][2] + sim.log[-1][3] - r_dev.thermostat_work)) <= 1e-9
     assert abs(sim.log[-1][2] - ke) <= 1e-4 * ke
+
+
+def test_pimd_invariant_reporter_matches_state():
+    """pimd_print_invariant (md.py:512-521): Invariant = (KE + sum of bead
+    energies + spring energy - thermostat work) / P, recomputed from the
+    returned final state with float64 oracle energies and the oracle's
+    unwrap across beads (relative 1e-5)."""
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+    P = 4
+    rng = np.random.default_rng(5)
+    pos = w["position"][None] + rng.normal(scale=0.02, size=(P, 192, 3))
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVT", 0.25, pos,
+                     temperature=300.0, n_bead=P, tau_t=100.0, seed=7, pimd_print_invariant=True,
+                     report_interval=10, verbose=False)
+    traj = sim.run(10)
+    assert sim.log_headers[4] == "Invariant"
+    r_dev = sim._report_struct()
+    m = om.OracleModel(p, v, torch.float64)
+    R, V = traj["position"][-1], traj["velocity"][-1]
+    mass = (w["mass"] * MU)[:, None]
+    E = sum(om.energy_force(m, R[b], w["box"], w["type_idx"], virial=False)["energy"] for b in range(P))
+    KE = 0.5 * float((mass * V ** 2).sum())
+    Ru = oi.unwrap_across_beads(R, w["box"])
+    omega = P * 300.0 * KB / oi.HBAR
+    spring = 0.5 * omega ** 2 * float((mass * (Ru - np.roll(Ru, 1, axis=0)) ** 2).sum())
+    want = (KE + E + spring - r_dev.thermostat_work) / P
+    scale = (abs(E) + KE + spring) / P
+    assert abs(sim.log[-1][4] - want) <= 1e-5 * scale, (sim.log[-1][4], want)
