@@ -1,7 +1,9 @@
 """Host-side logic of the reference-facing API that needs no GPU: the box
 shapes evaluate() accepts and its error message (deepmd_jax/train.py:718-740),
-the neighbour capacity rule (deepmd_jax/md_utils.py:394-403) and the
-conversion between the packed list and the reference's nested nbrs_nm."""
+the neighbour capacity rule (deepmd_jax/md_utils.py:394-403), the
+conversion between the packed list and the reference's nested nbrs_nm, the
+DeepMD data loader and error metrics of test(), periodic_replicate, and the
+host arithmetic of the PIMD Invariant and Model_Devi reporters."""
 import numpy as np
 import pytest
 import torch
@@ -190,3 +192,53 @@ def test_periodic_replicate():
     c3, b3 = periodic_replicate(2, c, np.diag([3.0, 4.0, 5.0]))
     assert np.array_equal(b3, np.diag([6.0, 8.0, 10.0]))
     assert np.allclose(c3[-1], c[-1] + [3.0, 4.0, 5.0])
+
+
+def _stub_simulation(**attrs):
+    """A Simulation object without an engine: only the attributes the
+    report helpers read (no GPU)."""
+    from deepmd_jax_b200.md import Simulation
+    sim = Simulation.__new__(Simulation)
+    for k, v in attrs.items():
+        setattr(sim, k, v)
+    return sim
+
+
+def test_pimd_invariant_formula_on_host():
+    """The ring-polymer Invariant of md.py:512-557 as the host computes it
+    from the engine's report and bead positions: NVT and NPT forms against
+    an independent evaluation with the oracle's unwrap across beads."""
+    import types
+    from oracle import integrators as oi
+    from deepmd_jax_b200.md import PRESS_UNIT_CONVERSION
+    rng = np.random.default_rng(2)
+    P, N = 4, 6
+    box = np.array([7.0, 8.0, 9.0])
+    R = rng.uniform(0, 1, size=(P, N, 3)) * box + rng.integers(-1, 2, size=(P, N, 3)) * box
+    mass = rng.uniform(1, 16, size=N)
+    kT = 300.0 * 8.617333e-5
+    rep = types.SimpleNamespace(kinetic_energy=1.7, potential_energy=-40.2, thermostat_work=0.3,
+                                box=tuple(box * 1.01), ngroups=2, box_momentum=(0.2, -0.1, 0.0),
+                                box_mass=(50.0, 70.0, 1.0), box_thermostat_work=0.05)
+    m = (mass * 103.6427)[:, None]
+    omega = P * kT / oi.HBAR
+    for routine, bx in (("NVT", box), ("NPT", box * 1.01)):
+        sim = _stub_simulation(_n_bead=P, _routine=routine, _box=box, _mass=mass, _kT=kT, _pressure=2.0,
+                               getPosition=lambda: R)
+        Ru = oi.unwrap_across_beads(R, bx)
+        spring = 0.5 * omega ** 2 * float((m * (Ru - np.roll(Ru, 1, axis=0)) ** 2).sum())
+        want = (1.7 - 40.2 + spring - 0.3) / P
+        if routine == "NPT":
+            want += 0.5 * 0.2 ** 2 / 50.0 + 0.5 * 0.1 ** 2 / 70.0 + 2.0 * PRESS_UNIT_CONVERSION * np.prod(bx) - 0.05
+        assert np.isclose(sim._pimd_invariant(rep), want, rtol=1e-12, atol=1e-12)
+
+
+def test_model_deviation_is_max_std_over_models():
+    """Model_Devi (md.py:559-567): max over atoms and axes of the standard
+    deviation (ddof 0) over the deviation models' forces."""
+    rng = np.random.default_rng(4)
+    F = rng.normal(size=(3, 5, 3))
+    sim = _stub_simulation(_dev_models=[object()] * 3, _deviation_forces=lambda: F)
+    assert sim.model_deviation() == pytest.approx(float(np.max(np.std(F, axis=0))))
+    with pytest.raises(ValueError):
+        _stub_simulation(_dev_models=[]).model_deviation()
