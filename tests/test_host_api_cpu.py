@@ -242,3 +242,22 @@ def test_model_deviation_is_max_std_over_models():
     assert sim.model_deviation() == pytest.approx(float(np.max(np.std(F, axis=0))))
     with pytest.raises(ValueError):
         _stub_simulation(_dev_models=[]).model_deviation()
+
+
+@pytest.mark.parametrize("axes,gid", [(((0, 1, 2),), [0, 0, 0]), (((0, 1),), [0, 0, -1]), (((0,),), [0, -1, -1]),
+                                      (((0,), (1,), (2,)), [0, 1, 2]), (((0, 1), (2,)), [0, 0, 1])])
+def test_couple_axes_groups(axes, gid):
+    """couple_axes (deepmd_jax/routine.py:199-229): the documented examples
+    map each axis to its group, -1 for a fixed axis."""
+    from deepmd_jax_b200.md import parse_couple_axes
+    groups, got = parse_couple_axes(axes)
+    assert groups == axes and got == gid
+
+
+@pytest.mark.parametrize("bad,msg", [((0, 1), "tuple of tuples"), (((0, 3),), "must be in"),
+                                     (((0, 1), (1,)), "partition"), (((0,), ()), "non-empty"),
+                                     ((), "at least one group")])
+def test_couple_axes_errors(bad, msg):
+    from deepmd_jax_b200.md import parse_couple_axes
+    with pytest.raises(ValueError, match=msg):
+        parse_couple_axes(bad)
