@@ -50,3 +50,21 @@ def test_oracle_virial_trace_is_strain_derivative():
     em = om.energy_only(m, pos * (1 - eps), box * (1 - eps), typ)[0]
     assert abs((ep - em) / (2 * eps) + np.trace(W)) < 1e-6
     assert np.abs(W - W.T).max() < 1e-10      # rotation invariance -> symmetric
+
+
+def test_normal_modes_match_reference_source():
+    """Ring-polymer normal modes of the reference's pimd.normal_mode_transform
+    (deepmd_jax/pimd.py:22-44, P = 8 at 300 K, golden fixture) against the
+    oracle's and the product host's: frequencies to 1e-12 relative; C
+    orthogonal; and, since eigenvectors of a degenerate pair are defined
+    only up to a rotation, the same projector onto each frequency's modes."""
+    from deepmd_jax_b200.md import normal_mode_transform as host_nm
+    from oracle import integrators as oi
+    P, kT = 8, 300.0 * 8.617333e-5
+    fg, Cg = G["pimd_freqs"], G["pimd_C"]
+    for freqs, C in (oi.normal_mode_transform(P, kT), host_nm(P, kT)):
+        assert np.allclose(freqs, fg, rtol=1e-12, atol=1e-15)
+        assert np.allclose(C.T @ C, np.eye(P), atol=1e-12)
+        for f in np.unique(np.round(fg, 12)):
+            sel = np.isclose(fg, f, rtol=1e-9, atol=1e-15)
+            assert np.allclose(C[:, sel] @ C[:, sel].T, Cg[:, sel] @ Cg[:, sel].T, atol=1e-12)
