@@ -177,7 +177,7 @@ def main(ref_root):
     wE = water_box(4, 9.86, seed=5, n_water=32)
     EE, FE = ref_energy_force(ref, pB, vB, wE["position"], wE["box"], wE["type_idx"])
 
-    # --- ring-polymer normal modes and one PILE-L O step from pimd.py
+    # --- ring-polymer normal modes from pimd.py
     pimd = ref["pimd"]
     kT = 300 * 8.617333e-5
     freqs, C = pimd.normal_mode_transform(8, kT)
