@@ -33,6 +33,8 @@ METRIC = "atom-steps/s, 98k-atom water MD (NVE, dt 0.5 fs), mixed vs plain FP32 
 N_SIDE, BOX = 32, 99.3
 DT = 0.5
 CHUNK = 10
+WORKLOAD = ("98,304-atom water (32,768 H2O, L=99.3 A), NVE velocity Verlet dt 0.5 fs, "
+            "random-init se_a model 25-50-100/240^3/axis 16, rcut 6 A, skin 0.3 A")
 
 
 def parse():
@@ -189,7 +191,8 @@ def reference_arm(args):
     return {"metric": METRIC, "value": val, "unit": "atom-steps/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "water MD NVE; CPU sample: 12,288-atom box (4,096 H2O, L=49.66 A)",
+            "config": {"workload": WORKLOAD, "form": "reference (CPU restatement)", "parallelism": "single",
+                       "cpu_sample": "12,288-atom box (4,096 H2O, L=49.66 A), same model and step",
                        "sample_atoms": N},
             "cpu_baseline": {"value": val, "unit": "atom-steps/s", "cores": threads, "kind": "port",
                              "sample": "%d velocity-Verlet steps of the 12,288-atom water box with the FP32 "
@@ -343,8 +346,7 @@ def gpu_arm(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,
         "warmup": max(args.warmup, 3), "ms_per_step": R["ms"] / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16+f32" if head == "mixed" else "f32", "data": "synthetic",
-        "config": {"workload": "98,304-atom water (32,768 H2O, L=99.3 A), NVE velocity Verlet dt 0.5 fs, "
-                               "random-init se_a model 25-50-100/240^3/axis 16, rcut 6 A, skin 0.3 A",
+        "config": {"workload": WORKLOAD,
                    "form": head, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > L2 (per-step scratch ~2 GB)", "rows_per_atom_within_rcut": rows,
                    "algorithmic_gflop_per_step": flop_atom * N / 1e9},
