@@ -2,9 +2,10 @@
 
 Runs the UNMODIFIED reference integrator source — the NVT ring-polymer step
 (deepmd_jax/pimd.py:114-207), the NPT ring-polymer step with the Langevin
-barostat (pimd.py:299-518) and the classical BAOAB Langevin step with fixed
-atoms (deepmd_jax/routine.py:46-107) — in float64 on the torch-backed jax
-stand-in of jaxshim.py, and writes golden_integrators.npz next to this file.
+barostat (pimd.py:299-518), the classical BAOAB Langevin step with fixed
+atoms (deepmd_jax/routine.py:46-107) and the MTK NPT step with coupled axes
+(routine.py:230-426) — in float64 on the torch-backed jax stand-in of
+jaxshim.py, and writes golden_integrators.npz next to this file.
 
 The potential is a smooth Gaussian pair repulsion under the minimum image,
 evaluated per bead and averaged over beads as the reference's energy_fn is
@@ -15,7 +16,12 @@ replay the same step.  What the reference takes from jax_md (absent here, a
 third-party dependency) is restated from its published definitions:
 momentum_step p += dt F, position_step r = shift(r, dt p / m),
 canonicalize_force = -grad of an energy, canonicalize_mass = identity for an
-(N, 1) mass.  jax.grad / jax.value_and_grad are torch autograd.
+(N, 1) mass, the volume and kinetic energy of `quantity`; the Nose-Hoover
+chain the NPT step calls (jax_md's nose_hoover_chain, with one chain step
+and one Suzuki-Yoshida step) is the oracle's own restatement (oracle/
+integrators.py NHChain), so the NPT fixture pins the barostat, the coupled
+axes and the step order of routine.py but not the chain substep itself.
+jax.grad / jax.value_and_grad are torch autograd.
 
 Usage:  python tests/golden/make_golden_integrators.py [/path/to/reference]
 """
@@ -31,6 +37,7 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 import jaxshim  # noqa: E402
 from jaxshim import J, JArray  # noqa: E402
@@ -122,13 +129,32 @@ def _install_extras():
         position_step=lambda st, shift_fn, dt, **kw: st.set(
             position=shift_fn(st.position, dt * st.momentum / st.mass, **kw)),
         canonicalize_mass=lambda st: st,
+        initialize_momenta=lambda st, key, kT: st.set(momentum=_centred(
+            torch.sqrt(torch.as_tensor(st.mass) * kT) * jaxshim.jrandom.normal(key, tuple(st.position.shape)))),
+        kinetic_energy=lambda st: (0.5 * (torch.as_tensor(st.momentum) ** 2
+                                          / torch.as_tensor(st.mass)).sum()).as_subclass(JArray),
+        default_nhc_kwargs=lambda tau, kw: {"chain_length": 3, "chain_steps": 2, "sy_steps": 3, "tau": tau,
+                                            **(kw or {})},
+        nose_hoover_chain=_nose_hoover_chain,
     )
-    quantity = types.SimpleNamespace(canonicalize_force=lambda fn: (lambda R, **kw: -grad(fn)(R, **kw)))
+    quantity = types.SimpleNamespace(
+        canonicalize_force=lambda fn: (lambda R, **kw: -grad(fn)(R, **kw)),
+        volume=lambda dim, box: torch.prod(torch.as_tensor(box)).as_subclass(JArray),
+        kinetic_energy=lambda momentum=None, mass=None: (0.5 * (torch.as_tensor(momentum) ** 2
+                                                                / torch.as_tensor(mass)).sum()).as_subclass(JArray),
+        count_dof=lambda R: int(np.prod(tuple(torch.as_tensor(R).shape))))
+    util = types.SimpleNamespace(high_precision_sum=lambda x, axis=None: torch.sum(torch.as_tensor(x), dim=axis)
+                                 .as_subclass(JArray))
     jax_md = sys.modules["jax_md"]
     jax_md.simulate = simulate
     jax_md.quantity = quantity
-    jax_md.util = types.SimpleNamespace()
+    jax_md.util = util
     sys.modules["jax_md.simulate"] = simulate
+
+
+def _centred(p):
+    p = torch.as_tensor(p)
+    return (p - torch.mean(p, dim=0, keepdim=True)).as_subclass(JArray)
 
 
 def _noise_queue(arrays):
@@ -145,6 +171,46 @@ def _with_set(cls):
     cls.set = lambda self, **kw: dataclasses.replace(self, **kw)
 
 
+@dataclasses.dataclass
+class _Chain:
+    """jax_md's NoseHooverChain state: xi, p, Q, tau, KE, DOF."""
+    position: object
+    momentum: object
+    mass: object
+    tau: float
+    kinetic_energy: object
+    degrees_of_freedom: float
+
+    def set(self, **kw):
+        return dataclasses.replace(self, **kw)
+
+
+def _nose_hoover_chain(dt, chain_length=3, chain_steps=1, sy_steps=1, tau=100.0):
+    """initialize / update_mass / half_step of jax_md.simulate.nose_hoover_chain
+    for chain_steps = sy_steps = 1, the substep taken from the oracle."""
+    from oracle.integrators import NHChain
+    assert chain_steps == 1 and sy_steps == 1
+    L, dt, tau = chain_length, float(dt), float(tau)
+
+    def masses(kT, dof):
+        Q = kT * tau ** 2 * np.ones(L)
+        Q[0] *= dof
+        return Q
+
+    def initialize(dof, KE, kT):
+        return _Chain(np.zeros(L), np.zeros(L), masses(kT, dof), tau, float(KE), float(dof))
+
+    def update_mass(c, kT):
+        return c.set(mass=masses(kT, c.degrees_of_freedom))
+
+    def half_step(P, c, kT):
+        ch = NHChain(L, c.degrees_of_freedom, kT, tau, float(c.kinetic_energy))
+        ch.xi, ch.p, ch.Q = np.array(c.position), np.array(c.momentum), np.array(c.mass)
+        Pn = ch.substep(dt, np.asarray(torch.as_tensor(P)), kT)
+        return J(Pn), c.set(position=ch.xi, momentum=ch.p, kinetic_energy=ch.KE)
+    return types.SimpleNamespace(initialize=initialize, update_mass=update_mass, half_step=half_step)
+
+
 def main(ref_root):
     import importlib
     _install_extras()
@@ -153,7 +219,8 @@ def main(ref_root):
     sys.modules["deepmd_jax"] = pkg
     pimd = importlib.import_module("deepmd_jax.pimd")
     routine = importlib.import_module("deepmd_jax.routine")
-    for c in (pimd.PIMDLangevinState, pimd.PIMDNPTLangevinState, routine.NVTLangevinStateWithWork):
+    for c in (pimd.PIMDLangevinState, pimd.PIMDNPTLangevinState, routine.NVTLangevinStateWithWork,
+              routine.CachedNPTNoseHooverState):
         _with_set(c)
 
     rng = np.random.default_rng(2024)
@@ -233,6 +300,29 @@ def main(ref_root):
     st = step_fn(st)
     out.update(lan_mobile=mobile, lan_r0=r0, lan_p0=p0, lan_noise=noise, lan_R=st.position.numpy(),
                lan_P=st.momentum.numpy(), lan_F=st.force.numpy(), lan_work=float(st.thermostat_work))
+
+    # --- MTK NPT with NHC thermostat and barostat (routine.py:230-426), axes x alone, y,z coupled
+    gid = np.array([0, 1, 1])
+    tau_t, tau_p, pressure = 40.0, 150.0, 200.0 * 6.241509e-7
+    init_fn, apply_fn = routine.npt_nose_hoover(
+        lambda R, box=None, perturbation=1.0, **kw: energy_fn(R[None], box=box, perturbation=perturbation),
+        lambda R, dR, **kw: R + dR, dt, pressure, kT,
+        barostat_kwargs={"chain_length": 3, "chain_steps": 1, "sy_steps": 1, "tau": tau_p},
+        thermostat_kwargs={"chain_length": 3, "chain_steps": 1, "sy_steps": 1, "tau": tau_t},
+        couple_axes=((0,), (1, 2)))
+    jaxshim._NOISE["fn"] = _noise_queue([np.zeros((N, 3))])      # momenta of init_fn, replaced below
+    r0, p0 = R0[0], P0[0] / np.sqrt(P)
+    st = init_fn(0, J(r0), J(box), mass=J(mass))
+    st = st.set(momentum=J(p0), box_momentum=J(np.array([0.4, -0.3])),
+                thermostat=st.thermostat.set(kinetic_energy=0.5 * float((p0 ** 2 / mass).sum())))
+    out.update(mtk_gid=gid, mtk_tau_t=tau_t, mtk_tau_p=tau_p, mtk_pressure=pressure, mtk_Pb0=np.array([0.4, -0.3]),
+               mtk_dUdV0=st.dUdV.numpy())
+    for _ in range(3):
+        st = apply_fn(st)
+    out.update(mtk_R=st.position.numpy(), mtk_P=st.momentum.numpy(), mtk_F=st.force.numpy(),
+               mtk_Rb=st.box_position.numpy(), mtk_Pb=st.box_momentum.numpy(), mtk_dUdV=st.dUdV.numpy(),
+               mtk_xi=np.asarray(st.thermostat.position), mtk_pxi=np.asarray(st.thermostat.momentum),
+               mtk_bxi=np.asarray(st.barostat.position), mtk_bpxi=np.asarray(st.barostat.momentum))
 
     np.savez_compressed(os.path.join(HERE, "golden_integrators.npz"), **out)
     print("nvt work", out["nvt_work"], "npt box", out["npt_Rb"], "lan work", out["lan_work"])

@@ -3,9 +3,9 @@ integrator source (tests/golden/golden_integrators.npz, written by
 tests/golden/make_golden_integrators.py from deepmd_jax/pimd.py and
 deepmd_jax/routine.py): one NVT ring-polymer BAOAB step with PILE-L, one
 NPT ring-polymer step with the Langevin barostat (axes x, y coupled, z
-alone), and one classical BAOAB Langevin step with fixed atoms, each on a
-Gaussian pair potential with the saved noise.  float64 on both sides:
-agreement to 1e-9 relative."""
+alone), one classical BAOAB Langevin step with fixed atoms and three MTK
+NPT steps, each on a Gaussian pair potential with the saved noise.  float64
+on both sides: agreement to 1e-9 relative."""
 import os
 
 import numpy as np
@@ -94,3 +94,35 @@ def test_langevin_step_with_fixed_atoms_matches_reference():
     _close(F, G["lan_F"], "F")
     _close(dW, G["lan_work"], "work")
     assert np.array_equal(r[~mob], G["lan_r0"][~mob]) and np.all(p[~mob] == 0.0)
+
+
+def test_mtk_npt_steps_match_reference():
+    """Three MTK NPT steps with Nose-Hoover thermostat and barostat chains,
+    axis x alone and y, z coupled (routine.py:230-426).  The chain substep
+    of the fixture is the oracle's restatement of jax_md's (jax_md is
+    absent), so this pins the barostat, the coupled axes and the step order."""
+    m, kT, dt = G["mass"], float(G["kT"]), float(G["dt"])
+    r0 = G["R0"][0]
+    p0 = G["P0"][0] / np.sqrt(float(G["P"]))
+
+    def force_fn(r, box):
+        F, W = _forces_and_virials(r[None], box)
+        return F[0], (float(_bead_energies(r[None], box)[0]), W[0])
+
+    F0, (_, W0) = force_fn(r0, BOX)
+    st = oi.NPTState(r0, p0, F0, W0, m, BOX, float(G["mtk_pressure"]), kT, float(G["mtk_tau_t"]),
+                     float(G["mtk_tau_p"]), G["mtk_gid"])
+    _close(st.dUde, G["mtk_dUdV0"], "dU/deps at init")
+    st.Pb = G["mtk_Pb0"].copy()
+    for _ in range(3):
+        oi.npt_step(st, dt, kT, force_fn)
+    _close(st.r, G["mtk_R"], "R")
+    _close(st.p, G["mtk_P"], "P")
+    _close(st.F, G["mtk_F"], "F")
+    _close(st.Rb, G["mtk_Rb"], "box position")
+    _close(st.Pb, G["mtk_Pb"], "box momentum")
+    _close(st.dUde, G["mtk_dUdV"], "dU/deps")
+    _close(st.thermo.xi, G["mtk_xi"], "thermostat xi")
+    _close(st.thermo.p, G["mtk_pxi"], "thermostat p")
+    _close(st.baro.xi, G["mtk_bxi"], "barostat xi")
+    _close(st.baro.p, G["mtk_bpxi"], "barostat p")
