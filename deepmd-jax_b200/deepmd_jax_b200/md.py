@@ -21,11 +21,11 @@ import torch
 from . import _lib
 from .engine import DeviceModel, NeighborBuilder, sort_by_type, _ptr, _stream
 from . import dump
-from .md_utils import knbr_from_counts
+from .md_utils import knbr_from_counts, print_run_profile
+from .pimd import HBAR, normal_mode_transform, spring_energy, unwrap_across_beads
 from .systems import MASS_UNIT_CONVERSION, TEMP_UNIT_CONVERSION
 from .utils import load_model
 
-HBAR = 6.582119569e-16 * 1e15  # eV fs (deepmd_jax/pimd.py:19)
 
 
 class MDDesc(ctypes.Structure):
@@ -89,19 +89,6 @@ def _declare(lib):
 
 def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-
-
-def normal_mode_transform(n_bead, kT):
-    """Ring-polymer normal modes (deepmd_jax/pimd.py:22-44), numpy eigh."""
-    ring_poly_freq = n_bead * kT / HBAR
-    A = 2 * np.eye(n_bead) - np.roll(np.eye(n_bead), 1, axis=0) - np.roll(np.eye(n_bead), -1, axis=0)
-    eva, eve = np.linalg.eigh(A)
-    order = np.argsort(eva)
-    eva = eva[order]
-    eve = eve[:, order]
-    if n_bead >= 2:
-        eva[0] = 0.0
-    return ring_poly_freq * np.sqrt(np.maximum(eva, 0.0)), eve
 
 
 def sel_from_counts(max_counts, buffer_ratio):
@@ -468,13 +455,8 @@ class Simulation:
         / hbar; float64 on the host from the engine's state."""
         P = self._n_bead
         box = np.array(r.box) if self._routine == "NPT" else np.asarray(self._box, dtype=np.float64)
-        R = self.getPosition()
-        d = R - R[0:1]
-        R = R[0:1] + (d - box * np.round(d / box))
-        dR = R - np.roll(R, 1, axis=0)
         m = (self._mass * MASS_UNIT_CONVERSION)[:, None]
-        omega_P = P * self._kT / HBAR
-        spring = 0.5 * omega_P ** 2 * float((m * dR ** 2).sum())
+        spring = spring_energy(self.getPosition(), m, box, P * self._kT / HBAR)
         inv = (r.kinetic_energy + r.potential_energy + spring - r.thermostat_work) / P
         if self._routine == "NPT":
             inv += sum(0.5 * r.box_momentum[g] ** 2 / r.box_mass[g] for g in range(r.ngroups))
@@ -583,11 +565,8 @@ class Simulation:
         if pending is not None:
             self._copy_out(pending, traj)
         elapsed = time() - tic_run
-        if self.verbose:
-            nsd = 1e-6 * steps * self._dt * (86400 / max(elapsed, 1e-9))
-            print("# Finished %d steps in %.2f s." % (steps, elapsed))
-            print("# Performance: %.3f ns/day, %.3f step/us/atom" %
-                  (nsd, 1e-6 * steps * self._natoms * self._n_bead / (elapsed + 1e-6)))
+        if self.verbose:  # md.py:953,966-967
+            print_run_profile(steps, max(elapsed, 1e-9), self._natoms * self._n_bead, self._dt)
         if self._is_pimd and traj is not None:
             traj["centroid"] = np.stack([self._centroid(p, b) for p, b in zip(traj["position"], traj["box"])])
         return traj
@@ -662,11 +641,7 @@ class Simulation:
             print("# Neighborlist reallocated with size %s" % (self._sel,))
 
     def _centroid(self, R, box=None):
-        box = self._box if box is None else np.asarray(box)
-        ref = R[0:1]
-        d = R - ref
-        d = d - box * np.round(d / box)
-        return (ref + d).mean(0)
+        return unwrap_across_beads(R, self._box if box is None else box).mean(0)
 
     def _state(self):
         shape = (self._n_bead * self._natoms * 3,)

@@ -172,3 +172,26 @@ def exact_neighbor_list(pos, perm, type_count, boxes, rcut):
     for a, b in groups:
         NeighborBuilder(N, b - a, type_count, sel, boxes[a], rcut).build(pos[a:b], perm=perm, nbrs=nbrs[a:b])
     return nbrs, sel
+
+
+def min_image_unwrap(previous_position, current_position, box):
+    """A step's positions moved by whole box vectors onto the image nearest
+    the previous step's (deepmd_jax/md_utils.py:160-167); box (3,) or (3, 3)."""
+    prev = np.asarray(previous_position, dtype=np.float64)
+    cur = np.asarray(current_position, dtype=np.float64)
+    box = np.asarray(box, dtype=np.float64)
+    if box.size == 3:
+        b = box.reshape(3)
+        return prev + np.mod(cur - prev + b / 2, b) - b / 2
+    frac = (cur - prev) @ np.linalg.inv(box)
+    return prev + (frac - np.round(frac)) @ box
+
+
+def print_run_profile(steps, elapsed_time, natoms, dt):
+    """Per-run timing summary of deepmd_jax/md_utils.py:170-177."""
+    steps_per_microsecond_per_atom = 1e-6 * steps * natoms / (elapsed_time + 1e-6)
+    nanosecond_per_day = 1e-6 * steps * dt * (86400 / elapsed_time)
+    print("# Finished %d steps in %dh %dm %ds." %
+          (steps, elapsed_time // 3600, (elapsed_time % 3600) // 60, elapsed_time % 60))
+    print("# Performance: %.3f ns/day, %.3f step/μs/atom" %
+          (nanosecond_per_day, steps_per_microsecond_per_atom))

@@ -261,3 +261,31 @@ def test_couple_axes_errors(bad, msg):
     from deepmd_jax_b200.md import parse_couple_axes
     with pytest.raises(ValueError, match=msg):
         parse_couple_axes(bad)
+
+
+def test_trajectory_helpers_match_oracle():
+    """Host post-processing helpers with the reference's names: bead unwrap,
+    centroid and spring energy (deepmd_jax/pimd.py:82-89,210-248) against the
+    oracle's, and min_image_unwrap (md_utils.py:160-167) for (3,) and
+    diagonal (3, 3) boxes."""
+    from oracle import integrators as oi
+    from deepmd_jax_b200 import pimd
+    from deepmd_jax_b200.md_utils import min_image_unwrap
+    rng = np.random.default_rng(9)
+    box = np.array([5.0, 6.0, 7.0])
+    R = rng.uniform(0, 1, size=(4, 5, 3)) * box + rng.integers(-2, 3, size=(4, 5, 3)) * box
+    assert np.allclose(pimd.unwrap_across_beads(R, box), oi.unwrap_across_beads(R, box), atol=1e-12)
+    assert np.allclose(pimd.unwrap_across_beads(R, np.diag(box)), oi.unwrap_across_beads(R, box), atol=1e-12)
+    assert np.allclose(pimd.centroid(R, box), oi.unwrap_across_beads(R, box).mean(0), atol=1e-12)
+    sim = _stub_simulation(_box=box)  # the centroid frames Simulation.run returns under PIMD
+    assert np.allclose(sim._centroid(R), pimd.centroid(R, box)) and np.allclose(sim._centroid(R, box * 2),
+                                                                                 pimd.centroid(R, box * 2))
+    m = rng.uniform(1, 10, size=(5, 1))
+    Ru = oi.unwrap_across_beads(R, box)
+    want = 0.5 * 0.3 ** 2 * float((m * (Ru - np.roll(Ru, 1, axis=0)) ** 2).sum())
+    assert np.isclose(pimd.spring_energy(R, m, box, 0.3), want, rtol=1e-12)
+    prev = rng.uniform(0, 1, size=(5, 3)) * box
+    cur = prev + rng.normal(scale=0.1, size=(5, 3)) + rng.integers(-1, 2, size=(5, 3)) * box
+    want = oi.min_image_unwrap(prev, cur, box)
+    assert np.allclose(min_image_unwrap(prev, cur, box), want, atol=1e-12)
+    assert np.allclose(min_image_unwrap(prev, cur, np.diag(box)), want, atol=1e-12)
