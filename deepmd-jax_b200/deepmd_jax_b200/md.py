@@ -147,11 +147,43 @@ class Simulation:
             model, variables = load_model(model_path)
             params = model.params
         self._params = params
-        self.model = DeviceModel(params, variables)
+        # argument checks before any device work, with the reference's
+        # messages (md.py:136-165,176-181,242-244,228-229,324,382-383)
+        if float(pimd_lambda) < 0:
+            raise ValueError("pimd_lambda must be non-negative.")
+        if int(n_bead) > 1:
+            if routine not in ("NVT", "NPT"):
+                raise NotImplementedError(
+                    "Path-integral MD (n_bead > 1) currently supports routine='NVT' or 'NPT'.")
+            if fixed_indices is not None:
+                raise NotImplementedError("fixed_indices is not supported with n_bead > 1.")
+            if len(model_deviation_paths) > 0:
+                raise NotImplementedError("model_deviation_paths is not supported with n_bead > 1.")
+            if remove_com_motion:
+                raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
+            if np.ndim(initial_position) not in (2, 3):
+                raise ValueError("initial_position must have shape (N,3) or (P,N,3).")
+        ct = params.get("chemical_types")
+        if ct is not None:
+            unknown = set(np.asarray(type_idx, dtype=int).tolist()) - set(ct)
+            if unknown:
+                raise ValueError('Atomic numbers %s in type_idx are not in model.params["chemical_types"]=%s'
+                                 % (sorted(unknown), ct))
+        if not (isinstance(couple_axes, tuple) and couple_axes == ((0, 1, 2),)) and "NPT" not in routine:
+            raise ValueError("couple_axes is only meaningful for routine='NPT'")
         if routine not in ("NVE", "NVT", "NVT_langevin", "NPT"):
             raise NotImplementedError("routine currently limited to 'NVE', 'NVT', 'NVT_langevin', 'NPT'")
-        if len(model_deviation_paths) and int(n_bead) > 1:
-            raise NotImplementedError("model_deviation_paths is not supported with n_bead > 1.")
+        if fixed_indices is not None and routine not in ("NVE", "NVT", "NVT_langevin"):
+            raise NotImplementedError("Fixing atoms currently limited to NVE, NVT, and NVT_langevin routines.")
+        if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
+            raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
+        if routine == "NPT":
+            if pressure is None:
+                raise ValueError("Missing argument 'pressure' (in bar) for routine 'NPT'")
+            if temperature is None:
+                raise ValueError("Missing argument 'temperature' for routine 'NPT'")
+            self._couple_axes, self._group_ids = parse_couple_axes(couple_axes)
+        self.model = DeviceModel(params, variables)
         # models of the Model_Devi reporter (md.py:299-302,559-567): paths, or
         # (params, variables) pairs
         self._dev_models = []
@@ -165,26 +197,10 @@ class Simulation:
                 raise ValueError("deviation model has %d types, the simulated model %d"
                                  % (int(dp["ntypes"]), int(params["ntypes"])))
             self._dev_models.append(DeviceModel(dp, dv))
-        if fixed_indices is not None and int(n_bead) > 1:
-            raise NotImplementedError("fixed_indices is not supported with n_bead > 1.")
-        if fixed_indices is not None and routine not in ("NVE", "NVT", "NVT_langevin"):
-            raise NotImplementedError("Fixing atoms currently limited to NVE, NVT, and NVT_langevin routines.")
-        if remove_com_motion and int(n_bead) > 1:
-            raise NotImplementedError("remove_com_motion is not supported with n_bead > 1.")
         self._remove_com = bool(remove_com_motion)
         self._pimd_print_invariant = bool(pimd_print_invariant) and int(n_bead) > 1
-        if chain_steps_t != 1 or sy_steps_t != 1 or chain_steps_p != 1 or sy_steps_p != 1:
-            raise NotImplementedError("Nose-Hoover chain_steps/sy_steps other than 1")
         self._n_bead = int(n_bead)
         self._is_pimd = self._n_bead > 1
-        if self._is_pimd and routine not in ("NVT", "NPT"):
-            raise NotImplementedError("Path-integral MD (n_bead > 1) supports routine='NVT' or 'NPT'.")
-        if routine == "NPT":
-            if pressure is None:
-                raise ValueError("Missing argument 'pressure' (in bar) for routine 'NPT'")
-            if temperature is None:
-                raise ValueError("Missing argument 'temperature' for routine 'NPT'")
-            self._couple_axes, self._group_ids = parse_couple_axes(couple_axes)
         self._pressure = pressure
         pos0 = np.asarray(initial_position, dtype=np.float64)
         if self._is_pimd:
@@ -213,7 +229,6 @@ class Simulation:
         self._debug = debug
         self.precision = precision
         self._type_idx = np.asarray(type_idx, dtype=np.int32)
-        ct = params.get("chemical_types")
         if ct is not None:
             z2i = {z: i for i, z in enumerate(ct)}
             self._type_idx = np.array([z2i[int(z)] for z in self._type_idx], dtype=np.int32)

@@ -289,3 +289,44 @@ def test_trajectory_helpers_match_oracle():
     want = oi.min_image_unwrap(prev, cur, box)
     assert np.allclose(min_image_unwrap(prev, cur, box), want, atol=1e-12)
     assert np.allclose(min_image_unwrap(prev, cur, np.diag(box)), want, atol=1e-12)
+
+
+@pytest.mark.parametrize("kw,exc,msg", [
+    (dict(routine="NVT", pimd_lambda=-1.0), ValueError, "pimd_lambda must be non-negative"),
+    (dict(routine="NVE", n_bead=2), NotImplementedError, "currently supports routine='NVT' or 'NPT'"),
+    (dict(routine="NVT", n_bead=2, fixed_indices=[0]), NotImplementedError, "fixed_indices is not supported"),
+    (dict(routine="NVT", n_bead=2, model_deviation_paths=["m.pkl"]), NotImplementedError,
+     "model_deviation_paths is not supported"),
+    (dict(routine="NVT", n_bead=2, remove_com_motion=True), NotImplementedError, "remove_com_motion is not"),
+    (dict(routine="NVT", couple_axes=((0, 1),)), ValueError, "couple_axes is only meaningful"),
+    (dict(routine="NVT_berendsen"), NotImplementedError, "routine currently limited"),
+    (dict(routine="NPT", fixed_indices=[0], pressure=1.0), NotImplementedError, "Fixing atoms currently limited"),
+    (dict(routine="NPT"), ValueError, "Missing argument 'pressure'"),
+    (dict(routine="NPT", pressure=1.0, couple_axes=((0, 0),)), ValueError, "partition"),
+])
+def test_simulation_argument_errors_before_device_work(kw, exc, msg):
+    """Simulation's argument checks run before any device work and raise what
+    the reference raises (deepmd_jax/md.py:136-165,242-244,228-229,324,
+    382-383), so they hold on a machine without a GPU."""
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import init_dp_params, water_box
+    p, v = init_dp_params(seed=0)
+    w = water_box(2, 6.21, seed=0)
+    args = dict(temperature=300.0)
+    args.update(kw)
+    routine = args.pop("routine")
+    with pytest.raises(exc, match=msg):
+        Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], routine, 0.5, w["position"], **args)
+
+
+def test_simulation_rejects_unknown_atomic_numbers():
+    """type_idx holds atomic numbers when the model carries chemical_types;
+    unknown ones raise the reference's ValueError (md.py:176-181)."""
+    from deepmd_jax_b200.md import Simulation
+    from deepmd_jax_b200.systems import init_dp_params, water_box
+    p, v = init_dp_params(seed=0)
+    p = dict(p, chemical_types=(8, 1))
+    w = water_box(2, 6.21, seed=0)
+    z = np.where(w["type_idx"] == 0, 8, 6)
+    with pytest.raises(ValueError, match="not in model.params"):
+        Simulation((p, v), w["box"], z, w["mass_per_type"], "NVE", 0.5, w["position"])
