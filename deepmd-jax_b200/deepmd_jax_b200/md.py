@@ -692,13 +692,29 @@ class Simulation:
         return np.array(self._report_struct().virial).reshape(3, 3)
 
     def setPosition(self, position, box=None):
-        if box is not None:
-            raise ValueError("Box can only be changed in NPT simulations.")
+        """Set the positions (deepmd_jax/md.py:984-1015): (N, 3), or (P, N, 3)
+        / (N, 3) broadcast over beads; forces follow at once.  A new box is
+        refused outside NPT as in the reference; under NPT the device-side
+        barostat box is not reset from the host, so a box change raises
+        NotImplementedError (after the reference's own checks)."""
         pos = np.asarray(position, dtype=np.float64)
         if self._is_pimd and pos.ndim == 2:
             pos = np.broadcast_to(pos, self._frame_shape())
         if pos.shape != self._frame_shape():
-            raise ValueError("Position must have the same shape as the initial position.")
+            raise ValueError("Position must have the same shape as the initial position, "
+                             "or you have to create a new Simulation instance.")
+        if box is not None:
+            if "NPT" not in self._routine:
+                raise ValueError("Box can only be changed in NPT simulations.")
+            box = np.asarray(box, dtype=np.float64)
+            if box.size == 1:
+                box = box.item() * np.ones(3)
+            cur = self.getBox()
+            if box.shape != cur.shape:
+                raise ValueError("Box must have the same shape as the initial box.")
+            if not np.allclose(box, cur * (box[0] / cur[0]), rtol=1e-4, atol=1e-6):
+                raise ValueError("Only isotropic box fluctuations are allowed in the current implementation.")
+            raise NotImplementedError("setPosition(box=...) under NPT is not supported by the device engine")
         self._set_pos(pos)
         _lib.check(self.lib.dpb_md_init(self._h, 0, _stream()), "dpb_md_init")
         if int(self._report_struct().status) & 2:

@@ -330,3 +330,21 @@ def test_simulation_rejects_unknown_atomic_numbers():
     z = np.where(w["type_idx"] == 0, 8, 6)
     with pytest.raises(ValueError, match="not in model.params"):
         Simulation((p, v), w["box"], z, w["mass_per_type"], "NVE", 0.5, w["position"])
+
+
+def test_set_position_argument_errors():
+    """setPosition's checks (deepmd_jax/md.py:989-1006) on a stub engine:
+    wrong shape, a box outside NPT, a box of another shape or an
+    anisotropic change under NPT."""
+    sim = _stub_simulation(_is_pimd=False, _routine="NVT", _natoms=3, _n_bead=1,
+                           getBox=lambda: np.array([5.0, 5.0, 6.0]))
+    sim._frame_shape = lambda: (3, 3)
+    with pytest.raises(ValueError, match="same shape as the initial position"):
+        sim.setPosition(np.zeros((4, 3)))
+    with pytest.raises(ValueError, match="only be changed in NPT"):
+        sim.setPosition(np.zeros((3, 3)), box=5.0)
+    sim._routine = "NPT"
+    with pytest.raises(ValueError, match="same shape as the initial box"):
+        sim.setPosition(np.zeros((3, 3)), box=np.eye(3))
+    with pytest.raises(ValueError, match="isotropic"):
+        sim.setPosition(np.zeros((3, 3)), box=[5.0, 5.5, 6.0])
