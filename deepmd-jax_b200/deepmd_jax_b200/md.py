@@ -495,8 +495,12 @@ class Simulation:
         fs = self._frame_shape()
         traj = None
         if trajectory:
-            traj = {"position": np.zeros((L,) + fs), "velocity": np.zeros((L,) + fs),
-                    "box": np.tile(self._box, (L, 1))}
+            try:
+                traj = {"position": np.zeros((L,) + fs), "velocity": np.zeros((L,) + fs),
+                        "box": np.tile(self._box, (L, 1))}
+            except MemoryError:  # md.py:849-850
+                raise MemoryError("Trajectory too large to fit in CPU RAM. Please pass dump_prefix=... to stream "
+                                  "to disk, or split into multiple shorter runs.")
         if first and trajectory:
             traj["position"][0] = self.getPosition()
             traj["velocity"][0] = self.getVelocity()
