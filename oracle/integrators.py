@@ -21,9 +21,10 @@ jax_md is a third-party dependency that is absent here (unpinned git HEAD,
 setup.py:13); the Nose-Hoover substep below restates its published MTK
 algorithm (Martyna, Tuckerman, Tobias, Klein, Mol. Phys. 87, 1117 (1996)) with
 the operator order used by jax_md.  Parity of that order is unpinned.
-The ring-polymer steps (NVT and NPT), the BAOAB Langevin step and the MTK
-NPT step (all but its chain substep) are pinned to the reference's own
-source by tests/test_oracle_integrators_golden.py.
+The ring-polymer steps (NVT and NPT), the BAOAB Langevin step, the MTK NPT
+step (all but its chain substep) and the fixed-atom wrapper of NVE / NVT
+are pinned to the reference's own source by
+tests/test_oracle_integrators_golden.py.
 The Gaussian noise of the stochastic steps comes from oracle/philox.py, the
 same counter-based stream the device kernels draw, so a step can be compared
 deterministically.

@@ -3,8 +3,9 @@
 Runs the UNMODIFIED reference integrator source — the NVT ring-polymer step
 (deepmd_jax/pimd.py:114-207), the NPT ring-polymer step with the Langevin
 barostat (pimd.py:299-518), the classical BAOAB Langevin step with fixed
-atoms (deepmd_jax/routine.py:46-107) and the MTK NPT step with coupled axes
-(routine.py:230-426) — in float64 on the torch-backed jax stand-in of
+atoms (deepmd_jax/routine.py:46-107), the MTK NPT step with coupled axes
+(routine.py:230-426) and the fixed-atom wrapper of NVE and Nose-Hoover NVT
+(routine.py:110-158) — in float64 on the torch-backed jax stand-in of
 jaxshim.py, and writes golden_integrators.npz next to this file.
 
 The potential is a smooth Gaussian pair repulsion under the minimum image,
@@ -20,7 +21,10 @@ canonicalize_force = -grad of an energy, canonicalize_mass = identity for an
 chain the NPT step calls (jax_md's nose_hoover_chain, with one chain step
 and one Suzuki-Yoshida step) is the oracle's own restatement (oracle/
 integrators.py NHChain), so the NPT fixture pins the barostat, the coupled
-axes and the step order of routine.py but not the chain substep itself.
+axes and the step order of routine.py but not the chain substep itself;
+likewise jax_md's nve / nvt_nose_hoover (velocity Verlet, chain half steps
+around it) are restated, so the fixed-atom fixtures pin the wrapper's
+masking and its chain degrees of freedom, mass and kinetic energy.
 jax.grad / jax.value_and_grad are torch autograd.
 
 Usage:  python tests/golden/make_golden_integrators.py [/path/to/reference]
@@ -89,6 +93,7 @@ def _install_extras():
     jnp.float32 = f64
     jnp.isscalar = lambda x: np.isscalar(x)
     JArray.size = property(lambda self: _SizeInt(self))
+    JArray.at = property(lambda self: _At(self))
     JArray.mean = lambda self, axis=None, keepdims=False: (
         torch.Tensor.mean(self) if axis is None else torch.Tensor.mean(self, dim=axis, keepdim=keepdims))
     jaxshim.jrandom.split = lambda key, n=2: tuple([key] * n)
@@ -131,8 +136,9 @@ def _install_extras():
         canonicalize_mass=lambda st: st,
         initialize_momenta=lambda st, key, kT: st.set(momentum=_centred(
             torch.sqrt(torch.as_tensor(st.mass) * kT) * jaxshim.jrandom.normal(key, tuple(st.position.shape)))),
-        kinetic_energy=lambda st: (0.5 * (torch.as_tensor(st.momentum) ** 2
-                                          / torch.as_tensor(st.mass)).sum()).as_subclass(JArray),
+        kinetic_energy=_kinetic,
+        nve=_nve,
+        nvt_nose_hoover=_nvt_nose_hoover,
         default_nhc_kwargs=lambda tau, kw: {"chain_length": 3, "chain_steps": 2, "sy_steps": 3, "tau": tau,
                                             **(kw or {})},
         nose_hoover_chain=_nose_hoover_chain,
@@ -183,6 +189,91 @@ class _Chain:
 
     def set(self, **kw):
         return dataclasses.replace(self, **kw)
+
+
+@dataclasses.dataclass
+class _NVEState:
+    position: object
+    momentum: object
+    force: object
+    mass: object
+
+    velocity = property(lambda self: self.momentum / self.mass)
+
+    def set(self, **kw):
+        return dataclasses.replace(self, **kw)
+
+
+@dataclasses.dataclass
+class _NVTState(_NVEState):
+    chain: object = None
+
+
+def _kinetic(st):
+    return (0.5 * (torch.as_tensor(st.momentum) ** 2 / torch.as_tensor(st.mass)).sum()).as_subclass(JArray)
+
+
+def _momenta(R, mass, kT):
+    """jax_md initialize_momenta: sqrt(m kT) N(0, 1), mean momentum removed."""
+    p = torch.sqrt(torch.as_tensor(mass) * kT) * jaxshim.jrandom.normal(0, tuple(torch.as_tensor(R).shape))
+    return _centred(p)
+
+
+def _velocity_verlet(force_fn, shift_fn, dt, st, **kw):
+    st = st.set(momentum=st.momentum + 0.5 * dt * st.force)
+    st = st.set(position=shift_fn(st.position, dt * st.momentum / st.mass, **kw))
+    st = st.set(force=force_fn(st.position, **kw))
+    return st.set(momentum=st.momentum + 0.5 * dt * st.force)
+
+
+def _nve(energy_fn, shift_fn, dt, **kw):
+    """jax_md.simulate.nve: velocity Verlet."""
+    force_fn = lambda R, **k: -jaxshim.jax.grad(energy_fn)(R, **k)  # noqa: E731
+
+    def init_fn(key, R, mass=1.0, kT=0.0, **k):
+        return _NVEState(R, _momenta(R, mass, kT), force_fn(R, **k), mass)
+
+    def apply_fn(st, **k):
+        return _velocity_verlet(force_fn, shift_fn, dt, st, **k)
+    return init_fn, apply_fn
+
+
+def _nvt_nose_hoover(energy_fn, shift_fn, dt, kT, tau=None, chain_length=3, chain_steps=1, sy_steps=1):
+    """jax_md.simulate.nvt_nose_hoover: chain half step, velocity Verlet,
+    chain half step, the chain masses refreshed first."""
+    force_fn = lambda R, **k: -jaxshim.jax.grad(energy_fn)(R, **k)  # noqa: E731
+    chain = _nose_hoover_chain(dt, chain_length, chain_steps, sy_steps, tau)
+
+    def init_fn(key, R, mass=1.0, **k):
+        st = _NVTState(R, _momenta(R, mass, kT), force_fn(R, **k), mass)
+        c = chain.initialize(int(np.prod(tuple(torch.as_tensor(R).shape))), float(_kinetic(st)), kT)
+        return st.set(chain=c.set(mass=J(c.mass)))
+
+    def apply_fn(st, **k):
+        c = chain.update_mass(st.chain, kT)
+        p, c = chain.half_step(st.momentum, c, kT)
+        st = _velocity_verlet(force_fn, shift_fn, dt, st.set(momentum=p), **k)
+        c = c.set(kinetic_energy=float(_kinetic(st)))
+        p, c = chain.half_step(st.momentum, c, kT)
+        return st.set(momentum=p, chain=c)
+    return init_fn, apply_fn
+
+
+class _At:
+    """x.at[i].multiply(v) / .set(v) / .add(v) of jax arrays, out of place."""
+
+    def __init__(self, x):
+        self.x = x
+
+    def __getitem__(self, idx):
+        x = self.x
+
+        def upd(fn):
+            y = torch.as_tensor(x).clone()
+            y[idx] = fn(y[idx])
+            return y.as_subclass(JArray)
+        return types.SimpleNamespace(multiply=lambda v: upd(lambda a: a * v), set=lambda v: upd(lambda a: a * 0 + v),
+                                     add=lambda v: upd(lambda a: a + v))
 
 
 def _nose_hoover_chain(dt, chain_length=3, chain_steps=1, sy_steps=1, tau=100.0):
@@ -300,6 +391,25 @@ def main(ref_root):
     st = step_fn(st)
     out.update(lan_mobile=mobile, lan_r0=r0, lan_p0=p0, lan_noise=noise, lan_R=st.position.numpy(),
                lan_P=st.momentum.numpy(), lan_F=st.force.numpy(), lan_work=float(st.thermostat_work))
+
+    # --- fixed atoms under NVE and Nose-Hoover NVT (routine.py:110-158), three steps each
+    for name, make in (("fnve", lambda: routine.nve(e1, shift, dt, mobile_mask=J(mobile))),
+                       ("fnvt", lambda: routine.nvt_nose_hoover(e1, shift, dt, kT, tau=60.0, chain_length=3,
+                                                                chain_steps=1, sy_steps=1,
+                                                                mobile_mask=J(mobile)))):
+        init_fn, apply_fn = make()
+        noise = rng.normal(size=(N, 3))
+        jaxshim._NOISE["fn"] = _noise_queue([noise])
+        st = init_fn(0, J(r0), mass=J(mass), kT=kT) if name == "fnve" else init_fn(0, J(r0), mass=J(mass))
+        out[name + "_p0"] = st.momentum.numpy().copy()
+        if name == "fnvt":
+            out[name + "_Q0"] = np.asarray(st.chain.mass)
+            out[name + "_KE0"] = float(st.chain.kinetic_energy)
+        for _ in range(3):
+            st = apply_fn(st)
+        out[name + "_R"], out[name + "_P"] = st.position.numpy(), st.momentum.numpy()
+        if name == "fnvt":
+            out[name + "_xi"], out[name + "_pxi"] = np.asarray(st.chain.position), np.asarray(st.chain.momentum)
 
     # --- MTK NPT with NHC thermostat and barostat (routine.py:230-426), axes x alone, y,z coupled
     gid = np.array([0, 1, 1])

@@ -126,3 +126,37 @@ def test_mtk_npt_steps_match_reference():
     _close(st.thermo.p, G["mtk_pxi"], "thermostat p")
     _close(st.baro.xi, G["mtk_bxi"], "barostat xi")
     _close(st.baro.p, G["mtk_bpxi"], "barostat p")
+
+
+def test_fixed_atom_wrapper_nve_and_nvt_match_reference():
+    """with_fixed_atoms around NVE and Nose-Hoover NVT (routine.py:110-158),
+    three steps each: momenta masked at init and after every step, fixed
+    coordinates under stop_gradient, the masked shift of md.py:231-234, and
+    for NVT the chain over 3 n_mobile degrees of freedom with
+    Q0 = kT tau^2 DOF and the initial kinetic energy of the masked momenta.
+    jax_md's own NVE / NVT steps are restated in the fixture, so this pins
+    the wrapper."""
+    m, mob, kT, dt = G["mass"], G["lan_mobile"], float(G["kT"]), float(G["dt"])
+    fn = oi.fixed_atom_forces(lambda r: (_forces(r[None], BOX)[0], None), mob)
+    r0 = G["lan_r0"]
+    # NVE
+    p = G["fnve_p0"].copy()
+    assert np.all(p[~mob] == 0.0)
+    r, (F, _) = r0.copy(), fn(r0)
+    for _ in range(3):
+        r, p, F, _ = oi.vv_step(r, p, F, m, dt, fn, mob)
+        p = oi.mask_momenta(p, mob)
+    _close(r, G["fnve_R"], "NVE R")
+    _close(p, G["fnve_P"], "NVE P")
+    # NVT
+    p = G["fnvt_p0"].copy()
+    chain = oi.NHChain(3, 3 * int(mob.sum()), kT, 60.0, oi.kinetic_energy(p, m))
+    _close(chain.Q, G["fnvt_Q0"], "chain masses at init")
+    _close(chain.KE, G["fnvt_KE0"], "chain KE at init")
+    r, (F, _) = r0.copy(), fn(r0)
+    for _ in range(3):
+        r, p, F, _ = oi.nvt_step(r, p, F, m, dt, kT, chain, fn, mob)
+    _close(r, G["fnvt_R"], "NVT R")
+    _close(p, G["fnvt_P"], "NVT P")
+    _close(chain.xi, G["fnvt_xi"], "chain xi")
+    _close(chain.p, G["fnvt_pxi"], "chain p")
