@@ -469,7 +469,7 @@ __global__ void k_lan_baoa(float *__restrict__ pos, float *__restrict__ mom, con
                            const float *__restrict__ shift_im, const float *__restrict__ mobile, int N, float dt,
                            float c1, float c2, unsigned long long seed, MdScalars *sc) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  float dw = 0.f;
+  double dw = 0.0;
   if (e < N * 3) {
     const int atom = e / 3;
     const float sim = shift_im[atom];
@@ -478,13 +478,15 @@ __global__ void k_lan_baoa(float *__restrict__ pos, float *__restrict__ mom, con
     float xi = philox_normal(seed, (unsigned)sc->step, 3u, (unsigned)e);
     if (mobile) xi *= mobile[atom];
     const float pn = c1 * p + c2 * sqrtf(mass[atom]) * xi;
-    dw = 0.5f * (pn * pn - p * p) * inv_mass[atom];
+    // kinetic-energy change in FP64, factored to avoid the cancellation of pn^2 - p^2
+    dw = 0.5 * ((double)pn - (double)p) * ((double)pn + (double)p) * (double)inv_mass[atom];
     r += 0.5f * dt * pn * sim;
     pos[e] = r;
     mom[e] = pn;
   }
-  dw = warp_sum(dw);
-  if ((threadIdx.x & 31) == 0 && dw != 0.f) atomicAdd(&sc->twork, (double)dw);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dw += __shfl_xor_sync(0xffffffffu, dw, o);
+  if ((threadIdx.x & 31) == 0 && dw != 0.0) atomicAdd(&sc->twork, dw);
 }
 
 struct PimdParams {
@@ -509,7 +511,7 @@ __global__ void k_pimd_baoa(float *__restrict__ pos, float *__restrict__ mom, co
   __syncthreads();
   const int col = blockIdx.x * blockDim.x + threadIdx.x;  // atom * 3 + comp
   const int N3 = pp.N * 3;
-  float dke = 0.f;
+  double dke = 0.0;
   if (col < N3) {
     const int atom = col / 3, comp = col - atom * 3;
     const float Lc = comp == 0 ? pp.L.x : (comp == 1 ? pp.L.y : pp.L.z);
@@ -565,7 +567,7 @@ __global__ void k_pimd_baoa(float *__restrict__ pos, float *__restrict__ mom, co
           pv = fmaf(C[b * P + k], Pn[k], pv);
         }
         if (pass == 1) {
-          dke += 0.5f * (pv * pv - Pm[b] * Pm[b]) / m;
+          dke += 0.5 * ((double)pv - (double)Pm[b]) * ((double)pv + (double)Pm[b]) / (double)m;
         } else {
           R[b] = r;
         }
@@ -579,8 +581,9 @@ __global__ void k_pimd_baoa(float *__restrict__ pos, float *__restrict__ mom, co
       mom[(size_t)b * N3 + col] = Pm[b];
     }
   }
-  dke = warp_sum(dke);
-  if ((threadIdx.x & 31) == 0 && dke != 0.f) atomicAdd(&sc->twork, (double)dke);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dke += __shfl_xor_sync(0xffffffffu, dke, o);
+  if ((threadIdx.x & 31) == 0 && dke != 0.0) atomicAdd(&sc->twork, dke);
 }
 
 // ---------------------------------------------------------------- NPT-PIMD
@@ -752,7 +755,7 @@ __global__ void k_nptp_a(float *__restrict__ pos, float *__restrict__ mom, const
   __syncthreads();
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int N3 = pp.N * 3;
-  float dke = 0.f;
+  double dke = 0.0;
   if (col < N3) {
     const int atom = col / 3, comp = col - atom * 3;
     const float Lc = boxd[comp], m = mass[atom], h = 0.5f * pp.dt;
@@ -777,13 +780,14 @@ __global__ void k_nptp_a(float *__restrict__ pos, float *__restrict__ mom, const
     for (int b = 0; b < P; ++b) {
       float pv = 0.f;
       for (int k = 0; k < P; ++k) pv = fmaf(C[b * P + k], Pn[k], pv);
-      dke += 0.5f * (pv * pv - Pm[b] * Pm[b]) / m;
+      dke += 0.5 * ((double)pv - (double)Pm[b]) * ((double)pv + (double)Pm[b]) / (double)m;
       pos[(size_t)b * N3 + col] = R[b];
       mom[(size_t)b * N3 + col] = pv;
     }
   }
-  dke = warp_sum(dke);
-  if ((threadIdx.x & 31) == 0 && dke != 0.f) atomicAdd(&sc->twork, (double)dke);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dke += __shfl_xor_sync(0xffffffffu, dke, o);
+  if ((threadIdx.x & 31) == 0 && dke != 0.0) atomicAdd(&sc->twork, dke);
 }
 
 // A (centroid drift + internal ring, second box), then the per-bead

@@ -16,14 +16,19 @@
 //   * every GPU that loads the library holds this array until the process
 //     exits;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress with that device current) and caches it; make that
-//     first call before capturing a stream into a CUDA graph;
+//     (cudaGetSymbolAddress with that device current) and caches it, keyed
+//     on the unique id of the CUDA context current at the time; make that
+//     first call before capturing a stream into a CUDA graph.  A device reset
+//     (cudaDeviceReset) or a re-created primary context gives a new context
+//     id, so the next call looks the address up again instead of using a
+//     stale one (the first call after a reset is then again a set-up call);
 //   * all calls share the one array and the array keeps the last call's
 //     contents: the evaluation zeroes every accumulator it needs, but two
 //     calls that overlap on the GPU (different streams, or different host
 //     threads) race on the scratch and corrupt each other — serialise them;
 //   * no cudaMalloc, cudaFree or other allocating routine is called.
 #include "internal.cuh"
+#include <cuda.h>
 #include <mutex>
 
 namespace {
@@ -32,8 +37,39 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+struct ScratchEntry {
+  unsigned long long ctx_id;  // unique id of the context the address belongs to
+  void *ptr;
+};
 std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kMaxDevices] = {};
+ScratchEntry g_noalloc[kMaxDevices] = {};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context (0 when there is none
+// yet).  The two driver calls are reached through the runtime's entry-point
+// lookup, so the library needs no link against the driver library.
+bool current_ctx_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || !a)
+      return false;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qb != cudaDriverEntryPointSuccess || !b)
+      return false;
+    get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+    get_id = reinterpret_cast<CtxGetIdFn>(b);
+  }
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS) return false;
+  *id = 0;
+  return !c || get_id(c, id) == CUDA_SUCCESS;
+}
 }  // namespace
 
 extern "C" int dpb_eval_noalloc(const dpb_model *m, int precision, const float *pos, const int32_t *perm,
@@ -52,13 +88,20 @@ extern "C" int dpb_eval_noalloc(const dpb_model *m, int precision, const float *
   void *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    scratch = g_noalloc_ptr[dev];
-    if (!scratch) {
+    unsigned long long ctx = 0;
+    if (!current_ctx_id(&ctx)) return DPB_ERR_CUDA;
+    ScratchEntry &e = g_noalloc[dev];
+    if (ctx == 0 || e.ptr == nullptr || e.ctx_id != ctx) {
       // The host-side symbol is a stand-in, not a device address: resolve the
-      // device address of the array on this device, once.
+      // device address of the array in the current context (this creates the
+      // device's primary context if there is none yet), then key it on that
+      // context.
       if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch) return DPB_ERR_CUDA;
-      g_noalloc_ptr[dev] = scratch;
+      if (!current_ctx_id(&ctx) || ctx == 0) return DPB_ERR_CUDA;
+      e.ptr = scratch;
+      e.ctx_id = ctx;
     }
+    scratch = e.ptr;
   }
   return dpb::eval_impl(m, precision, pos, perm, natoms, nframes, type_count, box, nbrs, sel, energy, atom_energy,
                         force, virial, status, scratch, kNoAllocScratchBytes, (cudaStream_t)stream);

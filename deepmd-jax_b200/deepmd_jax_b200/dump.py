@@ -29,38 +29,49 @@ SYMBOLS = ("X H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn F
            "Lu Hf Ta W Re Os Ir Pt Au Hg Tl Pb Bi Po At Rn Fr Ra Ac Th Pa U Np Pu Am Cm Bk Cf Es Fm Md No Lr").split()
 
 
-def normalize_content(dump_content, n_bead):
-    """Requested kinds in file order (md_utils.py:30-68): 'positions' means
-    position (and centroid under PIMD), 'all' every kind that applies."""
-    pimd = n_bead > 1
+# The dump_content vocabulary (md_utils.py:30-68): each word names the kinds it
+# stands for, without and with beads; a kind name stands for itself.
+_CONTENT_WORDS = {
+    "all": (("position", "velocity"), KINDS),
+    "positions": (("position",), ("position", "centroid")),
+}
+_DEFAULT_CONTENT = tuple(_CONTENT_WORDS)  # the words allowed without a dump_prefix
+
+_MSG_NOT_ITERABLE = ("dump_content must be 'all', 'positions', a dump kind string, "
+                     "or an iterable of dump kind strings.")
+
+
+def _content_items(dump_content):
+    """dump_content as a tuple of entries: one string is one entry."""
     if isinstance(dump_content, str):
-        requested = (dump_content,)
-    else:
-        try:
-            requested = tuple(dump_content)
-        except TypeError as exc:
-            raise ValueError("dump_content must be 'all', 'positions', a dump kind string, "
-                             "or an iterable of dump kind strings.") from exc
-    if len(requested) == 0:
+        return (dump_content,)
+    try:
+        return tuple(dump_content)
+    except TypeError as exc:
+        raise ValueError(_MSG_NOT_ITERABLE) from exc
+
+
+def normalize_content(dump_content, n_bead):
+    """The kinds a dump_content asks for, in file order (md_utils.py:30-68):
+    words expand through _CONTENT_WORDS for a run with or without beads, kind
+    names stand for themselves, and the union is checked against KINDS."""
+    pimd = n_bead > 1
+    items = _content_items(dump_content)
+    if not items:
         raise ValueError("dump_content must not be empty when dump_prefix is set.")
-    bad = [x for x in requested if not isinstance(x, str)]
-    if bad:
-        raise ValueError("dump_content entries must be strings; got %r." % (bad,))
-    expanded = []
-    for item in requested:
-        if item == "all":
-            expanded += list(KINDS) if pimd else ["position", "velocity"]
-        elif item == "positions":
-            expanded += ["position", "centroid"] if pimd else ["position"]
-        else:
-            expanded.append(item)
-    unknown = sorted(set(expanded) - set(KINDS))
+    non_str = [x for x in items if not isinstance(x, str)]
+    if non_str:
+        raise ValueError("dump_content entries must be strings; got %r." % (non_str,))
+    wanted = set()
+    for item in items:
+        wanted.update(_CONTENT_WORDS[item][pimd] if item in _CONTENT_WORDS else (item,))
+    unknown = sorted(wanted.difference(KINDS))
     if unknown:
         raise ValueError("Unknown dump_content entries %s. Allowed entries are %s, 'positions', or 'all'."
                          % (unknown, list(KINDS)))
-    if "centroid" in expanded and not pimd:
+    if not pimd and "centroid" in wanted:
         raise ValueError("dump_content includes 'centroid', which is only meaningful when n_bead > 1.")
-    return tuple(k for k in KINDS if k in expanded)
+    return tuple(filter(wanted.__contains__, KINDS))
 
 
 def _bead_path(path, bead):
@@ -73,11 +84,12 @@ def prepare(type_idx, type_symbols, n_bead, default_interval, dump_interval=None
     """[(kind, path, symbols, bead or None)] and the write interval
     (md_utils.py:194-229); ([], None) when nothing is dumped."""
     if dump_prefix is None:
-        if not (isinstance(dump_content, str) and dump_content in ("all", "positions")):
-            raise ValueError("dump_content requires dump_prefix to be set.")
-        return [], None
+        # without a prefix only the default words are accepted, and nothing is written
+        if isinstance(dump_content, str) and dump_content in _DEFAULT_CONTENT:
+            return [], None
+        raise ValueError("dump_content requires dump_prefix to be set.")
     prefix = os.fspath(dump_prefix)
-    if prefix == "":
+    if not prefix:
         raise ValueError("dump_prefix must be a non-empty path prefix.")
     kinds = normalize_content(dump_content, n_bead)
     if dump_mode not in ("overwrite", "append"):

@@ -523,7 +523,8 @@ class Simulation:
         pending = None  # an accepted chunk whose frames are still on the device
         done, idx = 0, int(first)
         overflow_twice = False
-        while done < steps:
+        stop = False
+        while done < steps and not stop:
             n = min(self.report_interval - self.step % self.report_interval, self._step_chunk_size, steps - done)
             _lib.check(self.lib.dpb_md_snapshot(self._h, 0), "dpb_md_snapshot")
             if trajectory:
@@ -537,27 +538,37 @@ class Simulation:
                 pending = None
             r = self._report_struct()
             code = int(r.status)
-            if code & 16:
+            # the reference's accumulated error word (md.py:906-916): bit 4 marks
+            # a chunk re-run after one neighbour reallocation
+            ec = code | (4 if overflow_twice else 0)
+            if ec & 16:
+                # NaN / Inf: this chunk is the last one (md.py:909-911); it is
+                # still recorded below unless a hard overflow discards it
                 print("# Warning: Nan or Inf encountered in simulation. Terminating.")
-                self._error_code = code
-                break
-            if code & 1:
-                # box shrank past the skin: a larger skin, a list on the current box, re-run (md.py:649-654)
-                _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
-                self._neighbor_skin += 0.4
-                _lib.check(self.lib.dpb_md_set_skin(self._h, self._neighbor_skin, _stream()), "dpb_md_set_skin")
-                _lib.check(self.lib.dpb_md_clear_status(self._h, ~1 & 0xFFFFFFFF), "dpb_md_clear_status")
-                self._graphs = {}
-                if self.verbose:
-                    print("# Box shrank past the skin: neighbour skin now %.2f A" % self._neighbor_skin)
-                continue
-            if code & 2:
-                # reallocate (grow the buffer ratio on a repeat) and re-run the chunk (md.py:657-668,913-916)
-                _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
-                if overflow_twice:
-                    self._buffer_ratio += 0.05
-                overflow_twice = True
-                self._resize_capacity()
+                self._error_code = ec
+                stop = True
+            if ec not in (0, 4, 16):
+                if code & 1:
+                    # box shrank past the skin: a larger skin, a list on the current box, re-run (md.py:649-654)
+                    _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
+                    self._neighbor_skin += 0.4
+                    _lib.check(self.lib.dpb_md_set_skin(self._h, self._neighbor_skin, _stream()), "dpb_md_set_skin")
+                    _lib.check(self.lib.dpb_md_clear_status(self._h, ~1 & 0xFFFFFFFF), "dpb_md_clear_status")
+                    self._graphs = {}
+                    if self.verbose:
+                        print("# Box shrank past the skin: neighbour skin now %.2f A" % self._neighbor_skin)
+                elif code & 2:
+                    # reallocate (grow the buffer ratio on a repeat) and re-run the chunk (md.py:657-668,913-916)
+                    _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
+                    if overflow_twice:
+                        self._buffer_ratio += 0.05
+                    overflow_twice = True
+                    self._resize_capacity()
+                else:
+                    # NaN after a reallocation (error word 20): the reference
+                    # resolves, clears the word and leaves without this chunk
+                    _lib.check(self.lib.dpb_md_snapshot(self._h, 1), "dpb_md_snapshot(restore)")
+                    overflow_twice = False
                 continue
             overflow_twice = False
             boxes = self._box_history(n)
@@ -571,9 +582,7 @@ class Simulation:
                     tic = time()
                 continue
             traj["box"][idx:idx + n] = boxes
-            ev = torch.cuda.Event()
-            ev.record(torch.cuda.current_stream())
-            pending = (buf_p, buf_v, n, idx, ev)
+            pending = (buf_p, buf_v, n, idx, self._chunk_event())
             which ^= 1
             idx += n
             done += n
@@ -589,6 +598,13 @@ class Simulation:
         if self._is_pimd and traj is not None:
             traj["centroid"] = np.stack([self._centroid(p, b) for p, b in zip(traj["position"], traj["box"])])
         return traj
+
+    def _chunk_event(self):
+        """An event on the main stream after the chunk just launched: the
+        side-stream copy of its frames waits on it."""
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream())
+        return ev
 
     def _copy_out(self, pending, traj):
         """Frames of one accepted chunk into the host trajectory: user order

@@ -36,41 +36,80 @@ class DPModelStub:
 
 
 class _Opaque:
-    """Any other flax class the pickle mentions (module bookkeeping)."""
+    """Flax module bookkeeping the pickle carries along (internal state
+    dataclasses, the unspecified-parent sentinel): kept, never used."""
 
     def __init__(self, *a, **k):
         pass
 
     def __setstate__(self, state):
+        if isinstance(state, tuple):  # (dict, slots)
+            state = state[0] or {}
         if isinstance(state, dict):
             self.__dict__.update(state)
 
 
 def _reconstruct_array(fun, args, arr_state, aval_state):
-    """Stand-in for jax._src.array._reconstruct_array: returns numpy."""
+    """Stand-in for jax._src.array._reconstruct_array, the reducer jax.Array
+    pickles through: (numpy's reconstructor, its args, the ndarray state, the
+    abstract-value state).  Returns the numpy array."""
     a = fun(*args)
     a.__setstate__(arr_state)
     return np.asarray(a)
 
 
 def _frozen_dict(*args, **kw):
-    d = dict(*args, **kw)
-    return d
+    """flax.core.frozen_dict.FrozenDict pickles as FrozenDict(plain dict)."""
+    return dict(*args, **kw)
+
+
+def _enum_value(value):
+    """Enum members (flax's SetupState) pickle as EnumClass(value)."""
+    return value
+
+
+def _none():
+    return None
+
+
+# Every global a reference model.pkl may name, and what it loads as.  The
+# reference pickles {'model': DPModel (a flax Module), 'variables': pytree of
+# jax.Array} (deepmd_jax/utils.py:225-228); a flax Module pickles as its class
+# plus its instance dict (params, parent, name and flax's internal state), a
+# jax.Array through jax._src.array._reconstruct_array over numpy's array
+# reduction, a FrozenDict as FrozenDict(dict).  Anything else is refused.
+_STANDINS = {
+    ("deepmd_jax.dpmodel", "DPModel"): DPModelStub,
+    ("jax._src.array", "_reconstruct_array"): _reconstruct_array,
+    ("flax.core.frozen_dict", "FrozenDict"): _frozen_dict,
+    ("flax.linen.module", "_ModuleInternalState"): _Opaque,
+    ("flax.linen.module", "_Sentinel"): _Opaque,
+    ("flax.linen.module", "SetupState"): _enum_value,
+    ("flax.linen.module", "_get_unspecified_parent"): _none,
+}
+# numpy's own reducers (numpy 1.x names map to numpy 2.x's) and the plain
+# containers pickle needs for older protocols.
+_NUMPY = {
+    ("numpy", "ndarray"): ("numpy", "ndarray"),
+    ("numpy", "dtype"): ("numpy", "dtype"),
+    ("numpy.core.multiarray", "_reconstruct"): ("numpy._core.multiarray", "_reconstruct"),
+    ("numpy._core.multiarray", "_reconstruct"): ("numpy._core.multiarray", "_reconstruct"),
+    ("numpy.core.multiarray", "scalar"): ("numpy._core.multiarray", "scalar"),
+    ("numpy._core.multiarray", "scalar"): ("numpy._core.multiarray", "scalar"),
+}
+_PLAIN = {("builtins", n) for n in ("tuple", "list", "dict", "set", "frozenset", "complex", "bytearray", "object",
+                                      "int", "float", "bool", "str", "bytes", "slice")}
+_PLAIN |= {("collections", "OrderedDict"), ("copyreg", "_reconstructor"), ("_codecs", "encode")}
 
 
 class _Unpickler(pickle.Unpickler):
     def find_class(self, module, name):
-        if module.startswith("deepmd_jax") and name == "DPModel":
-            return DPModelStub
-        if module.startswith("jax") and name in ("_reconstruct_array",):
-            return _reconstruct_array
-        if module.startswith("jax") and "Array" in name:
-            return np.asarray
-        if module.startswith("flax") and name == "FrozenDict":
-            return _frozen_dict
-        if module.startswith("flax") or module.startswith("jax"):
-            return _Opaque
-        if module.startswith(("numpy", "builtins", "collections", "copyreg", "_codecs")):
+        key = (module, name)
+        if key in _STANDINS:
+            return _STANDINS[key]
+        if key in _NUMPY:
+            return super().find_class(*_NUMPY[key])
+        if key in _PLAIN:
             return super().find_class(module, name)
         raise pickle.UnpicklingError("model.pkl refers to %s.%s, which is not allowed" % (module, name))
 

@@ -197,8 +197,10 @@ DPB_API int dpb_nlist_pack(const int32_t *src, int natoms, int nframes, int ntyp
  * 64 MiB array inside the library image on each device that loads it; calls
  * whose dpb_eval_workspace_bytes exceed it return DPB_ERR_SCRATCH_LIMIT.
  * The first call on a device resolves the array's address (make it before any
- * stream capture).  Calls share the array: calls that overlap on the GPU race.
- * Arguments and outputs as dpb_eval.  Allocates nothing. */
+ * stream capture); the address is cached per CUDA context, so after a device
+ * reset the next call resolves it again.  Calls share the array: calls that
+ * overlap on the GPU race.  Arguments and outputs as dpb_eval.  Allocates
+ * nothing. */
 DPB_API int dpb_eval_noalloc(const dpb_model *model, int precision, const float *pos, const int32_t *perm,
                              int natoms, int nframes, const int *type_count, const float *box,
                              const int32_t *nbrs, const int *sel, double *energy, float *atom_energy,

@@ -10,7 +10,7 @@ jaxshim.py).  Neighbour lists fed to the reference model come from the
 oracle's brute-force list (jax_md, which builds them in the reference, is a
 third-party dependency that is absent).
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/deepmd-jax   (the source checkout)
 """
 from __future__ import annotations
 
@@ -193,4 +193,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path to the deepmd-jax source checkout>" % os.path.basename(sys.argv[0]))
+    main(sys.argv[1])

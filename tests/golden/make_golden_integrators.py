@@ -27,7 +27,7 @@ around it) are restated, so the fixed-atom fixtures pin the wrapper's
 masking and its chain degrees of freedom, mass and kinetic energy.
 jax.grad / jax.value_and_grad are torch autograd.
 
-Usage:  python tests/golden/make_golden_integrators.py [/path/to/reference]
+Usage:  python tests/golden/make_golden_integrators.py /path/to/deepmd-jax   (the source checkout)
 """
 from __future__ import annotations
 
@@ -439,4 +439,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path to the deepmd-jax source checkout>" % os.path.basename(sys.argv[0]))
+    main(sys.argv[1])

@@ -118,6 +118,29 @@ def test_xyz_dump_format_and_options(tmp_path):
                                   prefix + "_centroid.xyz"]
 
 
+@pytest.mark.parametrize("content,n_bead,want", [
+    ("positions", 1, ("position",)), ("positions", 3, ("position", "centroid")),
+    ("all", 1, ("position", "velocity")), ("all", 2, ("position", "velocity", "centroid")),
+    (["velocity", "position"], 1, ("position", "velocity")), (("centroid", "all"), 2, ("position", "velocity", "centroid")),
+    (iter(["velocity"]), 1, ("velocity",)), ("velocity", 1, ("velocity",)),
+])
+def test_dump_content_vocabulary(content, n_bead, want):
+    """dump_content words and kinds (deepmd_jax/md_utils.py:30-68): file
+    order position, velocity, centroid whatever the request order."""
+    from deepmd_jax_b200 import dump
+    assert dump.normalize_content(content, n_bead) == want
+
+
+@pytest.mark.parametrize("content,msg", [
+    ([], "must not be empty"), ([1, "position"], "entries must be strings"), (5, "or an iterable"),
+    (["pos"], r"Unknown dump_content entries \['pos'\]"), ("centroid", "only meaningful when n_bead > 1"),
+])
+def test_dump_content_errors(content, msg):
+    from deepmd_jax_b200 import dump
+    with pytest.raises(ValueError, match=msg):
+        dump.normalize_content(content, 1)
+
+
 def _write_dp_dir(root, type_idx, sets):
     """A DeepMD-format directory: type.raw and set.NNN/{coord,box,energy,force}.npy."""
     root.mkdir(parents=True, exist_ok=True)
@@ -348,3 +371,202 @@ def test_set_position_argument_errors():
         sim.setPosition(np.zeros((3, 3)), box=np.eye(3))
     with pytest.raises(ValueError, match="isotropic"):
         sim.setPosition(np.zeros((3, 3)), box=[5.0, 5.5, 6.0])
+
+
+class _FakeEngineLib:
+    """The dpb_md_* calls run() makes between chunks, as no-ops returning 0."""
+
+    def __init__(self):
+        self.restores = 0
+
+    def dpb_md_snapshot(self, h, restore):
+        self.restores += int(restore)
+        return 0
+
+    def dpb_md_clear_status(self, h, mask):
+        return 0
+
+
+def _scripted_run(codes, steps=30, chunk=10):
+    """Simulation.run on a stub engine whose chunk status words come from
+    `codes` in turn; each recorded chunk writes its call number into the
+    trajectory rows it covers."""
+    import types
+    import torch
+    N = 2
+    calls = []
+    sim = _stub_simulation(
+        _type_idx=np.zeros(N, dtype=int), _type_symbols=None, _n_bead=1, report_interval=chunk,
+        _step_chunk_size=chunk, _is_initial_state=False, _box=np.array([5.0, 5.0, 5.0]), _natoms=N,
+        _routine="NVE", _is_pimd=False, verbose=False, _dt=0.5, step=0, _buffer_ratio=1.2, _h=None,
+        _traj_bufs=[(torch.zeros(chunk, N * 3), torch.zeros(chunk, N * 3)) for _ in range(2)])
+    sim.lib = _FakeEngineLib()
+    sim._frame_shape = lambda: (N, 3)
+    script = list(codes)
+    reports, resized = [], []
+
+    def run_chunk(n, p, v):
+        calls.append(n)
+
+    def copy_out(pending, traj):
+        _, _, n, idx, tag = pending
+        traj["position"][idx:idx + n] = tag
+
+    sim._run_chunk = run_chunk
+    sim._report_struct = lambda: types.SimpleNamespace(status=script.pop(0) if script else 0)
+    sim._chunk_event = lambda: len(calls)
+    sim._copy_out = copy_out
+    sim._report_row = lambda tic: reports.append(sim.step)
+    sim._resize_capacity = lambda: resized.append(sim.step)
+    traj = sim.run(steps)
+    return sim, traj, calls, reports, resized
+
+
+def test_run_records_nan_chunk_then_stops():
+    """Status bit 16 (NaN/Inf) as the reference handles it (deepmd_jax/md.py:
+    906-950): the chunk is still committed - its frames recorded, the step
+    advanced, the report printed - and the run ends there."""
+    sim, traj, calls, reports, _ = _scripted_run([0, 16])
+    assert calls == [10, 10] and sim.step == 20 and reports == [10, 20]
+    assert np.all(traj["position"][:10] == 1) and np.all(traj["position"][10:20] == 2)
+    assert np.all(traj["position"][20:] == 0) and sim._error_code == 16
+
+
+@pytest.mark.parametrize("codes,restores", [([18], 1), ([2, 16], 2)])
+def test_run_discards_nan_chunk_with_overflow(codes, restores):
+    """NaN together with a hard overflow (error word not 0, 4 or 16), or right
+    after a neighbour reallocation (word 20): the reference resolves the
+    error and leaves without recording that chunk (md.py:906-916)."""
+    sim, traj, calls, reports, resized = _scripted_run(codes)
+    assert sim.step == 0 and reports == [] and np.all(traj["position"] == 0)
+    assert sim.lib.restores == restores and len(calls) == len(codes)
+    assert resized == [0]  # one reallocation, at step 0, in both scripts
+
+
+def _reference_style_pickle(params, variables):
+    """A model.pkl byte stream as the reference writes it (deepmd_jax/utils.py:
+    225-228) on a machine with jax and flax: the DPModel flax Module pickles as
+    its class deepmd_jax.dpmodel.DPModel plus its instance dict (params,
+    parent, name, flax's _ModuleInternalState with a SetupState member), the
+    variables tree as nested FrozenDicts, each leaf a jax.Array reduced to
+    jax._src.array._reconstruct_array(numpy reconstructor, args, ndarray
+    state, {'weak_type': False}).  Neither jax nor flax is installed here, so
+    the globals are served by stand-in modules registered under those names
+    only while pickling."""
+    import enum
+    import pickle
+    import sys
+    import types
+    names = ["deepmd_jax", "deepmd_jax.dpmodel", "jax", "jax._src", "jax._src.array", "flax", "flax.core",
+             "flax.core.frozen_dict", "flax.linen", "flax.linen.module"]
+    saved = {n: sys.modules.get(n) for n in names}
+    mods = {n: types.ModuleType(n) for n in names}
+
+    def _reconstruct_array(fun, args, arr_state, aval_state):  # never called while pickling
+        raise AssertionError
+
+    _reconstruct_array.__module__, _reconstruct_array.__qualname__ = "jax._src.array", "_reconstruct_array"
+    mods["jax._src.array"]._reconstruct_array = _reconstruct_array
+
+    class ArrayImpl:
+        def __init__(self, a):
+            self.a = np.asarray(a)
+
+        def __reduce__(self):
+            fun, args, arr_state = self.a.__reduce__()
+            return _reconstruct_array, (fun, args, arr_state, {"weak_type": False})
+
+    class FrozenDict(dict):
+        def __reduce__(self):
+            return FrozenDict, (dict(self),)
+
+    FrozenDict.__module__, FrozenDict.__qualname__ = "flax.core.frozen_dict", "FrozenDict"
+    mods["flax.core.frozen_dict"].FrozenDict = FrozenDict
+    SetupState = enum.IntEnum("SetupState", [("NEW", 0), ("TRANSFORMED", 1), ("DONE", 2)],
+                              module="flax.linen.module")
+    mods["flax.linen.module"].SetupState = SetupState
+
+    class _ModuleInternalState:
+        pass
+
+    _ModuleInternalState.__module__ = "flax.linen.module"
+    _ModuleInternalState.__qualname__ = "_ModuleInternalState"
+    mods["flax.linen.module"]._ModuleInternalState = _ModuleInternalState
+
+    class DPModel:
+        pass
+
+    DPModel.__module__, DPModel.__qualname__ = "deepmd_jax.dpmodel", "DPModel"
+    mods["deepmd_jax.dpmodel"].DPModel = DPModel
+
+    def tree(x):
+        if isinstance(x, dict):
+            return FrozenDict({k: tree(v) for k, v in x.items()})
+        return ArrayImpl(x)
+
+    try:
+        sys.modules.update(mods)
+        st = _ModuleInternalState()
+        st.__dict__.update(in_compact_method=False, in_setup=False, setup_called=SetupState.NEW,
+                           is_initialized=False, autoname_cursor={}, children={})
+        model = DPModel()
+        model.__dict__.update(params=params, parent=None, name=None, _state=st)
+        return pickle.dumps({"model": model, "variables": tree(variables)}, protocol=4)
+    finally:
+        for n, m in saved.items():
+            if m is None:
+                sys.modules.pop(n, None)
+            else:
+                sys.modules[n] = m
+
+
+def test_load_model_reads_reference_pickle_globals(tmp_path):
+    """load_model on a stream that names the real jax / flax globals: the
+    globals are exactly the allow-listed ones, the parameters and every
+    variable leaf come back as the writer's numpy values."""
+    import io
+    from deepmd_jax_b200 import utils
+    from deepmd_jax_b200.systems import init_dp_params
+    from deepmd_jax_b200.utils import load_model
+    p, v = init_dp_params(seed=3)
+    blob = _reference_style_pickle(p, v)
+    globs = set()
+
+    class Recorder(utils._Unpickler):
+        def find_class(self, module, name):
+            globs.add((module, name))
+            return super().find_class(module, name)
+
+    Recorder(io.BytesIO(blob)).load()
+    assert {("deepmd_jax.dpmodel", "DPModel"), ("jax._src.array", "_reconstruct_array"),
+            ("flax.core.frozen_dict", "FrozenDict"), ("flax.linen.module", "_ModuleInternalState"),
+            ("flax.linen.module", "SetupState")} <= globs
+    path = tmp_path / "model.pkl"
+    path.write_bytes(blob)
+    model, variables = load_model(str(path))
+    assert model.params["embed_widths"] == p["embed_widths"] and model.params["rcut"] == p["rcut"]
+
+    def leaves(t, pre=""):
+        for k, x in t.items():
+            if isinstance(x, dict):
+                yield from leaves(x, pre + k + "/")
+            else:
+                yield pre + k, x
+
+    got, want = dict(leaves(variables)), dict(leaves(v))
+    assert got.keys() == want.keys()
+    for k in want:
+        assert isinstance(got[k], np.ndarray) and got[k].dtype == np.asarray(want[k]).dtype
+        assert np.array_equal(got[k], want[k]), k
+
+
+def test_load_model_refuses_unknown_globals(tmp_path):
+    """A global outside the allow-list fails loudly instead of loading as a
+    stand-in."""
+    import pickle
+    import collections
+    from deepmd_jax_b200.utils import load_model
+    path = tmp_path / "bad.pkl"
+    path.write_bytes(pickle.dumps({"model": collections.Counter(), "variables": {}}))
+    with pytest.raises(pickle.UnpicklingError, match="collections.Counter"):
+        load_model(str(path))
