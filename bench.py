@@ -50,6 +50,8 @@ def parse():
                     help="profiling case: plain MD steps (direct launches, no timing) for ncu")
     ap.add_argument("--n-side", type=int, default=N_SIDE, help="waters per box side (profiling case)")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving study: seconds of arrivals")
+    ap.add_argument("--serve-in-bench", type=float, default=2.0,
+                    help="seconds of serving arrivals (mixed form) measured after the MD line; 0 skips")
     ap.add_argument("--study", default="none", choices=["none", "drift", "pimd", "serving"],
                     help="drift: NVE total-energy drift of both forms on the 98,304-atom box; "
                          "pimd: 32-bead PILE-L throughput of both forms (1,536-atom water)")
@@ -193,7 +195,9 @@ def reference_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "form": "reference (CPU restatement)", "parallelism": "single",
                        "cpu_sample": "12,288-atom box (4,096 H2O, L=49.66 A), same model and step",
-                       "sample_atoms": N},
+                       "sample_atoms": N, "same_config": False,
+                       "extrapolation": "atom-steps/s of the 12,288-atom sample, taken per atom-step for the "
+                                        "98,304-atom workload; neighbour list built outside the timed steps"},
             "cpu_baseline": {"value": val, "unit": "atom-steps/s", "cores": threads, "kind": "port",
                              "sample": "%d velocity-Verlet steps of the 12,288-atom water box with the FP32 "
                                        "torch restatement of the reference model (the reference is JAX and "
@@ -384,6 +388,19 @@ def gpu_arm(args, rank, world, local_rank):
                        "h2d_bytes_per_step": int(2 * N * 3 * 8 / K),
                        "d2h_bytes_per_step": int(2 * N * 3 * 8),  # user-order float64 positions + velocities
                        "api": "Simulation.setPosition + setVelocity + run(K) returning the per-step trajectory"}
+    if rank == 0 and world == 1 and args.serve_in_bench > 0:
+        # the serving workload's latency line (BASELINE's p50 / p99): Poisson
+        # arrivals at 200 requests/s of evaluate() and MD-continuation requests
+        sv = study_serving(args, forms=("mixed",), seconds=args.serve_in_bench)
+        f = sv["forms"]["mixed"]
+        line["serving"] = {"form": "mixed", "seconds_of_arrivals": sv["seconds_of_arrivals"],
+                           "requests": sv["requests"], "md_requests": sv["md_requests"],
+                           "eval_p50_s": f["latency"].get("eval", {}).get("p50_s"),
+                           "eval_p99_s": f["latency"].get("eval", {}).get("p99_s"),
+                           "md_p50_s": f["latency"].get("md", {}).get("p50_s"),
+                           "md_p99_s": f["latency"].get("md", {}).get("p99_s"),
+                           "frames_per_s": f["frames_per_s"], "atom_evals_per_s": f["atom_evals_per_s"],
+                           "wall_s": f["wall_s"]}
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_sample()
     for v in results.values():
@@ -493,7 +510,7 @@ def study_pimd(args):
     return out
 
 
-def study_serving(args):
+def study_serving(args, forms=("fp32", "mixed"), seconds=None):
     """Serving stream of the benchmark model: Poisson arrivals at 200
     requests/s for args.serve_seconds; 98 % are evaluate() requests of 1-16
     water frames with the atom count log-uniform in [96, 24,576] (multiples
@@ -518,7 +535,7 @@ def study_serving(args):
     sched, t = [], 0.0
     while True:
         t += rng.exponential(1.0 / 200.0)
-        if t > args.serve_seconds:
+        if t > (args.serve_seconds if seconds is None else seconds):
             break
         if rng.random() < 0.02:
             n_w = int(np.exp(rng.uniform(np.log(1000), np.log(10000))))
@@ -528,10 +545,11 @@ def study_serving(args):
             sched.append((t, "eval", n_w, int(rng.integers(1, 17))))
     for _, _, n_w, _ in sched:
         water(n_w)
-    out = {"study": "serving", "arrival_rate_per_s": 200, "seconds_of_arrivals": args.serve_seconds,
+    out = {"study": "serving", "arrival_rate_per_s": 200,
+           "seconds_of_arrivals": args.serve_seconds if seconds is None else seconds,
            "requests": len(sched), "md_requests": sum(1 for x in sched if x[1] == "md"),
            "hbm_budget_GB": 60, "forms": {}}
-    for prec in ("fp32", "mixed"):
+    for prec in forms:
         with Server((params, variables), precision=prec, hbm_budget=60e9) as srv:
             w = water(64)
             srv.submit_evaluate(w["position"], w["box"], w["type_idx"]).result()   # warm-up

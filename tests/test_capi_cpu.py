@@ -36,3 +36,15 @@ def test_version_string():
     if not os.path.exists(_lib.LIB_PATH):
         pytest.skip("libdpb200.so not built")
     assert b"sm_100a" in _lib.load().dpb_version()
+
+
+def test_jax_ffi_shim_build_target():
+    """The jax.ffi shim's make target builds only where jaxlib's FFI headers
+    exist and otherwise succeeds with a 'skipped' note (this image has no jax)."""
+    import subprocess
+    import importlib.util
+    d = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "deepmd-jax_b200", "csrc", "jax_ffi")
+    out = subprocess.run(["make", "-C", d], capture_output=True, text=True)
+    assert out.returncode == 0
+    if importlib.util.find_spec("jax") is None:
+        assert "skipped: no jaxlib" in out.stdout
