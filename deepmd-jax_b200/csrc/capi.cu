@@ -184,36 +184,48 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
         rc = upload_bf16(m, v, &M.ew_bf[k][l]);
       }
     }
-  // shared-memory images of the embedding nets for the tensor-core kernels
+  // shared-memory images of the embedding nets for the tensor-core kernels:
+  // FP16 B tiles (K-major) of layers 1 and 2 with the layer's bias as one
+  // more K row (the A operands carry a ones column there), and the FP32 first
+  // layer (w0, b0) plus w0 as FP16 pairs (mixed.cu, MixDims)
   {
-    const int K1 = (M.E0 + 15) / 16 * 16, N1 = (M.E1 + 15) / 16 * 16, K2 = N1, N2 = (M.E2 + 15) / 16 * 16;
+    const int K1 = (M.E0 + 1 + 15) / 16 * 16, N1 = (M.E1 + 15) / 16 * 16;
+    const int K2 = (M.E1 + 1 + 15) / 16 * 16, N2 = (M.E2 + 15) / 16 * 16;
     const int W1B = N1 * K1 * 2, W2B = N2 * K2 * 2;
+    const int npair0 = (M.E0 + 1) / 2;
     M.net_img_bytes = W1B + W2B;
-    M.net_small_floats = ((2 * M.E0 + M.E1 + M.E2) + 3) / 4 * 4;
+    M.net_small_floats = (2 * M.E0 + npair0 + 3) / 4 * 4;
     for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp; ++k) {
       std::vector<uint8_t> img(M.net_img_bytes, 0);
       const float *W1 = d->embed_kernel[k * 3 + 1], *W2 = d->embed_kernel[k * 3 + 2];
+      const float *b1 = d->embed_bias[k * 3 + 1], *b2 = d->embed_bias[k * 3 + 2];
       for (int n = 0; n < N1; ++n)
         for (int kk = 0; kk < K1; ++kk) {
-          const float v = (n < M.E1 && kk < M.E0) ? W1[kk * M.E1 + n] : 0.f;
-          *reinterpret_cast<__nv_bfloat16 *>(img.data() + dpb::tc::kmajor_off(n, kk, K1)) = __float2bfloat16_rn(v);
+          float v = 0.f;
+          if (n < M.E1 && kk < M.E0) v = W1[kk * M.E1 + n];
+          if (n < M.E1 && kk == M.E0) v = b1[n];
+          *reinterpret_cast<__half *>(img.data() + dpb::tc::kmajor_off(n, kk, K1)) = __float2half_rn(v);
         }
       for (int n = 0; n < N2; ++n)
         for (int kk = 0; kk < K2; ++kk) {
-          const float v = (n < M.E2 && kk < M.E1) ? W2[kk * M.E2 + n] : 0.f;
-          *reinterpret_cast<__nv_bfloat16 *>(img.data() + W1B + dpb::tc::kmajor_off(n, kk, K2)) =
-              __float2bfloat16_rn(v);
+          float v = 0.f;
+          if (n < M.E2 && kk < M.E1) v = W2[kk * M.E2 + n];
+          if (n < M.E2 && kk == M.E1) v = b2[n];
+          *reinterpret_cast<__half *>(img.data() + W1B + dpb::tc::kmajor_off(n, kk, K2)) = __float2half_rn(v);
         }
       const char *dimg = nullptr;
       rc = upload(m, reinterpret_cast<const char *>(img.data()), img.size(), &dimg);
       M.net_img[k] = dimg;
       std::vector<float> sm(M.net_small_floats, 0.f);
+      const float *w0 = d->embed_kernel[k * 3 + 0], *b0 = d->embed_bias[k * 3 + 0];
       for (int e = 0; e < M.E0; ++e) {
-        sm[e] = d->embed_kernel[k * 3 + 0][e];
-        sm[M.E0 + e] = d->embed_bias[k * 3 + 0][e];
+        sm[e] = w0[e];
+        sm[M.E0 + e] = b0[e];
       }
-      for (int e = 0; e < M.E1; ++e) sm[2 * M.E0 + e] = d->embed_bias[k * 3 + 1][e];
-      for (int e = 0; e < M.E2; ++e) sm[2 * M.E0 + M.E1 + e] = d->embed_bias[k * 3 + 2][e];
+      for (int j = 0; j < npair0; ++j) {
+        __half2 h = __floats2half2_rn(w0[2 * j], 2 * j + 1 < M.E0 ? w0[2 * j + 1] : 0.f);
+        std::memcpy(&sm[2 * M.E0 + j], &h, 4);
+      }
       if (rc == DPB_OK) rc = upload(m, sm.data(), sm.size(), &M.net_small[k]);
     }
   }

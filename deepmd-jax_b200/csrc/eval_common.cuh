@@ -34,9 +34,10 @@ struct DevModel {
   const __nv_bfloat16 *ew_bf[kMaxTypes * kMaxTypes][kMaxEmbedLayers];
   const __nv_bfloat16 *fw_bf[kMaxTypes][kMaxFitLayers + 1];
   const __nv_bfloat16 *fwT_bf[kMaxTypes][kMaxFitLayers + 1];
-  // per embedding net: the shared-memory image of its BF16 B tiles (layer 1
-  // and layer 2, K-major, zero padded to multiples of 16) and of its FP32
-  // first layer and biases (w0, b0, b1, b2), copied verbatim by the mixed kernels
+  // per embedding net: the shared-memory image of its FP16 B tiles (layer 1
+  // and layer 2, K-major, the layer's bias as the K row after the inputs,
+  // zero padded to multiples of 16) and of its first layer (w0, b0 in FP32,
+  // w0 as FP16 pairs), copied verbatim by the mixed kernels
   const char *net_img[kMaxTypes * kMaxTypes];
   const float *net_small[kMaxTypes * kMaxTypes];
   int net_img_bytes, net_small_floats;

@@ -66,26 +66,53 @@ __global__ void __launch_bounds__(128) k_selftest_umma(int variant, float *out, 
 }
 
 // ---------------------------------------------------------------- shared pieces
+// Tile geometry of one embedding net E0 -> E1 -> E2 on the tensor cores.  The
+// operands are FP16 (10 mantissa bits, against BF16's 7; every embedding
+// activation is a sum of at most three tanh values, far inside FP16's range).
+// The A operands of layers 1 and 2 carry a ones column at K index E0 (E1) and
+// the B tiles hold the layer's bias in that K row, so the MMA adds the bias.
+__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
+
 template <int E0, int E1, int E2>
 struct MixDims {
-  static constexpr int K1 = (E0 + 15) / 16 * 16;
+  static constexpr int K1 = (E0 + 1 + 15) / 16 * 16;  // layer-1 K: inputs and the ones column
   static constexpr int N1 = (E1 + 15) / 16 * 16;
-  static constexpr int K2 = N1;
+  static constexpr int K2 = (E1 + 1 + 15) / 16 * 16;
   static constexpr int N2 = (E2 + 15) / 16 * 16;
   static constexpr int W1B = N1 * K1 * 2;  // bytes of the layer-1 B tile (K-major)
   static constexpr int W2B = N2 * K2 * 2;  // bytes of the layer-2 B tile (K-major)
   static constexpr int NETB = W1B + W2B;
-  static constexpr int NSMALL = (2 * E0 + E1 + E2 + 3) / 4 * 4;  // w0, b0, b1, b2 (fp32)
+  static constexpr int NSMALL = (2 * E0 + (E0 + 1) / 2 + 3) / 4 * 4;  // w0, b0 (fp32), w0 pairs (fp16)
   static constexpr int OPA_A0 = 128 * K1 * 2, OPA_A1 = 128 * K2 * 2, OPA_H2 = 128 * N2 * 2;
-  static constexpr int OPA = OPA_A0 > OPA_A1 ? (OPA_A0 > OPA_H2 ? OPA_A0 : OPA_H2) : (OPA_A1 > OPA_H2 ? OPA_A1 : OPA_H2);
+  static constexpr int OPA = imax(OPA_A0, imax(OPA_A1, OPA_H2));
   static constexpr int Z1 = E1 / E0, Z2 = E2 / E1;
+  static_assert(Z1 * E0 == E1 && Z2 * E1 == E2 && Z1 >= 1 && Z1 <= 2 && Z2 >= 1 && Z2 <= 2,
+                "residual ratios 1 or 2");
+  static_assert(E1 % 2 == 0 && E2 % 2 == 0 && N1 <= 64 && N2 <= 128, "tile widths");
+};
+
+// Column split between the two threads of a row ("halves", tid / 128): half
+// 0 owns h1 columns [0, S1) and h2 columns [0, S2), half 1 the rest, with
+// S2 = S1 * Z2 so every residual source h1[c / Z2] of a half's h2 columns is
+// one of its own h1 columns; the A0 operand is split at A0C, A1 at S1, H2 at
+// S2.  Half 0 computes h0 on [0, H0HI0), half 1 on [H0LO1, E0): the operand
+// columns it writes and the residual sources of its h1 columns.
+template <int E0, int E1, int E2>
+struct HalfSplit {
+  using MD = MixDims<E0, E1, E2>;
+  static constexpr int S1 = (E1 / 2) / 8 * 8;
+  static constexpr int S2 = S1 * MD::Z2;
+  static constexpr int A0C = MD::K1 / 2;
+  static constexpr int H0HI0 = imax(imin(A0C, E0), S1 / MD::Z1);
+  static constexpr int H0LO1 = imin(A0C, S1 / MD::Z1);
+  static constexpr int NP0 = imax((H0HI0 + 1) / 2, (E0 - H0LO1 + 1) / 2);  // h0 pairs per half
+  static constexpr int NP1 = imax(S1 / 2, (E1 - S1 + 1) / 2);              // h1 pairs per half
+  static_assert(S1 % 8 == 0 && S2 % 8 == 0 && H0LO1 % 2 == 0 && A0C % 8 == 0, "pair-aligned split");
 };
 
 constexpr int kBlkAtoms = 8;    // centre atoms per block
-constexpr int kBwdCpt = 4;      // compaction candidates per thread, adjoint (128 threads)
-constexpr int kRowCap = 128 + 128 * kBwdCpt;  // compacted rows: the carry (< 128) + one compaction round
 constexpr int kRblkBytes = 128 * 128 * 2;
-constexpr int kDtN = kBlkAtoms * 10;  // N of the adjoint contraction: 8 slots x 10 channels
 
 __host__ __device__ constexpr int round1k(int x) { return (x + 1023) / 1024 * 1024; }
 
@@ -298,16 +325,174 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
                     tc::pack_bf16(v[6], v[7]));
 }
 
-// ---------------------------------------------------------------- embedding forward (BF16 tcgen05)
+// ---------------------------------------------------------------- embedding rows in packed FP16
+// The per-row epilogues of both embedding kernels work on pairs of adjacent
+// columns packed in one register (__half2): tanh.approx.f16x2 (one MUFU
+// operation per two columns), HADD2 for the residual, HFMA2 for the tangent
+// (1 - t^2) dz + d_prev of the adjoint's forward-mode recompute.  A pair
+// (c, c + 1) with c even; its residual source (utils.py:115-123, x_prev =
+// repeat(x, Z)) is the pair (c, c + 1) of the layer below when Z = 1 and
+// column c / 2, broadcast to both halves, when Z = 2.
+
+// residual source pair of the even column c from the pairs `src` of the layer
+// below, which start at column lo (compile-time indices after unrolling)
+template <int Z>
+__device__ __forceinline__ __half2 res_pair(const __half2 *src, int c, int lo) {
+  if (Z == 1) return src[(c - lo) >> 1];
+  const int k = (c >> 1) - lo;
+  return (k & 1) ? __high2half2(src[k >> 1]) : __low2half2(src[k >> 1]);
+}
+
+// Operand pair of columns (c, c + 1) of a layer with E real columns whose
+// pairs start at column lo: the values, the ones column at K index E (VALUE),
+// zeros beyond.
+template <int E, bool VALUE>
+__device__ __forceinline__ __half2 operand_pair(const __half2 *p, int c, int lo) {
+  const __half one = __float2half_rn(VALUE ? 1.f : 0.f), zero = __float2half_rn(0.f);
+  if (c + 1 < E) return p[(c - lo) >> 1];
+  if (c + 1 == E) return __halves2half2(__low2half(p[(c - lo) >> 1]), one);
+  if (c == E) return __halves2half2(one, zero);
+  return __halves2half2(zero, zero);
+}
+
+__device__ __forceinline__ void st_pairs(char *dst, __half2 a, __half2 b, __half2 c, __half2 d) {
+  *reinterpret_cast<uint4 *>(dst) = make_uint4(tc::as_u32(a), tc::as_u32(b), tc::as_u32(c), tc::as_u32(d));
+}
+
+// Layer 0 (1 -> E0) of one half, FP32 pre-activation then FP16 pairs:
+// h0 = tanh(s~ w0 + b0), with TANGENT also dh0/ds~ = (1 - h0^2) w0; writes
+// the half's K-major A0 chunks (value operand a0, tangent operand a0t).
+template <int E0, int E1, int E2, int HALF, bool TANGENT>
+__device__ __forceinline__ void emb_layer0(float st, const float *sm, int row, char *a0, char *a0t,
+                                           __half2 (&h0)[HalfSplit<E0, E1, E2>::NP0],
+                                           __half2 (&d0)[HalfSplit<E0, E1, E2>::NP0]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = HalfSplit<E0, E1, E2>;
+  constexpr int lo = HALF ? SP::H0LO1 : 0, hi = HALF ? E0 : SP::H0HI0;
+  const __half2 one2 = __float2half2_rn(1.f);
+  const uint32_t *w0p = reinterpret_cast<const uint32_t *>(sm + 2 * E0);
+#pragma unroll
+  for (int j = 0; j < (hi - lo + 1) / 2; ++j) {
+    const int c = lo + 2 * j;
+    const float za = fmaf(st, sm[c], sm[E0 + c]);
+    const float zb = (c + 1 < E0) ? fmaf(st, sm[c + 1], sm[E0 + c + 1]) : 0.f;
+    const __half2 t = tc::tanh_h2(tc::f2_to_h2(za, zb));
+    h0[j] = t;
+    if (TANGENT) d0[j] = __hmul2(__hfma2(__hneg2(t), t, one2), tc::as_h2(w0p[c >> 1]));
+  }
+  constexpr int c0 = HALF ? SP::A0C : 0, c1 = HALF ? MD::K1 : SP::A0C;
+#pragma unroll
+  for (int k8 = c0; k8 < c1; k8 += 8) {
+    const uint32_t o = tc::kmajor_off(row, k8, MD::K1);
+    st_pairs(a0 + o, operand_pair<E0, true>(h0, k8, lo), operand_pair<E0, true>(h0, k8 + 2, lo),
+             operand_pair<E0, true>(h0, k8 + 4, lo), operand_pair<E0, true>(h0, k8 + 6, lo));
+    if (TANGENT)
+      st_pairs(a0t + o, operand_pair<E0, false>(d0, k8, lo), operand_pair<E0, false>(d0, k8 + 2, lo),
+               operand_pair<E0, false>(d0, k8 + 4, lo), operand_pair<E0, false>(d0, k8 + 6, lo));
+  }
+}
+
+// Layer 1 epilogue of one half: h1 = tanh(D1) + rep(h0) from the TMEM
+// accumulator at tD (bias included), with TANGENT dh1 = (1 - t^2) D1t +
+// rep(dh0) from tDt; 8 accumulator columns per TMEM load; writes the half's
+// A1 chunks.
+template <int E0, int E1, int E2, int HALF, bool TANGENT>
+__device__ __forceinline__ void emb_epi1(uint32_t tD, uint32_t tDt, int row, char *a1, char *a1t,
+                                         const __half2 (&h0)[HalfSplit<E0, E1, E2>::NP0],
+                                         const __half2 (&d0)[HalfSplit<E0, E1, E2>::NP0],
+                                         __half2 (&h1)[HalfSplit<E0, E1, E2>::NP1],
+                                         __half2 (&d1)[HalfSplit<E0, E1, E2>::NP1]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = HalfSplit<E0, E1, E2>;
+  constexpr int c0 = HALF ? SP::S1 : 0, c1 = HALF ? E1 : SP::S1, h0lo = HALF ? SP::H0LO1 : 0;
+  const __half2 one2 = __float2half2_rn(1.f);
+#pragma unroll
+  for (int g = c0 / 8 * 8; g < c1; g += 8) {
+    uint32_t z[8], dz[8];
+    tc::tmem_ld8_issue(tD + g, z);
+    if (TANGENT) tc::tmem_ld8_issue(tDt + g, dz);
+    tc::tmem_wait();
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+      const int c = g + i;
+      if (c < c0 || c >= c1) continue;
+      const __half2 t = tc::tanh_h2(tc::f2_to_h2(__uint_as_float(z[i]), __uint_as_float(z[i + 1])));
+      h1[(c - c0) >> 1] = __hadd2(t, res_pair<MD::Z1>(h0, c, h0lo));
+      if (TANGENT) {
+        const __half2 u = __hfma2(__hneg2(t), t, one2);
+        d1[(c - c0) >> 1] = __hfma2(u, tc::f2_to_h2(__uint_as_float(dz[i]), __uint_as_float(dz[i + 1])),
+                                    res_pair<MD::Z1>(d0, c, h0lo));
+      }
+    }
+  }
+  constexpr int k0 = HALF ? SP::S1 : 0, k1 = HALF ? MD::K2 : SP::S1;
+#pragma unroll
+  for (int k8 = k0; k8 < k1; k8 += 8) {
+    const uint32_t o = tc::kmajor_off(row, k8, MD::K2);
+    st_pairs(a1 + o, operand_pair<E1, true>(h1, k8, c0), operand_pair<E1, true>(h1, k8 + 2, c0),
+             operand_pair<E1, true>(h1, k8 + 4, c0), operand_pair<E1, true>(h1, k8 + 6, c0));
+    if (TANGENT)
+      st_pairs(a1t + o, operand_pair<E1, false>(d1, k8, c0), operand_pair<E1, false>(d1, k8 + 2, c0),
+               operand_pair<E1, false>(d1, k8 + 4, c0), operand_pair<E1, false>(d1, k8 + 6, c0));
+  }
+}
+
+// Layer 2 epilogue of one half: h2 = tanh(D2) + rep(h1) (and with TANGENT
+// dh2) for the half's columns (split at S2), zero past E2, stored per
+// 8-column chunk at h2 + off(chunk) (and h2t + off(chunk)); OFF maps a column
+// to the byte offset of the row's chunk in the operand layout the caller uses.
+template <int E0, int E1, int E2, int HALF, bool TANGENT, typename OFF>
+__device__ __forceinline__ void emb_epi2(uint32_t tD, uint32_t tDt, char *h2, char *h2t, OFF off,
+                                         const __half2 (&h1)[HalfSplit<E0, E1, E2>::NP1],
+                                         const __half2 (&d1)[HalfSplit<E0, E1, E2>::NP1]) {
+  using MD = MixDims<E0, E1, E2>;
+  using SP = HalfSplit<E0, E1, E2>;
+  constexpr int c0 = HALF ? SP::S2 : 0, c1 = HALF ? MD::N2 : SP::S2, h1lo = HALF ? SP::S1 : 0;
+  const __half2 one2 = __float2half2_rn(1.f), zero2 = __float2half2_rn(0.f);
+#pragma unroll
+  for (int k8 = c0; k8 < c1; k8 += 8) {
+    uint32_t z[8], dz[8];
+    if (k8 < E2) {  // chunks past E2 are zero padding
+      tc::tmem_ld8_issue(tD + k8, z);
+      if (TANGENT) tc::tmem_ld8_issue(tDt + k8, dz);
+      tc::tmem_wait();
+    }
+    __half2 hv[4], dv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int c = k8 + 2 * u, i = 2 * u;
+      hv[u] = dv[u] = zero2;
+      if (c < E2) {
+        const __half2 t = tc::tanh_h2(tc::f2_to_h2(__uint_as_float(z[i]), __uint_as_float(z[i + 1])));
+        hv[u] = __hadd2(t, res_pair<MD::Z2>(h1, c, h1lo));
+        if (TANGENT)
+          dv[u] = __hfma2(__hfma2(__hneg2(t), t, one2),
+                          tc::f2_to_h2(__uint_as_float(dz[i]), __uint_as_float(dz[i + 1])),
+                          res_pair<MD::Z2>(d1, c, h1lo));
+      }
+    }
+    st_pairs(h2 + off(k8), hv[0], hv[1], hv[2], hv[3]);
+    if (TANGENT) st_pairs(h2t + off(k8), dv[0], dv[1], dv[2], dv[3]);
+  }
+}
+
+// Row geometry for layer 0 alone: s~ = (s(r) - mean) / std (the fast-reciprocal
+// form of row_geom_mixed).
+__device__ __forceinline__ float row_stilde(float4 rb, float rcut, float inv_std, float mean) {
+  RowGeom g;
+  row_geom_mixed(make_float3(rb.x, rb.y, rb.z), rcut, g);
+  return (g.s - mean) * inv_std;
+}
+
+// ---------------------------------------------------------------- embedding forward (FP16 tcgen05)
 // Per block of 8 centre atoms of type ti: neighbour rows with s(r) != 0 are
 // compacted block-wide into 128-row tiles.  Two threads serve each row (TMEM
 // lane): warps w and w + 4 share lane quarter w % 4 and split the columns of
-// every layer ("halves"), so 16 warps per SM hide the latencies of the three
+// every layer (HalfSplit), so 16 warps per SM hide the latencies of the three
 // MMA round trips per tile:
-//   layer 0 (1 -> E0) FP32 on CUDA cores (tanh.approx.f32: its ~2^-11 relative
-//           error is below the BF16 rounding of the h0 operand), h0 -> A0 (bf16)
-//   D  = A0 . W1   (tcgen05, 128 x N1)   -> h1 = tanh(D + b1) + rep(h0) -> A1
-//   D  = A1 . W2   (tcgen05, 128 x N2)   -> h2 = tanh(D + b2) + rep(h1) -> H2
+//   layer 0 (1 -> E0) on CUDA cores, h0 -> A0 (fp16, ones column at E0)
+//   D  = A0 . [W1; b1]   (tcgen05, 128 x N1)   -> h1 = tanh(D) + rep(h0) -> A1
+//   D  = A1 . [W2; b2]   (tcgen05, 128 x N2)   -> h2 = tanh(D) + rep(h1) -> H2
 //   D3 += Rblk . H2 (tcgen05, M = 8 slots x 16 channels, K = 128 rows)
 // where Rblk holds each row's env row R~ in its atom's 16-lane slot (zero
 // elsewhere), so D3 accumulates T_a = sum_rows R~^T h2 for the 8 atoms in
@@ -318,116 +503,6 @@ constexpr int kFwdThreads = 256;
 constexpr int kFwdCpt = 2;  // compaction candidates per thread, forward
 constexpr int kRowCapFwd = 128 + kFwdThreads * kFwdCpt;  // the carry (< 128) + one compaction round
 
-// Column split of the two halves: half 0 owns h1 columns [0, S1) and h2
-// columns [0, S2), half 1 the rest; S2 = S1 * Z2 so every residual source
-// h1[c / Z2] of a half's h2 columns is one of its own h1 columns.
-template <int E0, int E1, int E2>
-struct FwdSplit {
-  using MD = MixDims<E0, E1, E2>;
-  static constexpr int S1 = (E1 / 2) / 8 * 8;
-  static constexpr int S2 = S1 * MD::Z2;
-  static constexpr int A0C = MD::K1 / 2;                 // h0 operand columns of half 0
-  // h0 columns each half computes: its operand columns and its residual sources
-  static constexpr int H0LO1 = (S1 / MD::Z1 < A0C) ? S1 / MD::Z1 : A0C;
-  static constexpr int H0N0 = (A0C > (S1 + MD::Z1 - 1) / MD::Z1) ? A0C : (S1 + MD::Z1 - 1) / MD::Z1;
-  static constexpr int H0N1 = E0 - H0LO1;
-  static constexpr int H0MAX = H0N0 > H0N1 ? H0N0 : H0N1;
-  static constexpr int H1N1 = E1 - S1;
-  static constexpr int H1MAX = S1 > H1N1 ? S1 : H1N1;
-};
-
-// layer 0 of one half: h0 (FP32) for the half's columns and its A0 chunks
-template <int E0, int E1, int E2, int HALF>
-__device__ __forceinline__ void fwd_layer0(float st, const float *sm, int row, char *opa, float (&h0)[16]) {
-  using MD = MixDims<E0, E1, E2>;
-  using SP = FwdSplit<E0, E1, E2>;
-  constexpr int lo = HALF ? SP::H0LO1 : 0, n = HALF ? SP::H0N1 : SP::H0N0;
-  static_assert(n <= 16, "h0 registers");
-#pragma unroll
-  for (int k = 0; k < n; ++k) h0[k] = tc::tanh_fast(fmaf(st, sm[lo + k], sm[E0 + lo + k]));
-  constexpr int c0 = HALF ? SP::A0C : 0, c1 = HALF ? MD::K1 : SP::A0C;
-#pragma unroll
-  for (int k8 = c0; k8 < c1; k8 += 8) {
-    float t[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int c = k8 + u;
-      t[u] = (c < E0) ? h0[(c - lo) < 0 ? 0 : ((c - lo) >= n ? n - 1 : (c - lo))] : 0.f;
-    }
-    *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(row, k8, MD::K1)) = pack8(t);
-  }
-}
-
-// epilogue of layer 1 for one half: h1 columns and their A1 chunks
-template <int E0, int E1, int E2, int HALF>
-__device__ __forceinline__ void fwd_epi1(uint32_t tD, uint32_t lane_off, const float *sm, int row, char *opa,
-                                         const float (&h0)[16], float (&h1)[32]) {
-  using MD = MixDims<E0, E1, E2>;
-  using SP = FwdSplit<E0, E1, E2>;
-  constexpr int c0 = HALF ? SP::S1 : 0, c1 = HALF ? E1 : SP::S1;
-  constexpr int h0lo = HALF ? SP::H0LO1 : 0;
-  constexpr int g0 = c0 / 16 * 16, g1 = (c1 + 15) / 16 * 16, NG = (g1 - g0) / 16;
-  static_assert(c1 - c0 <= 32, "h1 registers");
-  uint32_t r[NG][16];
-#pragma unroll
-  for (int q = 0; q < NG; ++q) tc::tmem_ld16_issue(tD + lane_off + g0 + 16 * q, r[q]);
-  tc::tmem_wait();
-#pragma unroll
-  for (int q = 0; q < NG; ++q)
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int c = g0 + 16 * q + i;
-      if (c >= c0 && c < c1)
-        h1[c - c0] = tc::tanh_fast(__uint_as_float(r[q][i]) + sm[2 * E0 + c]) + h0[c / MD::Z1 - h0lo];
-    }
-  constexpr int k0 = HALF ? SP::S1 : 0, k1 = HALF ? MD::K2 : SP::S1;
-#pragma unroll
-  for (int k8 = k0; k8 < k1; k8 += 8) {
-    float t[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int c = k8 + u;
-      t[u] = (c < c1) ? h1[c - c0] : 0.f;
-    }
-    *reinterpret_cast<uint4 *>(opa + tc::kmajor_off(row, k8, MD::K2)) = pack8(t);
-  }
-}
-
-// epilogue of layer 2 for one half: h2 columns into the MN-major operand H2
-template <int E0, int E1, int E2, int HALF>
-__device__ __forceinline__ void fwd_epi2(uint32_t tD, uint32_t lane_off, const float *sm, int row, char *opa,
-                                         const float (&h1)[32]) {
-  using MD = MixDims<E0, E1, E2>;
-  using SP = FwdSplit<E0, E1, E2>;
-  constexpr int c0 = HALF ? SP::S2 : 0, c1 = HALF ? MD::N2 : SP::S2;
-  constexpr int h1lo = HALF ? SP::S1 : 0, h1n = HALF ? SP::H1N1 : SP::S1;
-#pragma unroll
-  for (int gg = c0 / 16 * 16; gg < c1; gg += 32) {
-    uint32_t r[2][16];
-    tc::tmem_ld16_issue(tD + lane_off + gg, r[0]);
-    if (gg + 16 < c1) tc::tmem_ld16_issue(tD + lane_off + gg + 16, r[1]);
-    tc::tmem_wait();
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int g = gg + 16 * q;
-#pragma unroll
-      for (int h8 = 0; h8 < 16; h8 += 8) {
-        if (g + h8 < c0 || g + h8 >= c1) continue;
-        float h2[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int col = g + h8 + i;
-          const int src = col / MD::Z2 - h1lo;
-          h2[i] = (col < E2) ? tc::tanh_fast(__uint_as_float(r[q][h8 + i]) + sm[2 * E0 + E1 + (col < E2 ? col : 0)]) +
-                                   h1[src < 0 ? 0 : (src >= h1n ? h1n - 1 : src)]
-                             : 0.f;
-        }
-        *reinterpret_cast<uint4 *>(opa + tc::mnmajor_off(row, g + h8, MD::N2)) = pack8(h2);
-      }
-    }
-  }
-}
-
 template <int E0, int E1, int E2>
 __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, SysDesc D, int ti,
                                                                   const float4 *__restrict__ posS,
@@ -437,6 +512,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
                                                                   __nv_bfloat16 *__restrict__ Gout,
                                                                   int *__restrict__ err) {
   using MD = MixDims<E0, E1, E2>;
+  using SP = HalfSplit<E0, E1, E2>;
   extern __shared__ __align__(1024) char smem[];
   char *netb = smem;
   float *small = reinterpret_cast<float *>(netb + round1k(MD::NETB));
@@ -465,11 +541,12 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
   const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
   const int nblk = nbpf * D.F;
   const float inv_std = M.inv_std[ti], mean = M.mean[ti];
-  const uint32_t idesc1 = tc::idesc_bf16(128, MD::N1, 0, 0);
-  const uint32_t idesc2 = tc::idesc_bf16(128, MD::N2, 0, 0);
-  const uint32_t idesc3 = tc::idesc_bf16(128, MD::N2, 1, 1);
+  const uint32_t idesc1 = tc::idesc_f16(128, MD::N1, 0, 0);
+  const uint32_t idesc2 = tc::idesc_f16(128, MD::N2, 0, 0);
+  const uint32_t idesc3 = tc::idesc_f16(128, MD::N2, 1, 1);
   const uint32_t opa_u = tc::smem_u32(opa), rblk_u = tc::smem_u32(rblk);
   const uint32_t w1_u = tc::smem_u32(netb), w2_u = w1_u + MD::W1B;
+  auto h2off = [row](int k8) { return tc::mnmajor_off(row, k8, MD::N2); };
   int loaded_net = -1;
 
   for (int blk = blockIdx.x; blk < nblk && ok; blk += gridDim.x) {
@@ -534,14 +611,15 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image visible; rowbuf read by every thread
-          float h0[16];
-          if (half == 0) fwd_layer0<E0, E1, E2, 0>(st, sm, row, opa, h0);
-          else fwd_layer0<E0, E1, E2, 1>(st, sm, row, opa, h0);
+          __half2 h0[SP::NP0], h1[SP::NP1];
+          if (half == 0) emb_layer0<E0, E1, E2, 0, false>(st, sm, row, opa, nullptr, h0, h0);
+          else emb_layer0<E0, E1, E2, 1, false>(st, sm, row, opa, nullptr, h0, h0);
           my_slot = slot;
           if (half == 0 && act) {
             const uint32_t o = tc::mnmajor_off(row, 16 * slot, 128);
-            *reinterpret_cast<uint4 *>(rblk + o) = pack8(R);
-            *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(tc::pack_bf16(R[8], R[9]), 0u, 0u, 0u);
+            st_pairs(rblk + o, tc::f2_to_h2(R[0], R[1]), tc::f2_to_h2(R[2], R[3]), tc::f2_to_h2(R[4], R[5]),
+                     tc::f2_to_h2(R[6], R[7]));
+            *reinterpret_cast<uint4 *>(rblk + o + 128) = make_uint4(tc::as_u32(tc::f2_to_h2(R[8], R[9])), 0u, 0u, 0u);
           }
           tc::fence_proxy_async();
           tc::fence_before_sync();
@@ -557,9 +635,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           }
           MIX_WAIT();
           if (!ok) break;
-          float h1[32];
-          if (half == 0) fwd_epi1<E0, E1, E2, 0>(tD, lane_off, sm, row, opa, h0, h1);
-          else fwd_epi1<E0, E1, E2, 1>(tD, lane_off, sm, row, opa, h0, h1);
+          if (half == 0) emb_epi1<E0, E1, E2, 0, false>(tD + lane_off, 0, row, opa, nullptr, h0, h0, h1, h1);
+          else emb_epi1<E0, E1, E2, 1, false>(tD + lane_off, 0, row, opa, nullptr, h0, h0, h1, h1);
           tc::fence_proxy_async();
           tc::fence_before_sync();
           __syncthreads();
@@ -574,8 +651,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           }
           MIX_WAIT();
           if (!ok) break;
-          if (half == 0) fwd_epi2<E0, E1, E2, 0>(tD, lane_off, sm, row, opa, h1);
-          else fwd_epi2<E0, E1, E2, 1>(tD, lane_off, sm, row, opa, h1);
+          if (half == 0) emb_epi2<E0, E1, E2, 0, false>(tD + lane_off, 0, opa, nullptr, h2off, h1, h1);
+          else emb_epi2<E0, E1, E2, 1, false>(tD + lane_off, 0, opa, nullptr, h2off, h1, h1);
           tc::fence_proxy_async();
           tc::fence_before_sync();
           __syncthreads();
@@ -738,12 +815,15 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
 
 // ---------------------------------------------------------------- dE/dT (SIMT, warp per atom)
 // Adjoint of the descriptor (dpmodel.py:74-78): from dE/dG (BF16, from the
-// fitting chain) and T, dE/dT / Nnbrs as BF16 rows [atom][c][w] (w padded to
-// N2 with zeros), the B operand rows of the tensor-core adjoint.
+// fitting chain) and T, dE/dT / Nnbrs as FP16 rows [atom][c][w] (w padded to
+// N2 with zeros), the B operand rows of the tensor-core adjoint.  Each atom's
+// rows are scaled by the power of two 2^k that puts their largest magnitude in
+// [2^13, 2^14) (exact in FP32, and FP16 keeps ~2^-24 of that range normal);
+// dTs[atom] = 2^-k undoes it.
 template <int E2, int N2, int W>
 __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
                                                 const __nv_bfloat16 *__restrict__ dG,
-                                                __nv_bfloat16 *__restrict__ dTb) {
+                                                __half *__restrict__ dTh, float *__restrict__ dTs) {
   // Warp per atom; lane owns the column pairs w = 2 lane + 64 j (+0, +1).
   // The atom's dE/dG rows stay in registers (D[a][2j + h]); X = T + Tbias
   // sits in shared memory.
@@ -863,8 +943,9 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
     if (lane < 16) dQ[c * 16 + lane] = p[0];  // the sum for a = lane
   }
   __syncwarp();
-  __nv_bfloat16 *out = dTb + g * 10 * N2;
-#pragma unroll 1
+  float o[10][NJ][2];
+  float amax = 0.f;
+#pragma unroll
   for (int c = 0; c < 10; ++c) {
     float q[16];
 #pragma unroll
@@ -872,7 +953,6 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
       const int w = 2 * lane + 64 * j;
-      float v2[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int ww = w + h;
@@ -895,66 +975,76 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
             }
           }
         }
-        v2[h] = ww < E2 ? v * M.inv_nnbrs : 0.f;
+        v = ww < E2 ? v * M.inv_nnbrs : 0.f;
+        o[c][j][h] = v;
+        amax = fmaxf(amax, fabsf(v));
       }
-      if (w < N2) *reinterpret_cast<__nv_bfloat162 *>(out + c * N2 + w) = __floats2bfloat162_rn(v2[0], v2[1]);
     }
   }
-}
-
-// Columns 10 S .. 10 S + 9 of an 80-column TMEM row held in registers.
-template <int S>
-__device__ __forceinline__ void slot_cols(const uint32_t (&r)[kDtN / 16][16], float (&out)[10]) {
 #pragma unroll
-  for (int c = 0; c < 10; ++c) out[c] = __uint_as_float(r[(10 * S + c) / 16][(10 * S + c) % 16]);
+  for (int off = 16; off > 0; off >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+  // amax = m 2^e with m in [0.5, 1): scale 2^(14 - e) puts it in [2^13, 2^14)
+  int e = 0;
+  if (amax > 0.f && amax < INFINITY) frexpf(amax, &e);
+  const int k = (amax > 0.f && amax < INFINITY) ? 14 - e : 0;
+  const float scale = ldexpf(1.f, k);
+  if (lane == 0) dTs[g] = ldexpf(1.f, -k);
+  __half *out = dTh + g * 10 * N2;
+#pragma unroll
+  for (int c = 0; c < 10; ++c)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int w = 2 * lane + 64 * j;
+      if (w < N2)
+        *reinterpret_cast<__half2 *>(out + c * N2 + w) = tc::f2_to_h2(o[c][j][0] * scale, o[c][j][1] * scale);
+    }
 }
 
-__device__ __forceinline__ void slot_cols_rt(int slot, const uint32_t (&r)[kDtN / 16][16], float (&out)[10]) {
-  static_assert(kBlkAtoms == 8, "one case per slot");
-  switch (slot) {  // a warp's rows are sorted by slot: one or two cases run per warp
-    case 0: slot_cols<0>(r, out); break;
-    case 1: slot_cols<1>(r, out); break;
-    case 2: slot_cols<2>(r, out); break;
-    case 3: slot_cols<3>(r, out); break;
-    case 4: slot_cols<4>(r, out); break;
-    case 5: slot_cols<5>(r, out); break;
-    case 6: slot_cols<6>(r, out); break;
-    default: slot_cols<7>(r, out); break;
-  }
-}
+// ---------------------------------------------------------------- embedding adjoint (FP16 tcgen05)
+// Per block of 8 centre atoms: the B tile DTB holds the atoms' dE/dT rows
+// (FP16, each atom's rows scaled by a power of two, k_mix_dT) as rows
+// n = 16 slot + c (c < 10; rows 10..15 of a slot zero), K = N2.  The rows are
+// recomputed with their tangent along s~ (forward mode), two threads per row
+// as in the forward kernel: [h0, dh0] -> tcgen05 -> [h1, dh1] -> tcgen05 ->
+// [h2, dh2], then U = H2 . DTB and V = dH2 . DTB on the tensor cores over the
+// slots the tile's rows belong to only (N = 16 x the tile's slot count; rows
+// are sorted by slot); a row reads its slot's 16 columns: u = dE/dR~ and
+// dE/ds~ = R~ . v.  The FP32 row adjoint gives dE/dx (unscaled by the atom's
+// factor); half 0 scatters it as the neighbour's force and sums the virial,
+// half 1 reduces the centre atoms' forces.  One resident net, 2 CTAs per SM.
+constexpr int kBwdThreads = 256;
+constexpr int kBwdCpt = 1;  // compaction candidates per thread, adjoint
+constexpr int kRowCapBwd = 128 + kBwdThreads * kBwdCpt;
+constexpr int kDtbRows = 16 * kBlkAtoms;  // DTB rows: 16 per atom slot
 
-// ---------------------------------------------------------------- embedding adjoint (BF16 tcgen05)
-// Per block of 8 centre atoms: the B tile DTB (N = 8 slots x 10 channels,
-// K = N2) is copied from the per-atom dE/dT rows.  The rows are recomputed
-// with their tangent along s~ (forward mode): [h0, dh0] -> tcgen05 ->
-// [h1, dh1] -> tcgen05 -> [h2, dh2], then U = H2 . DTB and V = dH2 . DTB on
-// the tensor cores; a row reads its atom's slot: u = dE/dR~ and
-// dE/ds~ = R~ . v.  The FP32 row adjoint gives dE/dx, scattered as forces and
-// reduced into the virial.  One resident net, 2 CTAs per SM.
 template <int E0, int E1, int E2>
-__global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D, int ti,
-                                                          const float4 *__restrict__ posS,
-                                                          const float *__restrict__ box,
-                                                          const int32_t *__restrict__ nbrs,
-                                                          const __nv_bfloat16 *__restrict__ dTb,
-                                                          float4 *__restrict__ F4, double *__restrict__ virial,
-                                                          int *__restrict__ err) {
+__global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, SysDesc D, int ti,
+                                                                  const float4 *__restrict__ posS,
+                                                                  const float *__restrict__ box,
+                                                                  const int32_t *__restrict__ nbrs,
+                                                                  const __half *__restrict__ dTh,
+                                                                  const float *__restrict__ dTs,
+                                                                  float4 *__restrict__ F4,
+                                                                  double *__restrict__ virial,
+                                                                  int *__restrict__ err) {
   using MD = MixDims<E0, E1, E2>;
-  constexpr int DTB_BYTES = kDtN * MD::N2 * 2;
-  constexpr int OPB = 2 * MD::OPA_H2;
+  using SP = HalfSplit<E0, E1, E2>;
+  constexpr int DTB_BYTES = kDtbRows * MD::N2 * 2;
   extern __shared__ __align__(1024) char smem[];
   char *netb = smem;
   float *small = reinterpret_cast<float *>(netb + round1k(MD::NETB));
   char *dtb = reinterpret_cast<char *>(small) + round1k(MD::NSMALL * 4);
   char *opb = dtb + round1k(DTB_BYTES);
-  float4 *rowbuf = reinterpret_cast<float4 *>(opb + round1k(OPB));
-  __shared__ int wcnt[4];
+  float4 *rowbuf = reinterpret_cast<float4 *>(opb + round1k(2 * MD::OPA));
+  __shared__ int wcnt[kBwdThreads / 32];
   __shared__ float3 ri_s[kBlkAtoms];
   __shared__ float fi_s[kBlkAtoms * 3];
+  __shared__ float sc_s[kBlkAtoms];
   __shared__ double vir_s[9];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tbase_s;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = tid & 127, half = tid >> 7;
 
   if (tid < 9) vir_s[tid] = 0.0;
   if (tid == 0) tc::mbar_init(&mbar, 1);
@@ -962,7 +1052,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t tbase = tbase_s, lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t tbase = tbase_s, lane_off = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t ph = 0;
   bool ok = true;
   float vir[9];
@@ -975,7 +1065,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       const float s = warp_sum(vir[k]);
-      if ((tid & 31) == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
+      if (lane == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
       vir[k] = 0.f;
     }
     __syncthreads();
@@ -990,12 +1080,13 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
   const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
   const int nblk = nbpf * D.F;
   const float inv_std = M.inv_std[ti], mean = M.mean[ti];
-  const uint32_t idesc1 = tc::idesc_bf16(128, MD::N1, 0, 0);
-  const uint32_t idesc2 = tc::idesc_bf16(128, MD::N2, 0, 0);
-  const uint32_t idesc3 = tc::idesc_bf16(128, kDtN, 0, 0);
+  const uint32_t idesc1 = tc::idesc_f16(128, MD::N1, 0, 0);
+  const uint32_t idesc2 = tc::idesc_f16(128, MD::N2, 0, 0);
   const uint32_t opb_u = tc::smem_u32(opb), dtb_u = tc::smem_u32(dtb);
   const uint32_t w1_u = tc::smem_u32(netb), w2_u = w1_u + MD::W1B;
-  const uint32_t oA0 = 0, oA0t = MD::OPA_A0, oA1 = 0, oA1t = MD::OPA_A1, oH2 = 0, oH2t = MD::OPA_H2;
+  // operand offsets in opb: each layer's value operand at 0, its tangent at OPA
+  constexpr uint32_t kTan = MD::OPA;
+  auto h2off = [row](int k8) { return tc::kmajor_off(row, k8, MD::N2); };
   int loaded_net = -1;
 
   for (int blk = blockIdx.x; blk < nblk && ok; blk += gridDim.x) {
@@ -1008,7 +1099,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
       const size_t gn = (size_t)fn * D.N + D.offs[ti] + an;
       const int nbn = min(kBlkAtoms, cnt_i - an);
       prefetch_range_l2(nbrs + gn * D.S, (size_t)nbn * D.S * 4);
-      prefetch_range_l2(dTb + gn * 10 * MD::N2, (size_t)nbn * 10 * MD::N2 * 2);
+      prefetch_range_l2(dTh + gn * 10 * MD::N2, (size_t)nbn * 10 * MD::N2 * 2);
     }
     const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
     if (bs != vframe) {
@@ -1021,14 +1112,15 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
     if (tid < nb) {
       const float4 q = posS[g0 + tid];
       ri_s[tid] = make_float3(q.x, q.y, q.z);
+      sc_s[tid] = dTs[g0 + tid];
     }
     if (tid < kBlkAtoms * 3) fi_s[tid] = 0.f;
-    // ---- DTB: rows n = 10 slot + c of the 8 atoms (K-major, K = N2); zero for missing atoms
-    for (int e = tid; e < kDtN * (MD::N2 / 8); e += 128) {
+    // ---- DTB: rows n = 16 slot + c of the 8 atoms (K-major, K = N2); zero for c >= 10 and missing atoms
+    for (int e = tid; e < kDtbRows * (MD::N2 / 8); e += kBwdThreads) {
       const int n = e / (MD::N2 / 8), k8 = (e - n * (MD::N2 / 8)) * 8;
-      const int slot = n / 10, c = n - slot * 10;
+      const int slot = n >> 4, c = n & 15;
       char *dst = dtb + tc::kmajor_off(n, k8, MD::N2);
-      if (slot < nb) tc::cp_async16(dst, dTb + ((g0 + slot) * 10 + c) * MD::N2 + k8);
+      if (slot < nb && c < 10) tc::cp_async16(dst, dTh + ((g0 + slot) * 10 + c) * MD::N2 + k8);
       else *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
     }
     tc::cp_async_commit();
@@ -1041,7 +1133,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
-      constexpr int kStep = 128 * kBwdCpt;
+      constexpr int kStep = kBwdThreads * kBwdCpt;
       for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
         if (!flush)
@@ -1054,35 +1146,19 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
             mix_load_net<E0, E1, E2>(M, knet, netb, small);
             loaded_net = knet;
           }
-          const bool act = tid < nrows;
-          const float4 rv = act ? rowbuf[rowstart + tid] : make_float4(100.f, 100.f, 100.f, 0.f);
-          const int packed = act ? __float_as_int(rv.w) : 0;
-          const int slot = packed & 7, jsrc = packed >> 3;
-          RowGeom gm;
-          float st, R[10];
-          mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
+          const bool act = row < nrows;
+          const float4 rv = act ? rowbuf[rowstart + row] : make_float4(100.f, 100.f, 100.f, 0.f);
+          // rows are sorted by slot: the tile's slots are [smin, smax]
+          const int smin = __float_as_int(rowbuf[rowstart].w) & 7;
+          const int smax = __float_as_int(rowbuf[rowstart + nrows - 1].w) & 7;
+          const float st = row_stilde(rv, M.rcut, inv_std, mean);
           tc::cp_async_wait<0>();
           __syncthreads();  // net image and DTB visible
-          float h1[E1], d1[E1];
+          __half2 h1[SP::NP1], d1[SP::NP1];
           {
-            float h0[E0], d0[E0];
-#pragma unroll
-            for (int k = 0; k < E0; ++k) {
-              const float t = tc::tanh_fast(fmaf(st, sm[k], sm[E0 + k]));
-              h0[k] = t;
-              d0[k] = (1.f - t * t) * sm[k];
-            }
-#pragma unroll
-            for (int k8 = 0; k8 < MD::K1; k8 += 8) {
-              float a_[8], b_[8];
-#pragma unroll
-              for (int u = 0; u < 8; ++u) {
-                a_[u] = (k8 + u < E0) ? h0[min(k8 + u, E0 - 1)] : 0.f;
-                b_[u] = (k8 + u < E0) ? d0[min(k8 + u, E0 - 1)] : 0.f;
-              }
-              *reinterpret_cast<uint4 *>(opb + oA0 + tc::kmajor_off(tid, k8, MD::K1)) = pack8(a_);
-              *reinterpret_cast<uint4 *>(opb + oA0t + tc::kmajor_off(tid, k8, MD::K1)) = pack8(b_);
-            }
+            __half2 h0[SP::NP0], d0[SP::NP0];
+            if (half == 0) emb_layer0<E0, E1, E2, 0, true>(st, sm, row, opb, opb + kTan, h0, d0);
+            else emb_layer0<E0, E1, E2, 1, true>(st, sm, row, opb, opb + kTan, h0, d0);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
@@ -1091,40 +1167,21 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 #pragma unroll
               for (int ks = 0; ks < MD::K1 / 16; ++ks) {
                 const uint64_t bd = tc::make_desc(w1_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128);
-                tc::mma_bf16(tbase, tc::make_desc(opb_u + oA0 + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
                                                   (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
-                tc::mma_bf16(tbase + 64, tc::make_desc(opb_u + oA0t + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                tc::mma_bf16(tbase + 64, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
                                                        (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
               }
               tc::commit(&mbar);
             }
             MIX_WAIT();
             if (!ok) break;
-#pragma unroll
-            for (int c0 = 0; c0 < MD::N1; c0 += 16) {
-              uint32_t z[16], dz[16];
-              tc::tmem_ld16_issue(tbase + lane_off + c0, z);
-              tc::tmem_ld16_issue(tbase + 64 + lane_off + c0, dz);
-              tc::tmem_wait();
-#pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if (c0 + i < E1) {
-                  const float t = tc::tanh_fast(__uint_as_float(z[i]) + sm[2 * E0 + c0 + i]);
-                  h1[c0 + i] = t + h0[(c0 + i) / MD::Z1];
-                  d1[c0 + i] = (1.f - t * t) * __uint_as_float(dz[i]) + d0[(c0 + i) / MD::Z1];
-                }
-            }
-          }
-#pragma unroll
-          for (int k8 = 0; k8 < MD::K2; k8 += 8) {
-            float a_[8], b_[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              a_[u] = (k8 + u < E1) ? h1[min(k8 + u, E1 - 1)] : 0.f;
-              b_[u] = (k8 + u < E1) ? d1[min(k8 + u, E1 - 1)] : 0.f;
-            }
-            *reinterpret_cast<uint4 *>(opb + oA1 + tc::kmajor_off(tid, k8, MD::K2)) = pack8(a_);
-            *reinterpret_cast<uint4 *>(opb + oA1t + tc::kmajor_off(tid, k8, MD::K2)) = pack8(b_);
+            if (half == 0)
+              emb_epi1<E0, E1, E2, 0, true>(tbase + lane_off, tbase + 64 + lane_off, row, opb, opb + kTan, h0, d0, h1,
+                                            d1);
+            else
+              emb_epi1<E0, E1, E2, 1, true>(tbase + lane_off, tbase + 64 + lane_off, row, opb, opb + kTan, h0, d0, h1,
+                                            d1);
           }
           tc::fence_proxy_async();
           tc::fence_before_sync();
@@ -1134,86 +1191,88 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 #pragma unroll
             for (int ks = 0; ks < MD::K2 / 16; ++ks) {
               const uint64_t bd = tc::make_desc(w2_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128);
-              tc::mma_bf16(tbase, tc::make_desc(opb_u + oA1 + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+              tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
                                                 (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
-              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + oA1t + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
                                                       (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
             }
             tc::commit(&mbar);
           }
           MIX_WAIT();
           if (!ok) break;
-#pragma unroll
-          for (int c0 = 0; c0 < MD::N2; c0 += 16) {
-            uint32_t z[16], dz[16];
-            tc::tmem_ld16_issue(tbase + lane_off + c0, z);
-            tc::tmem_ld16_issue(tbase + 128 + lane_off + c0, dz);
-            tc::tmem_wait();
-            float hh[16], dd[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              if (c0 + i < E2) {
-                const float t = tc::tanh_fast(__uint_as_float(z[i]) + sm[2 * E0 + E1 + min(c0 + i, E2 - 1)]);
-                hh[i] = t + h1[min((c0 + i) / MD::Z2, E1 - 1)];
-                dd[i] = (1.f - t * t) * __uint_as_float(dz[i]) + d1[min((c0 + i) / MD::Z2, E1 - 1)];
-              } else {
-                hh[i] = 0.f;
-                dd[i] = 0.f;
-              }
-            }
-            *reinterpret_cast<uint4 *>(opb + oH2 + tc::kmajor_off(tid, c0, MD::N2)) = pack8(hh);
-            *reinterpret_cast<uint4 *>(opb + oH2 + tc::kmajor_off(tid, c0 + 8, MD::N2)) = pack8(hh + 8);
-            *reinterpret_cast<uint4 *>(opb + oH2t + tc::kmajor_off(tid, c0, MD::N2)) = pack8(dd);
-            *reinterpret_cast<uint4 *>(opb + oH2t + tc::kmajor_off(tid, c0 + 8, MD::N2)) = pack8(dd + 8);
-          }
+          if (half == 0)
+            emb_epi2<E0, E1, E2, 0, true>(tbase + lane_off, tbase + 128 + lane_off, opb, opb + kTan, h2off, h1, d1);
+          else
+            emb_epi2<E0, E1, E2, 1, true>(tbase + lane_off, tbase + 128 + lane_off, opb, opb + kTan, h2off, h1, d1);
           tc::fence_proxy_async();
           tc::fence_before_sync();
           __syncthreads();
           if (tid == 0) {
             tc::fence_after_sync();
+            const uint32_t idesc3 = tc::idesc_f16(128, 16 * (smax - smin + 1), 0, 0);
 #pragma unroll
             for (int ks = 0; ks < MD::N2 / 16; ++ks) {
-              const uint64_t bd = tc::make_desc(dtb_u + tc::kmajor_off(0, 16 * ks, MD::N2), 128, (MD::N2 / 8) * 128);
-              tc::mma_bf16(tbase, tc::make_desc(opb_u + oH2 + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+              const uint64_t bd =
+                  tc::make_desc(dtb_u + tc::kmajor_off(16 * smin, 16 * ks, MD::N2), 128, (MD::N2 / 8) * 128);
+              tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
                                                 (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
-              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + oH2t + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
                                                       (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
             }
             tc::commit(&mbar);
           }
           MIX_WAIT();
           if (!ok) break;
-          // ---- u, v of this row's atom slot (columns 10 slot .. 10 slot + 9)
+          // ---- u, v of this row's slot: the warp loads the 16-column block of
+          // each slot among its rows (sorted, so one or two blocks)
+          const int packed = act ? __float_as_int(rv.w) : 0;
+          const int slot = packed & 7, jsrc = packed >> 3;
+          const int wmin = __reduce_min_sync(0xffffffffu, act ? slot : 7);
+          const int wmax = __reduce_max_sync(0xffffffffu, act ? slot : 0);
           float u[10], v[10];
-          {
-            uint32_t r[kDtN / 16][16];
 #pragma unroll
-            for (int q = 0; q < kDtN / 16; ++q) tc::tmem_ld16_issue(tbase + lane_off + 16 * q, r[q]);
-            tc::tmem_wait();
-            slot_cols_rt(slot, r, u);
+          for (int c = 0; c < 10; ++c) u[c] = v[c] = 0.f;
+          for (int uv = 0; uv < 2; ++uv)
+            for (int sl = wmin; sl <= wmax; ++sl) {
+              uint32_t r16[16];
+              tc::tmem_ld16_issue(tbase + 128 * uv + lane_off + (uint32_t)(16 * (sl - smin)), r16);
+              tc::tmem_wait();
+              if (slot == sl) {
 #pragma unroll
-            for (int q = 0; q < kDtN / 16; ++q) tc::tmem_ld16_issue(tbase + 128 + lane_off + 16 * q, r[q]);
-            tc::tmem_wait();
-            slot_cols_rt(slot, r, v);
-          }
+                for (int c = 0; c < 10; ++c) {
+                  if (uv == 0) u[c] = __uint_as_float(r16[c]);
+                  else v[c] = __uint_as_float(r16[c]);
+                }
+              }
+            }
           tc::fence_before_sync();
+          RowGeom gm;
           float gst = 0.f;
+          {
+            float st2, R[10];
+            mix_row_env(rv, M.rcut, inv_std, mean, gm, st2, R);
 #pragma unroll
-          for (int c = 0; c < 10; ++c) gst = fmaf(R[c], v[c], gst);
+            for (int c = 0; c < 10; ++c) gst = fmaf(R[c], v[c], gst);
+          }
           float gx[3];
           row_adjoint_mixed(gm, inv_std, u, gst, gx);
-          if (act) {
-            atomicAdd(&F4[frame_base + jsrc], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
+          const float scl = act ? sc_s[slot] : 0.f;  // undo the atom's dE/dT scale
+          gx[0] *= scl;
+          gx[1] *= scl;
+          gx[2] *= scl;
+          if (half == 0) {
+            if (act) {
+              atomicAdd(&F4[frame_base + jsrc], make_float4(-gx[0], -gx[1], -gx[2], 0.f));
 #pragma unroll
-            for (int p3 = 0; p3 < 3; ++p3)
+              for (int p3 = 0; p3 < 3; ++p3)
 #pragma unroll
-              for (int q3 = 0; q3 < 3; ++q3) vir[p3 * 3 + q3] -= gm.x[p3] * gx[q3];
-          }
-          {
+                for (int q3 = 0; q3 < 3; ++q3) vir[p3 * 3 + q3] -= gm.x[p3] * gx[q3];
+            }
+          } else {
             // centre-atom force: the warp's rows are sorted by slot, so a
             // segmented suffix sum leaves each slot's total on its first lane
-            const int lane = tid & 31, key = act ? slot : -1 - lane;
-            float s0 = act ? gx[0] : 0.f, s1 = act ? gx[1] : 0.f, s2 = act ? gx[2] : 0.f;
+            const int key = act ? slot : -1 - lane;
+            float s0 = gx[0], s1 = gx[1], s2 = gx[2];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
               const int ko = __shfl_down_sync(0xffffffffu, key, o);
@@ -1246,7 +1305,7 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     const float s = warp_sum(vir[k]);
-    if ((tid & 31) == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
+    if (lane == 0 && s != 0.f) atomicAdd(&vir_s[k], (double)s);
   }
   if (!ok) {
     if (tid == 0) atomicOr(err, 1);
@@ -1262,13 +1321,13 @@ __global__ void __launch_bounds__(128, 2) k_mix_embed_bwd(DevModel M, SysDesc D,
 template <int E0, int E1, int E2>
 size_t mix_bwd_smem() {
   using MD = MixDims<E0, E1, E2>;
-  return (size_t)round1k(MD::NETB) + round1k(MD::NSMALL * 4) + round1k(kDtN * MD::N2 * 2) +
-         round1k(2 * MD::OPA_H2) + kRowCap * 16;
+  return (size_t)round1k(MD::NETB) + round1k(MD::NSMALL * 4) + round1k(kDtbRows * MD::N2 * 2) +
+         round1k(2 * MD::OPA) + kRowCapBwd * 16;
 }
 
 template <int E0, int E1, int E2>
 int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
-                         const float *box, const int32_t *nbrs, const __nv_bfloat16 *dTb, float4 *F4,
+                         const float *box, const int32_t *nbrs, const __half *dTh, const float *dTs, float4 *F4,
                          double *virial, int *err, cudaStream_t st) {
   using MD = MixDims<E0, E1, E2>;
   const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -1284,9 +1343,9 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
     const int nb1 = (cnt + kBlkAtoms - 1) / kBlkAtoms;
     const int grid = nb1 < 2 * nsm ? nb1 : 2 * nsm;
     const size_t off = (size_t)f * D.N;
-    k_mix_embed_bwd<E0, E1, E2><<<grid, 128, smem, st>>>(M, Df, ti, posS + off, box + f * 3,
-                                                          nbrs + off * D.S, dTb + off * 10 * MD::N2, F4 + off,
-                                                          virial + f * 9, err);
+    k_mix_embed_bwd<E0, E1, E2><<<grid, kBwdThreads, smem, st>>>(M, Df, ti, posS + off, box + f * 3,
+                                                                  nbrs + off * D.S, dTh + off * 10 * MD::N2,
+                                                                  dTs + off, F4 + off, virial + f * 9, err);
     count_launch();
   }
   DPB_LAUNCH_CHECK();
@@ -1741,26 +1800,27 @@ size_t mixed_workspace_fixed(const DevModel &M) {
 
 size_t mixed_workspace_per_atom(const DevModel &M) {
   const int FW = M.FW[0], K0 = M.A * M.E2;
-  return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 + 16 +
+  return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 + 4 + 16 +
          (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
 }
 
 // dE/dT with W atoms (warps) per block, W in {2, 4, 8} (launch shape only).
 template <int W>
 static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb,
-                            __nv_bfloat16 *dTb, cudaStream_t st) {
+                            __half *dTh, float *dTs, cudaStream_t st) {
   const unsigned grid = (unsigned)((NF + W - 1) / W);
-  if (M.E2 == 100) k_mix_dT<100, 112, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTb);
-  else k_mix_dT<64, 64, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTb);
+  if (M.E2 == 100) k_mix_dT<100, 112, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTh, dTs);
+  else k_mix_dT<64, 64, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTh, dTs);
   count_launch();
 }
 
-static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb, __nv_bfloat16 *dTb,
+static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb, __half *dTh,
+                         float *dTs,
                          int warps, cudaStream_t st) {
   switch (warps) {
-    case 2: launch_mix_dT_w<2>(M, NF, T, dGb, dTb, st); break;
-    case 8: launch_mix_dT_w<8>(M, NF, T, dGb, dTb, st); break;
-    default: launch_mix_dT_w<4>(M, NF, T, dGb, dTb, st); break;
+    case 2: launch_mix_dT_w<2>(M, NF, T, dGb, dTh, dTs, st); break;
+    case 8: launch_mix_dT_w<8>(M, NF, T, dGb, dTh, dTs, st); break;
+    default: launch_mix_dT_w<4>(M, NF, T, dGb, dTh, dTs, st); break;
   }
   DPB_LAUNCH_CHECK();
   return DPB_OK;
@@ -1884,7 +1944,8 @@ struct MixedWs {
   float *T;
   __nv_bfloat16 *Gb;
   float *dG;
-  __nv_bfloat16 *dTb;
+  __half *dTh;   // dE/dT rows (FP16, scaled per atom)
+  float *dTs;    // per-atom inverse scale of dTh
   float4 *posS;
   float *scratch;
 };
@@ -1897,7 +1958,8 @@ static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
   o.T = (float *)w; w += al256(NF * 10 * M.E2 * 4);
   o.Gb = (__nv_bfloat16 *)w; w += al256(NF * K0 * 2);
   o.dG = (float *)w; w += al256(NF * K0 * 4);
-  o.dTb = (__nv_bfloat16 *)w; w += al256(NF * 10 * N2 * 2);
+  o.dTh = (__half *)w; w += al256(NF * 10 * N2 * 2);
+  o.dTs = (float *)w; w += al256(NF * 4);
   o.posS = (float4 *)w; w += al256(NF * 16);
   o.scratch = (float *)w;
   return o;
@@ -1915,9 +1977,9 @@ int mixed_tune_dT(const DevModel &M, size_t NF, void *ws, cudaStream_t st, int *
   *best = 4;
   int rc = DPB_OK;
   for (int c = 0; c < 3 && !rc; ++c) {
-    rc = launch_mix_dT(M, NF, w.T, dGb, w.dTb, cand[c], st);  // warm-up (idempotent: dTb from dG, T)
+    rc = launch_mix_dT(M, NF, w.T, dGb, w.dTh, w.dTs, cand[c], st);  // warm-up (idempotent: dTh from dG, T)
     cudaEventRecord(a, st);
-    for (int r = 0; r < 5 && !rc; ++r) rc = launch_mix_dT(M, NF, w.T, dGb, w.dTb, cand[c], st);
+    for (int r = 0; r < 5 && !rc; ++r) rc = launch_mix_dT(M, NF, w.T, dGb, w.dTh, w.dTs, cand[c], st);
     cudaEventRecord(b, st);
     if (cudaEventSynchronize(b) != cudaSuccess) rc = DPB_ERR_CUDA;
     float ms = 0.f;
@@ -1936,7 +1998,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   const MixedWs mw = mixed_ws(M, NF, ws);
   int *err = mw.err;
   float *T = mw.T, *dG = mw.dG, *scratch = mw.scratch;
-  __nv_bfloat16 *Gb = mw.Gb, *dTb = mw.dTb;
+  __nv_bfloat16 *Gb = mw.Gb;
   float4 *posS = mw.posS;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
   if (M.ngrids > 0)
@@ -1952,14 +2014,14 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);
-  rc = launch_mix_dT(M, NF, T, dGb, dTb, dT_warps, st);
+  rc = launch_mix_dT(M, NF, T, dGb, mw.dTh, mw.dTs, dT_warps, st);
   if (rc) return rc;
   prof_end(PROF_MIXED_DT, st);
   prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     rc = (M.E2 == 100)
-             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, posS, box, nbrs, dTb, F4, virial, err, st)
-             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, posS, box, nbrs, dTb, F4, virial, err, st);
+             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, F4, virial, err, st)
+             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, F4, virial, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_BWD, st);
