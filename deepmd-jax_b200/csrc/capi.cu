@@ -64,12 +64,18 @@ template <int E0, int E1, int E2>
 int launch_embed_bwd(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
                      const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
 int launch_sgemm(int, int, int, const float *, int, RowMap, const float *, const Epi &, cudaStream_t);
+// any embedding shape (eval_general.cu)
+int launch_embed_fwd_gen(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                         const int32_t *, float *, float *, cudaStream_t);
+int launch_embed_bwd_gen(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                         const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
 int launch_fit_energy(int, RowMap, int, const float *, const float *, const float *, const float *,
                       const float *, float *, float *, double *, int, const int32_t *, cudaStream_t);
 int launch_finalize(int, int, const float4 *, float *, const float *, const int32_t *, float *, double *, int,
                     const float *, const int32_t *, uint32_t *, cudaStream_t);
 // mixed path (mixed.cu)
 int mixed_supported(const DevModel &M);
+int mixed_fit_width(const DevModel &M);
 size_t mixed_workspace_per_atom(const DevModel &M);
 size_t mixed_workspace_fixed(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
@@ -123,8 +129,28 @@ static int upload_fit_tiles(dpb_model *m, const std::vector<float> &a, int rows,
   return upload_bf16(m, t, dev);
 }
 
-static bool embed_supported(const DevModel &M) {
-  return (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
+// The tuned three-layer embedding instantiations (FP32 and tensor-core kernels).
+static bool embed_tuned(const DevModel &M) {
+  return M.nemb == 3 && ((M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64));
+}
+
+// Shapes the reference's embedding_net builds (utils.py:110-124): widths whose
+// consecutive ratio is an integer one way or the other.
+static bool embed_shape_ok(const dpb_model_desc *d) {
+  if (d->n_embed < 1 || d->n_embed > kMaxEmbedLayers) return false;
+  for (int l = 0; l < d->n_embed; ++l) {
+    const int w = d->embed_widths[l];
+    if (w < 1 || w > 256) return false;
+    if (l > 0) {
+      const int p = d->embed_widths[l - 1];
+      if (w % p != 0 && p % w != 0) return false;
+    }
+  }
+  return true;
+}
+
+namespace dpb {
+bool embed_general_fits(const DevModel &M);
 }
 
 extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
@@ -133,30 +159,40 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DPB_ERR_NO_DEVICE;
   const int nt = d->ntypes;
-  if (nt < 1 || nt > kMaxTypes || d->n_embed != 3 || d->n_fit < 1 || d->n_fit > kMaxFitLayers)
+  if (nt < 1 || nt > kMaxTypes || !embed_shape_ok(d) || d->n_fit < 1 || d->n_fit > kMaxFitLayers)
     return DPB_ERR_UNSUPPORTED;
+  for (int l = 0; l < d->n_fit; ++l)
+    if (d->fit_widths[l] < 1 || d->fit_widths[l] > 1024) return DPB_ERR_UNSUPPORTED;
   dpb_model *m = new dpb_model();
   cudaGetDevice(&m->device);
   DevModel &M = m->dm;
   std::memset(&M, 0, sizeof(M));
   M.ntypes = nt;
-  M.E0 = d->embed_widths[0]; M.E1 = d->embed_widths[1]; M.E2 = d->embed_widths[2];
+  M.nemb = d->n_embed;
+  for (int l = 0; l < d->n_embed; ++l) M.EW[l] = d->embed_widths[l];
+  // E2 is the output width everywhere; E0 / E1 name the tuned kernels' layers
+  M.E2 = d->embed_widths[d->n_embed - 1];
+  M.E0 = d->n_embed == 3 ? d->embed_widths[0] : 0;
+  M.E1 = d->n_embed == 3 ? d->embed_widths[1] : 0;
+  M.emb_tuned = embed_tuned(M) ? 1 : 0;
   M.A = d->axis;
   M.nfit = d->n_fit;
   for (int l = 0; l < d->n_fit; ++l) M.FW[l] = d->fit_widths[l];
   M.rcut = (float)d->rcut;
   M.inv_nnbrs = (float)(1.0 / d->nnbrs);
-  if (!embed_supported(M) || M.A < 1 || 2 * M.A > 32 || 2 * M.A > M.E2) {
+  if (M.A < 1 || 2 * M.A > 32 || 2 * M.A > M.E2) {
     delete m;
     return DPB_ERR_UNSUPPORTED;
   }
-  for (int l = 1; l < d->n_fit; ++l)
-    if (M.FW[l] != M.FW[0]) { delete m; return DPB_ERR_UNSUPPORTED; }
   for (int t = 0; t < nt; ++t) {
     M.mean[t] = (float)d->sr_mean[t];
     M.inv_std[t] = (float)(1.0 / d->sr_std[t]);
   }
-  const int ew_in[3] = {1, M.E0, M.E1}, ew_out[3] = {M.E0, M.E1, M.E2};
+  int ew_in[kMaxEmbedLayers], ew_out[kMaxEmbedLayers];
+  for (int l = 0; l < M.nemb; ++l) {
+    ew_in[l] = l == 0 ? 1 : M.EW[l - 1];
+    ew_out[l] = M.EW[l];
+  }
   int rc = DPB_OK;
   const bool have_mlp = d->embed_kernel != nullptr && d->embed_bias != nullptr;
   if (d->n_grids < 0 || (d->n_grids == 0 && !have_mlp) ||
@@ -175,14 +211,11 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
     M.cmp_srmin[k] = lo;
     M.cmp_delta[k] = span / (float)M.ngrids;
   }
+  const int ne = M.nemb;
   for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp; ++k)
-    for (int l = 0; l < 3 && rc == DPB_OK; ++l) {
-      rc = upload(m, d->embed_kernel[k * 3 + l], (size_t)ew_in[l] * ew_out[l], &M.ew[k][l]);
-      if (rc == DPB_OK) rc = upload(m, d->embed_bias[k * 3 + l], (size_t)ew_out[l], &M.eb[k][l]);
-      if (rc == DPB_OK) {
-        std::vector<float> v(d->embed_kernel[k * 3 + l], d->embed_kernel[k * 3 + l] + (size_t)ew_in[l] * ew_out[l]);
-        rc = upload_bf16(m, v, &M.ew_bf[k][l]);
-      }
+    for (int l = 0; l < ne && rc == DPB_OK; ++l) {
+      rc = upload(m, d->embed_kernel[k * ne + l], (size_t)ew_in[l] * ew_out[l], &M.ew[k][l]);
+      if (rc == DPB_OK) rc = upload(m, d->embed_bias[k * ne + l], (size_t)ew_out[l], &M.eb[k][l]);
     }
   // shared-memory images of the embedding nets for the tensor-core kernels:
   // FP16 B tiles (K-major) of layers 1 and 2 with the layer's bias as one
@@ -195,7 +228,7 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
     const int npair0 = (M.E0 + 1) / 2;
     M.net_img_bytes = W1B + W2B;
     M.net_small_floats = (2 * M.E0 + npair0 + 3) / 4 * 4;
-    for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp; ++k) {
+    for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp && M.emb_tuned; ++k) {
       std::vector<uint8_t> img(M.net_img_bytes, 0);
       const float *W1 = d->embed_kernel[k * 3 + 1], *W2 = d->embed_kernel[k * 3 + 2];
       const float *b1 = d->embed_bias[k * 3 + 1], *b2 = d->embed_bias[k * 3 + 2];
@@ -231,6 +264,7 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   }
   if (rc == DPB_OK) rc = upload(m, d->tbias, (size_t)M.E2, &M.tbias);
   const int K0 = M.A * M.E2;
+  M.mfw = dpb::mixed_fit_width(M);
   for (int t = 0; t < nt && rc == DPB_OK; ++t) {
     for (int l = 0; l <= M.nfit && rc == DPB_OK; ++l) {
       const int in = l == 0 ? K0 : M.FW[l - 1];
@@ -250,17 +284,35 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
       if (rc == DPB_OK) rc = upload(m, kt.data(), kt.size(), &M.fwT[t][l]);
       if (rc == DPB_OK) rc = upload_bf16(m, kv, &M.fw_bf[t][l]);
       if (rc == DPB_OK) rc = upload_bf16(m, kt, &M.fwT_bf[t][l]);
-      if (rc == DPB_OK && l < M.nfit && mixed_supported(M)) {
-        rc = upload_fit_tiles(m, kt, outw, in, outw, &M.fit_bt[t][kFitBtFwd + l]);
-        if (rc == DPB_OK && l >= 1) rc = upload_fit_tiles(m, kv, in, outw, in, &M.fit_bt[t][kFitBtAdj + l]);
-        if (rc == DPB_OK && l == 0) rc = upload_fit_tiles(m, kv, K0, outw, 128, &M.fit_bt[t][kFitBtDg]);
-      }
-      if (rc == DPB_OK && l < M.nfit) {
-        const float *dt = d->fit_dt ? d->fit_dt[t * M.nfit + l] : nullptr;
-        if (dt) rc = upload(m, dt, (size_t)outw, &M.fdt[t][l]);
+      const float *dt = (l < M.nfit && d->fit_dt) ? d->fit_dt[t * M.nfit + l] : nullptr;
+      if (rc == DPB_OK && dt) rc = upload(m, dt, (size_t)outw, &M.fdt[t][l]);
+      if (rc == DPB_OK && M.mfw > 0) {
+        // the tensor-core fitting's copy: every hidden width padded to mfw with zeros
+        const int P = M.mfw, inp = l == 0 ? K0 : P, outp = l == M.nfit ? 1 : P;
+        std::vector<float> kp((size_t)inp * outp, 0.f), ktp((size_t)outp * inp, 0.f);
+        for (int i = 0; i < in; ++i)
+          for (int o = 0; o < outw; ++o) {
+            kp[(size_t)i * outp + o] = kv[(size_t)i * outw + o];
+            ktp[(size_t)o * inp + i] = kv[(size_t)i * outw + o];
+          }
+        if (l < M.nfit) {
+          std::vector<float> bp(P, 0.f), dp(P, 0.f);
+          for (int o = 0; o < outw; ++o) {
+            bp[o] = bv[o];
+            if (dt) dp[o] = dt[o];
+          }
+          rc = upload(m, bp.data(), bp.size(), &M.mfb[t][l]);
+          if (rc == DPB_OK && dt) rc = upload(m, dp.data(), dp.size(), &M.mfdt[t][l]);
+          if (rc == DPB_OK) rc = upload_fit_tiles(m, ktp, outp, inp, outp, &M.fit_bt[t][kFitBtFwd + l]);
+          if (rc == DPB_OK && l >= 1) rc = upload_fit_tiles(m, kp, inp, outp, inp, &M.fit_bt[t][kFitBtAdj + l]);
+          if (rc == DPB_OK && l == 0) rc = upload_fit_tiles(m, kp, K0, outp, 128, &M.fit_bt[t][kFitBtDg]);
+        } else {
+          rc = upload(m, kp.data(), kp.size(), &M.mfwout[t]);
+        }
       }
     }
   }
+  if (rc == DPB_OK && !M.emb_tuned && !dpb::embed_general_fits(M)) rc = DPB_ERR_UNSUPPORTED;
   if (rc != DPB_OK) {
     dpb_model_destroy(m);
     return rc;
@@ -276,9 +328,16 @@ extern "C" int dpb_model_destroy(dpb_model *m) {
   return DPB_OK;
 }
 
+static int fit_width_max(const DevModel &M) {
+  int w = 0;
+  for (int l = 0; l < M.nfit; ++l) w = std::max(w, M.FW[l]);
+  return w;
+}
+
 static size_t fp32_ws_per_atom(const DevModel &M) {
-  const int FW = M.FW[0];
-  return (size_t)(10 * M.E2 + M.A * M.E2 + 2 * M.nfit * FW + 4 * FW + 1) * 4 + 16;
+  int hid = 0;
+  for (int l = 0; l < M.nfit; ++l) hid += M.FW[l];
+  return (size_t)(10 * M.E2 + M.A * M.E2 + 2 * hid + 4 * fit_width_max(M) + 1) * 4 + 16;
 }
 
 // Workspace of NF atoms with nE energy / virial rows.
@@ -321,19 +380,21 @@ static int fill_sys(const dpb_model *m, int natoms, int nframes, const int *type
 
 // FP32 fitting chain (tiled SGEMMs with fused epilogues) for every centre
 // type: G -> per-atom energies (FP64 frame sums) and dE/dG written over G.
+// Hidden layer l has width FW[l]; a dt residual (utils.py:158-163) exists
+// only where FW[l] == FW[l-1], so every residual pairs equal widths.
 // w: scratch for the per-layer activations and adjoints.
 int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Eatom, double *energy, char *w,
                         cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
-  const int E2 = M.E2, A = M.A, K0 = A * E2, FW = M.FW[0], L = M.nfit;
+  const int E2 = M.E2, A = M.A, K0 = A * E2, L = M.nfit, FWM = fit_width_max(M);
   float *tb[kMaxFitLayers], *hb[kMaxFitLayers];
-  for (int l = 0; l < L; ++l) { tb[l] = (float *)w; w += al(NF * FW * 4); }
-  for (int l = 0; l < L; ++l) { hb[l] = (float *)w; w += al(NF * FW * 4); }
+  for (int l = 0; l < L; ++l) { tb[l] = (float *)w; w += al(NF * M.FW[l] * 4); }
+  for (int l = 0; l < L; ++l) { hb[l] = (float *)w; w += al(NF * M.FW[l] * 4); }
   float *gz[2], *gh[2];
-  gz[0] = (float *)w; w += al(NF * FW * 4);
-  gz[1] = (float *)w; w += al(NF * FW * 4);
-  gh[0] = (float *)w; w += al(NF * FW * 4);
-  gh[1] = (float *)w; w += al(NF * FW * 4);
+  gz[0] = (float *)w; w += al(NF * FWM * 4);
+  gz[1] = (float *)w; w += al(NF * FWM * 4);
+  gh[0] = (float *)w; w += al(NF * FWM * 4);
+  gh[1] = (float *)w; w += al(NF * FWM * 4);
   int rc;
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -341,11 +402,12 @@ int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Ea
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
     for (int l = 0; l < L; ++l) {
+      const int out = M.FW[l], in = l == 0 ? K0 : M.FW[l - 1];
       Epi ep{};
       ep.bias = M.fb[ti][l];
       ep.out1 = tb[l];
       ep.out2 = hb[l];
-      ep.ld = FW;
+      ep.ld = out;
       if (l > 0 && M.fdt[ti][l]) {
         ep.mode = EPI_TANH_RES;
         ep.dt = M.fdt[ti][l];
@@ -353,19 +415,21 @@ int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Ea
       } else {
         ep.mode = EPI_TANH;
       }
-      if (l == 0) rc = launch_sgemm(Mrows, FW, K0, G, K0, rm, M.fw[ti][0], ep, st);
-      else rc = launch_sgemm(Mrows, FW, FW, hb[l - 1], FW, rm, M.fw[ti][l], ep, st);
+      if (l == 0) rc = launch_sgemm(Mrows, out, in, G, K0, rm, M.fw[ti][0], ep, st);
+      else rc = launch_sgemm(Mrows, out, in, hb[l - 1], in, rm, M.fw[ti][l], ep, st);
       if (rc) return rc;
     }
     int cur = 0;
-    rc = launch_fit_energy(Mrows, rm, FW, hb[L - 1], tb[L - 1], M.fw[ti][L], M.fb[ti][L], M.fdt[ti][L - 1], Eatom,
-                           gz[cur], energy, D.N, D.seg, st);
+    rc = launch_fit_energy(Mrows, rm, M.FW[L - 1], hb[L - 1], tb[L - 1], M.fw[ti][L], M.fb[ti][L],
+                           M.fdt[ti][L - 1], Eatom, gz[cur], energy, D.N, D.seg, st);
     if (rc) return rc;
     for (int l = L - 1; l >= 1; --l) {
+      // gH_{l-1} = gZ_l W_l^T (+ gH_l through layer l's residual)
+      const int out = M.FW[l - 1], in = M.FW[l];
       Epi ep{};
-      ep.ld = FW;
+      ep.ld = out;
       ep.tin = tb[l - 1];
-      if (M.fdt[ti][l]) {  // residual at layer l: gH_{l-1} += gH_l
+      if (M.fdt[ti][l]) {
         if (l == L - 1) ep.gvec = M.fw[ti][L];
         else ep.gmat = gh[cur];
       }
@@ -377,7 +441,7 @@ int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Ea
       } else {
         ep.mode = EPI_GRAD;
       }
-      rc = launch_sgemm(Mrows, FW, FW, gz[cur], FW, rm, M.fwT[ti][l], ep, st);
+      rc = launch_sgemm(Mrows, out, in, gz[cur], in, rm, M.fwT[ti][l], ep, st);
       if (rc) return rc;
       cur ^= 1;
     }
@@ -385,7 +449,7 @@ int dpb::fit_fp32_chain(const DevModel &M, const SysDesc &D, float *G, float *Ea
     ep.mode = EPI_STORE;
     ep.out1 = G;
     ep.ld = K0;
-    rc = launch_sgemm(Mrows, K0, FW, gz[cur], FW, rm, M.fwT[ti][0], ep, st);
+    rc = launch_sgemm(Mrows, K0, M.FW[0], gz[cur], M.FW[0], rm, M.fwT[ti][0], ep, st);
     if (rc) return rc;
   }
   return DPB_OK;
@@ -401,7 +465,8 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
   int rc;
   prof_begin(PROF_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    if (!M.emb_tuned) rc = launch_embed_fwd_gen(M, D, ti, pos, perm, box, nbrs, T, G, st);
+    else if (M.E2 == 100) rc = launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st);
     else rc = launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
     if (rc) return rc;
   }
@@ -412,7 +477,8 @@ static int eval_fp32(const DevModel &M, const SysDesc &D, const float *pos, cons
   prof_end(PROF_FIT, st);
   prof_begin(PROF_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    if (M.E2 == 100) rc = launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    if (!M.emb_tuned) rc = launch_embed_bwd_gen(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
+    else if (M.E2 == 100) rc = launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
     else rc = launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, F4, virial, st);
     if (rc) return rc;
   }
@@ -508,7 +574,8 @@ extern "C" int dpb_profile_read(int id, double *ms, uint64_t *count) {
 static int descriptors_fp32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                             const float *box, const int32_t *nbrs, float *T, float *G, cudaStream_t st) {
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    int rc = (M.E2 == 100) ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st)
+    int rc = !M.emb_tuned   ? launch_embed_fwd_gen(M, D, ti, pos, perm, box, nbrs, T, G, st)
+             : M.E2 == 100 ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, G, st)
                            : launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, G, st);
     if (rc) return rc;
   }
@@ -531,6 +598,8 @@ extern "C" int dpb_eval_descriptors(const dpb_model *m, int precision, const flo
   if (precision == DPB_PREC_FP32) return descriptors_fp32(m->dm, D, pos, perm, box, nbrs, T, G, st);
   if (precision == DPB_PREC_MIXED) {
     if (!mixed_supported(m->dm)) return DPB_ERR_UNSUPPORTED;
+    // the mixed form's embedding runs in the FP32 kernels for tables and untuned shapes
+    if (m->dm.ngrids > 0 || !m->dm.emb_tuned) return descriptors_fp32(m->dm, D, pos, perm, box, nbrs, T, G, st);
     return mixed_descriptors_f32(m->dm, D, pos, perm, box, nbrs, T, G, err, workspace, st);
   }
   return DPB_ERR_INVALID_ARG;

@@ -5,12 +5,15 @@
 
 namespace dpb {
 
-constexpr int kMaxEmbedLayers = 3;
+constexpr int kMaxEmbedLayers = 4;
 constexpr int kMaxFitLayers = 4;  // hidden layers
 
 struct DevModel {
   int ntypes;
-  int E0, E1, E2;      // embedding widths
+  int E0, E1, E2;      // embedding widths of the tuned three-layer kernels
+  int nemb;            // embedding layers (1 .. kMaxEmbedLayers) and their widths
+  int EW[kMaxEmbedLayers];
+  int emb_tuned;       // 1: a tuned instantiation (25-50-100 or 32-32-64) serves the shape
   int A;               // axis neurons
   int nfit;            // hidden fitting layers
   int FW[kMaxFitLayers];
@@ -30,8 +33,7 @@ struct DevModel {
   const float *fdt[kMaxTypes][kMaxFitLayers];
   // transposed fitting kernels (out,in) for the adjoint GEMMs
   const float *fwT[kMaxTypes][kMaxFitLayers + 1];
-  // BF16 copies for the mixed path (layouts documented in mixed.cu)
-  const __nv_bfloat16 *ew_bf[kMaxTypes * kMaxTypes][kMaxEmbedLayers];
+  // BF16 copies of the fitting kernels for the mixed path (layouts documented in mixed.cu)
   const __nv_bfloat16 *fw_bf[kMaxTypes][kMaxFitLayers + 1];
   const __nv_bfloat16 *fwT_bf[kMaxTypes][kMaxFitLayers + 1];
   // per embedding net: the shared-memory image of its FP16 B tiles (layer 1
@@ -51,6 +53,15 @@ struct DevModel {
   // at kFitBtFwd + l (W_l^T), adjoint layer l >= 1 at kFitBtAdj + l (W_l), and
   // W_0 in passes of 128 rows at kFitBtDg; null when the mixed form is unsupported
   const __nv_bfloat16 *fit_bt[kMaxTypes][2 * kMaxFitLayers + 1];
+  // the tensor-core fitting runs every hidden layer at one width mfw (a
+  // multiple of 16 with a kernel instantiation, >= every FW[l]; 0: no
+  // tensor-core fitting for this shape); the padding columns carry zero
+  // weights, biases and dt, which keeps them exactly zero through the chain.
+  // Padded FP32 biases, dt and output weights (out_norm folded) of that path:
+  int mfw;
+  const float *mfb[kMaxTypes][kMaxFitLayers];
+  const float *mfdt[kMaxTypes][kMaxFitLayers];
+  const float *mfwout[kMaxTypes];
 };
 
 constexpr int kFitBtFwd = 0, kFitBtAdj = kMaxFitLayers, kFitBtDg = 2 * kMaxFitLayers;

@@ -1574,7 +1574,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
     // ---- forward; the last layer's epilogue also forms the atom energy and
     // the first adjoint gate g = w_out dt (1 - t^2), the A operand of adjoint
     // layer L-1 (its t and h never go to the scratch)
-    const float *wf = M.fw[ti][L];
+    const float *wf = M.mfwout[ti];
     float e_sum = 0.f;
     for (int l = 0; l < L && ok; ++l) {
       ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
@@ -1582,7 +1582,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       if (!ok) break;
       tc::fence_after_sync();
       const bool last = l == L - 1;
-      const float *bias = M.fb[ti][l], *dt = M.fdt[ti][l];
+      const float *bias = M.mfb[ti][l], *dt = M.mfdt[ti][l];
       // residual sources of the current chunk, loaded one chunk ahead so the
       // scratch reads overlap the TMEM loads and the previous chunk's math
       float hp[16];
@@ -1655,8 +1655,8 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       ++accf_n;
       if (!ok) break;
       tc::fence_after_sync();
-      const bool res_l = M.fdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.fdt[ti][l - 1] != nullptr;
-      const float *dtm1 = M.fdt[ti][l - 1], *wf = M.fw[ti][L];
+      const bool res_l = M.mfdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.mfdt[ti][l - 1] != nullptr;
+      const float *dtm1 = M.mfdt[ti][l - 1], *wf = M.mfwout[ti];
       const bool use_gh = res_l && l != L - 1;
       float ghc[16], tcur[16];
 #pragma unroll
@@ -1781,13 +1781,37 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
   return DPB_OK;
 }
 
-// ---------------------------------------------------------------- dispatch
-int mixed_supported(const DevModel &M) {
-  const bool emb = (M.E0 == 25 && M.E1 == 50 && M.E2 == 100) || (M.E0 == 32 && M.E1 == 32 && M.E2 == 64);
-  bool fit = M.FW[0] == 240 || M.FW[0] == 128;
-  for (int l = 1; l < M.nfit; ++l) fit = fit && M.FW[l] == M.FW[0];
-  return emb && fit && (M.A * M.E2) % 16 == 0;
+// The instantiation of the model's padded hidden width.
+template <typename DGT>
+int launch_mix_fit_any(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, DGT *dG, float *scratch,
+                       float *Eatom, double *energy, int *err, cudaStream_t st) {
+  switch (M.mfw) {
+    case 64: return launch_mix_fit<64, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    case 128: return launch_mix_fit<128, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    case 208: return launch_mix_fit<208, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    case 240: return launch_mix_fit<240, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    case 256: return launch_mix_fit<256, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    default: return DPB_ERR_UNSUPPORTED;
+  }
 }
+
+// ---------------------------------------------------------------- dispatch
+// Hidden widths with a tensor-core fitting instantiation; a model's hidden
+// layers all run at the smallest one that holds its widest layer.
+static const int kFitWidths[] = {64, 128, 208, 240, 256};
+
+int mixed_fit_width(const DevModel &M) {
+  int w = 0;
+  for (int l = 0; l < M.nfit; ++l) w = w > M.FW[l] ? w : M.FW[l];
+  for (int c : kFitWidths)
+    if (w <= c) return c;
+  return 0;
+}
+
+// The mixed form needs the tensor-core fitting (padded width, dE/dG passes of
+// whole 16-column chunks); the embedding runs on the tensor cores for the
+// tuned shapes and in the FP32 kernels otherwise.
+int mixed_supported(const DevModel &M) { return M.mfw > 0 && (M.A * M.E2) % 16 == 0; }
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -1795,11 +1819,11 @@ static int n2_of(const DevModel &M) { return (M.E2 + 15) / 16 * 16; }
 
 // Fitting scratch rounds each centre type's rows up to whole 128-row tiles.
 size_t mixed_workspace_fixed(const DevModel &M) {
-  return (size_t)127 * M.ntypes * (2 * M.nfit + 1) * M.FW[0] * 4 + 1024;
+  return (size_t)127 * M.ntypes * (2 * M.nfit + 1) * M.mfw * 4 + 1024;
 }
 
 size_t mixed_workspace_per_atom(const DevModel &M) {
-  const int FW = M.FW[0], K0 = M.A * M.E2;
+  const int FW = M.mfw, K0 = M.A * M.E2;
   return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 + 4 + 16 +
          (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
 }
@@ -1852,7 +1876,7 @@ static int launch_pos_sorted(const SysDesc &D, const float *pos, const int32_t *
 
 int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, const float *box,
                       const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, int *err, cudaStream_t st) {
-  if (M.ngrids > 0) return DPB_ERR_UNSUPPORTED;  // compressed nets: the FP32 table kernels give T and G
+  if (M.ngrids > 0 || !M.emb_tuned) return DPB_ERR_UNSUPPORTED;  // the FP32 kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, posS, box, nbrs, T, Gb, err, st)
@@ -1883,10 +1907,15 @@ template <int E0, int E1, int E2>
 int launch_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float *pos, const int32_t *perm,
                      const float *box, const int32_t *nbrs, const float *T, const float *dG, float4 *F4,
                      double *virial, cudaStream_t st);
+int launch_embed_fwd_gen(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                         const int32_t *, float *, float *, cudaStream_t);
+int launch_embed_bwd_gen(const DevModel &, const SysDesc &, int, const float *, const int32_t *, const float *,
+                         const int32_t *, const float *, const float *, float4 *, double *, cudaStream_t);
 
-// Compressed embedding nets in the mixed form: the table lookup has no GEMM,
-// so the FP32 table kernels produce T and G (FP32) and take the adjoint; the
-// fitting chain runs on the tensor cores from a BF16 copy of G.
+// Embedding nets without tensor-core kernels in the mixed form - compressed
+// tables (a lookup, no GEMM) and shapes other than the tuned ones: the FP32
+// kernels produce T and G (FP32) and take the adjoint; the fitting chain runs
+// on the tensor cores from a BF16 copy of G.
 static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                                  const float *box, const int32_t *nbrs, double *energy, float *Eatom, float4 *F4,
                                  double *virial, float *T, __nv_bfloat16 *Gb, float *dG, float *scratch, int *err,
@@ -1896,7 +1925,8 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
   int rc;
   prof_begin(PROF_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    rc = (M.E2 == 100) ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, st)
+    rc = !M.emb_tuned   ? launch_embed_fwd_gen(M, D, ti, pos, perm, box, nbrs, T, dG, st)
+         : M.E2 == 100 ? launch_embed_fwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, st)
                        : launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, dG, st);
     if (rc) return rc;
   }
@@ -1906,13 +1936,13 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
   DPB_LAUNCH_CHECK();
   prof_end(PROF_EMBED_FWD, st);
   prof_begin(PROF_MIXED_FIT, st);
-  rc = (M.FW[0] == 240) ? launch_mix_fit<240, float>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
-                        : launch_mix_fit<128, float>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+  rc = launch_mix_fit_any<float>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    rc = (M.E2 == 100) ? launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st)
+    rc = !M.emb_tuned   ? launch_embed_bwd_gen(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st)
+         : M.E2 == 100 ? launch_embed_bwd<25, 50, 100>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st)
                        : launch_embed_bwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, dG, F4, virial, st);
     if (rc) return rc;
   }
@@ -1966,7 +1996,7 @@ static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
 }
 
 int mixed_tune_dT(const DevModel &M, size_t NF, void *ws, cudaStream_t st, int *best) {
-  if (M.ngrids > 0 || !best) return DPB_ERR_UNSUPPORTED;  // compressed nets take the FP32 adjoint
+  if (M.ngrids > 0 || !M.emb_tuned || !best) return DPB_ERR_UNSUPPORTED;  // these take the FP32 adjoint
   const MixedWs w = mixed_ws(M, NF, ws);
   const __nv_bfloat16 *dGb = reinterpret_cast<const __nv_bfloat16 *>(w.dG);
   cudaEvent_t a, b;
@@ -2001,7 +2031,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   __nv_bfloat16 *Gb = mw.Gb;
   float4 *posS = mw.posS;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
-  if (M.ngrids > 0)
+  if (M.ngrids > 0 || !M.emb_tuned)
     return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
   int rc = launch_pos_sorted(D, pos, perm, posS, st);
   if (rc) return rc;
@@ -2009,8 +2039,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
   __nv_bfloat16 *dGb = reinterpret_cast<__nv_bfloat16 *>(dG);  // dE/dG in BF16 (the dE/dT input)
-  rc = (M.FW[0] == 240) ? launch_mix_fit<240, __nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st)
-                        : launch_mix_fit<128, __nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
+  rc = launch_mix_fit_any<__nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);

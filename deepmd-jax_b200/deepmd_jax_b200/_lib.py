@@ -85,6 +85,9 @@ def load():
     lib.dpb_nlist_build.restype = ctypes.c_int
     lib.dpb_eval_workspace_bytes.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
     lib.dpb_eval_workspace_bytes.restype = ctypes.c_int
+    lib.dpb_eval_descriptors.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, ctypes.c_int, c_int_p, f32p,
+                                         i32p, c_int_p, vp, vp, vp, vp, ctypes.c_size_t, vp]
+    lib.dpb_eval_descriptors.restype = ctypes.c_int
     lib.dpb_eval.argtypes = [vp, ctypes.c_int, f32p, i32p, ctypes.c_int, ctypes.c_int, c_int_p, f32p, i32p,
                              c_int_p, f64p, f32p, f32p, f64p, vp, vp, ctypes.c_size_t, vp]
     lib.dpb_eval.restype = ctypes.c_int

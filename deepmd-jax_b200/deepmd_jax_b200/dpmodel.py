@@ -2,7 +2,8 @@
 se_a energy models, evaluated by libdpb200 on the GPU.
 
 ``DPModel(params).apply(variables, coord_N3, box_33, static_args, nbrs_nm)``
-returns ``(energy, debug)`` like the flax module; ``energy_and_force``
+returns ``(energy, debug)`` like the flax module (debug: the descriptor T);
+``energy_and_force``
 returns ``(energy, force)`` with the force as the negative coordinate
 gradient (dpmodel.py:106-108), computed by the hand-written adjoint.
 
@@ -82,14 +83,21 @@ class DPModel:
         st = int(out["status"].item())
         if st & 2:
             raise RuntimeError("neighbour list overflow (status %d): reallocate the typed neighbour list" % st)
+        out["_inputs"] = (dm, pos, box, nbrs, count, sel, perm_dev)
         return out
 
     def apply(self, variables, coord_N3, box_33, static_args, nbrs_nm=None):
+        """(energy, debug) like the flax module: debug is the descriptor
+        T_NselXW (N, 10, W), T / Nnbrs without Tbias, atoms in type-sorted
+        order (deepmd_jax/dpmodel.py:50-51,99-100)."""
         out = self._run(variables, coord_N3, box_33, static_args, nbrs_nm)
-        return float(out["energy"][0].item()), {}
+        dm, pos, box, nbrs, count, sel, perm_dev = out["_inputs"]
+        T, _ = dm.descriptors(pos, box, nbrs, count, sel, perm=perm_dev, precision=self.precision)
+        return float(out["energy"][0].item()), T.cpu().numpy()
 
     def energy(self, variables, coord_N3, box_33, static_args, nbrs_nm=None):
-        return self.apply(variables, coord_N3, box_33, static_args, nbrs_nm)[0]
+        out = self._run(variables, coord_N3, box_33, static_args, nbrs_nm)
+        return float(out["energy"][0].item())
 
     def energy_and_force(self, variables, coord_N3, box_33, static_args, nbrs_nm=None):
         out = self._run(variables, coord_N3, box_33, static_args, nbrs_nm)

@@ -181,6 +181,23 @@ class DeviceModel:
         out["status"] = status
         return out
 
+    def descriptors(self, pos, box, nbrs, type_count, sel, perm=None, precision="fp32"):
+        """The descriptor stage alone: T (F*N, 10, W) / Nnbrs without Tbias
+        (the reference's T_NselXW, deepmd_jax/dpmodel.py:50-51) and G (F*N,
+        A*W), atoms in type-sorted order, float32 on the device."""
+        F, N = pos.shape[0], pos.shape[1]
+        W, A = int(self.params["embed_widths"][-1]), int(self.params["axis"])
+        dev = pos.device
+        T = torch.empty((F * N, 10, W), dtype=torch.float32, device=dev)
+        G = torch.empty((F * N, A * W), dtype=torch.float32, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        ws = self.eval_workspace(N, F)
+        rc = self.lib.dpb_eval_descriptors(self.handle, PRECISIONS[precision], _ptr(pos), _ptr(perm), N, F,
+                                           _lib.int_array(type_count), _ptr(box), _ptr(nbrs), _lib.int_array(sel),
+                                           _ptr(T), _ptr(G), _ptr(err), _ptr(ws), ws.numel(), _stream())
+        _lib.check(rc, "dpb_eval_descriptors")
+        return T, G
+
 
 class NeighborBuilder:
     """Typed neighbour lists (reference nbrs_nm semantics) via dpb_nlist_build."""

@@ -122,8 +122,13 @@ class OracleModel:
             if i == 0:
                 x = torch.tanh(x @ Wk + b)
             else:
-                Z = Wk.shape[1] // Wk.shape[0]
-                x_prev = torch.repeat_interleave(x, Z, dim=-1)
+                # utils.py:115-117: repeat(x, Z) for a widening layer, the mean
+                # over the 1/Z groups of reshape(..., 1/Z, width) for a narrowing one
+                n_in, n_out = Wk.shape
+                if n_out % n_in == 0:
+                    x_prev = torch.repeat_interleave(x, n_out // n_in, dim=-1)
+                else:
+                    x_prev = x.reshape(x.shape[:-1] + (n_in // n_out, n_out)).mean(-2)
                 x = torch.tanh(x @ Wk + b) + x_prev
         return x
 

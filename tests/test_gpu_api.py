@@ -254,3 +254,23 @@ def test_test_on_dp_directories_matches_golden_and_metrics(tmp_path):
     assert np.isclose(metrics["rmse"]["force"], np.sqrt((f_err ** 2).mean()), rtol=1e-5)
     # the metrics are those of the planted offsets to the FP32 error
     assert abs(metrics["rmse"]["energy"] - np.sqrt(np.mean([(x[2] / x[4]) ** 2 for x in expect]))) < 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_apply_debug_descriptor_matches_oracle(precision):
+    """DPModel.apply returns (energy, T_NselXW) like the reference
+    (deepmd_jax/dpmodel.py:50-51,99-100): T (N, 10, W) / Nnbrs without Tbias,
+    type-sorted, against the FP64 oracle's T - to 1e-5 of max |T| in FP32,
+    to 2e-2 RMS (relative) in the mixed form (FP16 embedding operands)."""
+    from deepmd_jax_b200.dpmodel import DPModel
+    from deepmd_jax_b200.systems import water_box
+    p, v = golden_models()["B"]
+    w = water_box(4, 12.42, seed=0)
+    e, T = DPModel(p, precision=precision).apply(v, w["position"], w["box"], {"type_idx": tuple(w["type_idx"])})
+    _, _, T_ref = om.energy_only(om.OracleModel(p, v, torch.float64), w["position"], w["box"], w["type_idx"])
+    T_ref = T_ref.numpy()
+    assert T.shape == T_ref.shape == (192, 10, p["embed_widths"][-1])
+    if precision == "fp32":
+        assert np.abs(T - T_ref).max() <= 1e-5 * np.abs(T_ref).max()
+    else:
+        assert np.sqrt(((T - T_ref) ** 2).mean()) <= 2e-2 * np.sqrt((T_ref ** 2).mean())

@@ -68,3 +68,23 @@ def test_normal_modes_match_reference_source():
         for f in np.unique(np.round(fg, 12)):
             sel = np.isclose(fg, f, rtol=1e-9, atol=1e-15)
             assert np.allclose(C[:, sel] @ C[:, sel].T, Cg[:, sel] @ Cg[:, sel].T, atol=1e-12)
+
+
+GS = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "golden_shapes.npz"))
+
+
+@pytest.mark.parametrize("key", ["F", "G", "H", "I", "L"])
+def test_oracle_matches_reference_source_other_shapes(key):
+    """Embedding / fitting shapes beyond the benchmark's (make_golden_shapes.py):
+    (24,48,96)/(200,200,200)/axis 12, (16,32,64)/(240,120,240), a four-layer
+    net with a narrowing layer, a compressed width-96 table, and F through a
+    neighbour list."""
+    from make_golden_shapes import shape_models
+    mk = "F" if key == "L" else key
+    p, v = shape_models()[mk]
+    m = om.OracleModel(p, v, torch.float64)
+    pre = "L_" if key == "L" else ""
+    r = om.energy_force(m, GS[pre + "pos"], GS[pre + "box"], GS[pre + "type"],
+                        nbrs=(GS["L_nbrs"] if key == "L" else None), sel=[46, 92])
+    assert abs(r["energy"] - float(GS[key + "_E"])) <= 1e-12 * max(1.0, abs(float(GS[key + "_E"])))
+    assert np.abs(r["force"] - GS[key + "_F"]).max() <= 1e-12
