@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(128) k_selftest_umma(int variant, float *out, 
         ad = tc::make_desc(a0 + tc::mnmajor_off(ks * 16, 0, M), (M / 8) * 128, 128);
         bd = tc::make_desc(b0 + tc::mnmajor_off(ks * 16, 0, N), (N / 8) * 128, 128);
       }
-      tc::mma_bf16(d, ad, bd, idesc, ks > 0);
+      tc::mma_f16kind(d, ad, bd, idesc, ks > 0);
     }
     tc::commit(&mbar);
   }
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
             tc::fence_after_sync();
 #pragma unroll
             for (int ks = 0; ks < MD::K1 / 16; ++ks)
-              tc::mma_bf16(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128),
+              tc::mma_f16kind(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128),
                            tc::make_desc(w1_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128),
                            idesc1, ks > 0);
             tc::commit(&mbar);
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
             tc::fence_after_sync();
 #pragma unroll
             for (int ks = 0; ks < MD::K2 / 16; ++ks)
-              tc::mma_bf16(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128),
+              tc::mma_f16kind(tD, tc::make_desc(opa_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128),
                            tc::make_desc(w2_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128),
                            idesc2, ks > 0);
             tc::commit(&mbar);
@@ -660,7 +660,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
             tc::fence_after_sync();
 #pragma unroll
             for (int ks = 0; ks < 8; ++ks)
-              tc::mma_bf16(tD3, tc::make_desc(rblk_u + tc::mnmajor_off(16 * ks, 0, 128), (128 / 8) * 128, 128),
+              tc::mma_f16kind(tD3, tc::make_desc(rblk_u + tc::mnmajor_off(16 * ks, 0, 128), (128 / 8) * 128, 128),
                            tc::make_desc(opa_u + tc::mnmajor_off(16 * ks, 0, MD::N2), (MD::N2 / 8) * 128, 128),
                            idesc3, (ntile > 0 || ks > 0) ? 1u : 0u);
             tc::commit(&mbar);
@@ -1167,9 +1167,9 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
 #pragma unroll
               for (int ks = 0; ks < MD::K1 / 16; ++ks) {
                 const uint64_t bd = tc::make_desc(w1_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128, (MD::K1 / 8) * 128);
-                tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                tc::mma_f16kind(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
                                                   (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
-                tc::mma_bf16(tbase + 64, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
+                tc::mma_f16kind(tbase + 64, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K1), 128,
                                                        (MD::K1 / 8) * 128), bd, idesc1, ks > 0);
               }
               tc::commit(&mbar);
@@ -1191,9 +1191,9 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
 #pragma unroll
             for (int ks = 0; ks < MD::K2 / 16; ++ks) {
               const uint64_t bd = tc::make_desc(w2_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128, (MD::K2 / 8) * 128);
-              tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+              tc::mma_f16kind(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
                                                 (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
-              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
+              tc::mma_f16kind(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::K2), 128,
                                                       (MD::K2 / 8) * 128), bd, idesc2, ks > 0);
             }
             tc::commit(&mbar);
@@ -1214,9 +1214,9 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
             for (int ks = 0; ks < MD::N2 / 16; ++ks) {
               const uint64_t bd =
                   tc::make_desc(dtb_u + tc::kmajor_off(16 * smin, 16 * ks, MD::N2), 128, (MD::N2 / 8) * 128);
-              tc::mma_bf16(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+              tc::mma_f16kind(tbase, tc::make_desc(opb_u + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
                                                 (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
-              tc::mma_bf16(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
+              tc::mma_f16kind(tbase + 128, tc::make_desc(opb_u + kTan + tc::kmajor_off(0, 16 * ks, MD::N2), 128,
                                                       (MD::N2 / 8) * 128), bd, idesc3, ks > 0);
             }
             tc::commit(&mbar);
@@ -1523,7 +1523,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           const uint64_t ad = (g == 0) ? tc::make_desc(st_u, 128 * 16, 128)
                                        : tc::make_desc(ha_u + tc::kmajor_off(0, 16 * k, FW), 128, (FW / 8) * 128);
           const uint64_t bd = tc::make_desc(st_u + kFitStageA, (uint32_t)gi.br * 16, 128);
-          tc::mma_bf16(td + gi.col, ad, bd, idesc, k > 0 ? 1u : 0u);
+          tc::mma_f16kind(td + gi.col, ad, bd, idesc, k > 0 ? 1u : 0u);
           tc::commit(&empty[s]);
         }
         if (!ok) break;

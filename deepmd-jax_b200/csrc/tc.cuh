@@ -50,7 +50,10 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int a_mn, int b_m
          ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+// tcgen05.mma kind::f16 issued by one thread: D (TMEM) (+)= A . B with FP32
+// accumulation; A and B are both BF16 or both FP16, as the instruction
+// descriptor says (idesc_bf16 / idesc_f16).
+__device__ __forceinline__ void mma_f16kind(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
