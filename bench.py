@@ -449,6 +449,20 @@ def study_drift(args):
     w = water_box(N_SIDE, BOX, seed=0)
     N = len(w["position"])
     out = {"study": "nve_drift", "atoms": N, "dt_fs": DT, "steps": args.steps, "forms": {}}
+    # the 192-atom NVE workload over its full 1,000 steps, energy every 10 steps
+    w0 = water_box(4, 12.42, seed=0)
+    out["config0_1000_steps"] = {}
+    for prec in ("fp32", "mixed"):
+        sim = Simulation((params, variables), w0["box"], w0["type_idx"], w0["mass_per_type"], "NVE", DT,
+                         w0["position"], initial_velocity=w0["velocity"], report_interval=10, precision=prec,
+                         verbose=False)
+        sim.run(1000, trajectory=False)
+        rows = np.array([[r[0], r[4]] for r in sim.log])
+        e = rows[:, 1] / len(w0["position"])
+        out["config0_1000_steps"][prec] = {
+            "drift_eV_per_atom_per_ps": float(np.polyfit(rows[:, 0] * DT / 1000.0, e, 1)[0]),
+            "max_dev_eV_per_atom": float(np.abs(e - e[0]).max()),
+            "first_100_steps_max_dev_eV_per_atom": float(np.abs(e[:11] - e[0]).max())}
     for prec in ("fp32", "mixed"):
         sim = Simulation((params, variables), w["box"], w["type_idx"], w["mass_per_type"], "NVE", DT,
                          w["position"], initial_velocity=w["velocity"], report_interval=args.report_every,

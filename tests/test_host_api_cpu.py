@@ -570,3 +570,16 @@ def test_load_model_refuses_unknown_globals(tmp_path):
     path.write_bytes(pickle.dumps({"model": collections.Counter(), "variables": {}}))
     with pytest.raises(pickle.UnpicklingError, match="collections.Counter"):
         load_model(str(path))
+
+
+@pytest.mark.parametrize("n_side,L", [(4, 12.42), (8, 24.83), (16, 49.66)])
+def test_no_pair_within_an_ulp_of_the_cutoff(n_side, L):
+    """jax_md's float32 summation order of d^2 is unpinned (oracle/nlist.py);
+    the neighbour sets cannot depend on it when no pair's float32 d^2 lies
+    within one ulp of (rcut + skin)^2.  Checked on the initial frames of the
+    192-, 1,536- and 12,288-atom water boxes (rcut 6 A, skin 0.3 A)."""
+    from oracle import nlist as onl
+    from deepmd_jax_b200.systems import water_box
+    w = water_box(n_side, L, seed=0)
+    c = onl.canonicalize(w["position"], w["box"], w["type_idx"])
+    assert onl.boundary_pairs(c, w["box"].astype(np.float32), onl.cutoff_sq(6.3)) == 0
