@@ -320,6 +320,34 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
   __syncthreads();
 }
 
+// The forward kernel keeps, in list mode (one image per pair), the rows it
+// compacted for each block and neighbour type: rows of block g0 and type tj at
+// rows_g + g0 * kRowStoreCap + nb * col[tj], their count at rcnt[g0 * ntypes
+// + tj].  The adjoint then streams them back instead of compacting again.
+constexpr int kRowStoreCap = 192;  // neighbour slots per atom the store holds (sum of sel)
+
+// One round of the adjoint's row stream: the unread rows of earlier rounds
+// move to the front (as in mix_compact_round), then up to blockDim rows
+// [base, total) of the stored list are appended, one coalesced 16-byte load
+// per thread.
+__device__ __forceinline__ void mix_stream_round(const float4 *__restrict__ src, int base, int total, float4 *rowbuf,
+                                                 int &rowstart, int &rowcount) {
+  const int tid = threadIdx.x;
+  if (rowstart > 0) {
+    const int rem = rowcount - rowstart;  // < 128 <= blockDim
+    float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tid < rem) carry = rowbuf[rowstart + tid];
+    __syncthreads();
+    if (tid < rem) rowbuf[tid] = carry;
+    rowstart = 0;
+    rowcount = rem;
+  }
+  const int n = min((int)blockDim.x, total - base);
+  if (tid < n) rowbuf[rowcount + tid] = src[base + tid];
+  rowcount += n;
+  __syncthreads();
+}
+
 __device__ __forceinline__ uint4 pack8(const float *v) {
   return make_uint4(tc::pack_bf16(v[0], v[1]), tc::pack_bf16(v[2], v[3]), tc::pack_bf16(v[4], v[5]),
                     tc::pack_bf16(v[6], v[7]));
@@ -510,6 +538,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
                                                                   const int32_t *__restrict__ nbrs,
                                                                   float *__restrict__ Tout,
                                                                   __nv_bfloat16 *__restrict__ Gout,
+                                                                  float4 *__restrict__ rows_g,
+                                                                  int *__restrict__ rcnt,
                                                                   int *__restrict__ err) {
   using MD = MixDims<E0, E1, E2>;
   using SP = HalfSplit<E0, E1, E2>;
@@ -563,6 +593,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
+    const bool store = rows_g != nullptr && nim == 1 && D.S <= kRowStoreCap;  // keep the rows for the adjoint
     if (tid < nb) {
       const float4 q = posS[g0 + tid];
       ri_s[tid] = make_float3(q.x, q.y, q.z);
@@ -580,6 +611,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
+      float4 *rdst = store ? rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj] : nullptr;
+      int tjdone = 0;  // rows of this neighbour type processed so far
       constexpr int kStep = kFwdThreads * kFwdCpt;
       for (int base = 0; base < total + kStep && ok; base += kStep) {
         const bool flush = base >= total;
@@ -606,6 +639,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           const bool act = row < nrows;
           const float4 rv = act ? rowbuf[rowstart + row] : make_float4(100.f, 100.f, 100.f, 0.f);
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
+          if (store && half == 0 && act) rdst[tjdone + row] = rv;
           RowGeom gm;
           float st, R[10];
           mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
@@ -668,8 +702,10 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           pending = true;
           ++ntile;
           rowstart += nrows;
+          tjdone += nrows;
         }
       }
+      if (store && tid == 0 && ok) rcnt[g0 * M.ntypes + tj] = tjdone;
     }
     if (!ok) break;
     if (pending) {
@@ -798,8 +834,8 @@ static int num_sms() {
 
 template <int E0, int E1, int E2>
 int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
-                         const float *box, const int32_t *nbrs, float *T, __nv_bfloat16 *G, int *err,
-                         cudaStream_t st) {
+                         const float *box, const int32_t *nbrs, float *T, __nv_bfloat16 *G, float4 *rows_g,
+                         int *rcnt, int *err, cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
   const int nblk = (cnt + kBlkAtoms - 1) / kBlkAtoms * D.F;
@@ -807,7 +843,8 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
   DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_fwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   const int grid = nblk < 2 * num_sms() ? nblk : 2 * num_sms();
-  k_mix_embed_fwd<E0, E1, E2><<<grid, kFwdThreads, smem, st>>>(M, D, ti, posS, box, nbrs, T, G, err);
+  k_mix_embed_fwd<E0, E1, E2><<<grid, kFwdThreads, smem, st>>>(M, D, ti, posS, box, nbrs, T, G, rows_g, rcnt,
+                                                                err);
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
@@ -1024,6 +1061,8 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
                                                                   const int32_t *__restrict__ nbrs,
                                                                   const __half *__restrict__ dTh,
                                                                   const float *__restrict__ dTs,
+                                                                  const float4 *__restrict__ rows_g,
+                                                                  const int *__restrict__ rcnt,
                                                                   float4 *__restrict__ F4,
                                                                   double *__restrict__ virial,
                                                                   int *__restrict__ err) {
@@ -1098,7 +1137,8 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
       const int bn = blk + gridDim.x, fn = bn / nbpf, an = (bn - fn * nbpf) * kBlkAtoms;
       const size_t gn = (size_t)fn * D.N + D.offs[ti] + an;
       const int nbn = min(kBlkAtoms, cnt_i - an);
-      prefetch_range_l2(nbrs + gn * D.S, (size_t)nbn * D.S * 4);
+      if (rows_g != nullptr && D.S <= kRowStoreCap) prefetch_range_l2(rows_g + gn * kRowStoreCap, (size_t)nbn * D.S * 16);
+      else prefetch_range_l2(nbrs + gn * D.S, (size_t)nbn * D.S * 4);
       prefetch_range_l2(dTh + gn * 10 * MD::N2, (size_t)nbn * 10 * MD::N2 * 2);
     }
     const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
@@ -1109,6 +1149,9 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
     const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
+    // the rows the forward kernel kept for this block (list mode), else compact again
+    const bool stream = rows_g != nullptr && nim == 1 && D.S <= kRowStoreCap;
+    if (stream && blk == (int)blockIdx.x) prefetch_range_l2(rows_g + g0 * kRowStoreCap, (size_t)nb * D.S * 16);
     if (tid < nb) {
       const float4 q = posS[g0 + tid];
       ri_s[tid] = make_float3(q.x, q.y, q.z);
@@ -1134,11 +1177,17 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
       constexpr int kStep = kBwdThreads * kBwdCpt;
-      for (int base = 0; base < total + kStep && ok; base += kStep) {
-        const bool flush = base >= total;
-        if (!flush)
-          mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS, nbrs,
-                                     rowbuf, wcnt, rowstart, rowcount);
+      const float4 *rsrc = stream ? rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj] : nullptr;
+      const int nsrc = stream ? rcnt[g0 * M.ntypes + tj] : total;  // stored rows, or candidates
+      for (int base = 0; base < nsrc + kStep && ok; base += kStep) {
+        const bool flush = base >= nsrc;
+        if (!flush) {
+          if (stream)
+            mix_stream_round(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
+          else
+            mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS,
+                                       nbrs, rowbuf, wcnt, rowstart, rowcount);
+        }
         while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
           const int nrows = min(rowcount - rowstart, 128);
           if (loaded_net != knet) {
@@ -1327,8 +1376,9 @@ size_t mix_bwd_smem() {
 
 template <int E0, int E1, int E2>
 int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
-                         const float *box, const int32_t *nbrs, const __half *dTh, const float *dTs, float4 *F4,
-                         double *virial, int *err, cudaStream_t st) {
+                         const float *box, const int32_t *nbrs, const __half *dTh, const float *dTs,
+                         const float4 *rows_g, const int *rcnt, float4 *F4, double *virial, int *err,
+                         cudaStream_t st) {
   using MD = MixDims<E0, E1, E2>;
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
@@ -1345,7 +1395,10 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
     const size_t off = (size_t)f * D.N;
     k_mix_embed_bwd<E0, E1, E2><<<grid, kBwdThreads, smem, st>>>(M, Df, ti, posS + off, box + f * 3,
                                                                   nbrs + off * D.S, dTh + off * 10 * MD::N2,
-                                                                  dTs + off, F4 + off, virial + f * 9, err);
+                                                                  dTs + off,
+                                                                  rows_g ? rows_g + off * kRowStoreCap : nullptr,
+                                                                  rcnt ? rcnt + off * M.ntypes : nullptr, F4 + off,
+                                                                  virial + f * 9, err);
     count_launch();
   }
   DPB_LAUNCH_CHECK();
@@ -1825,7 +1878,7 @@ size_t mixed_workspace_fixed(const DevModel &M) {
 size_t mixed_workspace_per_atom(const DevModel &M) {
   const int FW = M.mfw, K0 = M.A * M.E2;
   return (size_t)10 * M.E2 * 4 + (size_t)K0 * 2 + (size_t)K0 * 4 + (size_t)10 * n2_of(M) * 2 + 4 + 16 +
-         (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
+         (size_t)kRowStoreCap * 16 + (size_t)M.ntypes * 4 + (size_t)(2 * M.nfit + 1) * FW * 4 + 64;
 }
 
 // dE/dT with W atoms (warps) per block, W in {2, 4, 8} (launch shape only).
@@ -1874,13 +1927,17 @@ static int launch_pos_sorted(const SysDesc &D, const float *pos, const int32_t *
   return DPB_OK;
 }
 
+// rows / rcnt (may be null): where the forward keeps its compacted rows for
+// the adjoint.
 int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, const float *box,
-                      const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, int *err, cudaStream_t st) {
+                      const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, float4 *rows, int *rcnt, int *err,
+                      cudaStream_t st) {
   if (M.ngrids > 0 || !M.emb_tuned) return DPB_ERR_UNSUPPORTED;  // the FP32 kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
-    int rc = (M.E2 == 100) ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, posS, box, nbrs, T, Gb, err, st)
-                           : launch_mix_embed_fwd<32, 32, 64>(M, D, ti, posS, box, nbrs, T, Gb, err, st);
+    int rc = (M.E2 == 100)
+                 ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, posS, box, nbrs, T, Gb, rows, rcnt, err, st)
+                 : launch_mix_embed_fwd<32, 32, 64>(M, D, ti, posS, box, nbrs, T, Gb, rows, rcnt, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_FWD, st);
@@ -1960,7 +2017,7 @@ int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos,
   float4 *posS = reinterpret_cast<float4 *>(static_cast<char *>(ws) + al256(NG * 2));
   int rc = launch_pos_sorted(D, pos, perm, posS, st);
   if (rc) return rc;
-  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, err, st);
+  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, nullptr, nullptr, err, st);
   if (rc) return rc;
   k_bf16_to_f32<<<(unsigned)((NG + 255) / 256), 256, 0, st>>>(Gb, G, NG);
   count_launch();
@@ -1977,6 +2034,8 @@ struct MixedWs {
   __half *dTh;   // dE/dT rows (FP16, scaled per atom)
   float *dTs;    // per-atom inverse scale of dTh
   float4 *posS;
+  float4 *rows;  // the forward's compacted neighbour rows (kRowStoreCap per atom)
+  int *rcnt;     // their count per block and neighbour type
   float *scratch;
 };
 
@@ -1991,6 +2050,8 @@ static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
   o.dTh = (__half *)w; w += al256(NF * 10 * N2 * 2);
   o.dTs = (float *)w; w += al256(NF * 4);
   o.posS = (float4 *)w; w += al256(NF * 16);
+  o.rows = (float4 *)w; w += al256(NF * kRowStoreCap * 16);
+  o.rcnt = (int *)w; w += al256(NF * M.ntypes * 4);
   o.scratch = (float *)w;
   return o;
 }
@@ -2035,7 +2096,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
     return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
   int rc = launch_pos_sorted(D, pos, perm, posS, st);
   if (rc) return rc;
-  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, err, st);
+  rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, mw.rows, mw.rcnt, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
   __nv_bfloat16 *dGb = reinterpret_cast<__nv_bfloat16 *>(dG);  // dE/dG in BF16 (the dE/dT input)
@@ -2049,8 +2110,10 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   prof_begin(PROF_MIXED_EMBED_BWD, st);
   for (int ti = 0; ti < M.ntypes; ++ti) {
     rc = (M.E2 == 100)
-             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, F4, virial, err, st)
-             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, F4, virial, err, st);
+             ? launch_mix_embed_bwd<25, 50, 100>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, mw.rows, mw.rcnt, F4,
+                                                 virial, err, st)
+             : launch_mix_embed_bwd<32, 32, 64>(M, D, ti, posS, box, nbrs, mw.dTh, mw.dTs, mw.rows, mw.rcnt, F4,
+                                               virial, err, st);
     if (rc) return rc;
   }
   prof_end(PROF_MIXED_EMBED_BWD, st);
