@@ -2,6 +2,7 @@
 #include "internal.cuh"
 #include "tc.cuh"
 #include <cuda_bf16.h>
+#include <cmath>
 #include <cstring>
 #include <vector>
 #include <algorithm>
@@ -104,17 +105,12 @@ static int upload(dpb_model *m, const T *host, size_t n, const T **dev) {
   return DPB_OK;
 }
 
-static int upload_bf16(dpb_model *m, const std::vector<float> &v, const __nv_bfloat16 **dev) {
-  std::vector<__nv_bfloat16> b(v.size());
-  for (size_t i = 0; i < v.size(); ++i) b[i] = __float2bfloat16_rn(v[i]);
-  return upload(m, b.data(), b.size(), dev);
-}
-
 // B operand chunks of the mixed fitting kernel from a row-major matrix
-// (rows x K): for pass p of br rows and K chunk k (16 wide), the chunk is
-// [half (2)][row (br)][8] BF16, rows past `rows` zero (mixed.cu, k_mix_fit).
-static int upload_fit_tiles(dpb_model *m, const std::vector<float> &a, int rows, int K, int br,
-                            const __nv_bfloat16 **dev) {
+// (rows x K) times `scale`: for pass p of br rows and K chunk k (16 wide), the
+// chunk is [half (2)][row (br)][8] FP16, rows past `rows` zero (mixed.cu,
+// k_mix_fit).
+static int upload_fit_tiles(dpb_model *m, const std::vector<float> &a, int rows, int K, int br, float scale,
+                            const __half **dev) {
   const int nk = K / 16, npass = (rows + br - 1) / br;
   std::vector<float> t((size_t)npass * nk * 2 * br * 8, 0.f);
   for (int p = 0; p < npass; ++p)
@@ -126,7 +122,18 @@ static int upload_fit_tiles(dpb_model *m, const std::vector<float> &a, int rows,
           for (int e = 0; e < 8; ++e)
             t[((((size_t)p * nk + k) * 2 + h) * br + r) * 8 + e] = a[(size_t)row * K + k * 16 + h * 8 + e];
         }
-  return upload_bf16(m, t, dev);
+  std::vector<__half> b(t.size());
+  for (size_t i = 0; i < t.size(); ++i) b[i] = __float2half_rn(t[i] * scale);
+  return upload(m, b.data(), b.size(), dev);
+}
+
+// 2^k with x 2^k in (2^13, 2^14] (x > 0; 1 for x = 0 or non-finite), k
+// clamped to [-40, 40].
+static float pow2_scale_to_2p14(double x) {
+  if (!(x > 0.0) || !std::isfinite(x)) return 1.f;
+  int k = 14 - (int)std::ceil(std::log2(x));
+  k = std::max(-40, std::min(40, k));
+  return std::ldexp(1.f, k);
 }
 
 // The tuned three-layer embedding instantiations (FP32 and tensor-core kernels).
@@ -266,6 +273,10 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   const int K0 = M.A * M.E2;
   M.mfw = dpb::mixed_fit_width(M);
   for (int t = 0; t < nt && rc == DPB_OK; ++t) {
+    // per layer: max over inputs i of sum_o |W[i][o]|, max |dt| (1 without
+    // residual), and max |w_out|: the bounds behind fit_gsc
+    std::vector<double> rowsum(M.nfit + 1, 0.0), maxdt(M.nfit + 1, 1.0);
+    double wout_max = 0.0;
     for (int l = 0; l <= M.nfit && rc == DPB_OK; ++l) {
       const int in = l == 0 ? K0 : M.FW[l - 1];
       const int outw = l == M.nfit ? 1 : M.FW[l];
@@ -282,10 +293,21 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
       for (int i = 0; i < in; ++i)
         for (int o = 0; o < outw; ++o) kt[(size_t)o * in + i] = kv[(size_t)i * outw + o];
       if (rc == DPB_OK) rc = upload(m, kt.data(), kt.size(), &M.fwT[t][l]);
-      if (rc == DPB_OK) rc = upload_bf16(m, kv, &M.fw_bf[t][l]);
-      if (rc == DPB_OK) rc = upload_bf16(m, kt, &M.fwT_bf[t][l]);
       const float *dt = (l < M.nfit && d->fit_dt) ? d->fit_dt[t * M.nfit + l] : nullptr;
       if (rc == DPB_OK && dt) rc = upload(m, dt, (size_t)outw, &M.fdt[t][l]);
+      double wmax = 0.0;
+      for (int i = 0; i < in; ++i) {
+        double rs = 0.0;
+        for (int o = 0; o < outw; ++o) {
+          rs += std::fabs((double)kv[(size_t)i * outw + o]);
+          wmax = std::max(wmax, std::fabs((double)kv[(size_t)i * outw + o]));
+        }
+        rowsum[l] = std::max(rowsum[l], rs);
+      }
+      if (dt)  // the kernel multiplies by dt or by 1: bound by both
+        for (int o = 0; o < outw; ++o) maxdt[l] = std::max(maxdt[l], std::fabs((double)dt[o]));
+      if (l == M.nfit) wout_max = wmax;
+      else M.fit_wsc[t][l] = pow2_scale_to_2p14(wmax);
       if (rc == DPB_OK && M.mfw > 0) {
         // the tensor-core fitting's copy: every hidden width padded to mfw with zeros
         const int P = M.mfw, inp = l == 0 ? K0 : P, outp = l == M.nfit ? 1 : P;
@@ -303,14 +325,29 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
           }
           rc = upload(m, bp.data(), bp.size(), &M.mfb[t][l]);
           if (rc == DPB_OK && dt) rc = upload(m, dp.data(), dp.size(), &M.mfdt[t][l]);
-          if (rc == DPB_OK) rc = upload_fit_tiles(m, ktp, outp, inp, outp, &M.fit_bt[t][kFitBtFwd + l]);
-          if (rc == DPB_OK && l >= 1) rc = upload_fit_tiles(m, kp, inp, outp, inp, &M.fit_bt[t][kFitBtAdj + l]);
-          if (rc == DPB_OK && l == 0) rc = upload_fit_tiles(m, kp, K0, outp, 128, &M.fit_bt[t][kFitBtDg]);
+          const float ws = M.fit_wsc[t][l];
+          if (rc == DPB_OK) rc = upload_fit_tiles(m, ktp, outp, inp, outp, ws, &M.fit_bt[t][kFitBtFwd + l]);
+          if (rc == DPB_OK && l >= 1) rc = upload_fit_tiles(m, kp, inp, outp, inp, ws, &M.fit_bt[t][kFitBtAdj + l]);
+          if (rc == DPB_OK && l == 0) rc = upload_fit_tiles(m, kp, K0, outp, 128, ws, &M.fit_bt[t][kFitBtDg]);
         } else {
           rc = upload(m, kp.data(), kp.size(), &M.mfwout[t]);
         }
       }
     }
+    // bound on the adjoint gate g_l of every layer (what the kernel packs as
+    // layer l's A operand): g_{L-1} = w_out dt (1 - t^2); the accumulator
+    // g_l W_l^T of row i is at most G_l rowsum_l, plus the residual's
+    // dE/dh term where layer l has one
+    const int L = M.nfit;
+    std::vector<double> G(L, 0.0);
+    double Hb = wout_max;  // bound on dE/dh_{L-1}
+    G[L - 1] = Hb * maxdt[L - 1];
+    for (int l = L - 1; l >= 1; --l) {
+      const bool res_l = d->fit_dt && d->fit_dt[t * M.nfit + l];
+      Hb = G[l] * rowsum[l] + (res_l ? Hb : 0.0);
+      G[l - 1] = Hb * maxdt[l - 1];
+    }
+    for (int l = 0; l < L; ++l) M.fit_gsc[t][l] = pow2_scale_to_2p14(G[l]);
   }
   if (rc == DPB_OK && !M.emb_tuned && !dpb::embed_general_fits(M)) rc = DPB_ERR_UNSUPPORTED;
   if (rc != DPB_OK) {

@@ -2,6 +2,7 @@
 #pragma once
 #include "dpb_common.cuh"
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace dpb {
 
@@ -33,9 +34,6 @@ struct DevModel {
   const float *fdt[kMaxTypes][kMaxFitLayers];
   // transposed fitting kernels (out,in) for the adjoint GEMMs
   const float *fwT[kMaxTypes][kMaxFitLayers + 1];
-  // BF16 copies of the fitting kernels for the mixed path (layouts documented in mixed.cu)
-  const __nv_bfloat16 *fw_bf[kMaxTypes][kMaxFitLayers + 1];
-  const __nv_bfloat16 *fwT_bf[kMaxTypes][kMaxFitLayers + 1];
   // per embedding net: the shared-memory image of its FP16 B tiles (layer 1
   // and layer 2, K-major, the layer's bias as the K row after the inputs,
   // zero padded to multiples of 16) and of its first layer (w0, b0 in FP32,
@@ -48,11 +46,17 @@ struct DevModel {
   int ngrids;
   const float *cmp_coeff[kMaxTypes * kMaxTypes];
   float cmp_srmin[kMaxTypes * kMaxTypes], cmp_delta[kMaxTypes * kMaxTypes];
-  // BF16 fitting weights pre-tiled as the B operand chunks of the mixed
+  // FP16 fitting weights pre-tiled as the B operand chunks of the mixed
   // fitting kernel (K = 16 per chunk, [chunk][k8 (2)][row][8]): forward layer l
   // at kFitBtFwd + l (W_l^T), adjoint layer l >= 1 at kFitBtAdj + l (W_l), and
-  // W_0 in passes of 128 rows at kFitBtDg; null when the mixed form is unsupported
-  const __nv_bfloat16 *fit_bt[kMaxTypes][2 * kMaxFitLayers + 1];
+  // W_0 in passes of 128 rows at kFitBtDg; null when the mixed form is unsupported.
+  // Layer l's weights are stored times fit_wsc[t][l] = 2^k (largest magnitude
+  // in (2^13, 2^14]), and the adjoint's A operand of layer l (the gate g of
+  // dE/dz_l) times fit_gsc[t][l] = 2^k' with k' from a bound on |g| that
+  // propagates max |w_out|, max |dt| and the row sums of |W| down the chain;
+  // the kernel divides each accumulator by its two powers of two (exact).
+  const __half *fit_bt[kMaxTypes][2 * kMaxFitLayers + 1];
+  float fit_wsc[kMaxTypes][kMaxFitLayers], fit_gsc[kMaxTypes][kMaxFitLayers];
   // the tensor-core fitting runs every hidden layer at one width mfw (a
   // multiple of 16 with a kernel instantiation, >= every FW[l]; 0: no
   // tensor-core fitting for this shape); the padding columns carry zero

@@ -348,6 +348,13 @@ __device__ __forceinline__ void mix_stream_round(const float4 *__restrict__ src,
   __syncthreads();
 }
 
+// 8 floats times s as FP16, round to nearest, saturating at the largest
+// finite FP16 value.
+__device__ __forceinline__ uint4 pack8h(const float *v, float s) {
+  return make_uint4(tc::as_u32(tc::f2_to_h2(v[0] * s, v[1] * s)), tc::as_u32(tc::f2_to_h2(v[2] * s, v[3] * s)),
+                    tc::as_u32(tc::f2_to_h2(v[4] * s, v[5] * s)), tc::as_u32(tc::f2_to_h2(v[6] * s, v[7] * s)));
+}
+
 __device__ __forceinline__ uint4 pack8(const float *v) {
   return make_uint4(tc::pack_bf16(v[0], v[1]), tc::pack_bf16(v[2], v[3]), tc::pack_bf16(v[4], v[5]),
                     tc::pack_bf16(v[6], v[7]));
@@ -404,7 +411,7 @@ __device__ __forceinline__ void emb_layer0(float st, const float *sm, int row, c
     const int c = lo + 2 * j;
     const float za = fmaf(st, sm[c], sm[E0 + c]);
     const float zb = (c + 1 < E0) ? fmaf(st, sm[c + 1], sm[E0 + c + 1]) : 0.f;
-    const __half2 t = tc::tanh_h2(tc::f2_to_h2(za, zb));
+    const __half2 t = tc::tanh_pair(za, zb);
     h0[j] = t;
     if (TANGENT) d0[j] = __hmul2(__hfma2(__hneg2(t), t, one2), tc::as_h2(w0p[c >> 1]));
   }
@@ -444,7 +451,7 @@ __device__ __forceinline__ void emb_epi1(uint32_t tD, uint32_t tDt, int row, cha
     for (int i = 0; i < 8; i += 2) {
       const int c = g + i;
       if (c < c0 || c >= c1) continue;
-      const __half2 t = tc::tanh_h2(tc::f2_to_h2(__uint_as_float(z[i]), __uint_as_float(z[i + 1])));
+      const __half2 t = tc::tanh_pair(__uint_as_float(z[i]), __uint_as_float(z[i + 1]));
       h1[(c - c0) >> 1] = __hadd2(t, res_pair<MD::Z1>(h0, c, h0lo));
       if (TANGENT) {
         const __half2 u = __hfma2(__hneg2(t), t, one2);
@@ -491,7 +498,7 @@ __device__ __forceinline__ void emb_epi2(uint32_t tD, uint32_t tDt, char *h2, ch
       const int c = k8 + 2 * u, i = 2 * u;
       hv[u] = dv[u] = zero2;
       if (c < E2) {
-        const __half2 t = tc::tanh_h2(tc::f2_to_h2(__uint_as_float(z[i]), __uint_as_float(z[i + 1])));
+        const __half2 t = tc::tanh_pair(__uint_as_float(z[i]), __uint_as_float(z[i + 1]));
         hv[u] = __hadd2(t, res_pair<MD::Z2>(h1, c, h1lo));
         if (TANGENT)
           dv[u] = __hfma2(__hfma2(__hneg2(t), t, one2),
@@ -537,7 +544,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
                                                                   const float *__restrict__ box,
                                                                   const int32_t *__restrict__ nbrs,
                                                                   float *__restrict__ Tout,
-                                                                  __nv_bfloat16 *__restrict__ Gout,
+                                                                  __half *__restrict__ Gout,
                                                                   float4 *__restrict__ rows_g,
                                                                   int *__restrict__ rcnt,
                                                                   int *__restrict__ err) {
@@ -792,7 +799,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
         xa[0] += M.tbias[w];
         xb[0] += M.tbias[w + 1];
         const float *Q = Qs + slot * 160;
-        __nv_bfloat162 *Gs = reinterpret_cast<__nv_bfloat162 *>(Gout + (g0 + slot) * (size_t)A * E2 + w);
+        __half2 *Gs = reinterpret_cast<__half2 *>(Gout + (g0 + slot) * (size_t)A * E2 + w);
         for (int aa = 0; aa < A; ++aa) {
           float va = 0.f, vb = 0.f;
 #pragma unroll
@@ -801,7 +808,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
             va = fmaf(qv, xa[c], va);
             vb = fmaf(qv, xb[c], vb);
           }
-          Gs[aa * (E2 / 2)] = __floats2bfloat162_rn(va, vb);
+          Gs[aa * (E2 / 2)] = __floats2half2_rn(va, vb);  // no saturation: |G| > 65504 -> inf -> NaN energy
         }
       }
     }
@@ -834,7 +841,7 @@ static int num_sms() {
 
 template <int E0, int E1, int E2>
 int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
-                         const float *box, const int32_t *nbrs, float *T, __nv_bfloat16 *G, float4 *rows_g,
+                         const float *box, const int32_t *nbrs, float *T, __half *G, float4 *rows_g,
                          int *rcnt, int *err, cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
@@ -1488,7 +1495,7 @@ __device__ __forceinline__ FitGemm fit_gemm_info(const DevModel &M, int ti, int 
 template <int FW, typename DGT>
 __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
                                                            int Mrows, RowMap rm,
-                                                           const __nv_bfloat16 *__restrict__ Gb,
+                                                           const __half *__restrict__ Gh,
                                                            DGT *__restrict__ dGout, float *__restrict__ scratch,
                                                            float *__restrict__ Eatom, double *__restrict__ energy,
                                                            int N, int *__restrict__ err,
@@ -1565,7 +1572,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         }
         if (!ok) break;
         tc::fence_after_sync();
-        const uint32_t idesc = tc::idesc_bf16(128, gi.N, 0, 0);
+        const uint32_t idesc = tc::idesc_f16(128, gi.N, 0, 0);
         for (int k = 0; k < gi.nk; ++k, ++q) {
           const int s = q % ST;
           const uint32_t par = (q / ST) & 1;
@@ -1595,7 +1602,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
     // ---- layer 0's A operand: this atom's G row, ST - 1 chunks in flight
     {
       const int nch0 = K0 / 16;
-      const char *grow = reinterpret_cast<const char *>(Gb + me * (size_t)K0);
+      const char *grow = reinterpret_cast<const char *>(Gh + me * (size_t)K0);
       for (int c = 0; c < nch0 + ST - 1; ++c) {
         if (c < nch0) {
           const int s = c % ST;
@@ -1636,6 +1643,8 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       tc::fence_after_sync();
       const bool last = l == L - 1;
       const float *bias = M.mfb[ti][l], *dt = M.mfdt[ti][l];
+      const float usc = 1.f / M.fit_wsc[ti][l];         // a power of two: exact
+      const float gsc = last ? M.fit_gsc[ti][l] : 1.f;  // the gate's operand scale
       // residual sources of the current chunk, loaded one chunk ahead so the
       // scratch reads overlap the TMEM loads and the previous chunk's math
       float hp[16];
@@ -1663,7 +1672,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int n = c0 + i;
-          const float t = tc::tanh_fast(__uint_as_float(r[i]) + bv[i]);
+          const float t = tc::tanh_fast(fmaf(__uint_as_float(r[i]), usc, bv[i]));
           float h = t;
           if (dt) h = t * dv[i] + hp[i];
           if (!last) {
@@ -1677,8 +1686,8 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) hp[i] = hn[i];
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(hv);
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(hv + 8);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8h(hv, gsc);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8h(hv + 8, gsc);
       }
       fit_signal(&epid);
     }
@@ -1711,6 +1720,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       const bool res_l = M.mfdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.mfdt[ti][l - 1] != nullptr;
       const float *dtm1 = M.mfdt[ti][l - 1], *wf = M.mfwout[ti];
       const bool use_gh = res_l && l != L - 1;
+      const float usc = 1.f / (M.fit_wsc[ti][l] * M.fit_gsc[ti][l]), gsc = M.fit_gsc[ti][l - 1];
       float ghc[16], tcur[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -1740,7 +1750,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int n = c0 + i;
-          float g = __uint_as_float(r[i]);
+          float g = __uint_as_float(r[i]) * usc;
           if (res_l) g += (l == L - 1) ? wv[i] : ghc[i];
           const float t = tcur[i];
           gz[i] = g * dv[i] * (1.f - t * t);
@@ -1751,13 +1761,14 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           ghc[i] = ghn[i];
           tcur[i] = tn[i];
         }
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8(gz);
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8(gz + 8);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8h(gz, gsc);
+        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8h(gz + 8, gsc);
       }
       fit_signal(&epid);
     }
     // ---- dE/dG = gZ_0 W_0^T, 128 columns per pass from alternating accumulators
     const int npass = (K0 + kFitDgN - 1) / kFitDgN;
+    const float usc0 = 1.f / (M.fit_wsc[ti][0] * M.fit_gsc[ti][0]);
     for (int pp = 0; pp < npass && ok; ++pp) {
       ok = __all_sync(0xffffffffu, fit_wait(&accfD[pp & 1], (pp >> 1) & 1, abort));
       if (!ok) break;
@@ -1770,6 +1781,11 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         tc::tmem_ld16_issue(tcol + c0, ra);
         if (two) tc::tmem_ld16_issue(tcol + c0 + 16, rb);
         tc::tmem_wait();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          ra[i] = __float_as_uint(__uint_as_float(ra[i]) * usc0);
+          rb[i] = __float_as_uint(__uint_as_float(rb[i]) * usc0);
+        }
         if (act) {
           if constexpr (sizeof(DGT) == 4) {  // FP32 (for the FP32 embedding adjoint)
             float4 *dst = reinterpret_cast<float4 *>(dGout + me * K0 + n0 + c0);
@@ -1813,7 +1829,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
 }
 
 template <int FW, typename DGT>
-int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, DGT *dG, float *scratch,
+int launch_mix_fit(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *dG, float *scratch,
                    float *Eatom, double *energy, int *err, cudaStream_t st) {
   using C = FitCfg<FW>;
   if (!M.fit_bt[0][kFitBtDg]) return DPB_ERR_UNSUPPORTED;
@@ -1836,7 +1852,7 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb,
 
 // The instantiation of the model's padded hidden width.
 template <typename DGT>
-int launch_mix_fit_any(const DevModel &M, const SysDesc &D, const __nv_bfloat16 *Gb, DGT *dG, float *scratch,
+int launch_mix_fit_any(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *dG, float *scratch,
                        float *Eatom, double *energy, int *err, cudaStream_t st) {
   switch (M.mfw) {
     case 64: return launch_mix_fit<64, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
@@ -1930,7 +1946,7 @@ static int launch_pos_sorted(const SysDesc &D, const float *pos, const int32_t *
 // rows / rcnt (may be null): where the forward keeps its compacted rows for
 // the adjoint.
 int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, const float *box,
-                      const int32_t *nbrs, float *T, __nv_bfloat16 *Gb, float4 *rows, int *rcnt, int *err,
+                      const int32_t *nbrs, float *T, __half *Gb, float4 *rows, int *rcnt, int *err,
                       cudaStream_t st) {
   if (M.ngrids > 0 || !M.emb_tuned) return DPB_ERR_UNSUPPORTED;  // the FP32 kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
@@ -1944,16 +1960,18 @@ int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, c
   return DPB_OK;
 }
 
-__global__ void k_bf16_to_f32(const __nv_bfloat16 *__restrict__ a, float *__restrict__ b, size_t n) {
+__global__ void k_f16_to_f32(const __half *__restrict__ a, float *__restrict__ b, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = __bfloat162float(a[i]);
+  if (i < n) b[i] = __half2float(a[i]);
 }
 
-__global__ void k_f32_to_bf16(const float4 *__restrict__ a, uint2 *__restrict__ b, size_t n4) {
+// FP32 -> FP16 rounded to nearest, without saturation (as the embedding
+// kernel writes G).
+__global__ void k_f32_to_f16(const float4 *__restrict__ a, uint2 *__restrict__ b, size_t n4) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n4) {
     const float4 v = a[i];
-    b[i] = make_uint2(tc::pack_bf16(v.x, v.y), tc::pack_bf16(v.z, v.w));
+    b[i] = make_uint2(tc::as_u32(__floats2half2_rn(v.x, v.y)), tc::as_u32(__floats2half2_rn(v.z, v.w)));
   }
 }
 
@@ -1975,7 +1993,7 @@ int launch_embed_bwd_gen(const DevModel &, const SysDesc &, int, const float *, 
 // on the tensor cores from a BF16 copy of G.
 static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                                  const float *box, const int32_t *nbrs, double *energy, float *Eatom, float4 *F4,
-                                 double *virial, float *T, __nv_bfloat16 *Gb, float *dG, float *scratch, int *err,
+                                 double *virial, float *T, __half *Gb, float *dG, float *scratch, int *err,
                                  cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
   const size_t NG = NF * M.A * M.E2;  // a multiple of 16 (mixed_supported)
@@ -1987,7 +2005,7 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
                        : launch_embed_fwd<32, 32, 64>(M, D, ti, pos, perm, box, nbrs, T, dG, st);
     if (rc) return rc;
   }
-  k_f32_to_bf16<<<(unsigned)((NG / 4 + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(dG),
+  k_f32_to_f16<<<(unsigned)((NG / 4 + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(dG),
                                                                    reinterpret_cast<uint2 *>(Gb), NG / 4);
   count_launch();
   DPB_LAUNCH_CHECK();
@@ -2013,13 +2031,13 @@ int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos,
                           const float *box, const int32_t *nbrs, float *T, float *G, int *err, void *ws,
                           cudaStream_t st) {
   const size_t NG = (size_t)D.N * D.F * M.A * M.E2;
-  __nv_bfloat16 *Gb = reinterpret_cast<__nv_bfloat16 *>(ws);
+  __half *Gb = reinterpret_cast<__half *>(ws);
   float4 *posS = reinterpret_cast<float4 *>(static_cast<char *>(ws) + al256(NG * 2));
   int rc = launch_pos_sorted(D, pos, perm, posS, st);
   if (rc) return rc;
   rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, nullptr, nullptr, err, st);
   if (rc) return rc;
-  k_bf16_to_f32<<<(unsigned)((NG + 255) / 256), 256, 0, st>>>(Gb, G, NG);
+  k_f16_to_f32<<<(unsigned)((NG + 255) / 256), 256, 0, st>>>(Gb, G, NG);
   count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
@@ -2029,7 +2047,7 @@ int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos,
 struct MixedWs {
   int *err;
   float *T;
-  __nv_bfloat16 *Gb;
+  __half *Gb;  // the descriptor G (FP16), the fitting's input
   float *dG;
   __half *dTh;   // dE/dT rows (FP16, scaled per atom)
   float *dTs;    // per-atom inverse scale of dTh
@@ -2045,7 +2063,7 @@ static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
   MixedWs o;
   o.err = (int *)w; w += 256;
   o.T = (float *)w; w += al256(NF * 10 * M.E2 * 4);
-  o.Gb = (__nv_bfloat16 *)w; w += al256(NF * K0 * 2);
+  o.Gb = (__half *)w; w += al256(NF * K0 * 2);
   o.dG = (float *)w; w += al256(NF * K0 * 4);
   o.dTh = (__half *)w; w += al256(NF * 10 * N2 * 2);
   o.dTs = (float *)w; w += al256(NF * 4);
@@ -2089,7 +2107,7 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   const MixedWs mw = mixed_ws(M, NF, ws);
   int *err = mw.err;
   float *T = mw.T, *dG = mw.dG, *scratch = mw.scratch;
-  __nv_bfloat16 *Gb = mw.Gb;
+  __half *Gb = mw.Gb;
   float4 *posS = mw.posS;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
   if (M.ngrids > 0 || !M.emb_tuned)

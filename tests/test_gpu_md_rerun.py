@@ -3,7 +3,7 @@
 
 * Bit 2 (neighbour overflow): an engine whose capacity is the exact maximum
   neighbour count of the initial frame (buffer ratio 1.0) overflows at a
-  drift-gated rebuild in the middle of a 60-step chunk.  It must reallocate
+  drift-gated rebuild in the middle of a 40-step chunk.  It must reallocate
   and re-run that chunk, so its trajectory equals the one of an engine given
   the grown capacity from step 0; an engine that kept the truncated list for
   the rest of the chunk would miss pairs within rcut.
@@ -14,11 +14,12 @@
 "Equals" is measured against the engine's own run-to-run spread: the force
 scatter adds in float32 atomics, whose order varies from run to run, and the
 random-init model (no short-range repulsion, atoms heat up and pass close to
-one another) grows that last-bit noise by orders of magnitude within tens of
-steps.  So a second engine with the grown setting gives the yardstick: the
-re-run trajectory must lie within 10x the distance between the two clean
-runs (or 1e-5 A, whichever is larger), and within 1e-5 A over the first 10
-steps, where the noise has not grown yet.  A wrong re-run (a lost neighbour,
+one another) grows that last-bit noise by orders of magnitude at a close
+approach (in this box one comes near step 55, where two clean runs part from
+2e-6 A to 2e-4 A within three steps).  The runs stop at 40 steps, before it,
+and a second engine with the grown setting gives the yardstick: the re-run
+trajectory must lie within 10x the distance between the two clean runs or
+1e-5 A, whichever is larger, and within 1e-5 A over the first 10 steps.  A wrong re-run (a lost neighbour,
 a chunk that does not restart from its saved state) moves atoms by a
 perturbation of a missing pair's force, not of a float32 last bit, and
 lands orders of magnitude outside.
@@ -61,17 +62,17 @@ def test_neighbour_overflow_mid_chunk_is_rerun_at_grown_capacity():
     tight = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.5, w["position"],
                        neighbor_buffer_ratio=1.0, **kw)
     sel0 = list(tight._sel)
-    traj_t = tight.run(60)
+    traj_t = tight.run(40)
     sel1 = list(tight._sel)
     assert any(b > a for a, b in zip(sel0, sel1)), "the tight capacity never overflowed (%s)" % sel0
-    assert tight.step == 60 and int(tight._report_struct().status) & 2 == 0
+    assert tight.step == 40 and int(tight._report_struct().status) & 2 == 0
 
     def clean():
         sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE", 0.5, w["position"], **kw)
         arr = (ctypes.c_int * len(sel1))(*sel1)
         _lib.check(sim.lib.dpb_md_set_capacity(sim._h, arr, None), "dpb_md_set_capacity")
         sim._sel = sel1
-        return sim.run(60)
+        return sim.run(40)
 
     print("capacity %s -> %s" % (sel0, sel1))
     _same_within_spread("neighbour overflow", traj_t, clean(), clean())
@@ -85,14 +86,14 @@ def test_npt_box_shrink_past_skin_is_rerun_with_grown_skin():
               report_interval=200, verbose=False)
     small = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NPT", 0.5, w["position"],
                        neighbor_skin=0.01, **kw)
-    traj_s = small.run(60)
+    traj_s = small.run(40)
     assert small._neighbor_skin > 0.01 + 0.3, "the box never shrank past the 0.01 A skin"
-    assert small.step == 60
+    assert small.step == 40
 
     def clean():
         sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NPT", 0.5, w["position"],
                          neighbor_skin=small._neighbor_skin, **kw)
-        return sim.run(60)
+        return sim.run(40)
 
     g1, g2 = clean(), clean()
     print("skin 0.01 -> %.2f A; box difference %.2e A (clean vs clean %.2e A)"
