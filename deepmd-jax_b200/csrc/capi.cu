@@ -227,14 +227,13 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   // shared-memory images of the embedding nets for the tensor-core kernels:
   // FP16 B tiles (K-major) of layers 1 and 2 with the layer's bias as one
   // more K row (the A operands carry a ones column there), and the FP32 first
-  // layer (w0, b0) plus w0 as FP16 pairs (mixed.cu, MixDims)
+  // layer (w0, b0 in FP32) (mixed.cu, MixDims)
   {
     const int K1 = (M.E0 + 1 + 15) / 16 * 16, N1 = (M.E1 + 15) / 16 * 16;
     const int K2 = (M.E1 + 1 + 15) / 16 * 16, N2 = (M.E2 + 15) / 16 * 16;
     const int W1B = N1 * K1 * 2, W2B = N2 * K2 * 2;
-    const int npair0 = (M.E0 + 1) / 2;
     M.net_img_bytes = W1B + W2B;
-    M.net_small_floats = (2 * M.E0 + npair0 + 3) / 4 * 4;
+    M.net_small_floats = (2 * M.E0 + 3) / 4 * 4;
     for (int k = 0; k < nt * nt && rc == DPB_OK && have_mlp && M.emb_tuned; ++k) {
       std::vector<uint8_t> img(M.net_img_bytes, 0);
       const float *W1 = d->embed_kernel[k * 3 + 1], *W2 = d->embed_kernel[k * 3 + 2];
@@ -262,16 +261,13 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
         sm[e] = w0[e];
         sm[M.E0 + e] = b0[e];
       }
-      for (int j = 0; j < npair0; ++j) {
-        __half2 h = __floats2half2_rn(w0[2 * j], 2 * j + 1 < M.E0 ? w0[2 * j + 1] : 0.f);
-        std::memcpy(&sm[2 * M.E0 + j], &h, 4);
-      }
       if (rc == DPB_OK) rc = upload(m, sm.data(), sm.size(), &M.net_small[k]);
     }
   }
   if (rc == DPB_OK) rc = upload(m, d->tbias, (size_t)M.E2, &M.tbias);
   const int K0 = M.A * M.E2;
   M.mfw = dpb::mixed_fit_width(M);
+  double dg_bound = 0.0;  // largest bound on |dE/dG| over the types
   for (int t = 0; t < nt && rc == DPB_OK; ++t) {
     // per layer: max over inputs i of sum_o |W[i][o]|, max |dt| (1 without
     // residual), and max |w_out|: the bounds behind fit_gsc
@@ -348,7 +344,9 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
       G[l - 1] = Hb * maxdt[l - 1];
     }
     for (int l = 0; l < L; ++l) M.fit_gsc[t][l] = pow2_scale_to_2p14(G[l]);
+    dg_bound = std::max(dg_bound, G[0] * rowsum[0]);
   }
+  M.fit_dgsc = pow2_scale_to_2p14(dg_bound);
   if (rc == DPB_OK && !M.emb_tuned && !dpb::embed_general_fits(M)) rc = DPB_ERR_UNSUPPORTED;
   if (rc != DPB_OK) {
     dpb_model_destroy(m);

@@ -36,8 +36,8 @@ struct DevModel {
   const float *fwT[kMaxTypes][kMaxFitLayers + 1];
   // per embedding net: the shared-memory image of its FP16 B tiles (layer 1
   // and layer 2, K-major, the layer's bias as the K row after the inputs,
-  // zero padded to multiples of 16) and of its first layer (w0, b0 in FP32,
-  // w0 as FP16 pairs), copied verbatim by the mixed kernels
+  // zero padded to multiples of 16) and of its first layer (w0, b0 in FP32),
+  // copied verbatim by the mixed kernels
   const char *net_img[kMaxTypes * kMaxTypes];
   const float *net_small[kMaxTypes * kMaxTypes];
   int net_img_bytes, net_small_floats;
@@ -57,6 +57,10 @@ struct DevModel {
   // the kernel divides each accumulator by its two powers of two (exact).
   const __half *fit_bt[kMaxTypes][2 * kMaxFitLayers + 1];
   float fit_wsc[kMaxTypes][kMaxFitLayers], fit_gsc[kMaxTypes][kMaxFitLayers];
+  // dE/dG leaves the fitting kernel as FP16 times fit_dgsc = 2^k, k from the
+  // gate bound of layer 0 times the row sums of |W_0| (largest over
+  // the types), and k_mix_dT divides it out
+  float fit_dgsc;
   // the tensor-core fitting runs every hidden layer at one width mfw (a
   // multiple of 16 with a kernel instantiation, >= every FW[l]; 0: no
   // tensor-core fitting for this shape); the padding columns carry zero

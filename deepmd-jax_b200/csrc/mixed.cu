@@ -83,7 +83,7 @@ struct MixDims {
   static constexpr int W1B = N1 * K1 * 2;  // bytes of the layer-1 B tile (K-major)
   static constexpr int W2B = N2 * K2 * 2;  // bytes of the layer-2 B tile (K-major)
   static constexpr int NETB = W1B + W2B;
-  static constexpr int NSMALL = (2 * E0 + (E0 + 1) / 2 + 3) / 4 * 4;  // w0, b0 (fp32), w0 pairs (fp16)
+  static constexpr int NSMALL = (2 * E0 + 3) / 4 * 4;  // w0, b0 (fp32)
   static constexpr int OPA_A0 = 128 * K1 * 2, OPA_A1 = 128 * K2 * 2, OPA_H2 = 128 * N2 * 2;
   static constexpr int OPA = imax(OPA_A0, imax(OPA_A1, OPA_H2));
   static constexpr int Z1 = E1 / E0, Z2 = E2 / E1;
@@ -404,16 +404,16 @@ __device__ __forceinline__ void emb_layer0(float st, const float *sm, int row, c
   using MD = MixDims<E0, E1, E2>;
   using SP = HalfSplit<E0, E1, E2>;
   constexpr int lo = HALF ? SP::H0LO1 : 0, hi = HALF ? E0 : SP::H0HI0;
-  const __half2 one2 = __float2half2_rn(1.f);
-  const uint32_t *w0p = reinterpret_cast<const uint32_t *>(sm + 2 * E0);
 #pragma unroll
   for (int j = 0; j < (hi - lo + 1) / 2; ++j) {
     const int c = lo + 2 * j;
     const float za = fmaf(st, sm[c], sm[E0 + c]);
     const float zb = (c + 1 < E0) ? fmaf(st, sm[c + 1], sm[E0 + c + 1]) : 0.f;
-    const __half2 t = tc::tanh_pair(za, zb);
+    const float ta = tc::tanh_fast(za), tb = tc::tanh_fast(zb);
+    const __half2 t = tc::f2_to_h2(ta, tb);
     h0[j] = t;
-    if (TANGENT) d0[j] = __hmul2(__hfma2(__hneg2(t), t, one2), tc::as_h2(w0p[c >> 1]));
+    if (TANGENT)
+      d0[j] = tc::f2_to_h2(fmaf(-ta, ta, 1.f) * sm[c], (c + 1 < E0) ? fmaf(-tb, tb, 1.f) * sm[c + 1] : 0.f);
   }
   constexpr int c0 = HALF ? SP::A0C : 0, c1 = HALF ? MD::K1 : SP::A0C;
 #pragma unroll
@@ -440,7 +440,6 @@ __device__ __forceinline__ void emb_epi1(uint32_t tD, uint32_t tDt, int row, cha
   using MD = MixDims<E0, E1, E2>;
   using SP = HalfSplit<E0, E1, E2>;
   constexpr int c0 = HALF ? SP::S1 : 0, c1 = HALF ? E1 : SP::S1, h0lo = HALF ? SP::H0LO1 : 0;
-  const __half2 one2 = __float2half2_rn(1.f);
 #pragma unroll
   for (int g = c0 / 8 * 8; g < c1; g += 8) {
     uint32_t z[8], dz[8];
@@ -451,10 +450,11 @@ __device__ __forceinline__ void emb_epi1(uint32_t tD, uint32_t tDt, int row, cha
     for (int i = 0; i < 8; i += 2) {
       const int c = g + i;
       if (c < c0 || c >= c1) continue;
-      const __half2 t = tc::tanh_pair(__uint_as_float(z[i]), __uint_as_float(z[i + 1]));
+      const float ta = tc::tanh_fast(__uint_as_float(z[i])), tb = tc::tanh_fast(__uint_as_float(z[i + 1]));
+      const __half2 t = tc::f2_to_h2(ta, tb);
       h1[(c - c0) >> 1] = __hadd2(t, res_pair<MD::Z1>(h0, c, h0lo));
       if (TANGENT) {
-        const __half2 u = __hfma2(__hneg2(t), t, one2);
+        const __half2 u = tc::f2_to_h2(fmaf(-ta, ta, 1.f), fmaf(-tb, tb, 1.f));
         d1[(c - c0) >> 1] = __hfma2(u, tc::f2_to_h2(__uint_as_float(dz[i]), __uint_as_float(dz[i + 1])),
                                     res_pair<MD::Z1>(d0, c, h0lo));
       }
@@ -483,7 +483,7 @@ __device__ __forceinline__ void emb_epi2(uint32_t tD, uint32_t tDt, char *h2, ch
   using MD = MixDims<E0, E1, E2>;
   using SP = HalfSplit<E0, E1, E2>;
   constexpr int c0 = HALF ? SP::S2 : 0, c1 = HALF ? MD::N2 : SP::S2, h1lo = HALF ? SP::S1 : 0;
-  const __half2 one2 = __float2half2_rn(1.f), zero2 = __float2half2_rn(0.f);
+  const __half2 zero2 = __float2half2_rn(0.f);
 #pragma unroll
   for (int k8 = c0; k8 < c1; k8 += 8) {
     uint32_t z[8], dz[8];
@@ -498,10 +498,11 @@ __device__ __forceinline__ void emb_epi2(uint32_t tD, uint32_t tDt, char *h2, ch
       const int c = k8 + 2 * u, i = 2 * u;
       hv[u] = dv[u] = zero2;
       if (c < E2) {
-        const __half2 t = tc::tanh_pair(__uint_as_float(z[i]), __uint_as_float(z[i + 1]));
+        const float ta = tc::tanh_fast(__uint_as_float(z[i])), tb = tc::tanh_fast(__uint_as_float(z[i + 1]));
+        const __half2 t = tc::f2_to_h2(ta, tb);
         hv[u] = __hadd2(t, res_pair<MD::Z2>(h1, c, h1lo));
         if (TANGENT)
-          dv[u] = __hfma2(__hfma2(__hneg2(t), t, one2),
+          dv[u] = __hfma2(tc::f2_to_h2(fmaf(-ta, ta, 1.f), fmaf(-tb, tb, 1.f)),
                           tc::f2_to_h2(__uint_as_float(dz[i]), __uint_as_float(dz[i + 1])),
                           res_pair<MD::Z2>(d1, c, h1lo));
       }
@@ -866,7 +867,7 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
 // dTs[atom] = 2^-k undoes it.
 template <int E2, int N2, int W>
 __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
-                                                const __nv_bfloat16 *__restrict__ dG,
+                                                const __half *__restrict__ dG,
                                                 __half *__restrict__ dTh, float *__restrict__ dTs) {
   // Warp per atom; lane owns the column pairs w = 2 lane + 64 j (+0, +1).
   // The atom's dE/dG rows stay in registers (D[a][2j + h]); X = T + Tbias
@@ -909,16 +910,17 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
     }
   }
   float D[16][2 * NJ];
-  const __nv_bfloat162 *Gg = reinterpret_cast<const __nv_bfloat162 *>(dG + g * (size_t)A * E2);
+  const __half2 *Gg = reinterpret_cast<const __half2 *>(dG + g * (size_t)A * E2);
+  const float inv_dgsc = 1.f / M.fit_dgsc;  // dE/dG arrives times fit_dgsc (a power of two)
 #pragma unroll
   for (int a = 0; a < 16; ++a)
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
       const int w = 2 * lane + 64 * j;
       float2 v = make_float2(0.f, 0.f);
-      if (a < A && w < E2) v = __bfloat1622float2(Gg[(a * E2 + w) / 2]);
-      D[a][2 * j] = v.x;
-      D[a][2 * j + 1] = v.y;
+      if (a < A && w < E2) v = __half22float2(Gg[(a * E2 + w) / 2]);
+      D[a][2 * j] = v.x * inv_dgsc;
+      D[a][2 * j + 1] = v.y * inv_dgsc;
     }
   __syncwarp();
   if (lane < 16) {  // Q[c][a] (dpmodel.py:74-78), zero for a >= A
@@ -1799,19 +1801,20 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
                 dst[4 + i / 4] = make_float4(__uint_as_float(rb[i]), __uint_as_float(rb[i + 1]),
                                              __uint_as_float(rb[i + 2]), __uint_as_float(rb[i + 3]));
             }
-          } else {  // BF16
+          } else {  // FP16 times fit_dgsc (for the tensor-core embedding adjoint)
             float fa[16], fb[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
               fa[i] = __uint_as_float(ra[i]);
               fb[i] = __uint_as_float(rb[i]);
             }
+            const float dgsc = M.fit_dgsc;
             uint4 *dst = reinterpret_cast<uint4 *>(dGout + me * K0 + n0 + c0);
-            dst[0] = pack8(fa);
-            dst[1] = pack8(fa + 8);
+            dst[0] = pack8h(fa, dgsc);
+            dst[1] = pack8h(fa + 8, dgsc);
             if (two) {
-              dst[2] = pack8(fb);
-              dst[3] = pack8(fb + 8);
+              dst[2] = pack8h(fb, dgsc);
+              dst[3] = pack8h(fb + 8, dgsc);
             }
           }
         }
@@ -1899,7 +1902,7 @@ size_t mixed_workspace_per_atom(const DevModel &M) {
 
 // dE/dT with W atoms (warps) per block, W in {2, 4, 8} (launch shape only).
 template <int W>
-static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb,
+static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const __half *dGb,
                             __half *dTh, float *dTs, cudaStream_t st) {
   const unsigned grid = (unsigned)((NF + W - 1) / W);
   if (M.E2 == 100) k_mix_dT<100, 112, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTh, dTs);
@@ -1907,7 +1910,7 @@ static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const 
   count_launch();
 }
 
-static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __nv_bfloat16 *dGb, __half *dTh,
+static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __half *dGb, __half *dTh,
                          float *dTs,
                          int warps, cudaStream_t st) {
   switch (warps) {
@@ -2077,7 +2080,7 @@ static MixedWs mixed_ws(const DevModel &M, size_t NF, void *ws) {
 int mixed_tune_dT(const DevModel &M, size_t NF, void *ws, cudaStream_t st, int *best) {
   if (M.ngrids > 0 || !M.emb_tuned || !best) return DPB_ERR_UNSUPPORTED;  // these take the FP32 adjoint
   const MixedWs w = mixed_ws(M, NF, ws);
-  const __nv_bfloat16 *dGb = reinterpret_cast<const __nv_bfloat16 *>(w.dG);
+  const __half *dGb = reinterpret_cast<const __half *>(w.dG);
   cudaEvent_t a, b;
   DPB_CUDA_TRY(cudaEventCreate(&a));
   DPB_CUDA_TRY(cudaEventCreate(&b));
@@ -2117,8 +2120,8 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, mw.rows, mw.rcnt, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
-  __nv_bfloat16 *dGb = reinterpret_cast<__nv_bfloat16 *>(dG);  // dE/dG in BF16 (the dE/dT input)
-  rc = launch_mix_fit_any<__nv_bfloat16>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
+  __half *dGb = reinterpret_cast<__half *>(dG);  // dE/dG in FP16 times fit_dgsc (the dE/dT input)
+  rc = launch_mix_fit_any<__half>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);

@@ -125,6 +125,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// tanh.approx.f32: about 1e-5 relative error with no sign preference, far
+// below the FP16 rounding step of the embedding's operands.  (The packed
+// tanh.approx.f16x2 is cheaper but shrinks |tanh| by about 3.5e-4 on average,
+// a bias that the embedding's tangents turn into a systematic scaling of the
+// forces, so the FP16 kernels take tanh in FP32 and round the pair.)
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -147,12 +152,7 @@ __device__ __forceinline__ __half2 f2_to_h2(float a, float b) {
   asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
   return as_h2(r);
 }
-// tanh of an FP32 pair, rounded to nearest into one FP16 pair.  The FP32
-// approximation (about 1e-5 relative, no sign preference) sits far below the
-// FP16 rounding step; the packed FP16 form (tanh.approx.f16x2) is cheaper but
-// shrinks |tanh| by about 3.5e-4 on average, a bias that the embedding's
-// tangents amplify into a systematic scaling of the forces.
-__device__ __forceinline__ __half2 tanh_pair(float a, float b) { return f2_to_h2(tanh_fast(a), tanh_fast(b)); }
+
 
 // Asynchronous 16-byte global -> shared copies (no register round trip).
 __device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem) {
