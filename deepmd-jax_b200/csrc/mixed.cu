@@ -320,16 +320,76 @@ __device__ __forceinline__ void mix_compact_round(const SysDesc &D, const DevMod
   __syncthreads();
 }
 
-// The forward kernel keeps, in list mode (one image per pair), the rows it
-// compacted for each block and neighbour type: rows of block g0 and type tj at
-// rows_g + g0 * kRowStoreCap + nb * col[tj], their count at rcnt[g0 * ntypes
-// + tj].  The adjoint then streams them back instead of compacting again.
+// Row store of list mode (one image per pair, boxes wider than 2 rcut):
+// k_mix_rows compacts the neighbour rows of every block of 8 centre atoms and
+// neighbour type once per evaluation, rows of block g0 and type tj at rows_g
+// + g0 * kRowStoreCap + nb * col[tj] (in candidate order, so sorted by atom
+// slot, as mix_compact_round leaves them), their count at rcnt[g0 * ntypes +
+// tj].  The forward and the adjoint embedding kernels then stream them.
 constexpr int kRowStoreCap = 192;  // neighbour slots per atom the store holds (sum of sel)
 
-// One round of the adjoint's row stream: the unread rows of earlier rounds
-// move to the front (as in mix_compact_round), then up to blockDim rows
-// [base, total) of the stored list are appended, one coalesced 16-byte load
-// per thread.
+// The blocks whose rows the store holds.
+__device__ __forceinline__ bool row_store_covers(const SysDesc &D, const float4 *rows_g, int nim) {
+  return rows_g != nullptr && nim == 1 && D.S <= kRowStoreCap;
+}
+
+// One warp per (block of 8 centre atoms of type ti, neighbour type tj): 32
+// candidates (atom slot, list slot) per round in candidate order, the
+// neighbour's position gathered from posS, the nearest-image displacement and
+// keep test of mix_compact_round (same arithmetic, so the same rows), kept
+// rows appended with a ballot.  Blocks outside the store (several images) are
+// left to the embedding kernels' own compaction.
+__global__ void __launch_bounds__(256) k_mix_rows(DevModel M, SysDesc D, int ti, const float4 *__restrict__ posS,
+                                                 const float *__restrict__ box, const int32_t *__restrict__ nbrs,
+                                                 float4 *__restrict__ rows_g, int *__restrict__ rcnt) {
+  const int lane = threadIdx.x & 31;
+  const int wg = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int cnt_i = D.offs[ti + 1] - D.offs[ti];
+  const int nbpf = (cnt_i + kBlkAtoms - 1) / kBlkAtoms;
+  const int blk = wg / D.ntypes, tj = wg - blk * D.ntypes;
+  if (blk >= nbpf * D.F) return;
+  const int f = blk / nbpf, a0 = (blk - f * nbpf) * kBlkAtoms;
+  const int nb = min(kBlkAtoms, cnt_i - a0);
+  const size_t g0 = (size_t)f * D.N + D.offs[ti] + a0;
+  const size_t frame_base = (size_t)f * D.N;
+  const int bs = box_slot(D, g0, f);
+  const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
+  const int3 ni = image_range(L, M.rcut);
+  if (!row_store_covers(D, rows_g, (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1))) return;
+  const float3 inv_l = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
+  const float rk = M.rcut + 1e-3f, rk2 = rk * rk;
+  const int sel = D.sel[tj], cnt_j = D.offs[tj + 1] - D.offs[tj], total = nb * sel;
+  float4 *out = rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj];
+  int n = 0;
+  for (int base = 0; base < total; base += 32) {
+    const int p = base + lane;
+    float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool keep = false;
+    if (p < total) {
+      const int slot = p / sel, k = p - slot * sel;
+      const int idx = nbrs[(g0 + slot) * D.S + D.col[tj] + k] & DPB_NBR_INDEX_MASK;
+      if (idx < cnt_j) {
+        const float4 q = posS[frame_base + D.offs[tj] + idx];
+        const float4 c = posS[g0 + slot];
+        const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+        const float ax = fmaf(-L.x, rintf(dx * inv_l.x), dx), ay = fmaf(-L.y, rintf(dy * inv_l.y), dy),
+                    az = fmaf(-L.z, rintf(dz * inv_l.z), dz);
+        if (ax * ax + ay * ay + az * az < rk2) {
+          keep = true;
+          rv = make_float4(ax, ay, az, __int_as_float((__float_as_int(q.w) << 3) | slot));
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) out[n + __popc(m & ((1u << lane) - 1u))] = rv;
+    n += __popc(m);
+  }
+  if (lane == 0) rcnt[g0 * M.ntypes + tj] = n;
+}
+
+// One round of a row stream: the unread rows of earlier rounds move to the
+// front (as in mix_compact_round), then up to blockDim rows [base, total) of
+// the stored list are appended, one coalesced 16-byte load per thread.
 __device__ __forceinline__ void mix_stream_round(const float4 *__restrict__ src, int base, int total, float4 *rowbuf,
                                                  int &rowstart, int &rowcount) {
   const int tid = threadIdx.x;
@@ -546,8 +606,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
                                                                   const int32_t *__restrict__ nbrs,
                                                                   float *__restrict__ Tout,
                                                                   __half *__restrict__ Gout,
-                                                                  float4 *__restrict__ rows_g,
-                                                                  int *__restrict__ rcnt,
+                                                                  const float4 *__restrict__ rows_g,
+                                                                  const int *__restrict__ rcnt,
                                                                   int *__restrict__ err) {
   using MD = MixDims<E0, E1, E2>;
   using SP = HalfSplit<E0, E1, E2>;
@@ -595,13 +655,16 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
     if (blk + (int)gridDim.x < nblk) {  // the next block's neighbour rows
       const int bn = blk + gridDim.x, fn = bn / nbpf, an = (bn - fn * nbpf) * kBlkAtoms;
       const size_t gn = (size_t)fn * D.N + D.offs[ti] + an;
-      prefetch_range_l2(nbrs + gn * D.S, (size_t)min(kBlkAtoms, cnt_i - an) * D.S * 4);
+      const int nbn = min(kBlkAtoms, cnt_i - an);
+      if (rows_g != nullptr && D.S <= kRowStoreCap) prefetch_range_l2(rows_g + gn * kRowStoreCap, (size_t)nbn * D.S * 16);
+      else prefetch_range_l2(nbrs + gn * D.S, (size_t)nbn * D.S * 4);
     }
     const int bs = box_slot(D, g0, f);  // the block's 8 atoms share one frame
     const float3 L = make_float3(box[bs * 3], box[bs * 3 + 1], box[bs * 3 + 2]);
     const int3 ni = image_range(L, M.rcut);
     const int nim = (2 * ni.x + 1) * (2 * ni.y + 1) * (2 * ni.z + 1);
-    const bool store = rows_g != nullptr && nim == 1 && D.S <= kRowStoreCap;  // keep the rows for the adjoint
+    const bool stream = row_store_covers(D, rows_g, nim);  // the block's rows are in the store
+    if (stream && blk == (int)blockIdx.x) prefetch_range_l2(rows_g + g0 * kRowStoreCap, (size_t)nb * D.S * 16);
     if (tid < nb) {
       const float4 q = posS[g0 + tid];
       ri_s[tid] = make_float3(q.x, q.y, q.z);
@@ -619,14 +682,18 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       const int per_atom = sel * nim, total = nb * per_atom;
       const float *sm = small;
       const int knet = ti * M.ntypes + tj;
-      float4 *rdst = store ? rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj] : nullptr;
-      int tjdone = 0;  // rows of this neighbour type processed so far
-      constexpr int kStep = kFwdThreads * kFwdCpt;
-      for (int base = 0; base < total + kStep && ok; base += kStep) {
-        const bool flush = base >= total;
-        if (!flush)
-          mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS, nbrs,
-                                     rowbuf, wcnt, rowstart, rowcount);
+      const float4 *rsrc = stream ? rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj] : nullptr;
+      const int nsrc = stream ? rcnt[g0 * M.ntypes + tj] : total;  // stored rows, or candidates
+      const int step = stream ? kFwdThreads : kFwdThreads * kFwdCpt;
+      for (int base = 0; base < nsrc + step && ok; base += step) {
+        const bool flush = base >= nsrc;
+        if (!flush) {
+          if (stream)
+            mix_stream_round(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
+          else
+            mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS,
+                                       nbrs, rowbuf, wcnt, rowstart, rowcount);
+        }
         while (rowcount - rowstart >= 128 || (flush && rowcount > rowstart)) {
           const int nrows = min(rowcount - rowstart, 128);
           if (pending) {  // previous contraction done: operands free, clear its Rblk entries
@@ -647,7 +714,6 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           const bool act = row < nrows;
           const float4 rv = act ? rowbuf[rowstart + row] : make_float4(100.f, 100.f, 100.f, 0.f);
           const int slot = act ? (__float_as_int(rv.w) & 7) : -1;
-          if (store && half == 0 && act) rdst[tjdone + row] = rv;
           RowGeom gm;
           float st, R[10];
           mix_row_env(rv, M.rcut, inv_std, mean, gm, st, R);
@@ -710,10 +776,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
           pending = true;
           ++ntile;
           rowstart += nrows;
-          tjdone += nrows;
         }
       }
-      if (store && tid == 0 && ok) rcnt[g0 * M.ntypes + tj] = tjdone;
     }
     if (!ok) break;
     if (pending) {
@@ -842,8 +906,8 @@ static int num_sms() {
 
 template <int E0, int E1, int E2>
 int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const float4 *posS,
-                         const float *box, const int32_t *nbrs, float *T, __half *G, float4 *rows_g,
-                         int *rcnt, int *err, cudaStream_t st) {
+                         const float *box, const int32_t *nbrs, float *T, __half *G, const float4 *rows_g,
+                         const int *rcnt, int *err, cudaStream_t st) {
   const int cnt = D.offs[ti + 1] - D.offs[ti];
   if (cnt == 0) return DPB_OK;
   const int nblk = (cnt + kBlkAtoms - 1) / kBlkAtoms * D.F;
@@ -1946,13 +2010,21 @@ static int launch_pos_sorted(const SysDesc &D, const float *pos, const int32_t *
   return DPB_OK;
 }
 
-// rows / rcnt (may be null): where the forward keeps its compacted rows for
-// the adjoint.
+// rows / rcnt (may be null): the row store, built here by k_mix_rows and
+// streamed by the forward and the adjoint embedding kernels.
 int mixed_descriptors(const DevModel &M, const SysDesc &D, const float4 *posS, const float *box,
                       const int32_t *nbrs, float *T, __half *Gb, float4 *rows, int *rcnt, int *err,
                       cudaStream_t st) {
   if (M.ngrids > 0 || !M.emb_tuned) return DPB_ERR_UNSUPPORTED;  // the FP32 kernels give T and G
   prof_begin(PROF_MIXED_EMBED_FWD, st);
+  for (int ti = 0; ti < M.ntypes && rows; ++ti) {
+    const int cnt = D.offs[ti + 1] - D.offs[ti];
+    const size_t warps = (size_t)(cnt + kBlkAtoms - 1) / kBlkAtoms * D.F * D.ntypes;
+    if (!cnt) continue;
+    k_mix_rows<<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(M, D, ti, posS, box, nbrs, rows, rcnt);
+    count_launch();
+    DPB_LAUNCH_CHECK();
+  }
   for (int ti = 0; ti < M.ntypes; ++ti) {
     int rc = (M.E2 == 100)
                  ? launch_mix_embed_fwd<25, 50, 100>(M, D, ti, posS, box, nbrs, T, Gb, rows, rcnt, err, st)
