@@ -333,12 +333,17 @@ __device__ __forceinline__ bool row_store_covers(const SysDesc &D, const float4 
   return rows_g != nullptr && nim == 1 && D.S <= kRowStoreCap;
 }
 
-// One warp per (block of 8 centre atoms of type ti, neighbour type tj): 32
-// candidates (atom slot, list slot) per round in candidate order, the
-// neighbour's position gathered from posS, the nearest-image displacement and
-// keep test of mix_compact_round (same arithmetic, so the same rows), kept
-// rows appended with a ballot.  Blocks outside the store (several images) are
-// left to the embedding kernels' own compaction.
+// One warp per (block of 8 centre atoms of type ti, neighbour type tj),
+// kRowsCpt rounds of 32 candidates (atom slot, list slot) at a time in
+// candidate order: all of their list entries are loaded, then all of their
+// neighbour positions gathered from posS, before any is used (the chain is
+// two dependent loads per round); the nearest-image displacement and keep
+// test are those of mix_compact_round (same arithmetic, so the same rows),
+// and the kept rows are appended round by round with a ballot.  Blocks
+// outside the store (several images) are left to the embedding kernels' own
+// compaction.
+constexpr int kRowsCpt = 4;
+
 __global__ void __launch_bounds__(256) k_mix_rows(DevModel M, SysDesc D, int ti, const float4 *__restrict__ posS,
                                                  const float *__restrict__ box, const int32_t *__restrict__ nbrs,
                                                  float4 *__restrict__ rows_g, int *__restrict__ rcnt) {
@@ -359,37 +364,52 @@ __global__ void __launch_bounds__(256) k_mix_rows(DevModel M, SysDesc D, int ti,
   const float3 inv_l = make_float3(1.f / L.x, 1.f / L.y, 1.f / L.z);
   const float rk = M.rcut + 1e-3f, rk2 = rk * rk;
   const int sel = D.sel[tj], cnt_j = D.offs[tj + 1] - D.offs[tj], total = nb * sel;
-  float4 *out = rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj];
+  const int col = D.col[tj], jbase = D.offs[tj];
+  // the block's centre positions, one per lane
+  const float4 cl = lane < nb ? posS[g0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 *out = rows_g + g0 * kRowStoreCap + (size_t)nb * col;
   int n = 0;
-  for (int base = 0; base < total; base += 32) {
-    const int p = base + lane;
-    float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
-    bool keep = false;
-    if (p < total) {
-      const int slot = p / sel, k = p - slot * sel;
-      const int idx = nbrs[(g0 + slot) * D.S + D.col[tj] + k] & DPB_NBR_INDEX_MASK;
-      if (idx < cnt_j) {
-        const float4 q = posS[frame_base + D.offs[tj] + idx];
-        const float4 c = posS[g0 + slot];
-        const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+  for (int base = 0; base < total; base += 32 * kRowsCpt) {
+    int idx[kRowsCpt], slot[kRowsCpt];
+#pragma unroll
+    for (int k = 0; k < kRowsCpt; ++k) {
+      const int p = base + 32 * k + lane;
+      slot[k] = p / sel;
+      idx[k] = p < total ? nbrs[(g0 + slot[k]) * D.S + col + (p - slot[k] * sel)] & DPB_NBR_INDEX_MASK : cnt_j;
+    }
+    float4 q[kRowsCpt];
+#pragma unroll
+    for (int k = 0; k < kRowsCpt; ++k)
+      q[k] = idx[k] < cnt_j ? posS[frame_base + jbase + idx[k]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < kRowsCpt; ++k) {
+      const int sl = min(slot[k], kBlkAtoms - 1);
+      const float cx = __shfl_sync(0xffffffffu, cl.x, sl), cy = __shfl_sync(0xffffffffu, cl.y, sl),
+                  cz = __shfl_sync(0xffffffffu, cl.z, sl);
+      float4 rv = make_float4(0.f, 0.f, 0.f, 0.f);
+      bool keep = false;
+      if (idx[k] < cnt_j) {
+        const float dx = q[k].x - cx, dy = q[k].y - cy, dz = q[k].z - cz;
         const float ax = fmaf(-L.x, rintf(dx * inv_l.x), dx), ay = fmaf(-L.y, rintf(dy * inv_l.y), dy),
                     az = fmaf(-L.z, rintf(dz * inv_l.z), dz);
         if (ax * ax + ay * ay + az * az < rk2) {
           keep = true;
-          rv = make_float4(ax, ay, az, __int_as_float((__float_as_int(q.w) << 3) | slot));
+          rv = make_float4(ax, ay, az, __int_as_float((__float_as_int(q[k].w) << 3) | slot[k]));
         }
       }
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) out[n + __popc(m & ((1u << lane) - 1u))] = rv;
+      n += __popc(m);
     }
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (keep) out[n + __popc(m & ((1u << lane) - 1u))] = rv;
-    n += __popc(m);
   }
   if (lane == 0) rcnt[g0 * M.ntypes + tj] = n;
 }
 
 // One round of a row stream: the unread rows of earlier rounds move to the
-// front (as in mix_compact_round), then up to blockDim rows [base, total) of
-// the stored list are appended, one coalesced 16-byte load per thread.
+// front (as in mix_compact_round), then up to RPT * blockDim rows [base,
+// total) of the stored list are appended, RPT coalesced 16-byte loads per
+// thread issued before any store.
+template <int RPT>
 __device__ __forceinline__ void mix_stream_round(const float4 *__restrict__ src, int base, int total, float4 *rowbuf,
                                                  int &rowstart, int &rowcount) {
   const int tid = threadIdx.x;
@@ -402,8 +422,18 @@ __device__ __forceinline__ void mix_stream_round(const float4 *__restrict__ src,
     rowstart = 0;
     rowcount = rem;
   }
-  const int n = min((int)blockDim.x, total - base);
-  if (tid < n) rowbuf[rowcount + tid] = src[base + tid];
+  const int n = min(RPT * (int)blockDim.x, total - base);
+  float4 v[RPT];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * (int)blockDim.x;
+    if (i < n) v[k] = src[base + i];
+  }
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int i = tid + k * (int)blockDim.x;
+    if (i < n) rowbuf[rowcount + i] = v[k];
+  }
   rowcount += n;
   __syncthreads();
 }
@@ -684,12 +714,12 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_mix_embed_fwd(DevModel M, Sy
       const int knet = ti * M.ntypes + tj;
       const float4 *rsrc = stream ? rows_g + g0 * kRowStoreCap + (size_t)nb * D.col[tj] : nullptr;
       const int nsrc = stream ? rcnt[g0 * M.ntypes + tj] : total;  // stored rows, or candidates
-      const int step = stream ? kFwdThreads : kFwdThreads * kFwdCpt;
+      constexpr int step = kFwdThreads * kFwdCpt;  // candidates, or stored rows, per round
       for (int base = 0; base < nsrc + step && ok; base += step) {
         const bool flush = base >= nsrc;
         if (!flush) {
           if (stream)
-            mix_stream_round(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
+            mix_stream_round<kFwdCpt>(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
           else
             mix_compact_round<kFwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS,
                                        nbrs, rowbuf, wcnt, rowstart, rowcount);
@@ -1256,7 +1286,7 @@ __global__ void __launch_bounds__(kBwdThreads, 2) k_mix_embed_bwd(DevModel M, Sy
         const bool flush = base >= nsrc;
         if (!flush) {
           if (stream)
-            mix_stream_round(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
+            mix_stream_round<kBwdCpt>(rsrc, base, nsrc, rowbuf, rowstart, rowcount);
           else
             mix_compact_round<kBwdCpt>(D, M, tj, base, total, per_atom, nim, ni, L, g0, frame_base, ri_s, posS,
                                        nbrs, rowbuf, wcnt, rowstart, rowcount);
