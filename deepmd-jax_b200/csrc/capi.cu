@@ -81,7 +81,7 @@ size_t mixed_workspace_per_atom(const DevModel &M);
 size_t mixed_workspace_fixed(const DevModel &M);
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
-               cudaStream_t st, int dT_warps);
+               cudaStream_t st, int dT_warps, bool fit_deep);
 int mixed_descriptors_f32(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                           const float *box, const int32_t *nbrs, float *T, float *G, int *err, void *ws,
                           cudaStream_t st);
@@ -552,7 +552,7 @@ int dpb::eval_impl(const dpb_model *m, int precision, const float *pos, const in
     rc = eval_fp32(M, D, pos, perm, box, nbrs, energy, F4, Eatom, vir, w, st);
   } else {
     if (!mixed_supported(M)) return DPB_ERR_UNSUPPORTED;
-    rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st, m->dT_warps);
+    rc = mixed_eval(M, D, pos, perm, box, nbrs, energy, Eatom, F4, vir, w, st, m->dT_warps, m->fit_deep != 0);
   }
   if (rc) return rc;
   return launch_finalize((int)NF, natoms, F4, force, Eatom, perm, atom_energy, energy, (int)nE, pos, seg, status,

@@ -8,8 +8,11 @@ struct dpb_model {
   std::vector<void *> allocs;
   int device;
   // launch shapes chosen by dpb_md_autotune (they never change results):
-  // atoms (warps) per block of the mixed dE/dT kernel
+  // atoms (warps) per block of the mixed dE/dT kernel, and the mixed fitting
+  // kernel's deep weight ring (1 CTA per SM) instead of the shallow one (2
+  // CTAs per SM)
   mutable int dT_warps = 4;
+  mutable int fit_deep = 0;
 };
 
 namespace dpb {

@@ -1519,7 +1519,7 @@ extern "C" int dpb_md_eval_model(dpb_md *m, const dpb_model *model, double *ener
 // (a warm-up, then timed repetitions with CUDA events on the stream) and the
 // fastest is kept; shapes never change results.  Ends with the list and
 // forces of the current positions, like dpb_md_init.
-extern "C" int dpb_md_autotune(dpb_md *m, int *nl_warps, int *dT_warps, void *stream) {
+extern "C" int dpb_md_autotune(dpb_md *m, int *nl_warps, int *dT_warps, int *fit_stages, void *stream) {
   if (!m) return DPB_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   cudaEvent_t a, b;
@@ -1551,6 +1551,25 @@ extern "C" int dpb_md_autotune(dpb_md *m, int *nl_warps, int *dT_warps, void *st
       if (!r) m->model->dT_warps = bestT;
     }
   }
+  // mixed form: the fitting kernel's shallow (2 CTAs per SM) or deep (1 CTA
+  // per SM) weight ring, timed over whole evaluations of the current state
+  if (!rc && m->d.precision == DPB_PREC_MIXED) {
+    int bestd = m->model->fit_deep;
+    tbest = 1e30f;
+    for (int deep = 0; deep < 2 && !rc; ++deep) {
+      m->model->fit_deep = deep;
+      int r = md_forces(m, st);  // warm-up
+      cudaEventRecord(a, st);
+      for (int k = 0; k < 3 && !r; ++k) r = md_forces(m, st);
+      cudaEventRecord(b, st);
+      if (!r && cudaEventSynchronize(b) != cudaSuccess) r = DPB_ERR_CUDA;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (r) rc = r;
+      else if (ms < tbest) { tbest = ms; bestd = deep; }
+    }
+    m->model->fit_deep = bestd;
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (!rc) rc = md_build_list(m, nullptr, st);
@@ -1558,6 +1577,7 @@ extern "C" int dpb_md_autotune(dpb_md *m, int *nl_warps, int *dT_warps, void *st
   if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = DPB_ERR_CUDA;
   if (nl_warps) *nl_warps = m->nl_warps;
   if (dT_warps) *dT_warps = m->model->dT_warps;
+  if (fit_stages) *fit_stages = m->d.precision == DPB_PREC_MIXED ? (m->model->fit_deep ? 12 : 4) : 0;
   return rc;
 }
 

@@ -1536,13 +1536,17 @@ constexpr int kFitThreads = 192;
 constexpr int kFitDgN = 128;                 // N of one dE/dG pass
 constexpr int kFitStageA = 2 * 128 * 16;     // A chunk bytes (K = 16)
 
-template <int FW>
+// Ring depth: the shallow ring fits two CTAs per SM (one CTA's epilogue
+// overlaps the other's MMAs); the deep ring keeps 12 stages of weights in
+// flight for one CTA per SM.  dpb_md_autotune times both.
+template <int FW, bool DEEP>
 struct FitCfg {
   static constexpr int BR = FW > kFitDgN ? FW : kFitDgN;  // rows of the largest B box
   static constexpr int STAGE = kFitStageA + 2 * BR * 16;
-  static constexpr int ST = FW > 128 ? 4 : 8;              // ring depth (2 CTAs per SM)
+  static constexpr int ST = DEEP ? 12 : (FW > 128 ? 4 : 8);
   static constexpr int HAB = 128 * FW * 2;
   static constexpr size_t SMEM = (size_t)round1k(HAB) + (size_t)ST * STAGE;
+  static_assert(SMEM <= 220 * 1024, "fitting ring");
 };
 
 // Bounded mbarrier wait that also gives up once another role of the CTA gave
@@ -1588,7 +1592,7 @@ __device__ __forceinline__ FitGemm fit_gemm_info(const DevModel &M, int ti, int 
   return G;
 }
 
-template <int FW, typename DGT>
+template <int FW, typename DGT, bool DEEP>
 __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
                                                            int Mrows, RowMap rm,
                                                            const __half *__restrict__ Gh,
@@ -1596,7 +1600,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
                                                            float *__restrict__ Eatom, double *__restrict__ energy,
                                                            int N, int *__restrict__ err,
                                                            const int32_t *__restrict__ seg, int tile0) {
-  using C = FitCfg<FW>;
+  using C = FitCfg<FW, DEEP>;
   constexpr int ST = C::ST;
   static_assert(FW % 16 == 0 && FW <= 256, "fit width");
   extern __shared__ __align__(1024) char smem[];
@@ -1925,12 +1929,13 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   if (warp == 0) tc::tmem_dealloc(td, 256);
 }
 
-template <int FW, typename DGT>
+template <int FW, typename DGT, bool DEEP>
 int launch_mix_fit(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *dG, float *scratch,
                    float *Eatom, double *energy, int *err, cudaStream_t st) {
-  using C = FitCfg<FW>;
+  using C = FitCfg<FW, DEEP>;
   if (!M.fit_bt[0][kFitBtDg]) return DPB_ERR_UNSUPPORTED;
-  DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_fit<FW, DGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  DPB_CUDA_TRY(
+      cudaFuncSetAttribute(k_mix_fit<FW, DGT, DEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
   int tile0 = 0;  // scratch tiles of 128 rows, consecutive over the centre types
   for (int ti = 0; ti < M.ntypes; ++ti) {
     const int cnt = D.offs[ti + 1] - D.offs[ti];
@@ -1938,7 +1943,7 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *d
     const RowMap rm{cnt, D.N, D.offs[ti]};
     const int Mrows = cnt * D.F;
     const int ntile = (Mrows + 127) / 128;
-    k_mix_fit<FW, DGT><<<ntile, kFitThreads, C::SMEM, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
+    k_mix_fit<FW, DGT, DEEP><<<ntile, kFitThreads, C::SMEM, st>>>(M, ti, Mrows, rm, Gb, dG, scratch, Eatom, energy, D.N, err,
                                                         D.seg, tile0);
     tile0 += ntile;
     count_launch();
@@ -1947,16 +1952,23 @@ int launch_mix_fit(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *d
   return DPB_OK;
 }
 
-// The instantiation of the model's padded hidden width.
+// The instantiation of the model's padded hidden width and ring depth.
+template <int FW, typename DGT>
+static int launch_mix_fit_d(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *dG, float *scratch,
+                            float *Eatom, double *energy, int *err, bool deep, cudaStream_t st) {
+  return deep ? launch_mix_fit<FW, DGT, true>(M, D, Gb, dG, scratch, Eatom, energy, err, st)
+              : launch_mix_fit<FW, DGT, false>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+}
+
 template <typename DGT>
 int launch_mix_fit_any(const DevModel &M, const SysDesc &D, const __half *Gb, DGT *dG, float *scratch,
-                       float *Eatom, double *energy, int *err, cudaStream_t st) {
+                       float *Eatom, double *energy, int *err, bool deep, cudaStream_t st) {
   switch (M.mfw) {
-    case 64: return launch_mix_fit<64, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
-    case 128: return launch_mix_fit<128, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
-    case 208: return launch_mix_fit<208, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
-    case 240: return launch_mix_fit<240, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
-    case 256: return launch_mix_fit<256, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+    case 64: return launch_mix_fit_d<64, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, deep, st);
+    case 128: return launch_mix_fit_d<128, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, deep, st);
+    case 208: return launch_mix_fit_d<208, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, deep, st);
+    case 240: return launch_mix_fit_d<240, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, deep, st);
+    case 256: return launch_mix_fit_d<256, DGT>(M, D, Gb, dG, scratch, Eatom, energy, err, deep, st);
     default: return DPB_ERR_UNSUPPORTED;
   }
 }
@@ -2099,7 +2111,7 @@ int launch_embed_bwd_gen(const DevModel &, const SysDesc &, int, const float *, 
 static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm,
                                  const float *box, const int32_t *nbrs, double *energy, float *Eatom, float4 *F4,
                                  double *virial, float *T, __half *Gb, float *dG, float *scratch, int *err,
-                                 cudaStream_t st) {
+                                 bool fit_deep, cudaStream_t st) {
   const size_t NF = (size_t)D.N * D.F;
   const size_t NG = NF * M.A * M.E2;  // a multiple of 16 (mixed_supported)
   int rc;
@@ -2116,7 +2128,7 @@ static int mixed_eval_compressed(const DevModel &M, const SysDesc &D, const floa
   DPB_LAUNCH_CHECK();
   prof_end(PROF_EMBED_FWD, st);
   prof_begin(PROF_MIXED_FIT, st);
-  rc = launch_mix_fit_any<float>(M, D, Gb, dG, scratch, Eatom, energy, err, st);
+  rc = launch_mix_fit_any<float>(M, D, Gb, dG, scratch, Eatom, energy, err, fit_deep, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_EMBED_BWD, st);
@@ -2207,7 +2219,7 @@ int mixed_tune_dT(const DevModel &M, size_t NF, void *ws, cudaStream_t st, int *
 
 int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int32_t *perm, const float *box,
                const int32_t *nbrs, double *energy, float *Eatom, float4 *F4, double *virial, void *ws,
-               cudaStream_t st, int dT_warps) {
+               cudaStream_t st, int dT_warps, bool fit_deep) {
   const size_t NF = (size_t)D.N * D.F;
   const MixedWs mw = mixed_ws(M, NF, ws);
   int *err = mw.err;
@@ -2216,14 +2228,15 @@ int mixed_eval(const DevModel &M, const SysDesc &D, const float *pos, const int3
   float4 *posS = mw.posS;
   DPB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
   if (M.ngrids > 0 || !M.emb_tuned)
-    return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err, st);
+    return mixed_eval_compressed(M, D, pos, perm, box, nbrs, energy, Eatom, F4, virial, T, Gb, dG, scratch, err,
+                                 fit_deep, st);
   int rc = launch_pos_sorted(D, pos, perm, posS, st);
   if (rc) return rc;
   rc = mixed_descriptors(M, D, posS, box, nbrs, T, Gb, mw.rows, mw.rcnt, err, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_FIT, st);
   __half *dGb = reinterpret_cast<__half *>(dG);  // dE/dG in FP16 times fit_dgsc (the dE/dT input)
-  rc = launch_mix_fit_any<__half>(M, D, Gb, dGb, scratch, Eatom, energy, err, st);
+  rc = launch_mix_fit_any<__half>(M, D, Gb, dGb, scratch, Eatom, energy, err, fit_deep, st);
   prof_end(PROF_MIXED_FIT, st);
   if (rc) return rc;
   prof_begin(PROF_MIXED_DT, st);

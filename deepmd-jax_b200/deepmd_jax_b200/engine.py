@@ -316,10 +316,21 @@ def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energ
     Np, S = batch.natoms, int(sum(sel))
     nbrs = torch.full((Np, S), Np, dtype=torch.int32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    for it in batch.items:
+    # every host array of the batch (the items' type orders, the packed order,
+    # the segments, the boxes as float bits) in one pinned buffer and one
+    # asynchronous copy, so the host does not wait on the stream per item
+    parts = [it["perm"].astype(np.int32) for it in batch.items] + [batch.perm, batch.seg,
+                                                                    batch.boxes.reshape(-1).view(np.int32)]
+    offs = np.concatenate([[0], np.cumsum([len(x) for x in parts])])
+    host = torch.empty(int(offs[-1]), dtype=torch.int32, pin_memory=True)
+    hv = host.numpy()
+    for x, o in zip(parts, offs[:-1]):
+        hv[o:o + len(x)] = x
+    dbuf = host.to(dev, non_blocking=True)
+    views = [dbuf[offs[i]:offs[i + 1]] for i in range(len(parts))]
+    for it, perm in zip(batch.items, views):
         N, nf = it["natoms"], it["nframes"]
         pos = slot_pos[it["slot0"]:it["slot0"] + nf * N].view(nf, N, 3)
-        perm = torch.tensor(it["perm"].astype(np.int32), device=dev)
         nb, _ = NeighborBuilder(N, nf, it["type_count"], sel, it["box"], rcut).build(pos, perm=perm, status=status)
         _lib.check(lib.dpb_nlist_pack(_ptr(nb), N, nf, batch.ntypes, _lib.int_array(it["type_count"]),
                                       _lib.int_array(sel), _lib.int_array(it["row0"]), _lib.int_array(it["base0"]),
@@ -328,9 +339,8 @@ def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energ
     _lib.check(lib.dpb_eval_packed_workspace_bytes(dm.handle, Np, batch.nseg, ctypes.byref(n)),
                "dpb_eval_packed_workspace_bytes")
     ws = torch.empty(n.value, dtype=torch.uint8, device=dev)
-    perm = torch.tensor(batch.perm, device=dev)
-    seg = torch.tensor(batch.seg, device=dev)
-    box = torch.tensor(batch.boxes, device=dev)
+    perm, seg = views[-3], views[-2]
+    box = views[-1].view(torch.float32)
     out = dict(energy=torch.empty(batch.nseg, dtype=torch.float64, device=dev),
                force=torch.empty((Np, 3), dtype=torch.float32, device=dev),
                virial=torch.empty((batch.nseg, 9), dtype=torch.float64, device=dev),

@@ -76,7 +76,8 @@ def _declare(lib):
     lib.dpb_md_set_capacity.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp]
     lib.dpb_md_set_skin.argtypes = [vp, ctypes.c_double, vp]
     lib.dpb_md_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
-    lib.dpb_md_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp]
+    lib.dpb_md_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int), vp]
     lib.dpb_md_box_history.argtypes = [vp, ctypes.c_int, d64]
     lib.dpb_md_eval_model.argtypes = [vp, vp, d64, d64]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
@@ -310,10 +311,11 @@ class Simulation:
         # atom-beads or more, where its few timed launches are negligible)
         self.launch_shapes = None
         if autotune if autotune is not None else self._natoms * self._n_bead >= 10000:
-            nlw, dtw = ctypes.c_int(), ctypes.c_int()
-            _lib.check(self.lib.dpb_md_autotune(self._h, ctypes.byref(nlw), ctypes.byref(dtw), _stream()),
-                       "dpb_md_autotune")
-            self.launch_shapes = {"nlist_warps_per_block": nlw.value, "dT_atoms_per_block": dtw.value}
+            nlw, dtw, fst = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            _lib.check(self.lib.dpb_md_autotune(self._h, ctypes.byref(nlw), ctypes.byref(dtw), ctypes.byref(fst),
+                                                _stream()), "dpb_md_autotune")
+            self.launch_shapes = {"nlist_warps_per_block": nlw.value, "dT_atoms_per_block": dtw.value,
+                                  "fit_ring_stages": fst.value}
         self._is_initial_state = True
         self._error_code = 0
         if verbose:

@@ -324,13 +324,16 @@ DPB_API int dpb_md_set_capacity(dpb_md *md, const int *sel, void *stream);
 DPB_API int dpb_md_device_pointers(dpb_md *md, dpb_md_pointers_t *ptrs);
 /* Launch-shape autotuner (no counterpart in the reference, which leaves
  * launch shapes to XLA): times the neighbour search at 4 / 8 / 16 centres
- * per block and, for the mixed form, dE/dT at 2 / 4 / 8 atoms per block on
- * this engine's current state and keeps the fastest (*nl_warps, *dT_warps
- * report the choice; the dE/dT choice is stored on the model).  Results do
- * not depend on the shapes.  Call after dpb_md_init and before capturing
- * dpb_md_run into a graph; ends with the list and forces of the current
- * positions. */
-DPB_API int dpb_md_autotune(dpb_md *md, int *nl_warps, int *dT_warps, void *stream);
+ * per block and, for the mixed form, dE/dT at 2 / 4 / 8 atoms per block and
+ * the tensor-core fitting kernel with its shallow weight ring (4 stages, 2
+ * CTAs per SM) and its deep one (12 stages, 1 CTA per SM, timed over whole
+ * evaluations) on this engine's current state, and keeps the fastest
+ * (*nl_warps, *dT_warps and *fit_stages report the choice; *fit_stages is 0
+ * for the FP32 form; the dE/dT and ring choices are stored on the model).
+ * Results do not depend on the shapes.  Call after dpb_md_init and before
+ * capturing dpb_md_run into a graph; ends with the list and forces of the
+ * current positions. */
+DPB_API int dpb_md_autotune(dpb_md *md, int *nl_warps, int *dT_warps, int *fit_stages, void *stream);
 /* Box (3 per step, Angstrom) after each of the first nsteps (<= 1024) steps
  * of the last dpb_md_run call: the per-step box of the reference's scan
  * output (deepmd_jax/md.py:784-803, 938); constant except under NPT. */

@@ -284,6 +284,7 @@ def test_autotuned_launch_shapes_leave_results_unchanged():
         if tune:
             assert sim.launch_shapes["nlist_warps_per_block"] in (4, 8, 16)
             assert sim.launch_shapes["dT_atoms_per_block"] in (2, 4, 8)
+            assert sim.launch_shapes["fit_ring_stages"] in (4, 12)
         else:
             assert sim.launch_shapes is None
         F0 = sim.getForce()
