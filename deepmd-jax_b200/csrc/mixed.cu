@@ -1731,12 +1731,20 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
     // residual adjoint
     float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + row;
 #define FIT_SCR(slot, n) tile[((size_t)(slot) * FW + (n)) * 128]
+    // L2 prefetch of one scratch slot of this warp's 32 rows (one 128-byte
+    // line per column), issued before a layer's accumulator wait so that it
+    // overlaps the layer's MMAs instead of stalling the epilogue's reads
+    const float *tile_w = tile - (row & 31);
+    auto prefetch_slot = [&](int slot) {
+      for (int n = row & 31; n < FW; n += 32) tc::prefetch_l2(tile_w + ((size_t)slot * FW + n) * 128);
+    };
     // ---- forward; the last layer's epilogue also forms the atom energy and
     // the first adjoint gate g = w_out dt (1 - t^2), the A operand of adjoint
     // layer L-1 (its t and h never go to the scratch)
     const float *wf = M.mfwout[ti];
     float e_sum = 0.f;
     for (int l = 0; l < L && ok; ++l) {
+      if (M.mfdt[ti][l]) prefetch_slot(L + l - 1);
       ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
       ++accf_n;
       if (!ok) break;
@@ -1813,6 +1821,8 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
     }
     // ---- adjoint: layers L-1 .. 1, gH_{l-1} = gZ_l W_l^T (+ gH_l if residual)
     for (int l = L - 1; l >= 1 && ok; --l) {
+      if (M.mfdt[ti][l] != nullptr && l != L - 1) prefetch_slot(2 * L);
+      prefetch_slot(l - 1);
       ok = __all_sync(0xffffffffu, fit_wait(&accf, accf_n & 1, abort));
       ++accf_n;
       if (!ok) break;

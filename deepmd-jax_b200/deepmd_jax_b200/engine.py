@@ -305,12 +305,15 @@ class PackedBatch:
         self.boxes = np.asarray(boxes, np.float32).reshape(-1, 3)
 
 
-def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energy=False):
+def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energy=False, host_stage=None):
     """One packed evaluation of every frame of ``batch`` (a PackedBatch).
 
     slot_pos: (batch.natoms, 3) float32 CUDA, the frames' positions at their
-    slots (padding slots any finite value).  Returns energy (nseg,) f64,
-    force (natoms, 3) f32 at the slots, virial (nseg, 9) f64, status."""
+    slots (padding slots any finite value).  host_stage: optional pinned
+    int32 host tensor that stages the batch's index arrays (the caller keeps
+    it untouched until this batch completes); without it one is allocated.
+    Returns energy (nseg,) f64, force (natoms, 3) f32 at the slots, virial
+    (nseg, 9) f64, status."""
     lib = dm.lib
     dev = slot_pos.device
     Np, S = batch.natoms, int(sum(sel))
@@ -322,7 +325,10 @@ def evaluate_packed(dm, batch, slot_pos, sel, rcut, precision="fp32", atom_energ
     parts = [it["perm"].astype(np.int32) for it in batch.items] + [batch.perm, batch.seg,
                                                                     batch.boxes.reshape(-1).view(np.int32)]
     offs = np.concatenate([[0], np.cumsum([len(x) for x in parts])])
-    host = torch.empty(int(offs[-1]), dtype=torch.int32, pin_memory=True)
+    if host_stage is not None and host_stage.numel() >= int(offs[-1]):
+        host = host_stage[:int(offs[-1])]
+    else:
+        host = torch.empty(int(offs[-1]), dtype=torch.int32, pin_memory=True)
     hv = host.numpy()
     for x, o in zip(parts, offs[:-1]):
         hv[o:o + len(x)] = x

@@ -13,11 +13,13 @@ Here a ``Server`` owns one device model and three worker threads:
   batch: a neighbour list per request (dpb_nlist_build) remapped into the
   packed index space (dpb_nlist_pack), then one dpb_eval_packed launch
   sequence over all frames; requests that arrive while a batch is on the GPU
-  form the next batch;
+  form the next batch, which the host packs while the current one runs;
 * the MD worker steps every admitted MD-continuation request chunk by chunk
   (CUDA-graph replays of the device-resident engine; positions, velocities
   and thermostat state stay on the device) in round-robin, on its own CUDA
-  stream, so MD chunks and evaluation batches overlap on the device.
+  stream, so MD chunks and evaluation batches overlap on the device.  The
+  continuations run with the library's default launch shapes: timing
+  candidate shapes would cost more than a short continuation gains.
 
 A request's bytes are released when it completes.  Latency is measured from
 ``submit_*`` to the result being ready on the host.
@@ -109,6 +111,14 @@ class Server:
         self._stop = False
         self._device = torch.cuda.current_device()
         self._eval_stream = torch.cuda.Stream()
+        # pinned host staging of the evaluation batches, two of each (the batch
+        # on the GPU keeps its own), allocated once: positions and the packed
+        # index arrays of up to max_batch_atoms atom-frames
+        self._pin = [torch.empty((self.max_batch_atoms + (1 << 16), 3), dtype=torch.float32, pin_memory=True)
+                     for _ in range(2)]
+        self._pin_idx = [torch.empty(3 * self.max_batch_atoms + (1 << 16), dtype=torch.int32, pin_memory=True)
+                         for _ in range(2)]
+        self._pin_k = 0
         self._md_stream = torch.cuda.Stream()
         self.completed = []
         self.batches = 0
@@ -220,11 +230,13 @@ class Server:
         else:
             req.future.set_result(result)
 
-    def _take_eval_batch(self):
+    def _take_eval_batch(self, wait=True):
+        """The admitted evaluate() requests waiting now, up to max_batch_atoms
+        atom-frames; with ``wait`` block until there is one (None: stopped)."""
         with self._lock:
-            while not self._stop and not self._eval_ready:
+            while wait and not self._stop and not self._eval_ready:
                 self._lock.wait(0.05)
-            if self._stop and not self._eval_ready:
+            if not self._eval_ready:
                 return None
             batch, atoms = [], 0
             while self._eval_ready and (not batch or atoms + self._eval_ready[0].atoms * self._eval_ready[0].frames
@@ -235,20 +247,41 @@ class Server:
             return batch
 
     def _eval_loop(self):
+        """One batch on the GPU while the host packs the next: launch batch k,
+        pack batch k + 1, then wait for batch k and hand out its results."""
         torch.cuda.set_device(self._device)
         with torch.cuda.stream(self._eval_stream):
+            inflight = None
             while True:
-                reqs = self._take_eval_batch()
-                if reqs is None:
-                    return
-                try:
-                    self._run_eval_batch(reqs)
-                except Exception as ex:  # report to every caller of the batch
-                    for r in reqs:
-                        if not r.future.done():
-                            self._finish(r, exc=ex)
+                reqs = self._take_eval_batch(wait=inflight is None)
+                prep = None
+                if reqs:
+                    try:
+                        prep = self._pack_eval_batch(reqs)
+                    except Exception as ex:
+                        self._fail(reqs, ex)
+                if inflight is not None:
+                    self._complete_eval_batch(inflight)
+                    inflight = None
+                if prep is not None:
+                    try:
+                        inflight = self._launch_eval_batch(prep)
+                    except Exception as ex:
+                        self._fail(prep["reqs"], ex)
+                elif reqs is None and self._stop:
+                    with self._lock:
+                        if not self._eval_ready:
+                            return
 
-    def _run_eval_batch(self, reqs):
+    def _fail(self, reqs, ex):
+        for r in reqs:
+            if not r.future.done():
+                self._finish(r, exc=ex)
+
+    def _pack_eval_batch(self, reqs):
+        """Host side of a batch: the packed layout and the positions at their
+        slots in one of two pinned staging buffers (alternating, so the batch
+        on the GPU keeps its own)."""
         t0 = time.perf_counter()
         items, groups = [], []
         for r in reqs:
@@ -262,22 +295,44 @@ class Server:
                     groups.append((r, start, f))
                     start = f
         batch = PackedBatch(items, self.ntypes)
-        slots = np.zeros((batch.natoms, 3), dtype=np.float32)
+        self._pin_k ^= 1
+        pin = self._pin[self._pin_k]
+        if pin.shape[0] < batch.natoms:  # one request beyond max_batch_atoms
+            pin = torch.empty((batch.natoms, 3), dtype=torch.float32, pin_memory=True)
+            self._pin[self._pin_k] = pin
+        slots = pin[:batch.natoms].numpy()
+        slots[:] = 0.0
         for it, (r, a, b) in zip(batch.items, groups):
             n = it["natoms"] * it["nframes"]
             slots[it["slot0"]:it["slot0"] + n] = r.payload[0][a:b].reshape(-1, 3)
-        pos = torch.from_numpy(slots).pin_memory().to("cuda", non_blocking=True)
-        sel = list(self.sel)
-        while True:
-            out = evaluate_packed(self.dm, batch, pos, sel, self.rcut, self.precision)
-            st = int(out["status"].item())
-            if not st & 2:
-                break
-            sel = [2 * s for s in sel]          # neighbour overflow: grow and re-run the batch
-            self.sel = [max(a, b) for a, b in zip(self.sel, sel)]
-        energy = out["energy"].cpu().numpy()
-        force = out["force"].cpu().numpy()
-        virial = out["virial"].cpu().numpy().reshape(-1, 3, 3)
+        return {"reqs": reqs, "batch": batch, "groups": groups, "pin": pin, "pin_idx": self._pin_idx[self._pin_k]}
+
+    def _launch_eval_batch(self, prep):
+        batch = prep["batch"]
+        prep["pos"] = prep["pin"][:batch.natoms].to("cuda", non_blocking=True)
+        prep["sel"] = list(self.sel)
+        prep["out"] = evaluate_packed(self.dm, batch, prep["pos"], prep["sel"], self.rcut, self.precision,
+                                      host_stage=prep["pin_idx"])
+        return prep
+
+    def _complete_eval_batch(self, prep):
+        reqs, batch, groups = prep["reqs"], prep["batch"], prep["groups"]
+        try:
+            out, sel = prep["out"], prep["sel"]
+            while True:
+                st = int(out["status"].item())
+                if not st & 2:
+                    break
+                sel = [2 * s for s in sel]      # neighbour overflow: grow and re-run the batch
+                self.sel = [max(a, b) for a, b in zip(self.sel, sel)]
+                out = evaluate_packed(self.dm, batch, prep["pos"], sel, self.rcut, self.precision,
+                                      host_stage=prep["pin_idx"])
+            energy = out["energy"].cpu().numpy()
+            force = out["force"].cpu().numpy()
+            virial = out["virial"].cpu().numpy().reshape(-1, 3, 3)
+        except Exception as ex:
+            self._fail(reqs, ex)
+            return
         self.batches += 1
         self.batch_sizes.append(batch.nreal)
         res = {id(r): {"energy": np.empty(r.frames), "force": np.empty((r.frames, r.atoms, 3), np.float32),
@@ -312,7 +367,7 @@ class Server:
                                          a["routine"], a["dt"], a["position"], initial_velocity=a["velocity"],
                                          temperature=a["temperature"] if a["routine"] == "NVT" else None,
                                          tau_t=a["tau_t"], seed=a["seed"], report_interval=self.md_chunk,
-                                         precision=self.precision, verbose=False)
+                                         precision=self.precision, verbose=False, autotune=False)
                         active.append([r, sim, a["steps"]])
                     except Exception as ex:
                         self._finish(r, exc=ex)
