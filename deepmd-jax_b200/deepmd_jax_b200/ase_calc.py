@@ -2,7 +2,8 @@
 evaluated by libdpb200 on the GPU.
 
 ``DPJaxCalculator(model_path, type_idx)`` provides energy, forces and stress
-of an ``ase.Atoms`` (orthorhombic cell).  The reference takes the stress as
+of an ``ase.Atoms`` (any periodic cell; a general one is evaluated through
+the open ghost-atom system of ``lattice.ghost_eval``, V = |det cell|).  The reference takes the stress as
 jax_md.quantity.stress, -(1/V) dU/d(eps), and returns its negative in Voigt
 order (xx, yy, zz, yz, xz, xy); with the virial W = -sum r (x) dE/dr that the
 adjoint produces, dU/d(eps) = -W, so the returned stress is -W / V.
@@ -15,7 +16,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .dpmodel import DPModel, box_diagonal
+from .dpmodel import DPModel, box_diagonal, general_box
 from .utils import load_model
 
 try:  # pragma: no cover - depends on the environment
@@ -70,10 +71,10 @@ class DPJaxCalculator(Calculator):
         if atoms is not None:
             self.atoms = atoms.copy()
         cell = np.asarray(self.atoms.get_cell(complete=True), dtype=np.float64)
-        L = box_diagonal(cell)
+        box = box_diagonal(cell) if general_box(cell) is None else cell  # general cells: lattice.ghost_eval
         pos = np.asarray(self.atoms.get_positions(), dtype=np.float64)
-        E, F, W = self._model.energy_force_virial(self._variables, pos, L, {"type_idx": tuple(self._type_idx)})
-        V = float(np.prod(L))
+        E, F, W = self._model.energy_force_virial(self._variables, pos, box, {"type_idx": tuple(self._type_idx)})
+        V = abs(float(np.linalg.det(cell)))
         self.results["energy"] = float(E)
         self.results["forces"] = np.asarray(F)
         self.results["stress"] = -np.array([W[0, 0], W[1, 1], W[2, 2], W[1, 2], W[0, 2], W[0, 1]]) / V

@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from .engine import DeviceModel, _require_cuda, sort_by_type
+from .lattice import ghost_eval
 from .md_utils import exact_neighbor_list
 from .utils import load_model
 
@@ -82,7 +83,8 @@ def evaluate(model_path, coord, box, type_idx, batch_size=1, precision="fp32"):
     """Energies and forces of frames sharing ``type_idx``.
 
     coord (n_frames, n_atoms, 3); box (n_frames,) / (n_frames, 1) /
-    (n_frames, 3) / (n_frames, 9) / (n_frames, 3, 3), orthorhombic; type_idx
+    (n_frames, 3) / (n_frames, 9) / (n_frames, 3, 3), general boxes with the
+    lattice vectors as rows included; type_idx
     (n_atoms,) (atomic numbers when the model carries ``chemical_types``).
     Returns {'energy': (n_frames,) float64, 'force': (n_frames, n_atoms, 3)
     float32}, forces in the input atom order.  ``precision`` is 'fp32' (the
@@ -99,10 +101,11 @@ def evaluate(model_path, coord, box, type_idx, batch_size=1, precision="fp32"):
 
 def _evaluate_frames(model, dm, coord, box, type_idx, batch_size, precision):
     """Energies and forces of frames (F, N, 3) in boxes (F, 3, 3) with model
-    type indices type_idx (N,), batch_size frames per dpb_eval call."""
+    type indices type_idx (N,), batch_size frames per dpb_eval call.  Frames
+    in general (non-orthorhombic) boxes are evaluated one at a time through
+    their open ghost-atom system (lattice.ghost_eval)."""
     off = box - np.einsum("fii->fi", box)[:, :, None] * np.eye(3)
-    if np.any(off):
-        raise NotImplementedError("non-orthorhombic boxes are not supported by the B200 kernels")
+    general = np.any(off.reshape(len(box), -1) != 0, axis=1)
     L = np.einsum("fii->fi", box)
     F, N = coord.shape[0], coord.shape[1]
     nt = int(model.params["ntypes"])
@@ -111,9 +114,19 @@ def _evaluate_frames(model, dm, coord, box, type_idx, batch_size, precision):
     rcut = float(model.params["rcut"])
     energy = np.empty(F, dtype=np.float64)
     force = np.empty((F, N, 3), dtype=np.float32)
+    for f in np.nonzero(general)[0]:
+        r = ghost_eval(dm, coord[f], box[f], type_idx, nt, rcut, precision)
+        energy[f], force[f] = r["energy"], r["force"]
     bs = max(int(batch_size), 1)
-    for a in range(0, F, bs):
-        b = min(a + bs, F)
+    ortho = np.nonzero(~general)[0]
+    runs, i = [], 0                     # runs of at most bs consecutive orthorhombic frames
+    while i < len(ortho):
+        j = i + 1
+        while j < len(ortho) and j - i < bs and ortho[j] == ortho[j - 1] + 1:
+            j += 1
+        runs.append((int(ortho[i]), int(ortho[j - 1]) + 1))
+        i = j
+    for a, b in runs:
         pos = torch.tensor(np.ascontiguousarray(coord[a:b], dtype=np.float32), device="cuda")
         nbrs, sel = exact_neighbor_list(pos, perm_dev, count, L[a:b], rcut)
         bx = torch.tensor(np.ascontiguousarray(L[a:b], dtype=np.float32), device="cuda")
