@@ -952,192 +952,233 @@ int launch_mix_embed_fwd(const DevModel &M, const SysDesc &D, int ti, const floa
   return DPB_OK;
 }
 
-// ---------------------------------------------------------------- dE/dT (SIMT, warp per atom)
-// Adjoint of the descriptor (dpmodel.py:74-78): from dE/dG (BF16, from the
-// fitting chain) and T, dE/dT / Nnbrs as FP16 rows [atom][c][w] (w padded to
-// N2 with zeros), the B operand rows of the tensor-core adjoint.  Each atom's
-// rows are scaled by the power of two 2^k that puts their largest magnitude in
-// [2^13, 2^14) (exact in FP32, and FP16 keeps ~2^-24 of that range normal);
-// dTs[atom] = 2^-k undoes it.
+// ---------------------------------------------------------------- dE/dT (warp per atom, warp-level MMA)
+// Adjoint of the descriptor (dpmodel.py:74-78): G[a][w] = sum_c Q[c][a] X[c][w]
+// with X = T + Tbias on channel 0 and Q[c][a] = X[c][a] (c < 4), the y_c
+// products of X[1..3][A + a] plus X[c][A + a] (c >= 4).  From dE/dG (FP16
+// times fit_dgsc, from the fitting chain) and T, per atom
+//   dQ[c][a] = sum_w X[c][w] dG[a][w]       (16 x 16 x N2 on mma.sync)
+//   dX[c][w] = sum_a Q[c][a] dG[a][w]       (16 x N2 x 16 on mma.sync)
+//            + the Q -> X terms at w < 2A   (FP32)
+// and dE/dT / Nnbrs leaves as FP16 rows [atom][c][w] (w padded to N2 with
+// zeros), the B operand rows of the tensor-core adjoint, each atom's rows
+// scaled by the power of two 2^k that puts their largest magnitude in
+// [2^13, 2^14); dTs[atom] = 2^-k / fit_dgsc undoes both scales.  X and Q
+// enter the FP16 products as their rounded value plus the rounded remainder
+// (hi + lo, about 22 significant bits), dE/dG is FP16 already, and the
+// products accumulate in FP32.  Each warp stages its atom in shared memory
+// (X hi / lo and the dE/dG rows at a padded row stride, so the ldmatrix
+// reads of eight rows hit distinct banks).
+template <int E2, int N2>
+struct DtCfg {
+  static constexpr int XS = N2 + 8;       // row stride (halves) of X and dE/dG
+  static constexpr int QS = 24;           // row stride (halves) of Q
+  static constexpr int XB = 16 * XS * 2;  // one 16-row FP16 tile
+  static constexpr int QB = 16 * QS * 2;
+  static constexpr int WARP_BYTES = 3 * XB + 2 * QB + 16 * 16 * 4 + 48 * 4;
+  static_assert(XB % 16 == 0 && WARP_BYTES % 16 == 0, "16-byte aligned tiles");
+};
+
 template <int E2, int N2, int W>
 __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const float *__restrict__ Tin,
                                                 const __half *__restrict__ dG,
                                                 __half *__restrict__ dTh, float *__restrict__ dTs) {
-  // Warp per atom; lane owns the column pairs w = 2 lane + 64 j (+0, +1).
-  // The atom's dE/dG rows stay in registers (D[a][2j + h]); X = T + Tbias
-  // sits in shared memory.
-  //   dQ[c][a] = sum_w dG[a][w] X[c][w]   (per-lane partials, then a shuffle
-  //                                         reduce-scatter: lane l ends with a = l & 15)
-  //   dX[c][w] = sum_a dG[a][w] Q[c][a] + the Q -> X terms at w < 2A
-  constexpr int NJ = (E2 + 63) / 64;
-  static_assert(N2 <= 64 * NJ && E2 % 2 == 0, "padded width");
-  __shared__ __align__(16) float Xs[W][10 * E2];
-  __shared__ float Qs[W][160], dQs[W][160];
+  using C = DtCfg<E2, N2>;
+  constexpr int XS = C::XS, QS = C::QS;
+  static_assert(E2 % 4 == 0 && E2 >= 32 && N2 % 16 == 0 && N2 >= E2 && N2 - E2 < 16, "dE/dT tile widths");
+  extern __shared__ __align__(16) char dt_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t g = (size_t)blockIdx.x * W + warp;
   if (g >= (size_t)NF) return;
-  const int A = M.A;  // 1..16 (checked at model creation: 2A <= 32)
-  float *X = Xs[warp], *Q = Qs[warp], *dQ = dQs[warp];
-  {  // X = T + Tbias: every lane issues all of its float4 loads before the first use
-    static_assert(E2 % 4 == 0, "float4 rows");
-    constexpr int N4 = 10 * E2 / 4, K4 = (N4 + 31) / 32;
-    const float4 *Tg4 = reinterpret_cast<const float4 *>(Tin + g * 10 * E2);
-    float4 tv[K4];
+  char *wb = dt_smem + warp * C::WARP_BYTES;
+  __half *Xh = reinterpret_cast<__half *>(wb), *Xl = Xh + 16 * XS, *Dg = Xl + 16 * XS;
+  __half *Qh = Dg + 16 * XS, *Ql = Qh + 16 * QS;
+  float *dQs = reinterpret_cast<float *>(Ql + 16 * QS);  // [c][a], 16 x 16
+  float *ys = dQs + 256;                                 // [k][a]: y_{k+1}[a] = X[k + 1][A + a]
+  const int A = M.A;                                     // 1..16 (2A <= 32 <= E2)
+  // ---- every global load first: T rows (float4), dE/dG rows (4 halves), Q inputs
+  constexpr int N4 = 10 * E2 / 4, K4 = (N4 + 31) / 32;
+  const float *Tg = Tin + g * 10 * E2;
+  float4 tv[K4];
 #pragma unroll
-    for (int k = 0; k < K4; ++k) {
-      const int e4 = lane + 32 * k;
-      tv[k] = e4 < N4 ? Tg4[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int k = 0; k < K4; ++k) {
+    const int e4 = lane + 32 * k;
+    tv[k] = e4 < N4 ? reinterpret_cast<const float4 *>(Tg)[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  constexpr int P4 = E2 / 4, NP = 16 * P4, KP = (NP + 31) / 32;
+  const uint2 *Dg8 = reinterpret_cast<const uint2 *>(dG + g * (size_t)A * E2);
+  uint2 dv[KP];
+#pragma unroll
+  for (int k = 0; k < KP; ++k) {
+    const int p = lane + 32 * k, a = p / P4;
+    dv[k] = (p < NP && a < A) ? Dg8[p] : make_uint2(0u, 0u);
+  }
+  const int aq = lane & 15;
+  const bool qlane = lane < 16 && aq < A;
+  float xr[4], xt[10];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) xr[c] = qlane ? Tg[c * E2 + aq] : 0.f;
+#pragma unroll
+  for (int c = 1; c < 10; ++c) xt[c] = qlane ? Tg[c * E2 + A + aq] : 0.f;
+  // ---- shared-memory tiles: zero padding, then X hi / lo, dE/dG, Q hi / lo
+  const uint2 z2 = make_uint2(0u, 0u);
+  for (int e = lane; e < 6 * (XS / 4); e += 32) {  // X rows 10..15
+    reinterpret_cast<uint2 *>(Xh + 10 * XS)[e] = z2;
+    reinterpret_cast<uint2 *>(Xl + 10 * XS)[e] = z2;
+  }
+  for (int e = lane; e < (16 - A) * (XS / 4); e += 32) reinterpret_cast<uint2 *>(Dg + A * XS)[e] = z2;  // rows a >= A
+  if constexpr (N2 > E2) {  // columns [E2, N2) of the live rows
+    constexpr int PW = (N2 - E2) / 4;
+    for (int e = lane; e < 10 * PW; e += 32) {
+      const int r = e / PW, o = E2 + 4 * (e - r * PW);
+      *reinterpret_cast<uint2 *>(Xh + r * XS + o) = z2;
+      *reinterpret_cast<uint2 *>(Xl + r * XS + o) = z2;
     }
+    for (int e = lane; e < A * PW; e += 32) {
+      const int r = e / PW, o = E2 + 4 * (e - r * PW);
+      *reinterpret_cast<uint2 *>(Dg + r * XS + o) = z2;
+    }
+  }
 #pragma unroll
-    for (int k = 0; k < K4; ++k) {
-      const int e4 = lane + 32 * k, e = 4 * e4;
-      if (e4 < N4) {
-        float4 v = tv[k];
-        if (e < E2) {
-          v.x += M.tbias[e];
-          v.y += M.tbias[e + 1];
-          v.z += M.tbias[e + 2];
-          v.w += M.tbias[e + 3];
-        }
-        reinterpret_cast<float4 *>(X)[e4] = v;
+  for (int k = 0; k < K4; ++k) {
+    const int e4 = lane + 32 * k;
+    if (e4 < N4) {
+      const int e = 4 * e4, c = e / E2, w = e - c * E2;
+      float x[4] = {tv[k].x, tv[k].y, tv[k].z, tv[k].w};
+      if (c == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] += M.tbias[w + i];
       }
+      __half h[4], l[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        h[i] = __float2half_rn(x[i]);
+        l[i] = __float2half_rn(x[i] - __half2float(h[i]));
+      }
+      *reinterpret_cast<uint2 *>(Xh + c * XS + w) =
+          make_uint2(tc::as_u32(__halves2half2(h[0], h[1])), tc::as_u32(__halves2half2(h[2], h[3])));
+      *reinterpret_cast<uint2 *>(Xl + c * XS + w) =
+          make_uint2(tc::as_u32(__halves2half2(l[0], l[1])), tc::as_u32(__halves2half2(l[2], l[3])));
     }
   }
-  float D[16][2 * NJ];
-  const __half2 *Gg = reinterpret_cast<const __half2 *>(dG + g * (size_t)A * E2);
-  const float inv_dgsc = 1.f / M.fit_dgsc;  // dE/dG arrives times fit_dgsc (a power of two)
 #pragma unroll
-  for (int a = 0; a < 16; ++a)
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const int w = 2 * lane + 64 * j;
-      float2 v = make_float2(0.f, 0.f);
-      if (a < A && w < E2) v = __half22float2(Gg[(a * E2 + w) / 2]);
-      D[a][2 * j] = v.x * inv_dgsc;
-      D[a][2 * j + 1] = v.y * inv_dgsc;
-    }
-  __syncwarp();
-  if (lane < 16) {  // Q[c][a] (dpmodel.py:74-78), zero for a >= A
-    const int aa = lane;
+  for (int k = 0; k < KP; ++k) {
+    const int p = lane + 32 * k, a = p / P4;
+    if (p < NP && a < A) *reinterpret_cast<uint2 *>(Dg + a * XS + 4 * (p - a * P4)) = dv[k];
+  }
+  if (lane < 16) {  // Q[c][a] of column a = lane (zero for a >= A and rows c >= 10), and y
     float q[10];
+    const float y1 = xt[1], y2 = xt[2], y3 = xt[3];
+    q[0] = xr[0] + (qlane ? M.tbias[aq] : 0.f);
+    q[1] = xr[1]; q[2] = xr[2]; q[3] = xr[3];
+    const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
 #pragma unroll
-    for (int c = 0; c < 10; ++c) q[c] = 0.f;
-    if (aa < A) {
+    for (int m = 0; m < 6; ++m) q[4 + m] = b6[m] + xt[4 + m];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) q[c] = X[c * E2 + aa];
-      const float y1 = X[E2 + A + aa], y2 = X[2 * E2 + A + aa], y3 = X[3 * E2 + A + aa];
-      const float b6[6] = {y1 * y1, y2 * y2, y3 * y3, kSqrt2 * y1 * y3, kSqrt2 * y2 * y1, kSqrt2 * y3 * y2};
-#pragma unroll
-      for (int m = 0; m < 6; ++m) q[4 + m] = b6[m] + X[(4 + m) * E2 + A + aa];
+    for (int c = 0; c < 16; ++c) {
+      const float v = (c < 10 && qlane) ? fminf(fmaxf(q[c < 10 ? c : 0], -65504.f), 65504.f) : 0.f;
+      const __half h = __float2half_rn(v);
+      Qh[c * QS + aq] = h;
+      Ql[c * QS + aq] = __float2half_rn(v - __half2float(h));
     }
-#pragma unroll
-    for (int c = 0; c < 10; ++c) Q[c * 16 + aa] = q[c];
-  }
-#pragma unroll 1
-  for (int c = 0; c < 10; ++c) {
-    float p[16];
-    float xc[2 * NJ];
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const int w = 2 * lane + 64 * j;
-      const float2 x2 = w < E2 ? *reinterpret_cast<const float2 *>(X + c * E2 + w) : make_float2(0.f, 0.f);
-      xc[2 * j] = x2.x;
-      xc[2 * j + 1] = x2.y;
-    }
-#pragma unroll
-    for (int a = 0; a < 16; ++a) {
-      float v = 0.f;
-#pragma unroll
-      for (int k = 0; k < 2 * NJ; ++k) v = fmaf(D[a][k], xc[k], v);
-      p[a] = v;
-    }
-    // reduce-scatter of the 16 partials over the 32 lanes
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const bool hi = lane & 8;
-      const float send = hi ? p[k] : p[k + 8];
-      const float keep = hi ? p[k + 8] : p[k];
-      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const bool hi = lane & 4;
-      const float send = hi ? p[k] : p[k + 4];
-      const float keep = hi ? p[k + 4] : p[k];
-      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const bool hi = lane & 2;
-      const float send = hi ? p[k] : p[k + 2];
-      const float keep = hi ? p[k + 2] : p[k];
-      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-    }
-    {
-      const bool hi = lane & 1;
-      const float send = hi ? p[0] : p[1];
-      const float keep = hi ? p[1] : p[0];
-      p[0] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
-    }
-    p[0] += __shfl_xor_sync(0xffffffffu, p[0], 16);
-    if (lane < 16) dQ[c * 16 + lane] = p[0];  // the sum for a = lane
+    ys[aq] = y1;
+    ys[16 + aq] = y2;
+    ys[32 + aq] = y3;
   }
   __syncwarp();
-  float o[10][NJ][2];
+  // ---- dQ = X . dE/dG^T: M = c, N = a (two tiles of 8), K = w
+  const int g8 = lane >> 2, q4 = lane & 3, mi = lane >> 3, ri = lane & 7;
+  float acc[2][4];
+#pragma unroll
+  for (int n = 0; n < 2; ++n)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[n][i] = 0.f;
+#pragma unroll
+  for (int kt = 0; kt < N2 / 16; ++kt) {
+    uint32_t ah[4], al[4];
+    const int arow = (ri + 8 * (mi & 1)) * XS + 16 * kt + 8 * (mi >> 1);
+    tc::ldmatrix_x4(ah, Xh + arow);
+    tc::ldmatrix_x4(al, Xl + arow);
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+      uint32_t b0, b1;
+      tc::ldmatrix_x2(b0, b1, Dg + (8 * n + ri) * XS + 16 * kt + 8 * (mi & 1));
+      tc::mma_16816(acc[n], ah, b0, b1);
+      tc::mma_16816(acc[n], al, b0, b1);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    const int a = 8 * n + 2 * q4;
+    dQs[g8 * 16 + a] = acc[n][0];
+    dQs[g8 * 16 + a + 1] = acc[n][1];
+    dQs[(g8 + 8) * 16 + a] = acc[n][2];
+    dQs[(g8 + 8) * 16 + a + 1] = acc[n][3];
+  }
+  // ---- dX = Q . dE/dG: M = c, N = w (tiles of 8), K = a
+  uint32_t qh[4], ql[4];
+  {
+    const int qrow = (ri + 8 * (mi & 1)) * QS + 8 * (mi >> 1);
+    tc::ldmatrix_x4(qh, Qh + qrow);
+    tc::ldmatrix_x4(ql, Ql + qrow);
+  }
+  float o[N2 / 8][4];
+#pragma unroll
+  for (int nt = 0; nt < N2 / 8; ++nt) {
+    uint32_t b0, b1;
+    tc::ldmatrix_x2_trans(b0, b1, Dg + (ri + 8 * (mi & 1)) * XS + 8 * nt);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) o[nt][i] = 0.f;
+    tc::mma_16816(o[nt], qh, b0, b1);
+    tc::mma_16816(o[nt], ql, b0, b1);
+  }
+  __syncwarp();  // dQs of every lane
+  // ---- Q -> X terms (w < 2A), 1 / Nnbrs, zero past E2 and for rows c >= 10
   float amax = 0.f;
 #pragma unroll
-  for (int c = 0; c < 10; ++c) {
-    float q[16];
+  for (int nt = 0; nt < N2 / 8; ++nt)
 #pragma unroll
-    for (int a = 0; a < 16; ++a) q[a] = Q[c * 16 + a];
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const int w = 2 * lane + 64 * j;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int ww = w + h;
-        float v = 0.f;
-#pragma unroll
-        for (int a = 0; a < 16; ++a) v = fmaf(D[a][2 * j + h], q[a], v);
-        if (j == 0) {  // the Q -> X terms live at w < 2A <= 32
-          if (ww < A && c < 4) v += dQ[c * 16 + ww];
-          if (ww >= A && ww < 2 * A) {
-            const int aa = ww - A;
-            if (c >= 4) {
-              v += dQ[c * 16 + aa];
-            } else if (c >= 1) {
-              const float y1 = X[E2 + ww], y2 = X[2 * E2 + ww], y3 = X[3 * E2 + ww];
-              const float d0 = dQ[64 + aa], d1 = dQ[80 + aa], d2 = dQ[96 + aa], d3 = dQ[112 + aa],
-                          d4 = dQ[128 + aa], d5 = dQ[144 + aa];
-              if (c == 1) v += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
-              if (c == 2) v += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
-              if (c == 3) v += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
-            }
+    for (int i = 0; i < 4; ++i) {
+      const int c = g8 + 8 * (i >> 1), w = 8 * nt + 2 * q4 + (i & 1);
+      float x = o[nt][i];
+      if (8 * nt < 32 && c < 10) {
+        if (w < A) {
+          if (c < 4) x += dQs[c * 16 + w];
+        } else if (w < 2 * A) {
+          const int aa = w - A;
+          if (c >= 4) {
+            x += dQs[c * 16 + aa];
+          } else if (c >= 1) {
+            const float y1 = ys[aa], y2 = ys[16 + aa], y3 = ys[32 + aa];
+            const float d0 = dQs[64 + aa], d1 = dQs[80 + aa], d2 = dQs[96 + aa], d3 = dQs[112 + aa],
+                        d4 = dQs[128 + aa], d5 = dQs[144 + aa];
+            if (c == 1) x += 2.f * y1 * d0 + kSqrt2 * y3 * d3 + kSqrt2 * y2 * d4;
+            if (c == 2) x += 2.f * y2 * d1 + kSqrt2 * y1 * d4 + kSqrt2 * y3 * d5;
+            if (c == 3) x += 2.f * y3 * d2 + kSqrt2 * y1 * d3 + kSqrt2 * y2 * d5;
           }
         }
-        v = ww < E2 ? v * M.inv_nnbrs : 0.f;
-        o[c][j][h] = v;
-        amax = fmaxf(amax, fabsf(v));
       }
+      x = (c < 10 && w < E2) ? x * M.inv_nnbrs : 0.f;
+      o[nt][i] = x;
+      amax = fmaxf(amax, fabsf(x));
     }
-  }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, off));
   // amax = m 2^e with m in [0.5, 1): scale 2^(14 - e) puts it in [2^13, 2^14)
   int e = 0;
-  if (amax > 0.f && amax < INFINITY) frexpf(amax, &e);
-  const int k = (amax > 0.f && amax < INFINITY) ? 14 - e : 0;
+  const bool fin = amax > 0.f && amax < INFINITY;
+  if (fin) frexpf(amax, &e);
+  const int k = fin ? 14 - e : 0;
   const float scale = ldexpf(1.f, k);
-  if (lane == 0) dTs[g] = ldexpf(1.f, -k);
+  if (lane == 0) dTs[g] = ldexpf(1.f, -k) / M.fit_dgsc;
   __half *out = dTh + g * 10 * N2;
 #pragma unroll
-  for (int c = 0; c < 10; ++c)
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const int w = 2 * lane + 64 * j;
-      if (w < N2)
-        *reinterpret_cast<__half2 *>(out + c * N2 + w) = tc::f2_to_h2(o[c][j][0] * scale, o[c][j][1] * scale);
-    }
+  for (int nt = 0; nt < N2 / 8; ++nt) {
+    const int w = 8 * nt + 2 * q4;
+    *reinterpret_cast<__half2 *>(out + g8 * N2 + w) = tc::f2_to_h2(o[nt][0] * scale, o[nt][1] * scale);
+    if (g8 + 8 < 10)
+      *reinterpret_cast<__half2 *>(out + (g8 + 8) * N2 + w) = tc::f2_to_h2(o[nt][2] * scale, o[nt][3] * scale);
+  }
 }
 
 // ---------------------------------------------------------------- embedding adjoint (FP16 tcgen05)
@@ -2017,13 +2058,21 @@ size_t mixed_workspace_per_atom(const DevModel &M) {
 }
 
 // dE/dT with W atoms (warps) per block, W in {2, 4, 8} (launch shape only).
+template <int E2, int N2, int W>
+static void launch_mix_dT_s(const DevModel &M, size_t NF, const float *T, const __half *dGb, __half *dTh,
+                            float *dTs, cudaStream_t st) {
+  const unsigned grid = (unsigned)((NF + W - 1) / W);
+  const int smem = W * DtCfg<E2, N2>::WARP_BYTES;
+  cudaFuncSetAttribute(k_mix_dT<E2, N2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k_mix_dT<E2, N2, W><<<grid, 32 * W, smem, st>>>(M, (int)NF, T, dGb, dTh, dTs);
+  count_launch();
+}
+
 template <int W>
 static void launch_mix_dT_w(const DevModel &M, size_t NF, const float *T, const __half *dGb,
                             __half *dTh, float *dTs, cudaStream_t st) {
-  const unsigned grid = (unsigned)((NF + W - 1) / W);
-  if (M.E2 == 100) k_mix_dT<100, 112, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTh, dTs);
-  else k_mix_dT<64, 64, W><<<grid, 32 * W, 0, st>>>(M, (int)NF, T, dGb, dTh, dTs);
-  count_launch();
+  if (M.E2 == 100) launch_mix_dT_s<100, 112, W>(M, NF, T, dGb, dTh, dTs, st);
+  else launch_mix_dT_s<64, 64, W>(M, NF, T, dGb, dTh, dTs, st);
 }
 
 static int launch_mix_dT(const DevModel &M, size_t NF, const float *T, const __half *dGb, __half *dTh,

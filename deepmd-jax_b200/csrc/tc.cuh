@@ -154,6 +154,37 @@ __device__ __forceinline__ __half2 f2_to_h2(float a, float b) {
 }
 
 
+// ---- warp-level MMA (mma.sync m16n8k16, FP16 operands, FP32 accumulators)
+// for small per-warp products.  Fragments (PTX ISA layout; g = lane / 4,
+// q = lane % 4): A (16 x 16, row-major) a[0] = (row g, cols 2q, 2q+1),
+// a[1] = row g + 8, a[2] = cols + 8, a[3] = both; B (16 x 8, "col") b[0] =
+// (rows 2q, 2q+1, col g), b[1] = rows + 8; C (16 x 8 FP32) c[0], c[1] = (row g,
+// cols 2q, 2q+1), c[2], c[3] = row g + 8.
+__device__ __forceinline__ void mma_16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// Four 8x8 b16 matrices from shared memory; lane l gives the row address of
+// row l % 8 of matrix l / 8 (16-byte aligned); register i holds matrix i.
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void *row) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(row)));
+}
+// Two 8x8 b16 matrices (lanes 0-15 give the row addresses), as stored or
+// transposed (.trans: lane l receives column l / 4, rows 2 (l % 4), +1).
+__device__ __forceinline__ void ldmatrix_x2(uint32_t &r0, uint32_t &r1, const void *row) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(smem_u32(row)));
+}
+__device__ __forceinline__ void ldmatrix_x2_trans(uint32_t &r0, uint32_t &r1, const void *row) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];"
+               : "=r"(r0), "=r"(r1)
+               : "r"(smem_u32(row)));
+}
+
 // Asynchronous 16-byte global -> shared copies (no register round trip).
 __device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst_smem)), "l"(src_gmem) : "memory");
