@@ -988,7 +988,8 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
   static_assert(E2 % 4 == 0 && E2 >= 32 && N2 % 16 == 0 && N2 >= E2 && N2 - E2 < 16, "dE/dT tile widths");
   extern __shared__ __align__(16) char dt_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t g = (size_t)blockIdx.x * W + warp;
+  const size_t stride = (size_t)gridDim.x * W;  // warp-strided atoms
+  size_t g = (size_t)blockIdx.x * W + warp;
   if (g >= (size_t)NF) return;
   char *wb = dt_smem + warp * C::WARP_BYTES;
   __half *Xh = reinterpret_cast<__half *>(wb), *Xl = Xh + 16 * XS, *Dg = Xl + 16 * XS;
@@ -996,31 +997,7 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
   float *dQs = reinterpret_cast<float *>(Ql + 16 * QS);  // [c][a], 16 x 16
   float *ys = dQs + 256;                                 // [k][a]: y_{k+1}[a] = X[k + 1][A + a]
   const int A = M.A;                                     // 1..16 (2A <= 32 <= E2)
-  // ---- every global load first: T rows (float4), dE/dG rows (4 halves), Q inputs
-  constexpr int N4 = 10 * E2 / 4, K4 = (N4 + 31) / 32;
-  const float *Tg = Tin + g * 10 * E2;
-  float4 tv[K4];
-#pragma unroll
-  for (int k = 0; k < K4; ++k) {
-    const int e4 = lane + 32 * k;
-    tv[k] = e4 < N4 ? reinterpret_cast<const float4 *>(Tg)[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  constexpr int P4 = E2 / 4, NP = 16 * P4, KP = (NP + 31) / 32;
-  const uint2 *Dg8 = reinterpret_cast<const uint2 *>(dG + g * (size_t)A * E2);
-  uint2 dv[KP];
-#pragma unroll
-  for (int k = 0; k < KP; ++k) {
-    const int p = lane + 32 * k, a = p / P4;
-    dv[k] = (p < NP && a < A) ? Dg8[p] : make_uint2(0u, 0u);
-  }
-  const int aq = lane & 15;
-  const bool qlane = lane < 16 && aq < A;
-  float xr[4], xt[10];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) xr[c] = qlane ? Tg[c * E2 + aq] : 0.f;
-#pragma unroll
-  for (int c = 1; c < 10; ++c) xt[c] = qlane ? Tg[c * E2 + A + aq] : 0.f;
-  // ---- shared-memory tiles: zero padding, then X hi / lo, dE/dG, Q hi / lo
+  // ---- zero padding of the tiles, once (the atoms' stages never write it)
   const uint2 z2 = make_uint2(0u, 0u);
   for (int e = lane; e < 6 * (XS / 4); e += 32) {  // X rows 10..15
     reinterpret_cast<uint2 *>(Xh + 10 * XS)[e] = z2;
@@ -1039,6 +1016,36 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
       *reinterpret_cast<uint2 *>(Dg + r * XS + o) = z2;
     }
   }
+  // ---- an atom's global inputs in registers: T rows (float4), dE/dG rows
+  // (4 halves), the Q inputs; the next atom's are loaded right after this
+  // atom's are staged, so they arrive while this atom's products run
+  constexpr int N4 = 10 * E2 / 4, K4 = (N4 + 31) / 32;
+  constexpr int P4 = E2 / 4, NP = 16 * P4, KP = (NP + 31) / 32;
+  const int aq = lane & 15;
+  const bool qlane = lane < 16 && aq < A;
+  float4 tv[K4];
+  uint2 dv[KP];
+  float xr[4], xt[10];
+  auto load = [&](size_t ga) {
+    const float *Tg = Tin + ga * 10 * E2;
+#pragma unroll
+    for (int k = 0; k < K4; ++k) {
+      const int e4 = lane + 32 * k;
+      tv[k] = e4 < N4 ? reinterpret_cast<const float4 *>(Tg)[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const uint2 *Dg8 = reinterpret_cast<const uint2 *>(dG + ga * (size_t)A * E2);
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+      const int p = lane + 32 * k, a = p / P4;
+      dv[k] = (p < NP && a < A) ? Dg8[p] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) xr[c] = qlane ? Tg[c * E2 + aq] : 0.f;
+#pragma unroll
+    for (int c = 1; c < 10; ++c) xt[c] = qlane ? Tg[c * E2 + A + aq] : 0.f;
+  };
+  load(g);
+  for (; g < (size_t)NF; g += stride) {
 #pragma unroll
   for (int k = 0; k < K4; ++k) {
     const int e4 = lane + 32 * k;
@@ -1085,6 +1092,7 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
     ys[16 + aq] = y2;
     ys[32 + aq] = y3;
   }
+  if (g + stride < (size_t)NF) load(g + stride);
   __syncwarp();
   // ---- dQ = X . dE/dG^T: M = c, N = a (two tiles of 8), K = w
   const int g8 = lane >> 2, q4 = lane & 3, mi = lane >> 3, ri = lane & 7;
@@ -1178,6 +1186,8 @@ __global__ void __launch_bounds__(32 * W) k_mix_dT(DevModel M, int NF, const flo
     *reinterpret_cast<__half2 *>(out + g8 * N2 + w) = tc::f2_to_h2(o[nt][0] * scale, o[nt][1] * scale);
     if (g8 + 8 < 10)
       *reinterpret_cast<__half2 *>(out + (g8 + 8) * N2 + w) = tc::f2_to_h2(o[nt][2] * scale, o[nt][3] * scale);
+  }
+  __syncwarp();  // every lane is done with this atom's tiles before the next stage
   }
 }
 
@@ -2061,7 +2071,9 @@ size_t mixed_workspace_per_atom(const DevModel &M) {
 template <int E2, int N2, int W>
 static void launch_mix_dT_s(const DevModel &M, size_t NF, const float *T, const __half *dGb, __half *dTh,
                             float *dTs, cudaStream_t st) {
-  const unsigned grid = (unsigned)((NF + W - 1) / W);
+  // warp-strided atoms: at most the blocks every SM can hold by thread count
+  const size_t cap = (size_t)num_sms() * (2048 / (32 * W));
+  const unsigned grid = (unsigned)std::min((NF + W - 1) / W, cap);
   const int smem = W * DtCfg<E2, N2>::WARP_BYTES;
   cudaFuncSetAttribute(k_mix_dT<E2, N2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   k_mix_dT<E2, N2, W><<<grid, 32 * W, smem, st>>>(M, (int)NF, T, dGb, dTh, dTs);
