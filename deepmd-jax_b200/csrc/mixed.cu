@@ -1566,10 +1566,12 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
 //   g <  L           forward layer g        A: G rows (g = 0) or H    B: W_g^T  (out x in)
 //   L <= g < 2L - 1  adjoint layer 2L-1-g   A: gZ                     B: W_l    (in x out)
 //   g >= 2L - 1      dE/dG columns [128 p, 128 p + 128), p = g - (2L - 1), B: rows of W_0
-// Warp roles (192 threads): warps 0-3 are the epilogue, one thread per atom,
-// which also stream layer 0's G rows into the ring with cp.async; lane 0 of
-// warp 4 issues the MMAs and lane 0 of warp 5 the bulk (TMA) copies of the
-// weights, each waiting only on its own barriers so MMAs queue back to back.  Operands
+// Warp roles (320 threads): warps 0-7 are the epilogue, two threads per atom
+// (warps w and w + 4 share TMEM lane quarter w and take the two halves of
+// every layer's columns), which also stream layer 0's G rows into the ring
+// with cp.async; lane 0 of warp 8 issues the MMAs and lane 0 of warp 9 the
+// bulk (TMA) copies of the weights, each waiting only on its own barriers so
+// MMAs queue back to back.  Operands
 // pass through a ring of K = 16 stages (full / empty mbarriers), so the
 // weights of the next GEMM are already in flight while the epilogue of the
 // current one runs; the dE/dG passes alternate between two TMEM accumulators
@@ -1583,7 +1585,8 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
 // product (FP64 segment sums) and the adjoint gates; tanh values and residual
 // sources go to a per-atom FP32 scratch, the BF16 activation of the next GEMM
 // stays in shared memory.  2 CTAs per SM, 256 TMEM columns each.
-constexpr int kFitThreads = 192;
+constexpr int kFitThreads = 320;
+constexpr int kFitEpi = 256;                 // epilogue threads: 2 per atom
 constexpr int kFitDgN = 128;                 // N of one dE/dG pass
 constexpr int kFitStageA = 2 * 128 * 16;     // A chunk bytes (K = 16)
 
@@ -1660,6 +1663,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   __shared__ __align__(8) uint64_t full[ST], fullA[ST], empty[ST], accf, accfD[2], epid, accfree[2];
   __shared__ uint32_t tbase_s;
   __shared__ int abort_s;
+  __shared__ float esum_s[128];  // the second half's energy partial per atom
   const int tid = threadIdx.x, warp = tid >> 5;
   const int L = M.nfit, K0 = M.A * M.E2;
   const int NG = 2 * L - 1 + (K0 + kFitDgN - 1) / kFitDgN;
@@ -1667,15 +1671,15 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   if (tid == 0) {
     for (int s = 0; s < ST; ++s) {
       tc::mbar_init(&full[s], 1);
-      tc::mbar_init(&fullA[s], 128);
+      tc::mbar_init(&fullA[s], kFitEpi);
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(&accf, 1);
     tc::mbar_init(&accfD[0], 1);
     tc::mbar_init(&accfD[1], 1);
-    tc::mbar_init(&epid, 128);
-    tc::mbar_init(&accfree[0], 128);
-    tc::mbar_init(&accfree[1], 128);
+    tc::mbar_init(&epid, kFitEpi);
+    tc::mbar_init(&accfree[0], kFitEpi);
+    tc::mbar_init(&accfree[1], kFitEpi);
     abort_s = 0;
     tc::fence_mbar_init();
   }
@@ -1686,7 +1690,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
   const uint32_t td = tbase_s;
   const int r0 = blockIdx.x * 128, nrows = min(128, Mrows - r0);
 
-  if (warp == 5) {
+  if (warp == 9) {
     // ================= weight producer (one thread): bulk copies into free stages
     if ((tid & 31) == 0) {
       const uint32_t ring_u = tc::smem_u32(ring);
@@ -1705,7 +1709,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       // copies still in flight only after a give-up: the last ST issued chunks
       for (int c = p > ST ? p - ST : 0; c < p; ++c) tc::mbar_wait(&full[c % ST], (c / ST) & 1);
     }
-  } else if (warp == 4) {
+  } else if (warp == 8) {
     // ================= MMA issuer (one thread)
     if ((tid & 31) == 0) {
       const uint32_t ring_u = tc::smem_u32(ring), ha_u = tc::smem_u32(HA);
@@ -1744,13 +1748,19 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       if (q > 0) tc::mbar_wait(&empty[(q - 1) % ST], ((q - 1) / ST) & 1);
     }
   } else {
-    // ================= epilogue warps: thread = atom = TMEM lane
-    const int row = tid;
+    // ================= epilogue warps: two threads per atom = TMEM lane; half
+    // h = warp / 4 takes columns [h FH, h FH + FH) of every hidden layer and
+    // [64 h, 64 h + 64) of every dE/dG pass
+    constexpr int FH = FW / 2;
+    static_assert(FH % 8 == 0, "half-width column chunks");
+    const int row = tid & 127, half = tid >> 7;
     const bool act = row < nrows;
     const size_t me = rm.atom(act ? r0 + row : r0);
-    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+    const int cb = half * FH, ce = cb + FH;  // this half's hidden columns
     bool ok = true;
-    // ---- layer 0's A operand: this atom's G row, ST - 1 chunks in flight
+    // ---- layer 0's A operand: this atom's G row (each half copies its 16
+    // bytes of every 32-byte K chunk), ST - 1 chunks in flight
     {
       const int nch0 = K0 / 16;
       const char *grow = reinterpret_cast<const char *>(Gh + me * (size_t)K0);
@@ -1758,14 +1768,9 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
         if (c < nch0) {
           const int s = c % ST;
           if (c >= ST && !(ok = __all_sync(0xffffffffu, fit_wait(&empty[s], ((c / ST) - 1) & 1, abort)))) break;
-          char *dst = ring + s * C::STAGE + row * 16;
-          if (act) {
-            tc::cp_async16(dst, grow + c * 32);
-            tc::cp_async16(dst + 128 * 16, grow + c * 32 + 16);
-          } else {
-            *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4 *>(dst + 128 * 16) = make_uint4(0, 0, 0, 0);
-          }
+          char *dst = ring + s * C::STAGE + half * 128 * 16 + row * 16;
+          if (act) tc::cp_async16(dst, grow + c * 32 + half * 16);
+          else *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
         }
         tc::cp_async_commit();
         const int cc = c - (ST - 1);
@@ -1782,12 +1787,12 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
     // residual adjoint
     float *tile = scratch + ((size_t)tile0 + blockIdx.x) * 128 * (size_t)(2 * L + 1) * FW + row;
 #define FIT_SCR(slot, n) tile[((size_t)(slot) * FW + (n)) * 128]
-    // L2 prefetch of one scratch slot of this warp's 32 rows (one 128-byte
-    // line per column), issued before a layer's accumulator wait so that it
-    // overlaps the layer's MMAs instead of stalling the epilogue's reads
+    // L2 prefetch of one scratch slot of this warp's 32 rows and this half's
+    // columns (one 128-byte line per column), issued before a layer's
+    // accumulator wait so that it overlaps the layer's MMAs
     const float *tile_w = tile - (row & 31);
     auto prefetch_slot = [&](int slot) {
-      for (int n = row & 31; n < FW; n += 32) tc::prefetch_l2(tile_w + ((size_t)slot * FW + n) * 128);
+      for (int n = cb + (row & 31); n < ce; n += 32) tc::prefetch_l2(tile_w + ((size_t)slot * FW + n) * 128);
     };
     // ---- forward; the last layer's epilogue also forms the atom energy and
     // the first adjoint gate g = w_out dt (1 - t^2), the A operand of adjoint
@@ -1806,18 +1811,18 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       const float gsc = last ? M.fit_gsc[ti][l] : 1.f;  // the gate's operand scale
       // residual sources of the current chunk, loaded one chunk ahead so the
       // scratch reads overlap the TMEM loads and the previous chunk's math
-      float hp[16];
+      float hp[8];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) hp[i] = dt ? FIT_SCR(L + l - 1, i) : 0.f;
-      for (int c0 = 0; c0 < FW; c0 += 16) {
-        uint32_t r[16];
-        tc::tmem_ld16_issue(td + lane_off + c0, r);
-        float hn[16];
+      for (int i = 0; i < 8; ++i) hp[i] = dt ? FIT_SCR(L + l - 1, cb + i) : 0.f;
+      for (int c0 = cb; c0 < ce; c0 += 8) {
+        uint32_t r[8];
+        tc::tmem_ld8_issue(td + lane_off + c0, r);
+        float hn[8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) hn[i] = (dt && c0 + 16 < FW) ? FIT_SCR(L + l - 1, c0 + 16 + i) : 0.f;
-        float bv[16], dv[16], wv[16];
+        for (int i = 0; i < 8; ++i) hn[i] = (dt && c0 + 8 < ce) ? FIT_SCR(L + l - 1, c0 + 8 + i) : 0.f;
+        float bv[8], dv[8], wv[8];
 #pragma unroll
-        for (int i = 0; i < 16; i += 4) {
+        for (int i = 0; i < 8; i += 4) {
           const float4 b4 = __ldg(reinterpret_cast<const float4 *>(bias + c0 + i));
           bv[i] = b4.x; bv[i + 1] = b4.y; bv[i + 2] = b4.z; bv[i + 3] = b4.w;
           const float4 d4 =
@@ -1827,9 +1832,9 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
         }
         tc::tmem_wait();
-        float hv[16];
+        float hv[8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
+        for (int i = 0; i < 8; ++i) {
           const int n = c0 + i;
           const float t = tc::tanh_fast(fmaf(__uint_as_float(r[i]), usc, bv[i]));
           float h = t;
@@ -1844,20 +1849,24 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           }
         }
 #pragma unroll
-        for (int i = 0; i < 16; ++i) hp[i] = hn[i];
+        for (int i = 0; i < 8; ++i) hp[i] = hn[i];
         *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8h(hv, gsc);
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8h(hv + 8, gsc);
       }
       fit_signal(&epid);
     }
-    float e_me = 0.f;
-    if (ok) {
-      e_me = e_sum + M.fb[ti][L][0];
-      if (act) Eatom[me] = e_me;
-    }
-    {  // energy per segment (every lane of the warp takes part): rows run
-       // through the segments in order, so a warp suffix sum over equal keys
-       // leaves each run's total at its first lane
+    // the two halves' energy partials (every epilogue thread reaches this
+    // barrier once, whatever its wait outcomes)
+    if (half) esum_s[row] = e_sum;
+    asm volatile("bar.sync 1, %0;" ::"n"(kFitEpi) : "memory");
+    if (half == 0) {
+      float e_me = 0.f;
+      if (ok) {
+        e_me = e_sum + esum_s[row] + M.fb[ti][L][0];
+        if (act) Eatom[me] = e_me;
+      }
+      // energy per segment (every lane of the warp takes part): rows run
+      // through the segments in order, so a warp suffix sum over equal keys
+      // leaves each run's total at its first lane
       const int lane = row & 31;
       const int key = (ok && act) ? energy_slot(seg, me, N) : -2;
       double v = (ok && act) ? (double)e_me : 0.0;
@@ -1879,27 +1888,27 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       if (!ok) break;
       tc::fence_after_sync();
       const bool res_l = M.mfdt[ti][l] != nullptr, res_lm1 = (l - 1 > 0) && M.mfdt[ti][l - 1] != nullptr;
-      const float *dtm1 = M.mfdt[ti][l - 1], *wf = M.mfwout[ti];
+      const float *dtm1 = M.mfdt[ti][l - 1];
       const bool use_gh = res_l && l != L - 1;
       const float usc = 1.f / (M.fit_wsc[ti][l] * M.fit_gsc[ti][l]), gsc = M.fit_gsc[ti][l - 1];
-      float ghc[16], tcur[16];
+      float ghc[8], tcur[8];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        ghc[i] = use_gh ? FIT_SCR(2 * L, i) : 0.f;
-        tcur[i] = FIT_SCR(l - 1, i);
+      for (int i = 0; i < 8; ++i) {
+        ghc[i] = use_gh ? FIT_SCR(2 * L, cb + i) : 0.f;
+        tcur[i] = FIT_SCR(l - 1, cb + i);
       }
-      for (int c0 = 0; c0 < FW; c0 += 16) {
-        uint32_t r[16];
-        tc::tmem_ld16_issue(td + lane_off + c0, r);
-        float ghn[16], tn[16];
+      for (int c0 = cb; c0 < ce; c0 += 8) {
+        uint32_t r[8];
+        tc::tmem_ld8_issue(td + lane_off + c0, r);
+        float ghn[8], tn[8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          ghn[i] = (use_gh && c0 + 16 < FW) ? FIT_SCR(2 * L, c0 + 16 + i) : 0.f;
-          tn[i] = (c0 + 16 < FW) ? FIT_SCR(l - 1, c0 + 16 + i) : 0.f;
+        for (int i = 0; i < 8; ++i) {
+          ghn[i] = (use_gh && c0 + 8 < ce) ? FIT_SCR(2 * L, c0 + 8 + i) : 0.f;
+          tn[i] = (c0 + 8 < ce) ? FIT_SCR(l - 1, c0 + 8 + i) : 0.f;
         }
-        float wv[16], dv[16];
+        float wv[8], dv[8];
 #pragma unroll
-        for (int i = 0; i < 16; i += 4) {
+        for (int i = 0; i < 8; i += 4) {
           const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wf + c0 + i));
           wv[i] = w4.x; wv[i + 1] = w4.y; wv[i + 2] = w4.z; wv[i + 3] = w4.w;
           const float4 d4 =
@@ -1907,9 +1916,9 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           dv[i] = d4.x; dv[i + 1] = d4.y; dv[i + 2] = d4.z; dv[i + 3] = d4.w;
         }
         tc::tmem_wait();
-        float gz[16];
+        float gz[8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
+        for (int i = 0; i < 8; ++i) {
           const int n = c0 + i;
           float g = __uint_as_float(r[i]) * usc;
           if (res_l) g += (l == L - 1) ? wv[i] : ghc[i];
@@ -1918,16 +1927,16 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
           if (res_lm1) FIT_SCR(2 * L, n) = g;
         }
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
+        for (int i = 0; i < 8; ++i) {
           ghc[i] = ghn[i];
           tcur[i] = tn[i];
         }
         *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0, FW)) = pack8h(gz, gsc);
-        *reinterpret_cast<uint4 *>(HA + tc::kmajor_off(row, c0 + 8, FW)) = pack8h(gz + 8, gsc);
       }
       fit_signal(&epid);
     }
-    // ---- dE/dG = gZ_0 W_0^T, 128 columns per pass from alternating accumulators
+    // ---- dE/dG = gZ_0 W_0^T, 128 columns per pass from alternating
+    // accumulators, this half's 64 of them
     const int npass = (K0 + kFitDgN - 1) / kFitDgN;
     const float usc0 = 1.f / (M.fit_wsc[ti][0] * M.fit_gsc[ti][0]);
     for (int pp = 0; pp < npass && ok; ++pp) {
@@ -1936,7 +1945,7 @@ __global__ void __launch_bounds__(kFitThreads, 2) k_mix_fit(DevModel M, int ti,
       tc::fence_after_sync();
       const int n0 = kFitDgN * pp, nv = min(kFitDgN, K0 - n0);
       const uint32_t tcol = td + lane_off + kFitDgN * (pp & 1);
-      for (int c0 = 0; c0 < nv; c0 += 32) {
+      for (int c0 = 64 * half; c0 < min(nv, 64 * half + 64); c0 += 32) {
         const bool two = c0 + 16 < nv;
         uint32_t ra[16], rb[16];
         tc::tmem_ld16_issue(tcol + c0, ra);
