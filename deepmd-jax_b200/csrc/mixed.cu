@@ -1539,22 +1539,15 @@ int launch_mix_embed_bwd(const DevModel &M, const SysDesc &D, int ti, const floa
   const size_t smem = mix_bwd_smem<E0, E1, E2>();
   DPB_CUDA_TRY(cudaFuncSetAttribute(k_mix_embed_bwd<E0, E1, E2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-  const int nsm = num_sms();
-  // one launch per frame so that each block's virial belongs to one frame
-  for (int f = 0; f < D.F; ++f) {
-    SysDesc Df = D;
-    Df.F = 1;
-    const int nb1 = (cnt + kBlkAtoms - 1) / kBlkAtoms;
-    const int grid = nb1 < 2 * nsm ? nb1 : 2 * nsm;
-    const size_t off = (size_t)f * D.N;
-    k_mix_embed_bwd<E0, E1, E2><<<grid, kBwdThreads, smem, st>>>(M, Df, ti, posS + off, box + f * 3,
-                                                                  nbrs + off * D.S, dTh + off * 10 * MD::N2,
-                                                                  dTs + off,
-                                                                  rows_g ? rows_g + off * kRowStoreCap : nullptr,
-                                                                  rcnt ? rcnt + off * M.ntypes : nullptr, F4 + off,
-                                                                  virial + f * 9, err);
-    count_launch();
-  }
+  // one launch over every frame: a CTA's blocks run through the frames in
+  // increasing order, and it flushes its virial sum to a frame's row before it
+  // moves on to the next frame (flush_virial), so the frames of PIMD beads or
+  // of a batch share one full-width grid
+  const int nblk = (cnt + kBlkAtoms - 1) / kBlkAtoms * D.F;
+  const int grid = nblk < 2 * num_sms() ? nblk : 2 * num_sms();
+  k_mix_embed_bwd<E0, E1, E2><<<grid, kBwdThreads, smem, st>>>(M, D, ti, posS, box, nbrs, dTh, dTs, rows_g, rcnt, F4,
+                                                                virial, err);
+  count_launch();
   DPB_LAUNCH_CHECK();
   return DPB_OK;
 }
