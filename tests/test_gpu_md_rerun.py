@@ -18,11 +18,16 @@ one another) grows that last-bit noise by orders of magnitude at a close
 approach (in this box one comes near step 55, where two clean runs part from
 2e-6 A to 2e-4 A within three steps).  The runs stop at 40 steps, before it,
 and a second engine with the grown setting gives the yardstick: the re-run
-trajectory must lie within 10x the distance between the two clean runs or
-1e-5 A, whichever is larger, and within 1e-5 A over the first 10 steps.  A wrong re-run (a lost neighbour,
-a chunk that does not restart from its saved state) moves atoms by a
-perturbation of a missing pair's force, not of a float32 last bit, and
-lands orders of magnitude outside.
+trajectory must lie within 1e-5 A over the first 10 steps and, after them,
+within 10x the distance between the two clean runs or 1e-4 A, whichever is
+larger.  The floor covers a last-bit difference that appears in one run and
+not in the other (one float32 ulp of a coordinate near 24 A is 1.9e-6 A; one
+such difference in a velocity grows by about 8e-6 A per step over the last
+ten steps here).  A wrong re-run (a lost neighbour, a chunk that does not
+restart from its saved state) moves atoms by a perturbation of a missing
+pair's force: 1e-3 eV/A on a hydrogen for 30 steps of 0.5 fs displaces it by
+about 1e-3 A, ten times the floor, and a chunk that does not restart differs
+from the first frames on.
 """
 import ctypes
 
@@ -50,7 +55,7 @@ def _same_within_spread(name, got, ref, ref2):
     print("%s: re-run vs clean %.2e A (step 10: %.2e), clean vs clean %.2e A (step 10: %.2e)"
           % (name, d.max(), d[10], d0.max(), d0[10]))
     assert d[:11].max() < 1e-5
-    assert d.max() <= max(10.0 * d0.max(), 1e-5)
+    assert d.max() <= max(10.0 * d0.max(), 1e-4)
 
 
 def test_neighbour_overflow_mid_chunk_is_rerun_at_grown_capacity():
