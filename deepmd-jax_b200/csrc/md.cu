@@ -901,6 +901,10 @@ struct dpb_md {
   // snapshot for chunk re-runs
   float *s_pos = nullptr, *s_mom = nullptr, *s_force = nullptr, *s_ref = nullptr;
   MdScalars *s_sc = nullptr;
+  // trajectory frames (dpb_md_traj_frames): sorted slot and float64 mass
+  // (eV fs^2 / A^2) of each atom in user order
+  int32_t *user_slot = nullptr;
+  double *user_mass = nullptr;
   std::vector<void *> allocs;
 };
 
@@ -1001,6 +1005,8 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   rc_ |= md_alloc(m, (void **)&m->s_force, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_ref, NF * 12);
   rc_ |= md_alloc(m, (void **)&m->s_sc, sizeof(MdScalars));
+  rc_ |= md_alloc(m, (void **)&m->user_slot, N * 4);
+  rc_ |= md_alloc(m, (void **)&m->user_mass, N * 8);
   if (has_box) {
     rc_ |= md_alloc(m, (void **)&m->np, sizeof(NptScalars));
     rc_ |= md_alloc(m, (void **)&m->s_np, sizeof(NptScalars));
@@ -1020,6 +1026,17 @@ extern "C" int dpb_md_create(const dpb_model *model, const dpb_md_desc *d, dpb_m
   m->mass_sorted = ms;
   cudaMemcpy(m->mass, ms.data(), N * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(m->inv_mass, im.data(), N * 4, cudaMemcpyHostToDevice);
+  {  // user order: the sorted slot of each atom and its float64 mass (the host's mass * unit)
+    std::vector<int32_t> us(N);
+    std::vector<double> um(N);
+    for (size_t k = 0; k < N; ++k) {
+      const int u = m->perm[k];
+      us[u] = (int32_t)k;
+      um[u] = d->mass_per_type[t[u]] * 1.036427e2;
+    }
+    cudaMemcpy(m->user_slot, us.data(), N * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(m->user_mass, um.data(), N * 8, cudaMemcpyHostToDevice);
+  }
   m->n_mobile = n_mobile;
   if (n_mobile < m->N) {  // fixed atoms: the mask and the masked shift, sorted order
     std::vector<float> mob(N), sim(N);
@@ -1484,6 +1501,37 @@ extern "C" int dpb_md_box_history(dpb_md *m, int nsteps, double *out) {
   }
   for (size_t e = 0; e < h.size(); ++e) out[e] = h[e];
   return DPB_OK;
+}
+
+// Trajectory frames in user atom order as float64, one thread per output
+// element (grid-stride): out[f][b][u][c] = frame[f][b][slot[u]][c], the
+// momenta divided by the user atom's float64 mass.  Writes are coalesced;
+// reads gather 12-byte atom rows.
+__global__ void k_traj_frames(const float *__restrict__ tp, const float *__restrict__ tm,
+                              const int32_t *__restrict__ slot, const double *__restrict__ mass, int N,
+                              size_t total, double *__restrict__ op, double *__restrict__ ov) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+    const size_t row = e / 3;
+    const int c = (int)(e - row * 3);
+    const size_t fb = row / (size_t)N;
+    const int u = (int)(row - fb * (size_t)N);
+    const size_t src = (fb * (size_t)N + (size_t)slot[u]) * 3 + c;
+    if (op) op[e] = (double)tp[src];
+    if (ov) ov[e] = (double)tm[src] / mass[u];
+  }
+}
+
+extern "C" int dpb_md_traj_frames(dpb_md *m, int nframes, const float *traj_pos, const float *traj_mom,
+                                  double *pos_out, double *vel_out, void *stream) {
+  if (!m || nframes < 0 || (pos_out && !traj_pos) || (vel_out && !traj_mom)) return DPB_ERR_INVALID_ARG;
+  const size_t total = (size_t)nframes * m->P * m->N * 3;
+  if (!total || (!pos_out && !vel_out)) return DPB_OK;
+  const size_t blocks = std::min<size_t>((total + 255) / 256, (size_t)148 * 16);
+  k_traj_frames<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(traj_pos, traj_mom, m->user_slot, m->user_mass,
+                                                                    m->N, total, pos_out, vel_out);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
 }
 
 extern "C" int dpb_md_eval_model(dpb_md *m, const dpb_model *model, double *energy, double *force) {

@@ -80,10 +80,11 @@ def _declare(lib):
                                     ctypes.POINTER(ctypes.c_int), vp]
     lib.dpb_md_box_history.argtypes = [vp, ctypes.c_int, d64]
     lib.dpb_md_eval_model.argtypes = [vp, vp, d64, d64]
+    lib.dpb_md_traj_frames.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp]
     for f in ("dpb_md_create", "dpb_md_destroy", "dpb_md_set_positions", "dpb_md_set_velocities",
               "dpb_md_get_state", "dpb_md_init", "dpb_md_run", "dpb_md_report", "dpb_md_clear_status",
               "dpb_md_snapshot", "dpb_md_set_capacity", "dpb_md_set_skin", "dpb_md_device_bytes",
-              "dpb_md_autotune", "dpb_md_box_history", "dpb_md_eval_model"):
+              "dpb_md_autotune", "dpb_md_box_history", "dpb_md_eval_model", "dpb_md_traj_frames"):
         getattr(lib, f).restype = ctypes.c_int
     lib._md_declared = True
 
@@ -611,28 +612,25 @@ class Simulation:
     def _copy_out(self, pending, traj):
         """Frames of one accepted chunk into the host trajectory: user order
         and velocities = momenta / (m * unit) in float64, formed on the device
-        on a side stream (the next chunk keeps the main stream busy), then
-        copied into traj[idx:idx + n].  Same values as un-permuting and
-        dividing on the host: float32 -> float64 is exact and IEEE division is
-        correctly rounded on both."""
+        by dpb_md_traj_frames on a side stream (the next chunk keeps the main
+        stream busy), then copied into traj[idx:idx + n].  Same values as
+        un-permuting and dividing on the host (_unpack_frame): float32 ->
+        float64 is exact and IEEE division is correctly rounded on both."""
         buf_p, buf_v, n, idx, ev = pending
-        P, N = self._n_bead, self._natoms
         if getattr(self, "_copy_stream", None) is None:
             self._copy_stream = torch.cuda.Stream()
-            inv = np.empty_like(self._perm)
-            inv[self._perm] = np.arange(len(self._perm))
-            self._inv_perm_dev = torch.tensor(inv.astype(np.int64), device="cuda")
-            self._mass_unit_dev = torch.tensor(self._mass * MASS_UNIT_CONVERSION, dtype=torch.float64, device="cuda")
+            shape = (self._step_chunk_size, self._natoms * self._n_bead * 3)
+            self._frames64 = (torch.empty(shape, dtype=torch.float64, device="cuda"),
+                              torch.empty(shape, dtype=torch.float64, device="cuda"))
         cs = self._copy_stream
+        pos, vel = self._frames64
         with torch.cuda.stream(cs):
             cs.wait_event(ev)
-            pos = buf_p[:n].view(n, P, N, 3).index_select(2, self._inv_perm_dev).double()
-            vel = buf_v[:n].view(n, P, N, 3).index_select(2, self._inv_perm_dev).double()
-            vel = vel / self._mass_unit_dev[None, None, :, None]
-            if not self._is_pimd:
-                pos, vel = pos[:, 0], vel[:, 0]
-            torch.from_numpy(traj["position"][idx:idx + n]).copy_(pos)
-            torch.from_numpy(traj["velocity"][idx:idx + n]).copy_(vel)
+            _lib.check(self.lib.dpb_md_traj_frames(self._h, n, _ptr(buf_p), _ptr(buf_v), _ptr(pos), _ptr(vel),
+                                                   ctypes.c_void_p(cs.cuda_stream)), "dpb_md_traj_frames")
+            dst_p, dst_v = traj["position"][idx:idx + n], traj["velocity"][idx:idx + n]
+            torch.from_numpy(dst_p).copy_(pos[:n].view(dst_p.shape))
+            torch.from_numpy(dst_v).copy_(vel[:n].view(dst_v.shape))
         cs.synchronize()
 
     def _unpack_frame(self, p_row, v_row):

@@ -344,6 +344,16 @@ DPB_API int dpb_md_box_history(dpb_md *md, int nsteps, double *out);
  * reference's Model_Devi reporter (deepmd_jax/md.py:299-302,559-567).
  * Synchronous; allocates and frees its scratch; not with beads. */
 DPB_API int dpb_md_eval_model(dpb_md *md, const dpb_model *model, double *energy, double *force);
+/* Frames written by dpb_md_run (nframes x (P,N,3) float32, type-sorted
+ * positions and momenta) as float64 in user atom order: positions, and
+ * velocities in A/fs (momenta divided by the float64 mass per atom), in one
+ * launch on `stream`; either output may be NULL.  Same values as
+ * un-permuting and dividing on the host (float32 -> float64 is exact and the
+ * division is correctly rounded).  Replaces: the per-chunk trajectory
+ * stacking of the reference's run loop (deepmd_jax/md.py:938-944), whose
+ * state is already in user order. */
+DPB_API int dpb_md_traj_frames(dpb_md *md, int nframes, const float *traj_pos, const float *traj_mom,
+                               double *pos_out, double *vel_out, void *stream);
 
 /* Diagnostics: per-stage CUDA-event timing on the launching stream (off by
  * default; not for use inside graph capture).  Stage ids: 0 neighbour

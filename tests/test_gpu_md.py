@@ -543,3 +543,40 @@ def test_pimd_invariant_reporter_matches_state():
     want = (KE + E + spring - r_dev.thermostat_work) / P
     scale = (abs(E) + KE + spring) / P
     assert abs(sim.log[-1][4] - want) <= 1e-5 * scale, (sim.log[-1][4], want)
+
+
+@pytest.mark.parametrize("n_bead", [1, 3])
+def test_trajectory_frames_kernel_matches_host_unpermute(n_bead):
+    """dpb_md_traj_frames (type-sorted float32 frames -> user-order float64
+    positions and velocities) against the host's un-permute and float64
+    division (Simulation._unpack_frame), bit for bit, on random frames; then
+    a two-chunk run() whose last trajectory frame is the engine's own state."""
+    from deepmd_jax_b200.md import Simulation
+    p, v = golden_models()["B"]
+    w = _system()
+    if n_bead == 1:
+        pos, vel, kw = w["position"], w["velocity"], {}
+    else:
+        pos = np.broadcast_to(w["position"], (n_bead, 192, 3)).copy()
+        vel = np.broadcast_to(w["velocity"], (n_bead, 192, 3)).copy()
+        kw = dict(temperature=300.0, n_bead=n_bead, tau_t=100.0, seed=5)
+    sim = Simulation((p, v), w["box"], w["type_idx"], w["mass_per_type"], "NVE" if n_bead == 1 else "NVT",
+                     0.25, pos, initial_velocity=vel, report_interval=10, verbose=False, **kw)
+    n, nf3 = 5, n_bead * 192 * 3
+    g = torch.Generator(device="cuda").manual_seed(0)
+    bp = torch.randn((n, nf3), device="cuda", generator=g) * 20.0
+    bv = torch.randn((n, nf3), device="cuda", generator=g)
+    op = torch.full((n, nf3), np.nan, dtype=torch.float64, device="cuda")
+    ov = torch.full((n, nf3), np.nan, dtype=torch.float64, device="cuda")
+    rc = sim.lib.dpb_md_traj_frames(sim._h, n, bp.data_ptr(), bv.data_ptr(), op.data_ptr(), ov.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0
+    for i in range(n):
+        ep, ev = sim._unpack_frame(bp[i], bv[i])
+        assert np.array_equal(op[i].cpu().numpy().reshape(ep.shape), ep)
+        assert np.array_equal(ov[i].cpu().numpy().reshape(ev.shape), ev)
+    traj = sim.run(12)   # chunks of 10 and 2 steps: both frame buffers
+    assert traj["position"].shape[0] == 13
+    assert np.array_equal(traj["position"][-1], sim.getPosition())
+    assert np.allclose(traj["velocity"][-1], sim.getVelocity(), rtol=1e-6, atol=1e-12)
