@@ -397,6 +397,8 @@ def gpu_arm(args, rank, world, local_rank):
                            "requests": sv["requests"], "md_requests": sv["md_requests"],
                            "eval_p50_s": f["latency"].get("eval", {}).get("p50_s"),
                            "eval_p99_s": f["latency"].get("eval", {}).get("p99_s"),
+                           "eval_queue_p50_s": f["latency"].get("eval", {}).get("queue_p50_s"),
+                           "eval_service_p50_s": f["latency"].get("eval", {}).get("service_p50_s"),
                            "md_p50_s": f["latency"].get("md", {}).get("p50_s"),
                            "md_p99_s": f["latency"].get("md", {}).get("p99_s"),
                            "frames_per_s": f["frames_per_s"], "atom_evals_per_s": f["atom_evals_per_s"],
@@ -572,15 +574,20 @@ def study_serving(args, forms=("fp32", "mixed"), seconds=None):
             w = water(64)
             srv.submit_evaluate(w["position"], w["box"], w["type_idx"]).result()   # warm-up
             srv.completed.clear()
+            srv.batch_log.clear()
             futs, atoms_eval, frames = [], 0, 0
+            # the clients' frames are drawn before the stream starts, so the
+            # submitting thread does no numpy work between arrivals
+            frames_of = [(w["position"][None] + 0.01 * rng.standard_normal((k,) + w["position"].shape)
+                          ).astype(np.float32) if kind == "eval" else None
+                         for _, kind, n_w, k in sched for w in (water(n_w),)]
             t0 = time.perf_counter()
-            for ta, kind, n_w, k in sched:
+            for (ta, kind, n_w, k), pos in zip(sched, frames_of):
                 dt = t0 + ta - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
                 w = water(n_w)
                 if kind == "eval":
-                    pos = w["position"][None] + 0.01 * rng.standard_normal((k,) + w["position"].shape)
                     futs.append(srv.submit_evaluate(pos, w["box"], w["type_idx"]))
                     atoms_eval += k * len(w["type_idx"])
                     frames += k
@@ -592,7 +599,9 @@ def study_serving(args, forms=("fp32", "mixed"), seconds=None):
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0
             lat = srv.latency_summary()
-            out["forms"][prec] = {"latency": lat, "wall_s": wall, "frames_per_s": frames / wall,
+            del frames_of
+            out["forms"][prec] = {"latency": lat, "batch_phases": srv.batch_summary(), "wall_s": wall,
+                                  "frames_per_s": frames / wall,
                                   "atom_evals_per_s": atoms_eval / wall, "batches": srv.batches,
                                   "mean_batch_atoms": float(np.mean(srv.batch_sizes)) if srv.batch_sizes else 0,
                                   "peak_reserved_GB": srv.budget.peak / 1e9}

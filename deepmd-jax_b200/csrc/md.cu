@@ -1490,9 +1490,9 @@ extern "C" int dpb_md_set_capacity(dpb_md *m, const int *sel, void *stream) {
 
 extern "C" int dpb_md_box_history(dpb_md *m, int nsteps, double *out) {
   if (!m || !out || nsteps < 0 || nsteps > kBoxHist) return DPB_ERR_INVALID_ARG;
-  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
   std::vector<float> h((size_t)nsteps * 3);
-  if (m->box_hist) {
+  if (m->box_hist) {  // written by the steps on their stream: wait for them
+    if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
     if (nsteps && cudaMemcpy(h.data(), m->box_hist, h.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
       return DPB_ERR_CUDA;
   } else {

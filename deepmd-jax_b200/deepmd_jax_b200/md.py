@@ -131,7 +131,10 @@ class Simulation:
     (default, the reference's float32) or 'mixed' (BF16 tensor-core GEMMs);
     ``autotune`` (default: on from 10,000 atom-beads) lets the library time
     its launch-shape candidates on this system once, before any graph is
-    captured (``launch_shapes`` holds the choice)."""
+    captured (``launch_shapes`` holds the choice).  Besides a model.pkl path
+    or a (params, variables) pair, ``model_path`` may be a ``DeviceModel``
+    already resident on the device, whose weights the engine then shares
+    (the serving loop's MD continuations do this)."""
 
     def __init__(self, model_path, box, type_idx, mass, routine, dt, initial_position, initial_velocity=None,
                  report_interval=200, temperature=None, pressure=None, debug=False, seed=0,
@@ -143,7 +146,10 @@ class Simulation:
         self.lib = _lib.load()
         _declare(self.lib)
         self.verbose = verbose
-        if isinstance(model_path, (tuple, list)):
+        resident = None
+        if isinstance(model_path, DeviceModel):   # weights already on the device (the serving loop's)
+            resident, params, variables = model_path, model_path.params, None
+        elif isinstance(model_path, (tuple, list)):
             params, variables = model_path
         else:
             model, variables = load_model(model_path)
@@ -185,7 +191,7 @@ class Simulation:
             if temperature is None:
                 raise ValueError("Missing argument 'temperature' for routine 'NPT'")
             self._couple_axes, self._group_ids = parse_couple_axes(couple_axes)
-        self.model = DeviceModel(params, variables)
+        self.model = resident if resident is not None else DeviceModel(params, variables)
         # models of the Model_Devi reporter (md.py:299-302,559-567): paths, or
         # (params, variables) pairs
         self._dev_models = []

@@ -17,7 +17,8 @@ Here a ``Server`` owns one device model and three worker threads:
 * the MD worker steps every admitted MD-continuation request chunk by chunk
   (CUDA-graph replays of the device-resident engine; positions, velocities
   and thermostat state stay on the device) in round-robin, on its own CUDA
-  stream, so MD chunks and evaluation batches overlap on the device.  The
+  stream, so MD chunks and evaluation batches overlap on the device; the
+  engines share the server's resident weights (no model upload per request).  The
   continuations run with the library's default launch shapes: timing
   candidate shapes would cost more than a short continuation gains.
 
@@ -123,6 +124,9 @@ class Server:
         self.completed = []
         self.batches = 0
         self.batch_sizes = []
+        # per evaluation batch: requests, atom-frames and host seconds spent
+        # packing, launching, waiting for the GPU and handing out results
+        self.batch_log = []
         self._threads = []
         n = ctypes.c_size_t()
         _lib.check(self.dm.lib.dpb_eval_packed_workspace_bytes(self.dm.handle, 1024, 1, ctypes.byref(n)),
@@ -181,10 +185,29 @@ class Server:
         with self._lock:
             done = list(self.completed)
         for kind in ("eval", "md"):
-            lat = np.array([r.t_done - r.t_submit for r in done if r.kind == kind])
+            rs = [r for r in done if r.kind == kind]
+            lat = np.array([r.t_done - r.t_submit for r in rs])
             if len(lat):
+                # queue: submit -> taken into a batch (or an MD slot); service: the rest
+                q = np.array([(r.t_start if r.t_start is not None else r.t_done) - r.t_submit for r in rs])
                 out[kind] = {"n": int(len(lat)), "p50_s": float(np.percentile(lat, 50)),
-                             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean())}
+                             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
+                             "queue_p50_s": float(np.percentile(q, 50)), "queue_p99_s": float(np.percentile(q, 99)),
+                             "service_p50_s": float(np.percentile(lat - q, 50)),
+                             "service_p99_s": float(np.percentile(lat - q, 99))}
+        return out
+
+    def batch_summary(self):
+        """Mean / max host seconds per evaluation batch in each phase (pack,
+        launch, GPU wait, hand-out) and the mean batch size."""
+        log = list(self.batch_log)
+        if not log:
+            return {}
+        out = {"batches": len(log), "mean_requests": float(np.mean([b["requests"] for b in log])),
+               "mean_atom_frames": float(np.mean([b["atoms"] for b in log]))}
+        for k in ("pack_s", "launch_s", "wait_s", "handout_s"):
+            v = np.array([b[k] for b in log])
+            out[k] = {"mean": float(v.mean()), "max": float(v.max())}
         return out
 
     def eval_bytes(self, atoms):
@@ -305,18 +328,22 @@ class Server:
         for it, (r, a, b) in zip(batch.items, groups):
             n = it["natoms"] * it["nframes"]
             slots[it["slot0"]:it["slot0"] + n] = r.payload[0][a:b].reshape(-1, 3)
-        return {"reqs": reqs, "batch": batch, "groups": groups, "pin": pin, "pin_idx": self._pin_idx[self._pin_k]}
+        return {"reqs": reqs, "batch": batch, "groups": groups, "pin": pin, "pin_idx": self._pin_idx[self._pin_k],
+                "t_pack": (t0, time.perf_counter())}
 
     def _launch_eval_batch(self, prep):
         batch = prep["batch"]
+        t0 = time.perf_counter()
         prep["pos"] = prep["pin"][:batch.natoms].to("cuda", non_blocking=True)
         prep["sel"] = list(self.sel)
         prep["out"] = evaluate_packed(self.dm, batch, prep["pos"], prep["sel"], self.rcut, self.precision,
                                       host_stage=prep["pin_idx"])
+        prep["t_launch"] = (t0, time.perf_counter())
         return prep
 
     def _complete_eval_batch(self, prep):
         reqs, batch, groups = prep["reqs"], prep["batch"], prep["groups"]
+        t_wait = time.perf_counter()
         try:
             out, sel = prep["out"], prep["sel"]
             while True:
@@ -327,6 +354,7 @@ class Server:
                 self.sel = [max(a, b) for a, b in zip(self.sel, sel)]
                 out = evaluate_packed(self.dm, batch, prep["pos"], sel, self.rcut, self.precision,
                                       host_stage=prep["pin_idx"])
+            t_gpu = time.perf_counter()
             energy = out["energy"].cpu().numpy()
             force = out["force"].cpu().numpy()
             virial = out["virial"].cpu().numpy().reshape(-1, 3, 3)
@@ -345,6 +373,10 @@ class Server:
             d["force"][a:b] = force[it["slot0"]:it["slot0"] + n * it["natoms"]].reshape(n, it["natoms"], 3)
         for r in reqs:
             self._finish(r, res[id(r)])
+        pk, ln = prep["t_pack"], prep["t_launch"]
+        self.batch_log.append({"requests": len(reqs), "atoms": batch.nreal, "pack_s": pk[1] - pk[0],
+                               "launch_s": ln[1] - ln[0], "wait_s": t_gpu - t_wait,
+                               "handout_s": time.perf_counter() - t_gpu})
 
     def _md_loop(self):
         from .md import Simulation
@@ -363,7 +395,7 @@ class Server:
                     a = r.payload
                     try:
                         r.t_start = time.perf_counter()
-                        sim = Simulation((self.params, self.variables), a["box"], a["type_idx"], a["mass_per_type"],
+                        sim = Simulation(self.dm, a["box"], a["type_idx"], a["mass_per_type"],
                                          a["routine"], a["dt"], a["position"], initial_velocity=a["velocity"],
                                          temperature=a["temperature"] if a["routine"] == "NVT" else None,
                                          tau_t=a["tau_t"], seed=a["seed"], report_interval=self.md_chunk,
