@@ -583,3 +583,38 @@ def test_no_pair_within_an_ulp_of_the_cutoff(n_side, L):
     w = water_box(n_side, L, seed=0)
     c = onl.canonicalize(w["position"], w["box"], w["type_idx"])
     assert onl.boundary_pairs(c, w["box"].astype(np.float32), onl.cutoff_sq(6.3)) == 0
+
+
+def test_serving_latency_split_and_batch_phases():
+    """Server.latency_summary splits each request's latency into queue time
+    (submit -> taken into a batch or MD slot) and service time, and
+    batch_summary averages the host phases of the evaluation batches; the
+    HBM budget admits first come first served and never exceeds its total.
+    Host logic only (a stand-in for the server's state, no device)."""
+    import threading
+    import types
+    from deepmd_jax_b200.serving import HBMBudget, Server, _Req
+    reqs = []
+    for k, (kind, q, s) in enumerate([("eval", 0.01, 0.05), ("eval", 0.02, 0.03), ("eval", 0.03, 0.01),
+                                      ("md", 0.5, 1.0)]):
+        r = _Req(kind, None, 0, 10, 1)
+        r.t_submit, r.t_start, r.t_done = 100.0 + k, 100.0 + k + q, 100.0 + k + q + s
+        reqs.append(r)
+    stub = types.SimpleNamespace(completed=reqs, _lock=threading.Condition(),
+                                 batch_log=[{"requests": 2, "atoms": 100, "pack_s": 0.001, "launch_s": 0.002,
+                                             "wait_s": 0.004, "handout_s": 0.0005},
+                                            {"requests": 4, "atoms": 300, "pack_s": 0.003, "launch_s": 0.004,
+                                             "wait_s": 0.002, "handout_s": 0.0015}])
+    lat = Server.latency_summary(stub)
+    assert lat["eval"]["n"] == 3 and lat["md"]["n"] == 1
+    assert lat["eval"]["p50_s"] == pytest.approx(0.05)
+    assert lat["eval"]["queue_p50_s"] == pytest.approx(0.02)
+    assert lat["eval"]["service_p50_s"] == pytest.approx(0.03)
+    assert lat["md"]["queue_p50_s"] == pytest.approx(0.5) and lat["md"]["service_p50_s"] == pytest.approx(1.0)
+    ph = Server.batch_summary(stub)
+    assert ph["batches"] == 2 and ph["mean_requests"] == 3.0 and ph["mean_atom_frames"] == 200.0
+    assert ph["pack_s"]["mean"] == pytest.approx(0.002) and ph["wait_s"]["max"] == pytest.approx(0.004)
+    b = HBMBudget(100)
+    assert b.try_reserve(60) and not b.try_reserve(50) and b.try_reserve(40)
+    b.release(60)
+    assert b.try_reserve(50) and b.peak == 100 and b.used == 90
