@@ -41,6 +41,28 @@ from .engine import DeviceModel, PackedBatch, evaluate_packed
 from .utils import load_model
 
 
+def request_boxes(box, coord, type_idx):
+    """(F, 3) float32 box lengths of an evaluate() request: one box (3,) or
+    (3, 3) for every frame, or per-frame boxes in the shapes evaluate()
+    takes (a leading frame axis; a (3, 3) array with three frames counts as
+    three (3,) rows, as in evaluate()).  The packed batches are
+    orthorhombic: a box with off-diagonal entries raises NotImplementedError
+    (evaluate() takes general boxes)."""
+    from .train import normalize_boxes
+    F = coord.shape[0]
+    box = np.asarray(box, dtype=np.float64)
+    if box.shape == (3,):
+        mats = np.broadcast_to(np.diag(box), (F, 3, 3))
+    elif box.shape == (3, 3) and F != 3:
+        mats = np.broadcast_to(box, (F, 3, 3))
+    else:
+        mats = normalize_boxes(coord, box, type_idx)
+    diag = np.einsum("fii->fi", mats)
+    if np.any(mats - diag[:, :, None] * np.eye(3) != 0):
+        raise NotImplementedError("the serving loop packs orthorhombic boxes; evaluate() takes general boxes")
+    return np.ascontiguousarray(diag, dtype=np.float32)
+
+
 class HBMBudget:
     """Byte budget with first-come-first-served admission."""
 
@@ -156,16 +178,20 @@ class Server:
         self.stop()
 
     def submit_evaluate(self, coord, box, type_idx):
-        """coord (F, N, 3) or (N, 3); box (3,) or (F, 3) orthorhombic; returns
-        a Future of {'energy' (F,), 'force' (F, N, 3), 'virial' (F, 3, 3)}."""
+        """coord (F, N, 3) or (N, 3); box (3,), (3, 3), or per frame in any
+        shape evaluate() takes ((F,), (F, 1), (F, 3), (F, 9), (F, 3, 3));
+        orthorhombic only.  Returns a Future of {'energy' (F,), 'force'
+        (F, N, 3), 'virial' (F, 3, 3)}."""
         coord = np.asarray(coord, dtype=np.float32)
         if coord.ndim == 2:
             coord = coord[None]
+        if coord.ndim != 3 or coord.shape[2] != 3:
+            raise ValueError("coord must have shape (F, N, 3) or (N, 3)")
         F, N = coord.shape[:2]
-        box = np.ascontiguousarray(np.broadcast_to(np.asarray(box, np.float32).reshape(-1, 3), (F, 3)))
         type_idx = np.asarray(type_idx)
         if type_idx.shape != (N,):
             raise ValueError("type_idx must have one entry per atom")
+        box = request_boxes(box, coord, type_idx)
         return self._submit(_Req("eval", (coord, box, type_idx), self.eval_bytes(N * F), N, F))
 
     def submit_md(self, position, box, type_idx, mass_per_type, steps, routine="NVT", dt=0.5, temperature=300.0,

@@ -618,3 +618,30 @@ def test_serving_latency_split_and_batch_phases():
     assert b.try_reserve(60) and not b.try_reserve(50) and b.try_reserve(40)
     b.release(60)
     assert b.try_reserve(50) and b.peak == 100 and b.used == 90
+
+
+def test_serving_request_boxes():
+    """The serving loop's box shapes: one box (3,) or (3, 3) for every frame,
+    per-frame boxes in evaluate()'s shapes; general boxes and bad shapes
+    rejected before anything is queued."""
+    from deepmd_jax_b200.serving import request_boxes
+    t = np.zeros(5, dtype=int)
+    c2, c3 = np.zeros((2, 5, 3), np.float32), np.zeros((3, 5, 3), np.float32)
+    L = np.array([10.0, 11.0, 12.5])
+    assert np.array_equal(request_boxes(L, c2, t), np.stack([L, L]).astype(np.float32))
+    assert np.array_equal(request_boxes(np.diag(L), c2, t), np.stack([L, L]).astype(np.float32))
+    per = np.array([[10.0, 11.0, 12.0], [13.0, 14.0, 15.0]])
+    assert np.array_equal(request_boxes(per, c2, t), per.astype(np.float32))
+    assert np.array_equal(request_boxes(np.stack([np.diag(b) for b in per]), c2, t), per.astype(np.float32))
+    assert np.array_equal(request_boxes(np.array([9.0, 8.0]), c2, t), np.array([[9.0] * 3, [8.0] * 3], np.float32))
+    assert np.array_equal(request_boxes(np.stack([np.diag(b).reshape(9) for b in per]), c2, t),
+                          per.astype(np.float32))
+    # a (3, 3) array with three frames is three rows of lengths, as evaluate() reads it
+    rows = np.array([[10.0, 10.0, 10.0], [11.0, 11.0, 11.0], [12.0, 12.0, 12.0]])
+    assert np.array_equal(request_boxes(rows, c3, t), rows.astype(np.float32))
+    sheared = np.diag(L)
+    sheared[1, 0] = 2.0
+    with pytest.raises(NotImplementedError, match="orthorhombic"):
+        request_boxes(sheared, c2, t)
+    with pytest.raises(ValueError):
+        request_boxes(np.ones((4, 3)), c2, t)
