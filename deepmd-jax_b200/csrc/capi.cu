@@ -348,6 +348,10 @@ extern "C" int dpb_model_create(const dpb_model_desc *d, dpb_model **out) {
   }
   M.fit_dgsc = pow2_scale_to_2p14(dg_bound);
   if (rc == DPB_OK && !M.emb_tuned && !dpb::embed_general_fits(M)) rc = DPB_ERR_UNSUPPORTED;
+  // the uploads are blocking copies from pageable memory, whose DMA may land
+  // after they return and which order themselves only against the legacy
+  // stream: the weights are in place before any stream's kernel reads them
+  if (rc == DPB_OK && cudaDeviceSynchronize() != cudaSuccess) rc = DPB_ERR_CUDA;
   if (rc != DPB_OK) {
     dpb_model_destroy(m);
     return rc;

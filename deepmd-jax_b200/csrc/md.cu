@@ -1121,7 +1121,13 @@ static int md_upload(dpb_md *m, const double *host, float *dev, bool momentum) {
         buf[((size_t)b * N + k) * 3 + c] = (float)v;
       }
     }
-  return cudaMemcpy(dev, buf.data(), buf.size() * 4, cudaMemcpyHostToDevice) == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
+  // The engine's kernels may run on any stream the caller gives, and a
+  // blocking copy from pageable memory orders itself only against the legacy
+  // stream (and may return before its DMA lands): wait for the device on both
+  // sides.
+  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
+  if (cudaMemcpy(dev, buf.data(), buf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+  return cudaDeviceSynchronize() == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
 }
 
 static int md_download(const dpb_md *m, const float *dev, double *host, bool velocity) {
@@ -1211,7 +1217,11 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
     h.Q[0] *= h.dof;
     h.scale = 1.0;
     h.twork = 0.0;
-    cudaMemcpy(sc, &h, sizeof(h), cudaMemcpyHostToDevice);
+    // a blocking copy from pageable memory may return before its DMA lands
+    // and orders itself only against the legacy stream: wait for it before
+    // any step on the caller's stream reads the chain state
+    if (cudaMemcpy(sc, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
     if (m->np) {  // npt init_fn (routine.py:322-350; NPT-PIMD: pimd.py:417-441)
       NptScalars n;
       std::memset(&n, 0, sizeof(n));
@@ -1231,6 +1241,7 @@ extern "C" int dpb_md_init(dpb_md *m, int reset_thermostat, void *stream) {
       n.bdof = n.G;
       n.bQ[0] *= n.bdof;
       if (cudaMemcpy(m->np, &n, sizeof(n), cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+      if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
       if (m->d.routine == DPB_MD_NPT_PIMD) {
         // centroid-virial dU/d(eps) and centroid p^2/m of the initial state
         PimdParams pp;
@@ -1422,16 +1433,25 @@ extern "C" int dpb_md_report(dpb_md *m, dpb_md_report_t *r) {
 extern "C" int dpb_md_clear_status(dpb_md *m, uint32_t keep) {
   if (!m) return DPB_ERR_INVALID_ARG;
   uint32_t st = 0;
+  // the word is read after every step in flight on any stream, and the new
+  // word has landed before the call returns (see md_upload)
+  if (cudaDeviceSynchronize() != cudaSuccess) return DPB_ERR_CUDA;
   if (cudaMemcpy(&st, m->status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return DPB_ERR_CUDA;
   st &= keep;
-  return cudaMemcpy(m->status, &st, 4, cudaMemcpyHostToDevice) == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
+  if (cudaMemcpy(m->status, &st, 4, cudaMemcpyHostToDevice) != cudaSuccess) return DPB_ERR_CUDA;
+  return cudaDeviceSynchronize() == cudaSuccess ? DPB_OK : DPB_ERR_CUDA;
 }
 
 extern "C" int dpb_md_snapshot(dpb_md *m, int restore) {
   if (!m) return DPB_ERR_INVALID_ARG;
   const size_t n = (size_t)m->N * m->P * 12;
   cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
-  int bad = 0;
+  // device-to-device cudaMemcpy runs on the legacy stream without host
+  // synchronisation, while the steps may run on a non-blocking stream: the
+  // state is copied only after every step in flight, and the call returns
+  // only when the copies are done
+  int bad = cudaDeviceSynchronize() != cudaSuccess;
+  if (bad) return DPB_ERR_CUDA;
   if (!restore) {
     bad |= cudaMemcpy(m->s_pos, m->pos, n, k) != cudaSuccess;
     bad |= cudaMemcpy(m->s_mom, m->mom, n, k) != cudaSuccess;
@@ -1453,6 +1473,7 @@ extern "C" int dpb_md_snapshot(dpb_md *m, int restore) {
       bad |= cudaMemcpy(m->boxd, m->s_box, (size_t)m->P * 12, k) != cudaSuccess;
     }
   }
+  bad |= cudaDeviceSynchronize() != cudaSuccess;
   return bad ? DPB_ERR_CUDA : DPB_OK;
 }
 

@@ -296,6 +296,7 @@ DPB_API int dpb_md_create(const dpb_model *model, const dpb_md_desc *desc, dpb_m
 DPB_API int dpb_md_destroy(dpb_md *md);
 DPB_API int dpb_md_device_bytes(const dpb_md *md, size_t *bytes);
 /* State in user atom order, (P,N,3) float64 host arrays; velocities in A/fs.
+ * Synchronous (the device is idle before and after each call).
  * Replaces: setPosition / setVelocity / getPosition / getVelocity / getForce
  * (deepmd_jax/md.py:969-1047). */
 DPB_API int dpb_md_set_positions(dpb_md *md, const double *pos);
@@ -314,7 +315,9 @@ DPB_API int dpb_md_run(dpb_md *md, int nsteps, float *traj_pos, float *traj_mom,
 /* Synchronous read of the energies, status word and thermostat state. */
 DPB_API int dpb_md_report(dpb_md *md, dpb_md_report_t *report);
 DPB_API int dpb_md_clear_status(dpb_md *md, uint32_t keep_bits);
-/* restore == 0: save the state (chunk start); 1: restore it (chunk re-run). */
+/* restore == 0: save the state (chunk start); 1: restore it (chunk re-run).
+ * Synchronous: waits for the device before and after the copies, so the
+ * steps may run on any stream. */
 DPB_API int dpb_md_snapshot(dpb_md *md, int restore);
 /* New neighbour skin and a rebuild whose reference box is the current box
  * (box-shrink resolution, status bit 1; deepmd_jax/md.py:649-654). */
