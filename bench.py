@@ -61,31 +61,95 @@ def parse():
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    polled every 5 ms from a thread (the device found by its UUID, else by
+    index), which gives samples inside a region of a few tens of ms; where
+    NVML cannot be used, nvidia-smi at 200 ms intervals.  Read-only queries."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+    PERIOD_S = 0.005
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []      # (sm MHz, max sm MHz, [reason names])
         self.proc = None
+        self.nvml = None
+        self.source = None
 
     def __enter__(self):
+        self._stop = threading.Event()
+        if self._open_nvml():
+            self._sample_nvml()
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            self.source = "nvml, %g ms" % (1e3 * self.PERIOD_S)
+            return self
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.source = "nvidia-smi, 200 ms"
         except Exception:
             self.proc = None
         return self
 
+    def _open_nvml(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = None
+            try:
+                import torch
+                u = str(torch.cuda.get_device_properties(self.index).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.h = h
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.reasons_fn = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.nvml = pynvml
+            return True
+        except Exception:
+            self.nvml = None
+            return False
+
+    def _sample_nvml(self):
+        try:
+            sm = float(self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+            mask = int(self.reasons_fn(self.h))
+            self.rows.append((sm, self.mx, [n for n, bit in self.REASONS if mask & bit]))
+        except Exception:
+            pass
+
+    def _poll_nvml(self):
+        while not self._stop.wait(self.PERIOD_S):
+            self._sample_nvml()
+
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                sm, mx = float(r[1]), float(r[2])
+            except (ValueError, IndexError):
+                continue
+            self.rows.append((sm, mx, [n for k, (n, _) in enumerate(self.REASONS)
+                                       if len(r) > 5 + k and r[5 + k] == "Active"]))
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=5)
+            self._sample_nvml()   # the end of the region
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -95,13 +159,10 @@ class ClockSampler:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted({n for r in self.rows for n in r[2]}), "samples": len(self.rows),
+                "source": self.source}
 
 
 # ----------------------------------------------------------------------------- work model
