@@ -18,9 +18,10 @@ Here a ``Server`` owns one device model and three worker threads:
   (CUDA-graph replays of the device-resident engine; positions, velocities
   and thermostat state stay on the device) in round-robin, on its own CUDA
   stream, so MD chunks and evaluation batches overlap on the device; the
-  engines share the server's resident weights (no model upload per request).  The
-  continuations run with the library's default launch shapes: timing
-  candidate shapes would cost more than a short continuation gains.
+  engines share the server's resident weights (no model upload per
+  request).  The continuations run with the library's default launch
+  shapes: timing candidate shapes would cost more than a short continuation
+  gains.
 
 A request's bytes are released when it completes.  Latency is measured from
 ``submit_*`` to the result being ready on the host.
